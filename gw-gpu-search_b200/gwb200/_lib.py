@@ -1,0 +1,116 @@
+"""ctypes binding of libgwb200.so, the C ABI declared in include/gwb200.h.
+
+The library is built in-tree (gw-gpu-search_b200/build.py) and loaded from gwb200/lib. There is no fallback: if the
+library is missing or a call returns a non-zero status, the caller gets an exception."""
+import ctypes
+import os
+
+import torch
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'lib', 'libgwb200.so')
+_lib = None
+
+GWB_OK = 0
+GWB_ERR_SHAPE = 1
+GWB_ERR_NOT_POW2 = 2
+GWB_ERR_EDGE_ORDER = 3
+GWB_ERR_ALLOC = 4
+GWB_ERR_CUFFT = 5
+GWB_ERR_TIMEOUT = 6
+GWB_ERR_CUDA = 7
+GWB_ERR_ARG = 8
+GWB_ERR_NOT_IMPLEMENTED = 9
+GWB_ERR_ALIGN = 10
+GWB_ERR_CAPACITY = 11
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_LL = ctypes.c_longlong
+_F = ctypes.c_float
+_D = ctypes.c_double
+
+# name -> argument types (all entry points return int status)
+SIGNATURES = {
+    'gwb_device_error': [_P, _P, _P, _P, _I],
+    'gwb_window_peaks': [_P, _LL, _I, _LL, _I, _I, _P, _P, _P],
+    'gwb_fused_peaks_f16': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
+    'gwb_fused_peaks_bf16x3': [_P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
+    'gwb_fused_peaks_f32': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
+}
+
+
+class GwbError(RuntimeError):
+    def __init__(self, name, status, msg):
+        super().__init__('%s failed with status %d (%s): %s' % (name, status, _status_string(status), msg))
+        self.status = status
+
+
+def lib_path():
+    return _LIB_PATH
+
+
+def load():
+    """Load the shared library once; raise if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError('libgwb200.so is not built (%s); run gw-gpu-search_b200/build.py' % _LIB_PATH)
+        lib = ctypes.CDLL(_LIB_PATH)
+        lib.gwb_version.restype = ctypes.c_int
+        lib.gwb_status_string.restype = ctypes.c_char_p
+        lib.gwb_status_string.argtypes = [_I]
+        lib.gwb_last_error.restype = ctypes.c_char_p
+        lib.gwb_num_sms.restype = ctypes.c_int
+        for name, args in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def _status_string(status):
+    try:
+        return load().gwb_status_string(int(status)).decode()
+    except Exception:
+        return '?'
+
+
+def call(name, *args):
+    """Call an entry point; raise GwbError on a non-zero status."""
+    lib = load()
+    st = getattr(lib, name)(*args)
+    if st != GWB_OK:
+        raise GwbError(name, st, lib.gwb_last_error().decode())
+    return st
+
+
+def stream_ptr(device=None):
+    """The caller's current torch stream as the void* the C ABI takes."""
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def device_error(clear=True):
+    """(code, where, info0, info1) from the current device's error word (a synchronous read)."""
+    c, w, i0, i1 = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    call('gwb_device_error', ctypes.byref(c), ctypes.byref(w), ctypes.byref(i0), ctypes.byref(i1), int(clear))
+    return c.value, w.value, i0.value, i1.value
+
+
+def check_device_error():
+    """Raise if a kernel recorded an error (bounded wait gave up, failed self-check)."""
+    code, where, i0, i1 = device_error(clear=True)
+    if code:
+        raise GwbError('device', code, 'site %d info %d %d' % (where, i0, i1))
+
+
+def require_cuda(*tensors):
+    """The product path runs on the GPU only: every tensor argument must be a CUDA tensor."""
+    for t in tensors:
+        if t is not None and not t.is_cuda:
+            raise TypeError('gwb200 kernels take CUDA tensors (got a %s tensor)' % t.device)

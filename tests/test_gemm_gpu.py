@@ -1,0 +1,152 @@
+"""GPU parity of the fused reconstruction GEMM (+|z|^2 +argmax) and of the window-peak kernel.
+
+References: the reference's own Triton kernel outputs (tests/golden/fp_gemm_*.npz) and the numpy oracle
+(oracle/gemm.py, itself checked against those fixtures on the CPU). Peak indices must be identical wherever the
+block's maximum is not a near-tie (two values within the accumulation-order rounding), and bit-identical, ties
+included, when every product and sum is exact (integer operands)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import gemm as og
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 2e-5   # fp32 accumulation in a different order than numpy / Triton
+
+
+def _near_tie_mask(Are, Aim, Z, M, Tn, I_ref, rel=1e-5):
+    """True where the reference block's winner is within rel of another column (argmax legitimately ambiguous)."""
+    zr = Are[:M].astype(np.float32) @ Z[:, :Tn].astype(np.float32)
+    zi = Aim[:M].astype(np.float32) @ Z[:, :Tn].astype(np.float32)
+    pw = zr * zr + zi * zi
+    nblk = I_ref.shape[1]
+    pad = nblk * 128 - Tn
+    if pad:
+        pw = np.concatenate([pw, np.full((M, pad), -1.0, np.float32)], 1)
+    pw = pw.reshape(M, nblk, 128)
+    s = np.sort(pw, axis=2)
+    return (s[..., -1] - s[..., -2]) <= rel * np.abs(s[..., -1])
+
+
+def _grouped(Vb, Ib, tie, group):
+    """Group the block results as the kernel does; a group's winner is ambiguous where a block inside it is, or where
+    two block maxima of the group nearly tie."""
+    M, nblk = Vb.shape
+    Vr, Ir = og.group_reduce(Vb, Ib, group)
+    nout = Vr.shape[1]
+    pad = nout * group - nblk
+    t = np.pad(tie, ((0, 0), (0, pad))).reshape(M, nout, group).any(2)
+    s = np.sort(np.pad(Vb, ((0, 0), (0, pad)), constant_values=-1).reshape(M, nout, group), 2)
+    if group > 1:
+        t |= (s[..., -1] - s[..., -2]) <= 1e-5 * np.abs(s[..., -1])
+    return Vr, Ir, t
+
+
+def _dev(a, dt):
+    return torch.from_numpy(np.ascontiguousarray(a)).to('cuda', dt)
+
+
+def _check(V, I, Vr, Ir, tie):
+    np.testing.assert_allclose(V, Vr, rtol=RTOL, atol=1e-6)
+    bad = (I != Ir) & ~tie
+    assert not bad.any(), 'index mismatch away from near-ties at %s' % (np.argwhere(bad)[:5],)
+
+
+@pytest.mark.parametrize('name', ['fp_gemm_a', 'fp_gemm_ragged', 'fp_gemm_ties'])
+def test_f16_matches_reference_triton_kernel(golden, name):
+    from gwb200 import fp_gemm
+    g = golden(name)
+    M, Tn, K = int(g['M']), int(g['Tn']), g['Are'].shape[1]
+    Z = g['Z']
+    ldz = -(-Tn // 8) * 8   # TMA wants the row stride a multiple of 16 bytes
+    Zp = np.zeros((K, ldz), np.float16)
+    Zp[:, :Tn] = Z
+    V, I = fp_gemm.fused_peaks(_dev(g['Are'], torch.float16), _dev(g['Aim'], torch.float16),
+                               _dev(Zp, torch.float16)[:, :Tn], M, Tn, (64, 64, 4, 2))
+    V, I = V.cpu().numpy(), I.cpu().numpy()
+    if name == 'fp_gemm_ties':
+        assert np.array_equal(V, g['V']) and np.array_equal(I, g['I'])
+    else:
+        _check(V, I, g['V'], g['I'], _near_tie_mask(g['Are'], g['Aim'], Z, M, Tn, g['I']))
+
+
+@pytest.mark.parametrize('M,K,Tn,group', [(256, 64, 131072, 1), (256, 64, 131072, 16), (300, 128, 40000, 1),
+                                          (100, 64, 2048 * 7 + 640, 16), (128, 128, 8192, 4)])
+def test_f16_random_against_oracle(M, K, Tn, group):
+    from gwb200 import fp_gemm
+    rng = np.random.default_rng(M + K + Tn)
+    Are = rng.standard_normal((M, K)).astype(np.float16)
+    Aim = rng.standard_normal((M, K)).astype(np.float16)
+    Z = rng.standard_normal((K, Tn)).astype(np.float16)
+    V, I = fp_gemm.fused_peaks(_dev(Are, torch.float16), _dev(Aim, torch.float16), _dev(Z, torch.float16), M, Tn,
+                               group=group)
+    Vr, Ir = og.gemm_absmax(Are, Aim, Z, M, Tn)
+    tie = _near_tie_mask(Are, Aim, Z, M, Tn, Ir)
+    if group > 1:
+        Vr, Ir, tie = _grouped(Vr, Ir, tie, group)
+    _check(V.cpu().numpy(), I.cpu().numpy(), Vr, Ir, tie)
+
+
+def test_f16_integer_operands_bit_exact_with_ties():
+    from gwb200 import fp_gemm
+    rng = np.random.default_rng(7)
+    M, K, Tn = 256, 64, 128 * 300 + 16
+    Are = rng.integers(-2, 3, (M, K)).astype(np.float16)
+    Aim = rng.integers(-2, 3, (M, K)).astype(np.float16)
+    Z = rng.integers(-1, 2, (K, Tn)).astype(np.float16)
+    V, I = fp_gemm.fused_peaks(_dev(Are, torch.float16), _dev(Aim, torch.float16), _dev(Z, torch.float16), M, Tn)
+    Vr, Ir = og.gemm_absmax(Are, Aim, Z, M, Tn)
+    assert np.array_equal(V.cpu().numpy(), Vr)
+    assert np.array_equal(I.cpu().numpy(), Ir)
+
+
+@pytest.mark.parametrize('M,K,Tn,group', [(256, 64, 32768, 1), (130, 40, 5000, 16)])
+def test_f32_form_against_oracle(M, K, Tn, group):
+    from gwb200 import fp_gemm
+    rng = np.random.default_rng(11)
+    Are = rng.standard_normal((M, K)).astype(np.float32)
+    Aim = rng.standard_normal((M, K)).astype(np.float32)
+    Z = rng.standard_normal((K, Tn)).astype(np.float32)
+    V, I = fp_gemm.fused_peaks(_dev(Are, torch.float32), _dev(Aim, torch.float32), _dev(Z, torch.float32), M, Tn,
+                               group=group)
+    Vr, Ir = og.gemm_absmax(Are, Aim, Z, M, Tn)
+    tie = _near_tie_mask(Are, Aim, Z, M, Tn, Ir)
+    if group > 1:
+        Vr, Ir, tie = _grouped(Vr, Ir, tie, group)
+    _check(V.cpu().numpy(), I.cpu().numpy(), Vr, Ir, tie)
+
+
+def test_bf16x3_form_close_to_fp32():
+    from gwb200 import fp_gemm
+    rng = np.random.default_rng(5)
+    M, K, Tn = 256, 64, 65536
+    Are = rng.standard_normal((M, K)).astype(np.float32)
+    Aim = rng.standard_normal((M, K)).astype(np.float32)
+    Z = rng.standard_normal((K, Tn)).astype(np.float32)
+
+    def split(x):
+        t = torch.from_numpy(x).cuda()
+        hi = t.to(torch.bfloat16)
+        lo = (t - hi.float()).to(torch.bfloat16)
+        return hi.contiguous(), lo.contiguous()
+    (rh, rl), (ih, il), (zh, zl) = split(Are), split(Aim), split(Z)
+    V, I = fp_gemm.fused_peaks_split(rh, rl, ih, il, zh, zl, M, Tn)
+    Vr, Ir = og.gemm_absmax(Are, Aim, Z, M, Tn)
+    V = V.cpu().numpy()
+    rel = np.abs(V - Vr) / Vr
+    assert rel.max() < 1e-4, rel.max()
+    assert (I.cpu().numpy() == Ir).mean() > 0.995
+
+
+def test_window_peaks_bit_exact():
+    from gwb200 import peak_kernel
+    rng = np.random.default_rng(3)
+    rows, N, a0, cw, nwin = 37, 3 * 2048 + 500, 300, 2048, 3
+    z = (rng.standard_normal((rows, N)) + 1j * rng.standard_normal((rows, N))).astype(np.complex64)
+    z[5, a0 + 10] = z[5, a0 + 900] = 10 + 0j          # a planted tie: the first offset must win
+    p, i = peak_kernel.window_peaks(torch.from_numpy(z).cuda(), a0, cw, nwin)
+    pr, ir = og.window_peaks(z, a0, cw, nwin)
+    assert np.array_equal(p.cpu().numpy(), pr)
+    assert np.array_equal(i.cpu().numpy(), ir)
+    assert i[5, 0].item() == 10

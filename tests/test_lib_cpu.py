@@ -1,0 +1,74 @@
+"""CPU checks of the C ABI: the library loads, exports every entry point the header declares, and rejects bad
+arguments with a status before any device work."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+from gwb200 import _lib
+
+HEADER = os.path.join(ROOT, 'include', 'gwb200.h')
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    txt = re.sub(r'/\*.*?\*/', '', txt, flags=re.S)
+    return sorted(set(re.findall(r'\b(gwb_[a-z0-9_]+)\s*\(', txt)))
+
+
+def test_library_loads_and_reports_version():
+    lib = _lib.load()
+    assert lib.gwb_version() == 1
+    assert lib.gwb_status_string(0) == b'ok'
+    assert lib.gwb_status_string(_lib.GWB_ERR_TIMEOUT).startswith(b'a device wait')
+
+
+def test_every_declared_symbol_is_exported():
+    lib = _lib.load()
+    names = declared_symbols()
+    assert len(names) >= 5
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_every_declared_symbol_has_a_binding():
+    names = set(declared_symbols()) - {'gwb_version', 'gwb_status_string', 'gwb_last_error', 'gwb_num_sms'}
+    assert names <= set(_lib.SIGNATURES), sorted(names - set(_lib.SIGNATURES))
+
+
+def _p(v):
+    return ctypes.c_void_p(v)
+
+
+def test_gemm_rejects_k_not_multiple_of_64():
+    lib = _lib.load()
+    st = lib.gwb_fused_peaks_f16(_p(16), _p(16), 48, _p(16), 1024, 64, 48, 1024, 1, _p(16), _p(16), 8, None)
+    assert st == _lib.GWB_ERR_SHAPE
+    assert b'multiple of 64' in lib.gwb_last_error()
+
+
+def test_gemm_rejects_misaligned_operands():
+    lib = _lib.load()
+    st = lib.gwb_fused_peaks_f16(_p(18), _p(16), 64, _p(16), 1024, 64, 64, 1024, 1, _p(16), _p(16), 8, None)
+    assert st == _lib.GWB_ERR_ALIGN
+    st = lib.gwb_fused_peaks_f16(_p(16), _p(16), 64, _p(16), 1020, 64, 64, 1020, 1, _p(16), _p(16), 8, None)
+    assert st == _lib.GWB_ERR_ALIGN
+
+
+def test_gemm_rejects_small_output_stride():
+    lib = _lib.load()
+    st = lib.gwb_fused_peaks_f32(_p(16), _p(16), 64, _p(16), 1024, 64, 64, 1024, 1, _p(16), _p(16), 7, None)
+    assert st == _lib.GWB_ERR_SHAPE
+
+
+def test_window_peaks_rejects_windows_past_the_row():
+    lib = _lib.load()
+    st = lib.gwb_window_peaks(_p(16), 4096, 2, 100, 2048, 2, _p(16), _p(16), None)
+    assert st == _lib.GWB_ERR_SHAPE
+
+
+def test_call_raises_with_message():
+    with pytest.raises(_lib.GwbError, match='multiple of 64'):
+        _lib.call('gwb_fused_peaks_f16', _p(16), _p(16), 48, _p(16), 1024, 64, 48, 1024, 1, _p(16), _p(16), 8, None)
