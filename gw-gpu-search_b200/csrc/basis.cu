@@ -1,0 +1,316 @@
+// Basis series (fp_filter.basis_series, pipeline/fp_filter.py:597-613), stacked A (stacked_A :615-621) and the window
+// candidate selection with the rebuilt complex SNR (fp_filter.py:745-764).
+//
+// basis series for one segment and a batch of basis rows:
+//   premul: q[j, k] = conj(Vh[j, k]) * (D[k] * isw[k]) for k < flen (the caller keeps q's upper half zero), the input
+//           of a batched C2C inverse FFT (cuFFT, no 1/N: norm='forward' in the reference);
+//   scale:  rms of the first batch over the analysed span, sqrt(mean(re^2 + im^2) / 2), reduced in float64 in a fixed
+//           order (per-block partials, the last block to finish sums them);
+//   pack:   Z rows 0..r-1 = Re / scale, rows r..2r-1 = Im / scale, over samples a0..a0+Tn-1, written as fp16 (the
+//           reference's form), fp32, or a bf16 hi/lo pair (split form).
+#include "common.cuh"
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace gwb {
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void premul_kernel(const float2* __restrict__ Vh, long long ldvh, int rows, const float2* __restrict__ D,
+                              long long ldd, const float* __restrict__ isw, long long flen, float2* __restrict__ q,
+                              long long ldq) {
+    const int j = blockIdx.y % rows, s = blockIdx.y / rows;
+    const float2* v = Vh + (long long)j * ldvh;
+    const float2* d = D + (long long)s * ldd;
+    float2* o = q + ((long long)s * rows + j) * ldq;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < flen; k += (long long)gridDim.x * blockDim.x) {
+        const float2 a = v[k], dk = d[k];
+        const float w = isw[k];
+        const float dr = dk.x * w, di = dk.y * w;             // D * isw, rounded as the reference's product
+        o[k] = make_float2(fmaf(a.x, dr, a.y * di), fmaf(a.x, di, -(a.y * dr)));   // conj(v) * (D isw)
+    }
+}
+
+// Partial sums of |zb|^2 over the first `rows` rows, samples a0..a0+Tn-1; the last block sums the partials in order
+// and writes scale. ticket must be zero on entry; the last block resets it.
+__global__ void scale_kernel(const float2* __restrict__ zb, long long ldz, int rows, long long a0, long long Tn,
+                             double* __restrict__ partials, unsigned int* __restrict__ ticket,
+                             float* __restrict__ scale_out) {
+    double acc = 0.0;
+    const long long total = (long long)rows * Tn;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const long long j = e / Tn, t = e - j * Tn;
+        const float2 v = zb[j * ldz + a0 + t];
+        acc += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    __shared__ double red[kThreads / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) s += red[w];
+        partials[blockIdx.x] = s;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double s = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)partials)[b];
+        *scale_out = (float)sqrt(s / (double)total / 2.0);
+        *ticket = 0;
+    }
+}
+
+template <int FORM>   // 0 fp16, 1 fp32, 2 bf16 hi/lo
+__global__ void pack_kernel(const float2* __restrict__ zb, long long ldzb, int rows, int r, int row0, long long a0,
+                            long long Tn, const float* __restrict__ scale, void* __restrict__ Z, void* __restrict__ Zlo,
+                            long long ldz) {
+    const int j = blockIdx.y;
+    const float inv = 1.0f / *scale;
+    const float2* src = zb + (long long)j * ldzb + a0;
+    const long long re_row = row0 + j, im_row = r + row0 + j;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < Tn; t += (long long)gridDim.x * blockDim.x) {
+        const float2 v = src[t];
+        const float xr = v.x * inv, xi = v.y * inv;
+        if (FORM == 0) {
+            __half* z = static_cast<__half*>(Z);
+            z[re_row * ldz + t] = __float2half_rn(xr);
+            z[im_row * ldz + t] = __float2half_rn(xi);
+        } else if (FORM == 1) {
+            float* z = static_cast<float*>(Z);
+            z[re_row * ldz + t] = xr;
+            z[im_row * ldz + t] = xi;
+        } else {
+            __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(Z);
+            __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(Zlo);
+            const __nv_bfloat16 hr = __float2bfloat16_rn(xr), hm = __float2bfloat16_rn(xi);
+            hi[re_row * ldz + t] = hr;
+            hi[im_row * ldz + t] = hm;
+            lo[re_row * ldz + t] = __float2bfloat16_rn(xr - __bfloat162float(hr));
+            lo[im_row * ldz + t] = __float2bfloat16_rn(xi - __bfloat162float(hm));
+        }
+    }
+}
+
+template <int FORM>
+__global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, int n, int r, const double* __restrict__ nrm,
+                                 long long nrm_stride, const float* __restrict__ scale, int Kp, void* __restrict__ Are,
+                                 void* __restrict__ Aim, void* __restrict__ Are_lo, void* __restrict__ Aim_lo,
+                                 long long ldo) {
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    const float f = (float)nrm[(long long)i * nrm_stride] * *scale;
+    for (int c = threadIdx.x; c < Kp; c += blockDim.x) {
+        float re = 0.f, im = 0.f;
+        if (c < r) {
+            const float2 a = A[(long long)i * lda + c];
+            re = a.x * f;
+            im = a.y * f;
+        } else if (c < 2 * r) {
+            const float2 a = A[(long long)i * lda + c - r];
+            re = -(a.y * f);
+            im = a.x * f;
+        }
+        const long long o = (long long)i * ldo + c;
+        if (FORM == 0) {
+            static_cast<__half*>(Are)[o] = __float2half_rn(re);
+            static_cast<__half*>(Aim)[o] = __float2half_rn(im);
+        } else if (FORM == 1) {
+            static_cast<float*>(Are)[o] = re;
+            static_cast<float*>(Aim)[o] = im;
+        } else {
+            const __nv_bfloat16 hr = __float2bfloat16_rn(re), hm = __float2bfloat16_rn(im);
+            static_cast<__nv_bfloat16*>(Are)[o] = hr;
+            static_cast<__nv_bfloat16*>(Aim)[o] = hm;
+            static_cast<__nv_bfloat16*>(Are_lo)[o] = __float2bfloat16_rn(re - __bfloat162float(hr));
+            static_cast<__nv_bfloat16*>(Aim_lo)[o] = __float2bfloat16_rn(im - __bfloat162float(hm));
+        }
+    }
+}
+
+__device__ __forceinline__ float ld_as_float(const void* p, long long i, int form) {
+    if (form == 0) return __half2float(static_cast<const __half*>(p)[i]);
+    if (form == 1) return static_cast<const float*>(p)[i];
+    return __bfloat162float(static_cast<const __nv_bfloat16*>(p)[i]);
+}
+
+// Window candidates of one (tile, segment). One block per template row: windows whose maximum |z|^2 (the fused GEMM's
+// windowed output) exceeds thr2 become candidates, written contiguously in window order at an offset taken with one
+// atomic per row; the row's candidates are cut into groups of at most 8 (one group = one exact-stage work unit) and
+// the row is registered once as an edges unit. The rebuilt complex SNR Are[row].Z[:, col] + i Aim[row].Z[:, col]
+// (fp_filter.py:760-764) is computed for each candidate; for the split form the hi and lo parts are summed.
+__global__ void select_kernel(const float* __restrict__ vw, const int32_t* __restrict__ iw, long long ldv, int n,
+                              int nw, float thr2, long long a0, int row0, int seg, const void* __restrict__ Are,
+                              const void* __restrict__ Aim, const void* __restrict__ Are_lo,
+                              const void* __restrict__ Aim_lo, long long lda, const void* __restrict__ Z,
+                              const void* __restrict__ Zlo, long long ldz, int Kp, int form, GwbCand* __restrict__ cands,
+                              int cand_cap, GwbGroup* __restrict__ groups, int group_cap, GwbUnit* __restrict__ units,
+                              int unit_cap, int32_t* __restrict__ counters) {
+    const int row = blockIdx.x;
+    if (row >= n) return;
+    const float* v = vw + (long long)row * ldv;
+    __shared__ int s_cnt, s_base, s_unit, s_gbase;
+    __shared__ int s_warp[kThreads / 32];
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    // count
+    int cnt = 0;
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) cnt += v[w] > thr2;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_cnt, cnt);
+    __syncthreads();
+    const int total = s_cnt;
+    if (total == 0) return;
+    const int ng = (total + 7) / 8;
+    if (threadIdx.x == 0) {
+        s_base = atomicAdd(&counters[0], total);
+        s_gbase = atomicAdd(&counters[1], ng);
+        s_unit = atomicAdd(&counters[2], 1);
+        if (s_base + total > cand_cap || s_gbase + ng > group_cap || s_unit >= unit_cap) atomicOr(&counters[3], 1);
+        else units[s_unit] = GwbUnit{row0 + row, seg, s_base, total};
+    }
+    __syncthreads();
+    if (s_base + total > cand_cap || s_gbase + ng > group_cap || s_unit >= unit_cap) return;
+    for (int g = threadIdx.x; g < ng; g += blockDim.x)
+        groups[s_gbase + g] = GwbGroup{s_unit, s_base + 8 * g, min(8, total - 8 * g), 0};
+    // ordered write: chunks of blockDim windows, prefix over warps
+    int written = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int w0 = 0; w0 < nw; w0 += blockDim.x) {
+        const int w = w0 + threadIdx.x;
+        const bool hit = w < nw && v[w] > thr2;
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) s_warp[warp] = __popc(m);
+        __syncthreads();
+        int before = 0;
+        for (int k = 0; k < warp; ++k) before += s_warp[k];
+        int chunk_total = 0;
+        for (int k = 0; k < kThreads / 32; ++k) chunk_total += s_warp[k];
+        if (hit) {
+            const int pos = s_base + written + before + __popc(m & ((1u << lane) - 1));
+            const int col = iw[(long long)row * ldv + w];
+            float zr = 0.f, zi = 0.f;
+            for (int c = 0; c < Kp; ++c) {
+                const float zc = ld_as_float(Z, (long long)c * ldz + col, form) +
+                                 (form == 2 ? ld_as_float(Zlo, (long long)c * ldz + col, 2) : 0.f);
+                const float ar = ld_as_float(Are, (long long)row * lda + c, form) +
+                                 (form == 2 ? ld_as_float(Are_lo, (long long)row * lda + c, 2) : 0.f);
+                const float ai = ld_as_float(Aim, (long long)row * lda + c, form) +
+                                 (form == 2 ? ld_as_float(Aim_lo, (long long)row * lda + c, 2) : 0.f);
+                zr = fmaf(ar, zc, zr);
+                zi = fmaf(ai, zc, zi);
+            }
+            GwbCand cd;
+            cd.row = row0 + row;
+            cd.seg = seg;
+            cd.sample = (int)(a0 + col);
+            cd.window = w;
+            cd.approx = sqrtf(v[w]);
+            cd.zr = zr;
+            cd.zi = zi;
+            cd.unit = s_unit;
+            cands[pos] = cd;
+        }
+        written += chunk_total;
+        __syncthreads();
+    }
+}
+
+}  // namespace
+}  // namespace gwb
+
+extern "C" {
+
+int gwb_basis_premul(const float* Vh, long long ldvh, int rows, const float* D, long long ldd, int nseg,
+                     const float* isw, long long flen, float* q, long long ldq, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(Vh && D && isw && q, GWB_ERR_ARG, "basis_premul: null pointer");
+    GWB_CHECK_ARG(rows > 0 && nseg > 0 && flen > 0 && ldvh >= flen && ldd >= flen && ldq >= flen, GWB_ERR_SHAPE,
+                  "basis_premul: rows=%d nseg=%d flen=%lld", rows, nseg, flen);
+    GWB_CHECK_ARG((long long)rows * nseg < 65536, GWB_ERR_SHAPE, "basis_premul: too many rows");
+    const int gx = (int)std::min<long long>(cdiv(flen, kThreads), 512);
+    dim3 grid(gx, rows * nseg);
+    premul_kernel<<<grid, kThreads, 0, (cudaStream_t)stream>>>(reinterpret_cast<const float2*>(Vh), ldvh, rows,
+                                                                reinterpret_cast<const float2*>(D), ldd, isw, flen,
+                                                                reinterpret_cast<float2*>(q), ldq);
+    GWB_LAUNCH_CHECK("premul_kernel");
+    return GWB_OK;
+}
+
+int gwb_basis_scale(const float* zb, long long ldz, int rows, long long a0, long long Tn, double* partials,
+                    int npartials, uint32_t* ticket, float* scale_out, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(zb && partials && ticket && scale_out, GWB_ERR_ARG, "basis_scale: null pointer");
+    GWB_CHECK_ARG(rows > 0 && Tn > 0 && a0 >= 0 && a0 + Tn <= ldz && npartials > 0, GWB_ERR_SHAPE,
+                  "basis_scale: rows=%d a0=%lld Tn=%lld ldz=%lld", rows, a0, Tn, ldz);
+    const int nb = (int)std::min<long long>((long long)npartials, cdiv((long long)rows * Tn, kThreads * 8));
+    scale_kernel<<<nb, kThreads, 0, (cudaStream_t)stream>>>(reinterpret_cast<const float2*>(zb), ldz, rows, a0, Tn,
+                                                             partials, ticket, scale_out);
+    GWB_LAUNCH_CHECK("scale_kernel");
+    return GWB_OK;
+}
+
+int gwb_basis_pack(const float* zb, long long ldzb, int rows, int r, int row0, long long a0, long long Tn,
+                   const float* scale, int form, void* Z, void* Zlo, long long ldz, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(zb && scale && Z && (form != 2 || Zlo), GWB_ERR_ARG, "basis_pack: null pointer");
+    GWB_CHECK_ARG(form >= 0 && form <= 2, GWB_ERR_ARG, "basis_pack: form %d", form);
+    GWB_CHECK_ARG(rows > 0 && row0 >= 0 && row0 + rows <= r && Tn > 0 && a0 >= 0 && a0 + Tn <= ldzb && ldz >= Tn,
+                  GWB_ERR_SHAPE, "basis_pack: rows=%d row0=%d r=%d a0=%lld Tn=%lld", rows, row0, r, a0, Tn);
+    const int gx = (int)std::min<long long>(cdiv(Tn, kThreads), 1024);
+    dim3 grid(gx, rows);
+    const float2* src = reinterpret_cast<const float2*>(zb);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (form == 0) pack_kernel<0><<<grid, kThreads, 0, s>>>(src, ldzb, rows, r, row0, a0, Tn, scale, Z, Zlo, ldz);
+    else if (form == 1) pack_kernel<1><<<grid, kThreads, 0, s>>>(src, ldzb, rows, r, row0, a0, Tn, scale, Z, Zlo, ldz);
+    else pack_kernel<2><<<grid, kThreads, 0, s>>>(src, ldzb, rows, r, row0, a0, Tn, scale, Z, Zlo, ldz);
+    GWB_LAUNCH_CHECK("pack_kernel");
+    return GWB_OK;
+}
+
+int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
+                  const float* scale, int Kp, int form, void* Are, void* Aim, void* Are_lo, void* Aim_lo,
+                  long long ldo, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(A && nrm && scale && Are && Aim && (form != 2 || (Are_lo && Aim_lo)), GWB_ERR_ARG,
+                  "stacked_a: null pointer");
+    GWB_CHECK_ARG(form >= 0 && form <= 2, GWB_ERR_ARG, "stacked_a: form %d", form);
+    GWB_CHECK_ARG(n > 0 && r > 0 && Kp >= 2 * r && lda >= r && ldo >= Kp, GWB_ERR_SHAPE,
+                  "stacked_a: n=%d r=%d Kp=%d", n, r, Kp);
+    cudaStream_t s = (cudaStream_t)stream;
+    const float2* a = reinterpret_cast<const float2*>(A);
+    if (form == 0) stacked_a_kernel<0><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
+    else if (form == 1) stacked_a_kernel<1><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
+    else stacked_a_kernel<2><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
+    GWB_LAUNCH_CHECK("stacked_a_kernel");
+    return GWB_OK;
+}
+
+int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2, long long a0,
+                       int row0, int seg, const void* Are, const void* Aim, const void* Are_lo, const void* Aim_lo,
+                       long long lda, const void* Z, const void* Zlo, long long ldz, int Kp, int form, GwbCand* cands,
+                       int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units, int unit_cap, int32_t* counters,
+                       void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(vw && iw && Are && Aim && Z && cands && groups && units && counters, GWB_ERR_ARG,
+                  "select_windows: null pointer");
+    GWB_CHECK_ARG(form >= 0 && form <= 2 && (form != 2 || (Are_lo && Aim_lo && Zlo)), GWB_ERR_ARG,
+                  "select_windows: form %d", form);
+    GWB_CHECK_ARG(n > 0 && nw >= 0 && ldv >= nw && Kp > 0 && lda >= Kp, GWB_ERR_SHAPE, "select_windows: n=%d nw=%d", n,
+                  nw);
+    if (nw == 0) return GWB_OK;
+    select_kernel<<<n, kThreads, 0, (cudaStream_t)stream>>>(vw, iw, ldv, n, nw, thr2, a0, row0, seg, Are, Aim, Are_lo,
+                                                            Aim_lo, lda, Z, Zlo, ldz, Kp, form, cands, cand_cap, groups,
+                                                            group_cap, units, unit_cap, counters);
+    GWB_LAUNCH_CHECK("select_kernel");
+    return GWB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,325 @@
+// Chi-squared bin edges, binned sums at peaks and the exact-stage finalisation.
+//
+// edges (multi_filter.edges_per_template, pipeline/multi_filter.py:264-282; chisq_edges.edges_fused :92-143):
+//   one block per unit (template row, segment): float64 sums of |h_k|^2 IP_k over contiguous per-thread chunks of
+//   [kmin, k1), a block scan of the chunk sums, then every edge j < nb is the first k whose cumulative sum exceeds
+//   j / nb of the total, found by walking only the chunk that holds it. Edges are clipped to [kmin, k1] and padded
+//   with k1 up to B + 1 entries. The comparison is written as the reference writes it, so rounding at near-ties
+//   follows it too: offset_mode 1 compares cs / tot + u > u + j / nb (the flattened searchsorted of
+//   edges_per_template, u the unit's index), offset_mode 0 compares cs > (j / nb) tot (chisq_edges.py:70-82, 116-121).
+// binned sums (chisq_kernel.bin_power_sums :17-121, exact_stage dense path :425-439, :734-739):
+//   Z_j(t) = sum_{k in bin j} q_k exp(2 pi i ((k t) mod N) / N) with q_k = conj(h_k) D_k formed in registers (or q
+//   given). Work item = (group of <= 8 peaks of one unit, chunk of kChunk bins); threads take k = base + tid + NT m
+//   (coalesced) and advance each peak's phasor by a fixed rotation exp(2 pi i (NT t mod N) / N), reseeded exactly with
+//   sincospif every kReseed steps (the reference's regen kernel uses the same recurrence-with-reseed, exact_stage.py
+//   :548-585). Per bin the block reduces in a fixed order and writes one slot per (peak, chunk, bin).
+// finalize: per peak, Z_j = sum over chunks of its slots (fp32, chunk order); z = sum_j Z_j and pw = sum_j |Z_j|^2
+//   in float64; then snr = |z| norm, chisq = (nb pw - |z|^2) norm^2, dof = 2 nb - 2, newsnr, fpeak
+//   (fp_filter.py:837-853, exact_stage.py:236-238, coinc_rank.py:39-46) with norm = 4 df / sqrt(sigma^2).
+#include "common.cuh"
+
+namespace gwb {
+namespace {
+
+constexpr int kEdgeThreads = 512;
+constexpr int kSumThreads = 256;
+constexpr int kChunk = 32768;
+constexpr int kReseed = 16;
+constexpr int kMaxPeaks = 8;
+
+__device__ __forceinline__ int count_of(const int32_t* dev, int host_max) {
+    return dev ? min(*dev, host_max) : host_max;
+}
+
+__device__ __forceinline__ double wgt(const float2* h, const float* ip, long long k) {
+    const float2 v = h[k];
+    return ((double)v.x * (double)v.x + (double)v.y * (double)v.y) * (double)ip[k];
+}
+
+__global__ void __launch_bounds__(kEdgeThreads) edges_kernel(const GwbUnit* __restrict__ units, const int32_t* ucount,
+                                                             int umax, const float2* __restrict__ H, long long ldh,
+                                                             const float* __restrict__ IP, long long ldip,
+                                                             const int32_t* __restrict__ nbins,
+                                                             const int32_t* __restrict__ kmax, int kmin, int B,
+                                                             int offset_mode, int32_t* __restrict__ E) {
+    __shared__ double pre[kEdgeThreads + 1];
+    const int nu = count_of(ucount, umax);
+    const int t = threadIdx.x;
+    for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+        const GwbUnit un = units[u];
+        const float2* h = H + (long long)un.row * ldh;
+        const float* ip = IP + (long long)un.seg * ldip;
+        const int k1 = kmax[un.row];
+        const int nb = max(nbins[un.row], 1);
+        const int span = max(k1 - kmin, 0);
+        const int chunk = (span + kEdgeThreads - 1) / kEdgeThreads;
+        const int a = kmin + min(t * chunk, span), b = kmin + min((t + 1) * chunk, span);
+        double s = 0.0;
+        for (int k = a; k < b; ++k) s += wgt(h, ip, k);
+        // inclusive scan of chunk sums (Hillis-Steele over the block, float64)
+        pre[t + 1] = s;
+        if (t == 0) pre[0] = 0.0;
+        __syncthreads();
+        for (int off = 1; off < kEdgeThreads; off <<= 1) {
+            const double v = (t + 1 - off >= 1) ? pre[t + 1 - off] : 0.0;
+            __syncthreads();
+            pre[t + 1] += v;
+            __syncthreads();
+        }
+        const double tot = pre[kEdgeThreads];
+        const double uo = (double)u;
+        int32_t* e = E + (long long)u * (B + 1);
+        for (int j = t; j <= B; j += kEdgeThreads) {
+            int ej = k1;
+            if (j < nb) {
+                // mode 1: cs / tot + u > u + j / nb (the reference's flattened searchsorted);
+                // mode 0: cs > (j / nb) tot (its blocked and fused edge kernels)
+                const double frac = (double)j / (double)nb;
+                const double target = offset_mode ? uo + frac : frac * tot;
+                auto above = [&](double cs) { return offset_mode ? (cs / tot + uo > target) : (cs > target); };
+                // first chunk whose end-of-chunk sum is above the target
+                int lo = 0, hi = kEdgeThreads;
+                while (lo < hi) {
+                    const int m = (lo + hi) >> 1;
+                    if (above(pre[m + 1])) hi = m; else lo = m + 1;
+                }
+                ej = k1;
+                for (int c = lo; c < kEdgeThreads; ++c) {
+                    const int ca = kmin + min(c * chunk, span), cb = kmin + min((c + 1) * chunk, span);
+                    double cs = pre[c];
+                    int found = -1;
+                    for (int k = ca; k < cb; ++k) {
+                        cs += wgt(h, ip, k);
+                        if (above(cs)) {
+                            found = k;
+                            break;
+                        }
+                    }
+                    if (found >= 0) {
+                        ej = found;
+                        break;
+                    }
+                }
+                ej = min(max(ej, kmin), k1);
+                if (nbins[un.row] == 0 && j == 0) ej = kmin;
+            }
+            e[j] = ej;
+        }
+        __syncthreads();
+    }
+}
+
+// bin index of k among edges e[0..nb]: -1 below e[0], nb at or above e[nb]
+__device__ __forceinline__ int bin_of(const int32_t* e, int nb, int k) {
+    int lo = 0, hi = nb + 1;
+    while (lo < hi) {
+        const int m = (lo + hi) >> 1;
+        if (e[m] > k) hi = m; else lo = m + 1;
+    }
+    return lo - 1;
+}
+
+__global__ void __launch_bounds__(kSumThreads) binsum_kernel(const GwbGroup* __restrict__ groups, const int32_t* gcount,
+                                                             int gmax, const GwbUnit* __restrict__ units,
+                                                             const GwbCand* __restrict__ cands,
+                                                             const int32_t* __restrict__ E, int B,
+                                                             const int32_t* __restrict__ nbins,
+                                                             const float2* __restrict__ H, long long ldh,
+                                                             const float2* __restrict__ D, long long ldd, int kmin,
+                                                             int nchunk, unsigned nmask, float inv_half_n,
+                                                             float2* __restrict__ slots) {
+    __shared__ float2 red[kSumThreads / 32][kMaxPeaks];
+    const int ng = count_of(gcount, gmax);
+    const long long nitems = (long long)ng * nchunk;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int g = (int)(it / nchunk), c = (int)(it % nchunk);
+        const GwbGroup gr = groups[g];
+        const GwbUnit un = units[gr.unit];
+        const int np = gr.count;
+        const int nb = max(nbins[un.row], 1);
+        const int32_t* e = E + (long long)gr.unit * (B + 1);
+        const int c0 = kmin + c * kChunk, c1 = c0 + kChunk;
+        const int lo = max(c0, e[0]), hi = min(c1, e[nb]);
+        if (lo >= hi) continue;   // uniform
+        unsigned tp[kMaxPeaks];
+        float2 rot[kMaxPeaks];
+#pragma unroll
+        for (int p = 0; p < kMaxPeaks; ++p) {
+            tp[p] = p < np ? (unsigned)cands[gr.first + p].sample : 0u;
+            float sn, cs;
+            sincospif((float)(((unsigned)kSumThreads * tp[p]) & nmask) * inv_half_n, &sn, &cs);
+            rot[p] = make_float2(cs, sn);
+        }
+        const float2* h = H + (long long)un.row * ldh;
+        const float2* d = D ? D + (long long)un.seg * ldd : nullptr;
+        int j = bin_of(e, nb, lo);
+        int a = lo;
+        while (a < hi) {   // uniform over the block: one bin sub-range at a time
+            const int b = min(hi, e[j + 1]);
+            float2 acc[kMaxPeaks];
+            float2 w[kMaxPeaks];
+#pragma unroll
+            for (int p = 0; p < kMaxPeaks; ++p) acc[p] = make_float2(0.f, 0.f);
+            int step = 0;
+            for (int k = a + t; k < b; k += kSumThreads, ++step) {
+                if ((step & (kReseed - 1)) == 0) {
+#pragma unroll
+                    for (int p = 0; p < kMaxPeaks; ++p) {
+                        float sn, cs;
+                        sincospif((float)(((unsigned)k * tp[p]) & nmask) * inv_half_n, &sn, &cs);
+                        w[p] = make_float2(cs, sn);
+                    }
+                }
+                float qx, qy;
+                const float2 hk = h[k];
+                if (d) {
+                    const float2 dk = d[k];
+                    qx = fmaf(hk.x, dk.x, hk.y * dk.y);      // conj(h) D
+                    qy = fmaf(hk.x, dk.y, -(hk.y * dk.x));
+                } else {
+                    qx = hk.x;
+                    qy = hk.y;
+                }
+#pragma unroll
+                for (int p = 0; p < kMaxPeaks; ++p) {
+                    if (p < np) {
+                        acc[p].x = fmaf(qx, w[p].x, fmaf(-qy, w[p].y, acc[p].x));
+                        acc[p].y = fmaf(qx, w[p].y, fmaf(qy, w[p].x, acc[p].y));
+                        const float2 ww = w[p];
+                        w[p] = make_float2(fmaf(ww.x, rot[p].x, -(ww.y * rot[p].y)), fmaf(ww.x, rot[p].y, ww.y * rot[p].x));
+                    }
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < kMaxPeaks; ++p) {
+                float x = acc[p].x, y = acc[p].y;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    x += __shfl_down_sync(0xffffffffu, x, off);
+                    y += __shfl_down_sync(0xffffffffu, y, off);
+                }
+                if (lane == 0) red[warp][p] = make_float2(x, y);
+            }
+            __syncthreads();
+            if (t < np) {
+                float x = 0.f, y = 0.f;
+                for (int q = 0; q < kSumThreads / 32; ++q) {
+                    x += red[q][t].x;
+                    y += red[q][t].y;
+                }
+                slots[((long long)(gr.first + t) * nchunk + c) * B + j] = make_float2(x, y);
+            }
+            __syncthreads();
+            a = b;
+            ++j;
+        }
+    }
+}
+
+__global__ void finalize_kernel(const GwbCand* __restrict__ cands, const int32_t* ccount, int cmax,
+                                const GwbUnit* __restrict__ units, const int32_t* __restrict__ E, int B,
+                                const int32_t* __restrict__ nbins, int kmin, int nchunk,
+                                const float2* __restrict__ slots, const double* __restrict__ sig, long long ldsig,
+                                double df, GwbPeak* __restrict__ out) {
+    const int n = count_of(ccount, cmax);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const GwbCand cd = cands[i];
+        const GwbUnit un = units[cd.unit];
+        const int nbr = nbins[un.row];
+        const int nb = max(nbr, 1);
+        const int32_t* e = E + (long long)cd.unit * (B + 1);
+        const float2* sl = slots + (long long)i * nchunk * B;
+        double zx = 0.0, zy = 0.0, pw = 0.0;
+        for (int j = 0; j < nb; ++j) {
+            if (e[j] >= e[j + 1]) continue;
+            const int ca = (e[j] - kmin) / kChunk, cb = (e[j + 1] - 1 - kmin) / kChunk;
+            float x = 0.f, y = 0.f;
+            for (int c = ca; c <= cb; ++c) {
+                x += sl[(long long)c * B + j].x;
+                y += sl[(long long)c * B + j].y;
+            }
+            zx += x;
+            zy += y;
+            pw += (double)x * x + (double)y * y;
+        }
+        GwbPeak pk;
+        pk.zr = (float)zx;
+        pk.zi = (float)zy;
+        pk.pw = (float)pw;
+        const double z2 = zx * zx + zy * zy;
+        double norm = 0.0;
+        if (sig) norm = 4.0 * df / sqrt(sig[(long long)un.row * ldsig + un.seg]);
+        const double snr = sqrt(z2) * norm;
+        const double chisq = ((double)nbr * (double)pk.pw - z2) * norm * norm;
+        const int dof = 2 * nbr - 2;
+        double ns = snr;
+        const double rchisq = chisq / (double)max(dof, 1);
+        if (rchisq > 1.0) ns = snr / pow((1.0 + rchisq * rchisq * rchisq) / 2.0, 1.0 / 6.0);
+        pk.snr = (float)snr;
+        pk.chisq = (float)chisq;
+        pk.newsnr = (float)ns;
+        pk.dof = dof;
+        pk.fpeak = (float)((2.0 * e[max(nbr - 1, 0)] - e[max(nbr - 2, 0)]) * df);
+        out[i] = pk;
+    }
+}
+
+}  // namespace
+}  // namespace gwb
+
+extern "C" {
+
+int gwb_edges(const GwbUnit* units, const int32_t* ucount, int umax, const float* H, long long ldh, const float* IP,
+              long long ldip, const int32_t* nbins, const int32_t* kmax, int kmin, int B, int offset_mode, int32_t* E,
+              void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(units && H && IP && nbins && kmax && E, GWB_ERR_ARG, "edges: null pointer");
+    GWB_CHECK_ARG(umax >= 0 && B >= 1 && kmin >= 0, GWB_ERR_SHAPE, "edges: umax=%d B=%d kmin=%d", umax, B, kmin);
+    if (umax == 0) return GWB_OK;
+    const int grid = std::min(umax, 8 * num_sms());
+    edges_kernel<<<grid, kEdgeThreads, 0, (cudaStream_t)stream>>>(units, ucount, umax, reinterpret_cast<const float2*>(H),
+                                                                  ldh, IP, ldip, nbins, kmax, kmin, B, offset_mode, E);
+    GWB_LAUNCH_CHECK("edges_kernel");
+    return GWB_OK;
+}
+
+int gwb_bin_sums(const GwbGroup* groups, const int32_t* gcount, int gmax, const GwbUnit* units, const GwbCand* cands,
+                 const int32_t* E, int B, const int32_t* nbins, const float* H, long long ldh, const float* D,
+                 long long ldd, int kmin, int flen, long long tlen, float* slots, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(groups && units && cands && E && nbins && H && slots, GWB_ERR_ARG, "bin_sums: null pointer");
+    GWB_CHECK_ARG(is_pow2(tlen) && tlen <= (1ll << 31), GWB_ERR_NOT_POW2, "bin_sums: time length %lld is not a power of two",
+                  tlen);
+    GWB_CHECK_ARG(gmax >= 0 && B >= 1 && flen > kmin, GWB_ERR_SHAPE, "bin_sums: gmax=%d B=%d flen=%d kmin=%d", gmax, B,
+                  flen, kmin);
+    if (gmax == 0) return GWB_OK;
+    const int nchunk = (int)cdiv(flen - kmin, kChunk);
+    const long long items = (long long)gmax * nchunk;
+    const int grid = (int)std::min<long long>(items, 16ll * num_sms());
+    binsum_kernel<<<grid, kSumThreads, 0, (cudaStream_t)stream>>>(
+        groups, gcount, gmax, units, cands, E, B, nbins, reinterpret_cast<const float2*>(H), ldh,
+        reinterpret_cast<const float2*>(D), ldd, kmin, nchunk, (unsigned)(tlen - 1), (float)(2.0 / (double)tlen),
+        reinterpret_cast<float2*>(slots));
+    GWB_LAUNCH_CHECK("binsum_kernel");
+    return GWB_OK;
+}
+
+int gwb_exact_finalize(const GwbCand* cands, const int32_t* ccount, int cmax, const GwbUnit* units, const int32_t* E,
+                       int B, const int32_t* nbins, int kmin, int flen, const float* slots, const double* sig,
+                       long long ldsig, double df, GwbPeak* out, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(cands && units && E && nbins && slots && out, GWB_ERR_ARG, "exact_finalize: null pointer");
+    GWB_CHECK_ARG(cmax >= 0 && B >= 1 && flen > kmin, GWB_ERR_SHAPE, "exact_finalize: cmax=%d", cmax);
+    if (cmax == 0) return GWB_OK;
+    const int nchunk = (int)cdiv(flen - kmin, kChunk);
+    const int grid = (int)std::min<long long>(cdiv(cmax, 128), 4ll * num_sms());
+    finalize_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(cands, ccount, cmax, units, E, B, nbins, kmin, nchunk,
+                                                             reinterpret_cast<const float2*>(slots), sig, ldsig, df, out);
+    GWB_LAUNCH_CHECK("finalize_kernel");
+    return GWB_OK;
+}
+
+int gwb_exact_chunks(int flen, int kmin) { return (int)gwb::cdiv(flen - kmin, gwb::kChunk); }
+
+}  // extern "C"

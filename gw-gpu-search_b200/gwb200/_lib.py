@@ -32,10 +32,43 @@ _D = ctypes.c_double
 # name -> argument types (all entry points return int status)
 SIGNATURES = {
     'gwb_device_error': [_P, _P, _P, _P, _I],
+    'gwb_create': [_P],
+    'gwb_destroy': [_P],
+    'gwb_fft_c2c': [_P, _P, _P, _LL, _I, _LL, _LL, _I, _P],
+    'gwb_fft_r2c': [_P, _P, _P, _LL, _I, _LL, _LL, _P],
+    'gwb_fft_c2r': [_P, _P, _P, _LL, _I, _LL, _LL, _P],
     'gwb_window_peaks': [_P, _LL, _I, _LL, _I, _I, _P, _P, _P],
     'gwb_fused_peaks_f16': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_bf16x3': [_P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_f32': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
+    'gwb_basis_premul': [_P, _LL, _I, _P, _LL, _I, _P, _LL, _P, _LL, _P],
+    'gwb_basis_scale': [_P, _LL, _I, _LL, _LL, _P, _I, _P, _P, _P],
+    'gwb_basis_pack': [_P, _LL, _I, _I, _I, _LL, _LL, _P, _I, _P, _P, _LL, _P],
+    'gwb_stacked_a': [_P, _LL, _I, _I, _P, _LL, _P, _I, _I, _P, _P, _P, _P, _LL, _P],
+    'gwb_select_windows': [_P, _P, _LL, _I, _I, _F, _LL, _I, _I, _P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _P, _I,
+                           _P, _I, _P, _I, _P, _P],
+    'gwb_edges': [_P, _P, _I, _P, _LL, _P, _LL, _P, _P, _I, _I, _I, _P, _P],
+    'gwb_bin_sums': [_P, _P, _I, _P, _P, _P, _I, _P, _P, _LL, _P, _LL, _I, _I, _LL, _P, _P],
+    'gwb_exact_finalize': [_P, _P, _I, _P, _P, _I, _P, _I, _I, _P, _P, _LL, _D, _P, _P],
+    'gwb_exact_chunks': [_I, _I],
+    'gwb_sigma2': [_P, _LL, _I, _P, _LL, _I, _I, _I, _D, _P, _LL, _P, _LL, _P],
+    'gwb_gram': [_P, _LL, _I, _P, _I, _I, _P, _LL, _P, _P],
+    'gwb_basis_vh': [_P, _LL, _I, _I, _P, _LL, _P, _I, _I, _P, _LL, _P],
+    'gwb_taylorf2': [_P, _P, _P, _P, _P, _P, _I, _D, _I, _I, _D, _P, _LL, _P],
+    'gwb_frames': [_P, _LL, _I, _LL, _LL, _P, _I, _I, _P, _P, _LL, _P],
+    'gwb_welch_avg': [_P, _LL, _I, _I, _I, _F, _I, _D, _F, _P, _LL, _P],
+    'gwb_interp': [_P, _LL, _I, _I, _D, _D, _I, _P, _LL, _P],
+    'gwb_ist_pre': [_P, _LL, _I, _I, _I, _P, _LL, _P],
+    'gwb_ist_mid': [_P, _LL, _I, _I, _F, _I, _P, _P],
+    'gwb_ist_post': [_P, _LL, _I, _I, _F, _P, _LL, _P],
+    'gwb_d_ip': [_P, _LL, _I, _P, _LL, _P, _I, _I, _F, _P, _LL, _P, _LL, _P],
+    'gwb_sw': [_P, _LL, _I, _I, _P, _P, _P],
+    'gwb_taper_pad': [_P, _LL, _I, _LL, _LL, _P, _P, _P],
+    'gwb_whiten': [_P, _I, _P, _F, _F, _P],
+    'gwb_above': [_P, _LL, _LL, _I, _F, _F, _P, _P, _I, _P, _P],
+    'gwb_apply_gates': [_P, _LL, _P, _I, _P],
+    'gwb_highpass': [],
+    'gwb_resample': [],
 }
 
 
@@ -114,3 +147,18 @@ def require_cuda(*tensors):
     for t in tensors:
         if t is not None and not t.is_cuda:
             raise TypeError('gwb200 kernels take CUDA tensors (got a %s tensor)' % t.device)
+
+
+_handles = {}
+
+
+def handle(device=None):
+    """The per-device library handle (owns cached cuFFT plans), created on first use."""
+    dev = torch.cuda.current_device() if device is None else torch.device(device).index
+    h = _handles.get(dev)
+    if h is None:
+        p = ctypes.c_void_p()
+        with torch.cuda.device(dev):
+            call('gwb_create', ctypes.byref(p))
+        h = _handles[dev] = p
+    return h

@@ -1,0 +1,166 @@
+"""The compressed filter's tile-level steps: drop-in for the closures of pipeline/fp_filter.py.
+
+The reference defines these as closures inside its main loop (fp_filter.py:354-370 derive, :576-593 svd_tile,
+:597-613 basis_series, :615-621 stacked_A, :710-714 template norms). Here
+they are functions over explicit arguments, or made by make_closures(...) with the reference's closure variables, so
+a caller can keep the reference's call sites. All array work runs in libgwb200; the one host step is the Hermitian
+eigendecomposition of the tile's n x n Gram matrix (float64 LAPACK, n <= a few hundred), whose input (the Gram
+matrix, O(n^2 flen)) and outputs (Vh, O(r n flen)) are computed on the device in float64 / fp32."""
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+from . import _lib
+
+CH = 1 << 16       # fp_filter.py:42 (kept for reference; the kernels do not chunk)
+RB = 64            # basis rows per inverse-FFT batch (fp_filter.py:43)
+FORMS = {'f16': 0, 'f32': 1, 'bf16x3': 2}
+
+
+def _s():
+    return _lib.stream_ptr()
+
+
+def derive_sw(IPall):
+    """fp_filter.py:363-364: sw = sqrt(mean over segments of IP) (float64 mean), isw = 1/sw (0 where sw = 0)."""
+    _lib.require_cuda(IPall)
+    IPall = IPall.contiguous()
+    nseg, flen = IPall.shape
+    sw = torch.empty(flen, dtype=torch.float32, device=IPall.device)
+    isw = torch.empty_like(sw)
+    _lib.call('gwb_sw', _lib.ptr(IPall), IPall.stride(0), nseg, flen, _lib.ptr(sw), _lib.ptr(isw), _s())
+    return sw, isw
+
+
+def sigma2(H, IPall, df, kmin=0):
+    """Template norms (fp_filter.py:710-714) in float64: sig (n, nseg) = 4 df |H|^2 @ IP^T; norm = 4 df / sqrt(sig)."""
+    _lib.require_cuda(H, IPall)
+    n, flen = H.shape
+    nseg = IPall.shape[0]
+    part_elems = n * nseg * 64
+    part = torch.empty(part_elems, dtype=torch.float64, device=H.device)
+    sig = torch.empty((n, nseg), dtype=torch.float64, device=H.device)
+    _lib.call('gwb_sigma2', _lib.ptr(H), H.stride(0), n, _lib.ptr(IPall), IPall.stride(0), nseg, int(kmin), flen,
+              float(df), _lib.ptr(part), part_elems, _lib.ptr(sig), sig.stride(0), _s())
+    return sig, (4.0 * df) / torch.sqrt(sig)
+
+
+def gram(H, sw, kmin):
+    """G = sum_{k >= kmin} (H sw)(H sw)^H in float64 (complex128, n x n)."""
+    n, flen = H.shape
+    part_elems = 2 * n * n * 128
+    part = torch.empty(part_elems, dtype=torch.float64, device=H.device)
+    G = torch.empty((n, n), dtype=torch.complex128, device=H.device)
+    _lib.call('gwb_gram', _lib.ptr(H), H.stride(0), n, _lib.ptr(sw), int(kmin), flen, _lib.ptr(part), part_elems,
+              _lib.ptr(G), _s())
+    return G
+
+
+def svd_tile(H, sw, kmin, eps):
+    """fp_filter.py:576-593: Gram matrix (float64, device), normalised, Hermitian eigendecomposition (float64 LAPACK on
+    the host), rank r = smallest with worst lost power <= eps, basis filters Vh (device). Returns (r, A, Vh, worst)
+    with A (n, r) and Vh (r, flen) complex64 CUDA tensors."""
+    _lib.require_cuda(H, sw)
+    H = H.contiguous()
+    n, flen = H.shape
+    G = gram(H, sw, kmin).cpu().numpy()
+    nrm = np.sqrt(np.maximum(G.diagonal().real, 1e-30))
+    lam, W = np.linalg.eigh(G / (nrm[:, None] * nrm[None, :]))
+    lam, W = np.maximum(lam[::-1], 0), W[:, ::-1]
+    worst = (1 - ((np.abs(W) ** 2) * lam[None, :]).cumsum(1)).max(0)
+    r = min(int((worst > eps).sum()) + 1, n)
+    Wr = W[:, :r]
+    s_r = np.sqrt(np.maximum(lam[:r], 1e-12 * lam[0]))
+    Bm = ((Wr.conj().T / s_r[:, None]) / nrm[None, :]).astype(np.complex64)
+    A = ((Wr * s_r[None, :]).conj() * nrm[:, None]).astype(np.complex64)
+    Bm_d = torch.from_numpy(np.ascontiguousarray(Bm)).to(H.device)
+    Vh = torch.empty((r, flen), dtype=torch.complex64, device=H.device)
+    _lib.call('gwb_basis_vh', _lib.ptr(Bm_d), Bm_d.stride(0), r, n, _lib.ptr(H), H.stride(0), _lib.ptr(sw), int(kmin),
+              flen, _lib.ptr(Vh), Vh.stride(0), _s())
+    return r, torch.from_numpy(np.ascontiguousarray(A)).to(H.device), Vh, float(worst[r - 1])
+
+
+def kp_of(r):
+    """K padded to a multiple of 64 for 2 r real rows (fp_filter.py:601)."""
+    return ((2 * r + 63) // 64) * 64
+
+
+class BasisWorkspace:
+    """Device buffers of the basis series for one (tlen, batch) shape: the zero-padded transform input q, the
+    transform output, the scale reduction's partials and ticket. q's upper half is zeroed once and never written."""
+
+    def __init__(self, tlen, flen, rows=RB, device='cuda', npartials=1024):
+        self.tlen, self.flen, self.rows = tlen, flen, rows
+        self.q = torch.zeros((rows, tlen), dtype=torch.complex64, device=device)
+        self.zb = torch.empty((rows, tlen), dtype=torch.complex64, device=device)
+        self.partials = torch.empty(npartials, dtype=torch.float64, device=device)
+        self.ticket = torch.zeros(1, dtype=torch.int32, device=device)
+        self.scale = torch.empty(1, dtype=torch.float32, device=device)
+        self.ones = torch.ones(flen, dtype=torch.float32, device=device)
+
+
+def basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16'):
+    """Z rows: real parts of the r basis series over [a0, a0+Tn) divided by the first batch's rms, then the imaginary
+    parts (fp_filter.py:597-613), written into a preallocated Z (Kp, >= Tn) (rows >= 2r left as they are). D: one
+    segment's data (flen,) complex64; isw: 1/sw (or None when D is already divided by sw). Returns the device scale."""
+    r, flen = Vh.shape
+    assert flen == ws.flen and Tn <= ws.tlen - a0
+    f = FORMS[form]
+    iw = ws.ones if isw is None else isw
+    for c0 in range(0, r, ws.rows):
+        nb = min(ws.rows, r - c0)
+        _lib.call('gwb_basis_premul', _lib.ptr(Vh[c0:]), Vh.stride(0), nb, _lib.ptr(D), flen, 1, _lib.ptr(iw), flen,
+                  _lib.ptr(ws.q), ws.q.stride(0), _s())
+        _lib.call('gwb_fft_c2c', _lib.handle(), _lib.ptr(ws.q), _lib.ptr(ws.zb), ws.tlen, nb, ws.tlen, ws.tlen, 1, _s())
+        if c0 == 0:
+            _lib.call('gwb_basis_scale', _lib.ptr(ws.zb), ws.tlen, nb, int(a0), int(Tn), _lib.ptr(ws.partials),
+                      ws.partials.numel(), _lib.ptr(ws.ticket), _lib.ptr(ws.scale), _s())
+        _lib.call('gwb_basis_pack', _lib.ptr(ws.zb), ws.tlen, nb, r, c0, int(a0), int(Tn), _lib.ptr(ws.scale), f,
+                  _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0), _s())
+    return ws.scale
+
+
+def _z_dtype(form):
+    return {'f16': torch.float16, 'f32': torch.float32, 'bf16x3': torch.bfloat16}[form]
+
+
+def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='f16'):
+    """As = A (norm scale); Are = [Re As, -Im As], Aim = [Im As, Re As], zero-padded to Kp (fp_filter.py:615-621).
+    nrm: float64 CUDA vector (a strided view is fine); scale: device float32 scalar."""
+    n, r = A.shape
+    _lib.call('gwb_stacked_a', _lib.ptr(A), A.stride(0), n, r, _lib.ptr(nrm), nrm.stride(0), _lib.ptr(scale), Kp,
+              FORMS[form], _lib.ptr(Are), _lib.ptr(Aim), _lib.ptr(Are_lo), _lib.ptr(Aim_lo), Are.stride(0), _s())
+
+
+def make_closures(kmin, flen, tlen, sw, eps_b, dev='cuda', form='f16'):
+    """The reference's closures over (kmin, flen, tlen, sw, eps_b, RB, qz, dev) (fp_filter.py:576-621): returns an
+    object with svd_tile(H), basis_series(Vh, Dws, a0, Tn) and stacked_A(A, nrm_s, scale, Kp), same arguments and
+    results as the reference (CUDA tensors; scale a Python float, as the reference returns)."""
+    ws = BasisWorkspace(tlen, flen, RB, dev)
+
+    def _svd_tile(H):
+        return svd_tile(H, sw, kmin, eps_b)
+
+    def _basis_series(Vh, Dws, a0, Tn):
+        r = Vh.shape[0]
+        Kp = kp_of(r)
+        Z = torch.zeros((Kp, Tn), dtype=_z_dtype(form), device=Dws.device)
+        Zlo = torch.zeros_like(Z) if form == 'bf16x3' else None
+        sc = basis_series_into(ws, Vh, Dws.contiguous(), None, a0, Tn, Z, Zlo, form)
+        scale = float(sc.item())
+        return (Z, scale) if Zlo is None else ((Z, Zlo), scale)
+
+    def _stacked_A(A, nrm_s, scale, Kp):
+        n = A.shape[0]
+        dt = _z_dtype(form)
+        Are = torch.empty((n, Kp), dtype=dt, device=A.device)
+        Aim = torch.empty_like(Are)
+        lo = (torch.empty_like(Are), torch.empty_like(Are)) if form == 'bf16x3' else (None, None)
+        sc = torch.tensor([scale], dtype=torch.float32, device=A.device)
+        nrm = torch.as_tensor(nrm_s, device=A.device).to(torch.float64)
+        stacked_A_into(A.contiguous(), nrm, sc, Kp, Are, Aim, lo[0], lo[1], form)
+        return (Are, Aim) if form != 'bf16x3' else ((Are, lo[0]), (Aim, lo[1]))
+
+    return SimpleNamespace(svd_tile=_svd_tile, basis_series=_basis_series, stacked_A=_stacked_A, ws=ws)
+

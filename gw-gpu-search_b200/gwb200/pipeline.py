@@ -1,0 +1,204 @@
+"""Batched matched filter over many segments: the device-resident replacement of fp_filter.py's per (tile, segment)
+loop (pipeline/fp_filter.py:700-888).
+
+Layout in HBM (all resident for a run):
+  H      (M, flen) complex64   every template of the bank, tile after tile (rows sorted by chirp time); read by the
+                               Gram/Vh setup and by the exact stage
+  Vh_t   (r_t, flen) complex64 per tile basis filters; A_t (n_t, r_t) complex64 mixing matrices
+  D, IP  (S, flen)             over-whitened data and inverse PSD of every segment
+  sig    (M, S) float64        template norms
+  Z      (Kp, Tn)              basis series of the current (tile, segment), fp16 / fp32 / bf16 hi+lo
+  V, I   (n, nw)               per-window max |SNR|^2 and sample straight from the GEMM epilogue (group = cw/128)
+  cands, groups, units         candidate lists of the whole step, appended by the selection kernel
+One step = every tile against a batch of segments: basis series -> stacked A -> fused GEMM (+|z|^2, window argmax)
+-> selection, then one exact stage over all candidates (edges, binned sums, finalisation) and a single copy of the
+results to the host. The step's launch sequence is fixed, so it can be captured once in a CUDA graph and replayed.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _exact, _lib, fp_filter, templates
+
+BN = 128
+
+
+@dataclass
+class FilterConfig:
+    f_low: float = 20.0
+    sr: float = 2048.0
+    tile: int = 256
+    eps: float = 1e-3
+    nbins: int = 16
+    cluster_window: float = 1.0
+    snr_threshold: float = 5.5
+    margin: float = 0.04
+    form: str = 'bf16x3'
+    cand_cap: int = 1 << 20
+    seg_batch: int = 16
+
+
+class Bank:
+    """Template bank on the device: templates for every row (tile order), and each tile's SVD compression."""
+
+    def __init__(self, params, flen, df, sw, cfg: FilterConfig, device='cuda'):
+        self.cfg = cfg
+        self.flen, self.df = flen, df
+        self.kmin = int(cfg.f_low / df)
+        self.tiles = templates.tiles(params, cfg.tile, cfg.f_low)
+        self.order = np.concatenate(self.tiles)                     # global row -> bank index
+        M = len(self.order)
+        self.M = M
+        self.H = torch.empty((M, flen), dtype=torch.complex64, device=device)
+        km = np.empty(M, np.int32)
+        self.row0 = []
+        r0 = 0
+        for ids in self.tiles:
+            _, k = templates.generate(params, ids, flen, df, cfg.f_low, out=self.H[r0:r0 + len(ids)], device=device)
+            km[r0:r0 + len(ids)] = k
+            self.row0.append(r0)
+            r0 += len(ids)
+        self.kmax = torch.from_numpy(km).to(device)
+        self.kmax_h = km
+        self.nbins = torch.full((M,), cfg.nbins, dtype=torch.int32, device=device)
+        self.svd = []
+        for t, ids in enumerate(self.tiles):
+            Ht = self.H[self.row0[t]:self.row0[t] + len(ids)]
+            r, A, Vh, worst = fp_filter.svd_tile(Ht, sw, self.kmin, cfg.eps)
+            self.svd.append(dict(r=r, A=A, Vh=Vh, worst=worst, Kp=fp_filter.kp_of(r)))
+
+    @property
+    def r_over_n(self):
+        return sum(s['r'] for s in self.svd) / self.M
+
+
+class MatchedFilter:
+    """Runs steps of the batched filter for one bank and one segment geometry (tlen, analysed span)."""
+
+    def __init__(self, bank: Bank, tlen, a0, Tn, cfg: FilterConfig, device='cuda'):
+        self.bank, self.cfg = bank, cfg
+        self.tlen, self.a0 = tlen, a0
+        cw = int(cfg.cluster_window * cfg.sr)
+        assert cw % BN == 0, 'cluster window must be a multiple of %d samples' % BN
+        self.cw, self.group = cw, cw // BN
+        self.nw = Tn // cw
+        self.Tn = self.nw * cw
+        self.form = cfg.form
+        self.ws = fp_filter.BasisWorkspace(tlen, bank.flen, fp_filter.RB, device)
+        Kp = max(s['Kp'] for s in bank.svd)
+        nmax = max(len(t) for t in bank.tiles)
+        dt = fp_filter._z_dtype(self.form)
+        ldz = -(-self.Tn // 8) * 8
+        self.Z = torch.zeros((Kp, ldz), dtype=dt, device=device)
+        self.Zlo = torch.zeros_like(self.Z) if self.form == 'bf16x3' else None
+        self.Are = torch.zeros((nmax, Kp), dtype=dt, device=device)
+        self.Aim = torch.zeros_like(self.Are)
+        self.Are_lo = torch.zeros_like(self.Are) if self.form == 'bf16x3' else None
+        self.Aim_lo = torch.zeros_like(self.Are) if self.form == 'bf16x3' else None
+        self.V = torch.empty((nmax, self.nw), dtype=torch.float32, device=device)
+        self.I = torch.empty((nmax, self.nw), dtype=torch.int32, device=device)
+        cap = cfg.cand_cap
+        self.cands = torch.empty(cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
+        self.groups = torch.empty(cap * _exact.GROUP.itemsize, dtype=torch.uint8, device=device)
+        self.units = torch.empty(cap * _exact.UNIT.itemsize, dtype=torch.uint8, device=device)
+        self.counters = torch.zeros(4, dtype=torch.int32, device=device)
+        self.B = cfg.nbins
+        self.E = torch.empty((cap, self.B + 1), dtype=torch.int32, device=device)
+        self.nchunk = _lib.load().gwb_exact_chunks(bank.flen, bank.kmin)
+        self.slot_cap = cap
+        assert cap <= 1 << 22
+        self.slots = None
+        self.peaks = torch.empty(cap * _exact.PEAK.itemsize, dtype=torch.uint8, device=device)
+        self.thr2 = float((cfg.snr_threshold * (1 - cfg.margin)) ** 2)
+        self.kernel_launches = 0
+
+    def _gemm(self, n, Kp):
+        s = _lib.stream_ptr()
+        Zs = self.Z[:Kp]
+        if self.form == 'f16':
+            _lib.call('gwb_fused_peaks_f16', _lib.ptr(self.Are), _lib.ptr(self.Aim), self.Are.stride(0), _lib.ptr(Zs),
+                      Zs.stride(0), n, Kp, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
+        elif self.form == 'f32':
+            _lib.call('gwb_fused_peaks_f32', _lib.ptr(self.Are), _lib.ptr(self.Aim), self.Are.stride(0), _lib.ptr(Zs),
+                      Zs.stride(0), n, Kp, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
+        else:
+            _lib.call('gwb_fused_peaks_bf16x3', _lib.ptr(self.Are), _lib.ptr(self.Are_lo), _lib.ptr(self.Aim),
+                      _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(Zs), _lib.ptr(self.Zlo[:Kp]), Zs.stride(0), n,
+                      Kp, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
+
+    def tile_segment(self, t, D, isw, sig, seg):
+        """Basis series, stacked A, fused GEMM and window selection of tile t against segment seg (row of D)."""
+        b = self.bank
+        sv = b.svd[t]
+        n = len(b.tiles[t])
+        r, Kp = sv['r'], sv['Kp']
+        scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
+                                            self.Zlo, self.form)
+        nrm = sig[b.row0[t]:b.row0[t] + n, seg]
+        fp_filter.stacked_A_into(sv['A'], nrm, scale, Kp, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form)
+        self._gemm(n, Kp)
+        f = fp_filter.FORMS[self.form]
+        cap = self.cfg.cand_cap
+        _lib.call('gwb_select_windows', _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), n, self.nw, self.thr2,
+                  self.a0, b.row0[t], seg, _lib.ptr(self.Are), _lib.ptr(self.Aim), _lib.ptr(self.Are_lo),
+                  _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), Kp,
+                  f, _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
+                  _lib.ptr(self.counters), _lib.stream_ptr())
+        nlaunch = 2 + 2 * (-(-r // fp_filter.RB)) + 4     # premul+fft per batch, scale, pack per batch, A, GEMM, select
+        self.kernel_launches += nlaunch
+
+    def norms(self, IP):
+        """Template norms for every (row, segment): sig (M, S) float64 = 4 df sum |H|^2 IP (fp_filter.py:710-714)."""
+        b = self.bank
+        nseg = IP.shape[0]
+        sig = torch.empty((b.M, nseg), dtype=torch.float64, device=IP.device)
+        part_elems = b.M * nseg * 16
+        part = torch.empty(part_elems, dtype=torch.float64, device=IP.device)
+        _lib.call('gwb_sigma2', _lib.ptr(b.H), b.H.stride(0), b.M, _lib.ptr(IP), IP.stride(0), nseg, b.kmin, b.flen,
+                  float(b.df), _lib.ptr(part), part_elems, _lib.ptr(sig), sig.stride(0), _lib.stream_ptr())
+        self.kernel_launches += 2
+        return sig
+
+    def exact(self, D, IP, sig):
+        """Edges, binned sums and finalisation over every candidate of the step (device counts, no host sync)."""
+        b = self.bank
+        cap = self.cfg.cand_cap
+        s = _lib.stream_ptr()
+        cnt = self.counters
+        _lib.call('gwb_edges', _lib.ptr(self.units), _lib.ptr(cnt[2:]), cap, _lib.ptr(b.H), b.H.stride(0),
+                  _lib.ptr(IP), IP.stride(0), _lib.ptr(b.nbins), _lib.ptr(b.kmax), b.kmin, self.B, 0, _lib.ptr(self.E), s)
+        if self.slots is None:
+            # every slot the finalisation reads is written by the binned sums: no clearing between steps
+            self.slots = torch.empty((self.slot_cap, self.nchunk, self.B, 2), dtype=torch.float32, device=D.device)
+        _lib.call('gwb_bin_sums', _lib.ptr(self.groups), _lib.ptr(cnt[1:]), cap, _lib.ptr(self.units),
+                  _lib.ptr(self.cands), _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), _lib.ptr(b.H), b.H.stride(0),
+                  _lib.ptr(D), D.stride(0), b.kmin, b.flen, self.tlen, _lib.ptr(self.slots), s)
+        _lib.call('gwb_exact_finalize', _lib.ptr(self.cands), _lib.ptr(cnt[0:]), cap, _lib.ptr(self.units),
+                  _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), b.kmin, b.flen, _lib.ptr(self.slots), _lib.ptr(sig),
+                  sig.stride(0), float(b.df), _lib.ptr(self.peaks), s)
+        self.kernel_launches += 4
+
+    def step(self, D, IP, isw, seg_ids=None):
+        """Queue one step on the current stream: every tile against every segment in seg_ids (rows of D / IP).
+        Nothing is copied back; call results() after the stream is synchronised."""
+        self.counters.zero_()
+        sig = self.norms(IP)
+        segs = range(D.shape[0]) if seg_ids is None else seg_ids
+        for t in range(len(self.bank.tiles)):
+            for s in segs:
+                self.tile_segment(t, D, isw, sig, s)
+        self.exact(D, IP, sig)
+        return sig
+
+    def results(self, sig=None):
+        """Copy the step's candidates and exact values to the host; returns a dict of numpy arrays (all candidates
+        and the kept peaks with exact SNR above the threshold)."""
+        c = self.counters.cpu().numpy()
+        if c[3]:
+            raise _lib.GwbError('select', _lib.GWB_ERR_CAPACITY, 'candidate capacity %d exceeded' % self.cfg.cand_cap)
+        n = int(c[0])
+        cands = _exact.from_dev(self.cands, _exact.CAND, n)
+        peaks = _exact.from_dev(self.peaks, _exact.PEAK, n)
+        keep = peaks['snr'] > self.cfg.snr_threshold
+        return dict(n_candidates=n, n_units=int(c[2]), n_groups=int(c[1]), cands=cands, peaks=peaks, keep=keep)

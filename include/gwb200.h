@@ -39,6 +39,36 @@ extern "C" {
 #define GWB_ERR_ALIGN 10          /* pointer or row stride misaligned for TMA (16 bytes) */
 #define GWB_ERR_CAPACITY 11       /* a bounded output list overflowed (count still reported) */
 
+/* ---- shared record types (device arrays of these are exchanged between entry points) ---------------------- */
+/* A window candidate: global template row (row of the caller's template array), segment, sample index within the
+ * segment's time series, window index, rebuilt SNR sqrt(max |z|^2), the rebuilt complex SNR (zr, zi) and the index
+ * of its unit. */
+typedef struct {
+    int32_t row, seg, sample, window;
+    float approx, zr, zi;
+    int32_t unit;
+} GwbCand;
+/* One exact-stage work unit: up to 8 candidates of one unit (consecutive in the candidate array). */
+typedef struct {
+    int32_t unit, first, count, pad;
+} GwbGroup;
+/* A (template row, segment) pair that has candidates: its chi-squared bin edges are computed once. */
+typedef struct {
+    int32_t row, seg, first, count;
+} GwbUnit;
+/* Exact-stage result for one candidate. */
+typedef struct {
+    float zr, zi;      /* exact complex SNR numerator z = sum_j Z_j */
+    float pw;          /* sum_j |Z_j|^2 */
+    float snr;         /* |z| norm */
+    float chisq;       /* (nb pw - |z|^2) norm^2 */
+    float newsnr;      /* pycbc newsnr of snr and chisq / dof */
+    float fpeak;       /* (2 e[nb-1] - e[nb-2]) df */
+    int32_t dof;       /* 2 nb - 2 */
+} GwbPeak;
+
+typedef struct gwb_handle_s* gwb_handle_t;
+
 /* ---- library ---------------------------------------------------------------------------------------------- */
 GWB_API int gwb_version(void);
 GWB_API const char* gwb_status_string(int status);
@@ -69,7 +99,7 @@ GWB_API int gwb_window_peaks(const float* z, long long ldz, int rows, long long 
  *   lda and ldz multiples of 8, base pointers 16-byte aligned.
  * gwb_fused_peaks_bf16x3: split-bf16 form. Each operand is given as a hi and lo bf16 pair (x ~ hi + lo); the
  *   accumulator receives hi*hi + hi*lo + lo*hi. Same alignment rules as f16.
- * gwb_fused_peaks_f32: plain fp32 operands on the fp32 pipe (no tensor cores), same output. K a multiple of 8. */
+ * gwb_fused_peaks_f32: plain fp32 operands on the fp32 pipe (no tensor cores), same output, any K. */
 GWB_API int gwb_fused_peaks_f16(const uint16_t* Are, const uint16_t* Aim, long long lda, const uint16_t* Z, long long ldz,
                         int M, int K, long long Tn, int group, float* V, int32_t* I, long long ldv, void* stream);
 GWB_API int gwb_fused_peaks_bf16x3(const uint16_t* Are_hi, const uint16_t* Are_lo, const uint16_t* Aim_hi,
@@ -78,6 +108,140 @@ GWB_API int gwb_fused_peaks_bf16x3(const uint16_t* Are_hi, const uint16_t* Are_l
                            long long ldv, void* stream);
 GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long lda, const float* Z, long long ldz, int M,
                         int K, long long Tn, int group, float* V, int32_t* I, long long ldv, void* stream);
+
+/* ---- handle and transforms (cuFFT) ----------------------------------------------------------------------------- */
+/* The handle caches cuFFT plans per (kind, n, batch, strides); plans are made on first use of a shape. Transforms are
+ * unnormalised (cuFFT convention), as the reference's norm='forward' inverse transforms and its explicit dt / df
+ * scale factors expect (pipeline/gpu_prep.py:109,148,156,197-199,421; pipeline/fp_filter.py:608). A complex-to-real
+ * transform may overwrite its input. */
+GWB_API int gwb_create(gwb_handle_t* out);
+GWB_API int gwb_destroy(gwb_handle_t h);
+GWB_API int gwb_fft_c2c(gwb_handle_t h, const float* in, float* out, long long n, int batch, long long idist,
+                        long long odist, int inverse, void* stream);
+GWB_API int gwb_fft_r2c(gwb_handle_t h, const float* in, float* out, long long n, int batch, long long idist,
+                        long long odist, void* stream);
+GWB_API int gwb_fft_c2r(gwb_handle_t h, const float* in, float* out, long long n, int batch, long long idist,
+                        long long odist, void* stream);
+
+/* ---- strain conditioning (pipeline/gpu_prep.py) -------------------------------------------------------------- */
+/* Welch / segment frames: out[(r * nfr + f) * ldo + j] = x[r * ldx + s_f + j] * w[j] (w may be NULL), with
+ * s_f = starts[f] if starts is given, else start + f * stride. Replaces the gathers of gpu_prep.py:104-108 and :420. */
+GWB_API int gwb_frames(const float* x, long long ldx, int rows, long long start, long long stride,
+                       const long long* starts, int nfr, int L, const float* w, float* out, long long ldo, void* stream);
+/* Welch average over nfr frames of each row's rFFT X (complex, row stride ldx): p = |X dt|^2 in float32, bins 0 and
+ * nbin-1 halved, then the median (mean of the two middle values for an even count) divided by bias, or the mean;
+ * times fac. Replaces welch's per-row loop (gpu_prep.py:107-124). nfr <= 256. */
+GWB_API int gwb_welch_avg(const float* X, long long ldx, int rows, int nfr, int nbin, float dt, int median,
+                          double bias, float fac, float* psd, long long ldp, void* stream);
+/* np.interp of each PSD row (float64) from k df_old onto k df_new, k < nnew; replaces gpu_prep.interpolate
+ * (gpu_prep.py:128-135). */
+GWB_API int gwb_interp(const float* psd, long long ldp, int rows, int nold, double df_old, double df_new, int nnew,
+                       float* out, long long ldo, void* stream);
+/* Inverse spectrum truncation around two real transforms (gpu_prep.inverse_spectrum_truncation, :138-158):
+ * pre: out (complex) = sqrt(1/P) for kmin <= k < N/2, else 0;  [C2R of length N = 2 (flen - 1)]
+ * mid: q *= df, Hann taper of max_filter_len/2 samples at each end when taper != NULL, zero q[ts:te];  [R2C]
+ * post: out = 1 / |X scale|^2. */
+GWB_API int gwb_ist_pre(const float* P, long long ldp, int rows, int flen, int kmin, float* out, long long ldo,
+                        void* stream);
+GWB_API int gwb_ist_mid(float* q, long long ldq, int rows, int N, float df, int max_filter_len, const float* taper,
+                        void* stream);
+GWB_API int gwb_ist_post(const float* X, long long ldx, int rows, int flen, float scale, float* out, long long ldo,
+                         void* stream);
+/* D = stilde * IP and IP = 1/P (float64, 0 where P <= 0 or k < kmin), P = psd row pick[s] (gpu_stage2,
+ * gpu_prep.py:447-451); stilde = X * scale with X the segment rFFT (scale = 1/sample rate). */
+GWB_API int gwb_d_ip(const float* stilde, long long ldst, int nseg, const float* psd, long long ldp,
+                     const int32_t* pick, int flen, int kmin, float scale, float* D, long long ldd, float* IP,
+                     long long ldip, void* stream);
+/* SVD metric sw = sqrt(mean over segments of IP) (float64 mean) and isw = 1/sw or 0 (fp_filter.py:363-364). */
+GWB_API int gwb_sw(const float* IP, long long ldip, int nseg, int flen, float* sw, float* isw, void* stream);
+/* detect_loud_glitches pieces (gpu_prep.py:175-209): taper_pad ramps the first and last cl samples and centres the
+ * series in a zeroed buffer of length L; whiten scales a spectrum by dt (psd norm)^(-1/2) (0 where psd is inf);
+ * above appends (index, value) for |x df| > thr over samples cl .. n-cl-1 of the centred series, at most cap, with
+ * the true count in *count (zero it first). */
+GWB_API int gwb_taper_pad(const float* s, long long n, int cl, long long L, long long pad_start, float* tapered,
+                          float* sp, void* stream);
+GWB_API int gwb_whiten(float* st, int nbin, const float* psd, float dt, float norm, void* stream);
+GWB_API int gwb_above(const float* wt, long long pad_start, long long n, int cl, float df, float thr, int32_t* idx,
+                      float* val, int cap, int32_t* count, void* stream);
+/* Inverted-Tukey gates in place (gpu_prep.gate_taper, :212-231). gates: ngates x (offset, window samples, taper
+ * samples, i1, i2) as computed on the host from GPS arithmetic; the product is taken in float64. */
+GWB_API int gwb_apply_gates(float* x, long long n, const long long* gates, int ngates, void* stream);
+/* The lal IIR highpass (gpu_prep.py:56-64) and the ldas FIR resampler (:67-84) are not provided: both return
+ * GWB_ERR_NOT_IMPLEMENTED. */
+GWB_API int gwb_highpass(void);
+GWB_API int gwb_resample(void);
+
+/* ---- template bank: templates, norms, tile SVD ------------------------------------------------------------------ */
+/* TaylorF2 templates (the synthetic bank; the reference evaluates IMR waveforms, pipeline/imr_interp.py:56-85):
+ * H[i, k] = f^(-7/6) exp(-i (Psi(f) - pi/4)) for kmin <= k < kmax[i], f = k df, else 0. */
+GWB_API int gwb_taylorf2(const double* m1, const double* m2, const double* chi1, const double* chi2, const double* e0,
+                         const int32_t* kmax, int n, double df, int kmin, int flen, double f_ecc, float* H,
+                         long long ldh, void* stream);
+/* Template norms (fp_filter.py:710-714) in float64: sig[i * ldsig + s] = 4 df sum_{k >= kmin} |H_ik|^2 IP_sk.
+ * part: workspace of part_elems doubles (>= n * nseg; more allows more k-splits). */
+GWB_API int gwb_sigma2(const float* H, long long ldh, int n, const float* IP, long long ldip, int nseg, int kmin,
+                       int flen, double df, double* part, long long part_elems, double* sig, long long ldsig,
+                       void* stream);
+/* Tile Gram matrix (svd_tile, fp_filter.py:578-581) in float64: G (n x n complex128, interleaved) =
+ * sum_{k >= kmin} (H_k sw_k)(H_k sw_k)^H. part: workspace of part_elems doubles (>= 2 n^2). */
+GWB_API int gwb_gram(const float* H, long long ldh, int n, const float* sw, int kmin, int flen, double* part,
+                     long long part_elems, double* G, void* stream);
+/* Basis filters (svd_tile, fp_filter.py:589-591): Vh[j, k] = sum_i Bm[j, i] H[i, k] sw[k] for k >= kmin, else 0;
+ * Bm (r x n complex64). */
+GWB_API int gwb_basis_vh(const float* Bm, long long ldb, int r, int n, const float* H, long long ldh, const float* sw,
+                         int kmin, int flen, float* Vh, long long ldv, void* stream);
+
+/* ---- basis series and stacked A (fp_filter.basis_series / stacked_A, pipeline/fp_filter.py:597-621) ----------- */
+/* q[(s * rows + j) * ldq + k] = conj(Vh[j, k]) (D_s[k] isw[k]) for k < flen, for nseg consecutive segments D_s at
+ * stride ldd. The caller keeps q[.., flen:ldq) zero; q is the input of a C2C inverse transform of length ldq. */
+GWB_API int gwb_basis_premul(const float* Vh, long long ldvh, int rows, const float* D, long long ldd, int nseg,
+                             const float* isw, long long flen, float* q, long long ldq, void* stream);
+/* scale_out = sqrt(mean over rows x [a0, a0+Tn) of |zb|^2 / 2), float64 partial sums in a fixed order. partials:
+ * npartials doubles; ticket: one uint32, zero on entry (left zero). */
+GWB_API int gwb_basis_scale(const float* zb, long long ldz, int rows, long long a0, long long Tn, double* partials,
+                            int npartials, uint32_t* ticket, float* scale_out, void* stream);
+/* Z rows row0+j (real) and r+row0+j (imaginary) = zb[j, a0 + t] / scale for t < Tn. form 0 fp16, 1 fp32, 2 bf16 hi
+ * in Z and lo in Zlo. */
+GWB_API int gwb_basis_pack(const float* zb, long long ldzb, int rows, int r, int row0, long long a0, long long Tn,
+                           const float* scale, int form, void* Z, void* Zlo, long long ldz, void* stream);
+/* As = A (nrm_i scale); Are = [Re As, -Im As, 0...], Aim = [Im As, Re As, 0...] padded to Kp columns; nrm read at
+ * nrm[i * nrm_stride] (float64). form as gwb_basis_pack. */
+GWB_API int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
+                          const float* scale, int Kp, int form, void* Are, void* Aim, void* Are_lo, void* Aim_lo,
+                          long long ldo, void* stream);
+
+/* ---- candidate selection and the exact stage ---------------------------------------------------------------- */
+/* Window candidates of one (tile, segment) (fp_filter.py:745-764): rows i < n whose windowed maximum vw (the fused
+ * GEMM output with group = cw/128) exceeds thr2 become GwbCand records (row0 + i, seg, a0 + iw, window, sqrt(vw),
+ * rebuilt z), appended per row in window order; each row with candidates becomes one GwbUnit and groups of <= 8
+ * candidates become GwbGroup records. counters[0..3]: candidates, groups, units, overflow flag (1 when a capacity was
+ * exceeded; the row is then dropped). */
+GWB_API int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2,
+                               long long a0, int row0, int seg, const void* Are, const void* Aim, const void* Are_lo,
+                               const void* Aim_lo, long long lda, const void* Z, const void* Zlo, long long ldz, int Kp,
+                               int form, GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units,
+                               int unit_cap, int32_t* counters, void* stream);
+/* Chi-squared bin edges per unit (multi_filter.edges_per_template, pipeline/multi_filter.py:264-282; the fused
+ * kernel of chisq_edges.py:92-143): E[u, 0..B] int32, B >= max nbins. Unit count = min(*ucount, umax) when ucount is
+ * not NULL, else umax. nbins and kmax are indexed by the unit's row. offset_mode 1 reproduces the reference's
+ * row-offset comparison (cs/tot + u > u + j/nb). */
+GWB_API int gwb_edges(const GwbUnit* units, const int32_t* ucount, int umax, const float* H, long long ldh,
+                      const float* IP, long long ldip, const int32_t* nbins, const int32_t* kmax, int kmin, int B,
+                      int offset_mode, int32_t* E, void* stream);
+/* Binned sums at peaks (chisq_kernel.bin_power_sums, pipeline/chisq_kernel.py:17-121): for every group and every
+ * chunk of the band, Z_j partial sums into slots[(cand * nchunk + chunk) * B + j] (float2; zero slots first).
+ * q_k = conj(H_k) D_k when D is given (fused mode), else q_k = H_k. tlen: the time length N (a power of two). */
+GWB_API int gwb_bin_sums(const GwbGroup* groups, const int32_t* gcount, int gmax, const GwbUnit* units,
+                         const GwbCand* cands, const int32_t* E, int B, const int32_t* nbins, const float* H,
+                         long long ldh, const float* D, long long ldd, int kmin, int flen, long long tlen, float* slots,
+                         void* stream);
+/* Number of band chunks the slots are laid out for. */
+GWB_API int gwb_exact_chunks(int flen, int kmin);
+/* Per candidate: z, pw from the slots (float64 sums), and with sig given (float64, sig[row * ldsig + seg]) snr,
+ * chisq, dof, newsnr (fp_filter.py:837-853, coinc_rank.py:39-46); fpeak (exact_stage.py:236-238). */
+GWB_API int gwb_exact_finalize(const GwbCand* cands, const int32_t* ccount, int cmax, const GwbUnit* units,
+                               const int32_t* E, int B, const int32_t* nbins, int kmin, int flen, const float* slots,
+                               const double* sig, long long ldsig, double df, GwbPeak* out, void* stream);
 
 #ifdef __cplusplus
 }

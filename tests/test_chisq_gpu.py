@@ -1,0 +1,118 @@
+"""GPU parity of the chi-squared edges, the binned sums and the exact stage against the reference's own numpy code
+(tests/golden/edges_exact.npz) and the float64 oracle, with the reference's tolerances: edges within 1 bin and at most
+1e-3 of them different (the reference asserts exact equality of its blocked edges and <= 1 bin for its fused ones,
+fp_filter.py:812-824), snr_rel <= 1e-4, phase <= 1e-4 rad, chisq_rel <= 1e-3 (exact_stage.py:35), and the binned-sum
+test of the reference's tests/test_chisq_kernel_gpu.py (N = 2^21, relative error < 1e-3)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import chisq as oc
+
+pytestmark = pytest.mark.gpu
+
+
+def test_edges_per_template_matches_reference(golden):
+    from gwb200 import chisq_edges, multi_filter
+    g = golden('edges_exact')
+    H = torch.from_numpy(g['H']).cuda()
+    nb = np.maximum(g['nbins'], 1)
+    rows = np.arange(len(nb))
+    E = multi_filter.edges_per_template(None, rows, nb, int(g['kmin']), g['kmax'], H, torch.from_numpy(g['IP']).cuda())
+    d = np.abs(E - g['E'])
+    assert d.max() <= 1 and (d > 0).mean() <= 1e-3, (d.max(), (d > 0).mean())
+    E2 = chisq_edges.edges_blocked(None, rows, nb, int(g['kmin']), g['kmax'], H, torch.from_numpy(g['IP']).cuda())
+    d2 = np.abs(E2 - g['E'])
+    assert d2.max() <= 1 and (d2 > 0).mean() <= 1e-3
+
+
+def test_edges_on_random_rows_against_oracle():
+    from gwb200 import multi_filter
+    rng = np.random.default_rng(9)
+    n, flen, kmin = 40, 20001, 500
+    H = (rng.standard_normal((n, flen)) + 1j * rng.standard_normal((n, flen))).astype(np.complex64)
+    ip = rng.uniform(0.5, 2.0, flen).astype(np.float32)
+    ip[:kmin] = 0
+    rows = rng.integers(0, n, 100)
+    nb = rng.integers(1, 40, n)[rows]
+    k1 = rng.integers(flen // 2, flen, n)[rows]
+    # per-peak nb and k1 must be functions of the row
+    nb_row = dict(zip(rows, nb))
+    nb = np.array([nb_row[r] for r in rows])
+    k1_row = dict(zip(rows, k1))
+    k1 = np.array([k1_row[r] for r in rows])
+    E = multi_filter.edges_per_template(None, rows, nb, kmin, k1, torch.from_numpy(H).cuda(), torch.from_numpy(ip).cuda())
+    Er = oc.edges_per_template(rows, nb, kmin, k1, H, ip)
+    d = np.abs(E - Er)
+    assert d.max() <= 1 and (d > 0).mean() <= 1e-3
+
+
+def test_exact_stage_matches_reference(golden):
+    from gwb200 import exact_stage as es
+    g = golden('edges_exact')
+    tile = es.TemplateTile(torch.from_numpy(g['H']).cuda(), g['nbins'], int(g['kmin']), g['kmax'])
+    stage = es.ExactStage(tile)
+    seg = es.SegmentData(torch.from_numpy(g['D']).cuda(), torch.from_numpy(g['IP']).cuda(), float(g['df']),
+                         int(g['tlen']))
+    pv = stage.evaluate(seg, es.PeakRequest(g['rows'], g['samples']))
+    rep = es.compare_values(pv.z, pv.pw, g['z'], g['pw'], g['nbins'][g['rows']])
+    t = es.CHECK_TOL
+    assert rep['snr_rel_max'] <= t['snr_rel'] and rep['phase_max'] <= t['phase_rad'], rep
+    assert rep['chisq_rel_max'] <= t['chisq_rel'], rep
+    assert np.array_equal(pv.fpeak, g['fpeak'])
+    # edges of the stage equal the reference's
+    E = stage.edges(seg, np.arange(len(g['nbins'])))
+    assert np.abs(E - g['E']).max() <= 1
+    # an empty request
+    pv0 = stage.evaluate(seg, es.PeakRequest(np.zeros(0, int), np.zeros(0, int)))
+    assert len(pv0.z) == 0
+
+
+def test_regen_tile_is_refused():
+    from gwb200 import exact_stage as es
+    H = torch.zeros((2, 9), dtype=torch.complex64, device='cuda')
+    with pytest.raises(NotImplementedError):
+        es.ExactStage(es.TemplateTile(H, np.ones(2), 1, np.full(2, 8), coarse=object()))
+
+
+def test_bin_power_sums_reference_case():
+    """The reference's own GPU unit test (tests/test_chisq_kernel_gpu.py): N = 2^21, 4 rows, 15 peaks, 40 random
+    edges above bin 30 * 1024, seed 1; relative error below 1e-3 against a float64 direct sum."""
+    from gwb200 import chisq_kernel
+    rng = np.random.default_rng(1)
+    N = 2 ** 21
+    F = N // 2 + 1
+    nrow = 4
+    q = np.zeros((nrow, N), np.complex64)
+    q[:, :F] = (rng.standard_normal((nrow, F)) + 1j * rng.standard_normal((nrow, F))).astype(np.complex64)
+    rows = np.array([0, 0, 0, 1, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 3])
+    times = rng.integers(0, N, len(rows))
+    nb = 40
+    edges_row = np.sort(rng.choice(np.arange(30 * 1024, F), size=(nrow, nb + 1), replace=False), axis=1)
+    E = edges_row[rows]
+    got, z = chisq_kernel.bin_power_sums(torch.from_numpy(q).cuda(), rows, times, E, want_z=True)
+    ref, zr = oc.bin_power_sums(q, rows, times, E, want_z=True)
+    rel = np.abs(got - ref) / ref
+    assert rel.max() < 1e-3, rel.max()
+    assert (np.abs(z - zr) / np.abs(zr)).max() < 1e-3
+
+
+def test_bin_power_sums_fused_against_oracle():
+    from gwb200 import chisq_kernel
+    rng = np.random.default_rng(2)
+    tlen = 1 << 16
+    flen = tlen // 2 + 1
+    H = (rng.standard_normal((5, flen)) + 1j * rng.standard_normal((5, flen))).astype(np.complex64)
+    d = (rng.standard_normal(flen) + 1j * rng.standard_normal(flen)).astype(np.complex64)
+    rows = np.array([4, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 3])       # one row with 9 peaks: two groups
+    times = rng.integers(0, tlen, len(rows))
+    times[3] = times[2]                                           # a duplicate peak
+    times[0] = tlen - 1
+    edges_row = np.sort(rng.choice(np.arange(300, flen), size=(5, 17), replace=False), axis=1)
+    E = edges_row[rows]
+    pw, z = chisq_kernel.bin_power_sums(torch.from_numpy(H).cuda(), rows, times, E, want_z=True,
+                                        d=torch.from_numpy(d).cuda(), n_time=tlen)
+    pwr, zr = oc.bin_power_sums(H, rows, times, E, want_z=True, d=d, n_time=tlen)
+    assert (np.abs(pw - pwr) / pwr).max() < 1e-4
+    assert (np.abs(z - zr) / np.abs(zr)).max() < 1e-4
+    assert pw[3] == pw[2] and z[3] == z[2]

@@ -1,0 +1,92 @@
+"""GPU parity of the bank and tile steps: TaylorF2 templates, sigma^2 (float64), sw, the tile SVD, basis series and
+stacked A, against the oracle and the reference's own closures (tests/golden/filt_tile.npz)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import filt as of
+from oracle import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def test_taylorf2_matches_oracle():
+    from gwb200 import templates
+    flen, df = (1 << 17) + 1, 1 / 64.
+    bank = dict(mass1=np.array([30.0, 5.0, 60.0, 12.0]), mass2=np.array([25.0, 3.2, 40.0, 9.0]),
+                spin1z=np.array([0.0, 0.5, -0.8, 0.3]), spin2z=np.array([0.0, -0.2, 0.4, 0.0]),
+                ecc=np.array([0.0, 0.0, 0.2, 0.1]))
+    H, km = templates.generate(bank, np.arange(4), flen, df)
+    H = H.cpu().numpy()
+    for i in range(4):
+        ref = synth.taylorf2(flen, df, bank['mass1'][i], bank['mass2'][i], bank['spin1z'][i], bank['spin2z'][i],
+                             bank['ecc'][i])
+        ref[km[i]:] = 0                        # the bin at f_ISCO itself may fall on either side; compare below kend
+        k = np.arange(int(20 / df), km[i])
+        rel = np.abs(H[i, k] - ref[k]) / np.abs(ref[k])
+        assert rel.max() < 2e-5, (i, rel.max())
+        assert (H[i, :int(20 / df)] == 0).all() and (H[i, km[i]:] == 0).all()
+
+
+def test_sigma2_and_sw_match_oracle(golden):
+    from gwb200 import fp_filter
+    g = golden('filt_tile')
+    H = torch.from_numpy(g['H']).cuda()
+    IP = np.stack([g['IP'], g['IP'] * 0.5, g['IP'] * 2]).astype(np.float32)
+    sig, norm = fp_filter.sigma2(H, torch.from_numpy(IP).cuda(), float(g['df']))
+    sref, _ = of.sigma2(g['H'], IP, float(g['df']))
+    np.testing.assert_allclose(sig.cpu().numpy(), sref, rtol=1e-12)
+    sw, isw = fp_filter.derive_sw(torch.from_numpy(IP).cuda())
+    swr, iswr = of.derive_sw(IP)
+    assert np.array_equal(sw.cpu().numpy(), swr) and np.array_equal(isw.cpu().numpy(), iswr)
+
+
+def test_svd_tile_matches_reference(golden):
+    from gwb200 import fp_filter
+    g = golden('filt_tile')
+    H = torch.from_numpy(g['H']).cuda()
+    sw = torch.from_numpy(g['sw']).cuda()
+    G = fp_filter.gram(H, sw, int(g['kmin'])).cpu().numpy()
+    Gr = of.gram(g['H'], g['sw'], int(g['kmin']))
+    np.testing.assert_allclose(G, Gr, rtol=1e-10, atol=1e-12 * np.abs(Gr).max())
+    r, A, Vh, worst = fp_filter.svd_tile(H, sw, int(g['kmin']), float(g['eps']))
+    assert r == int(g['r'])
+    assert abs(worst - float(g['worst'])) < 2e-5
+    rec = A.cpu().numpy().astype(np.complex128) @ Vh.cpu().numpy().astype(np.complex128)
+    rec_ref = g['A'].astype(np.complex128) @ g['Vh'].astype(np.complex128)
+    assert (np.linalg.norm(rec - rec_ref, axis=1) / np.linalg.norm(rec_ref, axis=1)).max() < 2e-5
+
+
+@pytest.mark.parametrize('form', ['f16', 'f32', 'bf16x3'])
+def test_basis_series_and_gemm_rebuild_the_reference_snr(golden, form):
+    """Basis series + stacked A + fused GEMM (per-sample max over 128 blocks) rebuild the reference's SNR series."""
+    from gwb200 import fp_filter, fp_gemm
+    g = golden('filt_tile')
+    H = torch.from_numpy(g['H']).cuda()
+    sw = torch.from_numpy(g['sw']).cuda()
+    cl = fp_filter.make_closures(int(g['kmin']), H.shape[1], int(g['tlen']), sw, float(g['eps']), form=form)
+    r, A, Vh, worst = cl.svd_tile(H)
+    Dws = torch.from_numpy(g['D'] * g['isw']).cuda()
+    a0, Tn = int(g['a0']), int(g['Tn'])
+    Z, scale = cl.basis_series(Vh, Dws, a0, Tn)
+    assert abs(scale - float(g['scale'])) < 1e-5 * float(g['scale'])
+    Are, Aim = cl.stacked_A(A, torch.from_numpy(g['nrm_s']).cuda(), scale, fp_filter.kp_of(r))
+    if form == 'bf16x3':
+        V, I = fp_gemm.fused_peaks_split(Are[0], Are[1], Aim[0], Aim[1], Z[0], Z[1], H.shape[0], Tn)
+        zf = (Z[0].float() + Z[1].float()).cpu().numpy()
+        ar = (Are[0].float() + Are[1].float()).cpu().numpy()
+        ai = (Aim[0].float() + Aim[1].float()).cpu().numpy()
+    else:
+        V, I = fp_gemm.fused_peaks(Are, Aim, Z, H.shape[0], Tn)
+        zf, ar, ai = Z.float().cpu().numpy(), Are.float().cpu().numpy(), Aim.float().cpu().numpy()
+    # the SNR series these operands define, against the reference's fp16 operands
+    snr = np.hypot(ar @ zf, ai @ zf)
+    snr_ref = np.hypot(g['Are'].astype(np.float32) @ g['Z'].astype(np.float32),
+                       g['Aim'].astype(np.float32) @ g['Z'].astype(np.float32))
+    tol = 3e-3 if form == 'f16' else 2e-3          # the reference's own operands are fp16
+    assert np.abs(snr - snr_ref).max() < tol * snr_ref.max()
+    # the GEMM's block maxima are the maxima of that series
+    Vr = (snr ** 2).reshape(snr.shape[0], -1, 128).max(2)
+    np.testing.assert_allclose(V.cpu().numpy(), Vr, rtol=1e-4)
+    t = int(float(g['t0']) * 2048) - a0
+    assert abs(int(I[3].cpu().numpy()[np.argmax(V[3].cpu().numpy())]) - t) <= 2
