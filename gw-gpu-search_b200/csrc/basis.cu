@@ -100,12 +100,15 @@ __global__ void pack_kernel(const float2* __restrict__ zb, long long ldzb, int r
 
 template <int FORM>
 __global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, int n, int r, const double* __restrict__ nrm,
-                                 long long nrm_stride, const float* __restrict__ scale, int Kp, void* __restrict__ Are,
+                                 long long nrm_stride, double df4, const float* __restrict__ scale, int Kp,
+                                 void* __restrict__ Are,
                                  void* __restrict__ Aim, void* __restrict__ Are_lo, void* __restrict__ Aim_lo,
                                  long long ldo) {
     const int i = blockIdx.x;
     if (i >= n) return;
-    const float f = (float)nrm[(long long)i * nrm_stride] * *scale;
+    // nrm holds the norm itself, or sigma^2 when df4 = 4 df > 0 (norm = 4 df / sqrt(sigma^2), fp_filter.py:714)
+    const double v = nrm[(long long)i * nrm_stride];
+    const float f = (float)(df4 > 0.0 ? df4 / sqrt(v) : v) * *scale;
     for (int c = threadIdx.x; c < Kp; c += blockDim.x) {
         float re = 0.f, im = 0.f;
         if (c < r) {
@@ -275,7 +278,7 @@ int gwb_basis_pack(const float* zb, long long ldzb, int rows, int r, int row0, l
     return GWB_OK;
 }
 
-int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
+int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride, double df4,
                   const float* scale, int Kp, int form, void* Are, void* Aim, void* Are_lo, void* Aim_lo,
                   long long ldo, void* stream) {
     using namespace gwb;
@@ -286,9 +289,9 @@ int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm
                   "stacked_a: n=%d r=%d Kp=%d", n, r, Kp);
     cudaStream_t s = (cudaStream_t)stream;
     const float2* a = reinterpret_cast<const float2*>(A);
-    if (form == 0) stacked_a_kernel<0><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
-    else if (form == 1) stacked_a_kernel<1><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
-    else stacked_a_kernel<2><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
+    if (form == 0) stacked_a_kernel<0><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
+    else if (form == 1) stacked_a_kernel<1><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
+    else stacked_a_kernel<2><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
     GWB_LAUNCH_CHECK("stacked_a_kernel");
     return GWB_OK;
 }

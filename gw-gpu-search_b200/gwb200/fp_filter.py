@@ -125,11 +125,13 @@ def _z_dtype(form):
     return {'f16': torch.float16, 'f32': torch.float32, 'bf16x3': torch.bfloat16}[form]
 
 
-def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='f16'):
+def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='f16', df4=0.0):
     """As = A (norm scale); Are = [Re As, -Im As], Aim = [Im As, Re As], zero-padded to Kp (fp_filter.py:615-621).
-    nrm: float64 CUDA vector (a strided view is fine); scale: device float32 scalar."""
+    nrm: float64 CUDA vector (a strided view is fine), the norms, or sigma^2 when df4 = 4 df is given; scale: device
+    float32 scalar."""
     n, r = A.shape
-    _lib.call('gwb_stacked_a', _lib.ptr(A), A.stride(0), n, r, _lib.ptr(nrm), nrm.stride(0), _lib.ptr(scale), Kp,
+    _lib.call('gwb_stacked_a', _lib.ptr(A), A.stride(0), n, r, _lib.ptr(nrm), nrm.stride(0), float(df4),
+              _lib.ptr(scale), Kp,
               FORMS[form], _lib.ptr(Are), _lib.ptr(Aim), _lib.ptr(Are_lo), _lib.ptr(Aim_lo), Are.stride(0), _s())
 
 

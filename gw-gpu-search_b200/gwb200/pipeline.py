@@ -136,7 +136,8 @@ class MatchedFilter:
         scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
                                             self.Zlo, self.form)
         nrm = sig[b.row0[t]:b.row0[t] + n, seg]
-        fp_filter.stacked_A_into(sv['A'], nrm, scale, Kp, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form)
+        fp_filter.stacked_A_into(sv['A'], nrm, scale, Kp, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
+                                 df4=4.0 * b.df)
         self._gemm(n, Kp)
         f = fp_filter.FORMS[self.form]
         cap = self.cfg.cand_cap

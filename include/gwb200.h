@@ -204,11 +204,12 @@ GWB_API int gwb_basis_scale(const float* zb, long long ldz, int rows, long long 
  * in Z and lo in Zlo. */
 GWB_API int gwb_basis_pack(const float* zb, long long ldzb, int rows, int r, int row0, long long a0, long long Tn,
                            const float* scale, int form, void* Z, void* Zlo, long long ldz, void* stream);
-/* As = A (nrm_i scale); Are = [Re As, -Im As, 0...], Aim = [Im As, Re As, 0...] padded to Kp columns; nrm read at
- * nrm[i * nrm_stride] (float64). form as gwb_basis_pack. */
+/* As = A (norm_i scale); Are = [Re As, -Im As, 0...], Aim = [Im As, Re As, 0...] padded to Kp columns. nrm is read
+ * at nrm[i * nrm_stride] (float64): the norm itself when df4 <= 0, else sigma^2 with norm = df4 / sqrt(sigma^2)
+ * (df4 = 4 df). form as gwb_basis_pack. */
 GWB_API int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
-                          const float* scale, int Kp, int form, void* Are, void* Aim, void* Are_lo, void* Aim_lo,
-                          long long ldo, void* stream);
+                          double df4, const float* scale, int Kp, int form, void* Are, void* Aim, void* Are_lo,
+                          void* Aim_lo, long long ldo, void* stream);
 
 /* ---- candidate selection and the exact stage ---------------------------------------------------------------- */
 /* Window candidates of one (tile, segment) (fp_filter.py:745-764): rows i < n whose windowed maximum vw (the fused
