@@ -450,3 +450,74 @@ def prep(argv, xp, inj=None, strain=None):
     out['gates'] = gates
     out['timing'] = {**T1, **out['timing']}
     return out
+
+
+class BatchConditioner:
+    """gpu_stage2 for many datasets of equal length that each hold exactly one analysis segment and one PSD span
+    (a dataset as long as the segment and the Welch span, as the synthetic 512 s chunks are), batched: one set of
+    transforms and kernels for every dataset at once. Output rows are the datasets' D and IP (gpu_prep.py:405-454).
+    Buffers are allocated once for the batch shape, so repeated calls allocate nothing and can be graph-captured."""
+
+    def __init__(self, nds, n, sr, flow, psd_seg_len, psd_seg_stride, psd_num_segments, psd_inverse_length,
+                 trunc_method=None, avg='median', device='cuda'):
+        self.nds, self.n, self.sr, self.flow = nds, n, sr, flow
+        self.tlen = n
+        self.flen = n // 2 + 1
+        self.df = sr / n
+        self.kmin = int(flow / self.df)
+        self.L = int(psd_seg_len * sr + 0.5)
+        self.stride = int(psd_seg_stride * sr + 0.5)
+        nseg, start = _welch_layout(n, self.L, self.stride, psd_num_segments)
+        assert start == 0 and (nseg - 1) * self.stride + self.L == n, 'one PSD span per dataset'
+        self.nfr = nseg
+        self.median = avg == 'median'
+        self.bias = median_bias(nseg)
+        w = np.hanning(self.L).astype(np.float32)
+        self.w = torch.from_numpy(w).to(device)
+        self.fac = float(np.float32(2 * (1. / (1. / sr) / self.L) * self.L / (w * w).sum()))
+        self.pdf = 1. / (1. / sr) / self.L
+        self.mfl = int(psd_inverse_length * sr) if psd_inverse_length else 0
+        self.tw = torch.from_numpy(np.hanning(self.mfl).astype(np.float32)).to(device) if trunc_method == 'hann' else None
+        nb = self.L // 2 + 1
+        self.frames = torch.empty((nds * nseg, self.L), dtype=torch.float32, device=device)
+        self.F = torch.empty((nds * nseg, nb), dtype=torch.complex64, device=device)
+        self.psd_w = torch.empty((nds, nb), dtype=torch.float32, device=device)
+        self.psd = torch.empty((nds, self.flen), dtype=torch.float32, device=device)
+        self.inv = torch.empty((nds, self.flen), dtype=torch.complex64, device=device)
+        self.q = torch.empty((nds, n), dtype=torch.float32, device=device)
+        self.pt = torch.empty((nds, self.flen), dtype=torch.complex64, device=device)
+        self.st = torch.empty((nds, self.flen), dtype=torch.complex64, device=device)
+        self.pick = torch.arange(nds, dtype=torch.int32, device=device)
+        self.D = torch.empty((nds, self.flen), dtype=torch.complex64, device=device)
+        self.IP = torch.empty((nds, self.flen), dtype=torch.float32, device=device)
+        self.launches = 0
+
+    def __call__(self, x):
+        """x: (nds, n) float32 strain (DYN_RANGE_FAC units). Returns (D, IP), each (nds, flen)."""
+        assert tuple(x.shape) == (self.nds, self.n) and x.dtype == torch.float32 and x.is_contiguous()
+        h, s = _lib.handle(), _s()
+        nds, n, L, flen = self.nds, self.n, self.L, self.flen
+        _lib.call('gwb_frames', _lib.ptr(x), n, nds, 0, self.stride, None, self.nfr, L, _lib.ptr(self.w),
+                  _lib.ptr(self.frames), L, s)
+        _lib.call('gwb_fft_r2c', h, _lib.ptr(self.frames), _lib.ptr(self.F), L, nds * self.nfr, L, self.F.stride(0), s)
+        _lib.call('gwb_welch_avg', _lib.ptr(self.F), self.F.stride(0), nds, self.nfr, L // 2 + 1,
+                  float(np.float32(1.0 / self.sr)), int(self.median), float(self.bias), self.fac, _lib.ptr(self.psd_w),
+                  self.psd_w.stride(0), s)
+        _lib.call('gwb_interp', _lib.ptr(self.psd_w), self.psd_w.stride(0), nds, L // 2 + 1, float(self.pdf),
+                  float(self.df), flen, _lib.ptr(self.psd), flen, s)
+        self.launches += 3          # this library's kernels; the transforms are cuFFT's
+        P = self.psd
+        if self.mfl:
+            _lib.call('gwb_ist_pre', _lib.ptr(self.psd), flen, nds, flen, self.kmin, _lib.ptr(self.inv), flen, s)
+            _lib.call('gwb_fft_c2r', h, _lib.ptr(self.inv), _lib.ptr(self.q), n, nds, flen, n, s)
+            _lib.call('gwb_ist_mid', _lib.ptr(self.q), n, nds, n, float(np.float32(self.df)), self.mfl,
+                      _lib.ptr(self.tw), s)
+            _lib.call('gwb_fft_r2c', h, _lib.ptr(self.q), _lib.ptr(self.pt), n, nds, n, flen, s)
+            _lib.call('gwb_ist_post', _lib.ptr(self.pt), flen, nds, flen, float(np.float32(1.0 / (self.df * n))),
+                      _lib.ptr(self.psd), flen, s)
+            self.launches += 3
+        _lib.call('gwb_fft_r2c', h, _lib.ptr(x), _lib.ptr(self.st), n, nds, n, flen, s)
+        _lib.call('gwb_d_ip', _lib.ptr(self.st), flen, nds, _lib.ptr(P), flen, _lib.ptr(self.pick), flen, self.kmin,
+                  float(np.float32(1.0 / self.sr)), _lib.ptr(self.D), flen, _lib.ptr(self.IP), flen, s)
+        self.launches += 1
+        return self.D, self.IP

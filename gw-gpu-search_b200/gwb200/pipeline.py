@@ -112,6 +112,8 @@ class MatchedFilter:
         self.peaks = torch.empty(cap * _exact.PEAK.itemsize, dtype=torch.uint8, device=device)
         self.thr2 = float((cfg.snr_threshold * (1 - cfg.margin)) ** 2)
         self.kernel_launches = 0
+        self.fft_launches = 0
+        self.profile = None      # set to {} to record CUDA events around the GEMM and the basis series
 
     def _gemm(self, n, Kp):
         s = _lib.stream_ptr()
@@ -133,12 +135,21 @@ class MatchedFilter:
         sv = b.svd[t]
         n = len(b.tiles[t])
         r, Kp = sv['r'], sv['Kp']
+        prof = self.profile
+        if prof is not None:
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
         scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
                                             self.Zlo, self.form)
         nrm = sig[b.row0[t]:b.row0[t] + n, seg]
         fp_filter.stacked_A_into(sv['A'], nrm, scale, Kp, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
                                  df4=4.0 * b.df)
+        if prof is not None:
+            e[1].record()
         self._gemm(n, Kp)
+        if prof is not None:
+            e[2].record()
+            prof.setdefault('launches', []).append((e, n, r, Kp))
         f = fp_filter.FORMS[self.form]
         cap = self.cfg.cand_cap
         _lib.call('gwb_select_windows', _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), n, self.nw, self.thr2,
@@ -146,8 +157,9 @@ class MatchedFilter:
                   _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), Kp,
                   f, _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
                   _lib.ptr(self.counters), _lib.stream_ptr())
-        nlaunch = 2 + 2 * (-(-r // fp_filter.RB)) + 4     # premul+fft per batch, scale, pack per batch, A, GEMM, select
-        self.kernel_launches += nlaunch
+        nb = -(-r // fp_filter.RB)
+        self.kernel_launches += 2 * nb + 4      # premul and pack per batch; scale, stacked A, GEMM, selection
+        self.fft_launches += nb
 
     def norms(self, IP):
         """Template norms for every (row, segment): sig (M, S) float64 = 4 df sum |H|^2 IP (fp_filter.py:710-714)."""
@@ -178,7 +190,7 @@ class MatchedFilter:
         _lib.call('gwb_exact_finalize', _lib.ptr(self.cands), _lib.ptr(cnt[0:]), cap, _lib.ptr(self.units),
                   _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), b.kmin, b.flen, _lib.ptr(self.slots), _lib.ptr(sig),
                   sig.stride(0), float(b.df), _lib.ptr(self.peaks), s)
-        self.kernel_launches += 4
+        self.kernel_launches += 3
 
     def step(self, D, IP, isw, seg_ids=None):
         """Queue one step on the current stream: every tile against every segment in seg_ids (rows of D / IP).
