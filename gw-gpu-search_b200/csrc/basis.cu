@@ -67,14 +67,14 @@ __global__ void scale_kernel(const float2* __restrict__ zb, long long ldz, int r
     }
 }
 
-template <int FORM>   // 0 fp16, 1 fp32, 2 bf16 hi/lo
-__global__ void pack_kernel(const float2* __restrict__ zb, long long ldzb, int rows, int r, int row0, long long a0,
+template <int FORM>   // 0 fp16, 1 fp32, 2 bf16 hi/lo, 3 bf16
+__global__ void pack_kernel(const float2* __restrict__ zb, long long ldzb, int rows, int im_off, int row0, long long a0,
                             long long Tn, const float* __restrict__ scale, void* __restrict__ Z, void* __restrict__ Zlo,
                             long long ldz) {
     const int j = blockIdx.y;
     const float inv = 1.0f / *scale;
     const float2* src = zb + (long long)j * ldzb + a0;
-    const long long re_row = row0 + j, im_row = r + row0 + j;
+    const long long re_row = row0 + j, im_row = im_off + row0 + j;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < Tn; t += (long long)gridDim.x * blockDim.x) {
         const float2 v = src[t];
         const float xr = v.x * inv, xi = v.y * inv;
@@ -86,6 +86,10 @@ __global__ void pack_kernel(const float2* __restrict__ zb, long long ldzb, int r
             float* z = static_cast<float*>(Z);
             z[re_row * ldz + t] = xr;
             z[im_row * ldz + t] = xi;
+        } else if (FORM == 3) {
+            __nv_bfloat16* z = static_cast<__nv_bfloat16*>(Z);
+            z[re_row * ldz + t] = __float2bfloat16_rn(xr);
+            z[im_row * ldz + t] = __float2bfloat16_rn(xi);
         } else {
             __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(Z);
             __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(Zlo);
@@ -100,7 +104,7 @@ __global__ void pack_kernel(const float2* __restrict__ zb, long long ldzb, int r
 
 template <int FORM>
 __global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, int n, int r, const double* __restrict__ nrm,
-                                 long long nrm_stride, double df4, const float* __restrict__ scale, int Kp,
+                                 long long nrm_stride, double df4, const float* __restrict__ scale, int Kp, int kh,
                                  void* __restrict__ Are,
                                  void* __restrict__ Aim, void* __restrict__ Are_lo, void* __restrict__ Aim_lo,
                                  long long ldo) {
@@ -111,7 +115,14 @@ __global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, in
     const float f = (float)(df4 > 0.0 ? df4 / sqrt(v) : v) * *scale;
     for (int c = threadIdx.x; c < Kp; c += blockDim.x) {
         float re = 0.f, im = 0.f;
-        if (c < r) {
+        if (kh > 0) {
+            // compact: one row [Re As (Kh) | Im As (Kh)] in Are; Aim is not written
+            const int cc = c < kh ? c : c - kh;
+            if (cc < r) {
+                const float2 a = A[(long long)i * lda + cc];
+                re = c < kh ? a.x * f : a.y * f;
+            }
+        } else if (c < r) {
             const float2 a = A[(long long)i * lda + c];
             re = a.x * f;
             im = a.y * f;
@@ -121,7 +132,20 @@ __global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, in
             im = a.x * f;
         }
         const long long o = (long long)i * ldo + c;
-        if (FORM == 0) {
+        if (kh > 0) {
+            if (FORM == 0) static_cast<__half*>(Are)[o] = __float2half_rn(re);
+            else if (FORM == 1) static_cast<float*>(Are)[o] = re;
+            else {
+                const __nv_bfloat16 hr = __float2bfloat16_rn(re);
+                static_cast<__nv_bfloat16*>(Are)[o] = hr;
+                if (FORM == 2) static_cast<__nv_bfloat16*>(Are_lo)[o] = __float2bfloat16_rn(re - __bfloat162float(hr));
+            }
+            continue;
+        }
+        if (FORM == 3) {
+            static_cast<__nv_bfloat16*>(Are)[o] = __float2bfloat16_rn(re);
+            static_cast<__nv_bfloat16*>(Aim)[o] = __float2bfloat16_rn(im);
+        } else if (FORM == 0) {
             static_cast<__half*>(Are)[o] = __float2half_rn(re);
             static_cast<__half*>(Aim)[o] = __float2half_rn(im);
         } else if (FORM == 1) {
@@ -140,7 +164,7 @@ __global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, in
 __device__ __forceinline__ float ld_as_float(const void* p, long long i, int form) {
     if (form == 0) return __half2float(static_cast<const __half*>(p)[i]);
     if (form == 1) return static_cast<const float*>(p)[i];
-    return __bfloat162float(static_cast<const __nv_bfloat16*>(p)[i]);
+    return __bfloat162float(static_cast<const __nv_bfloat16*>(p)[i]);    // forms 2 (hi or lo) and 3
 }
 
 // Window candidates of one (tile, segment). One block per template row: windows whose maximum |z|^2 (the fused GEMM's
@@ -152,7 +176,8 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
                               int nw, float thr2, long long a0, int row0, int seg, const void* __restrict__ Are,
                               const void* __restrict__ Aim, const void* __restrict__ Are_lo,
                               const void* __restrict__ Aim_lo, long long lda, const void* __restrict__ Z,
-                              const void* __restrict__ Zlo, long long ldz, int Kp, int form, GwbCand* __restrict__ cands,
+                              const void* __restrict__ Zlo, long long ldz, int Kp, int kh, int form,
+                              GwbCand* __restrict__ cands,
                               int cand_cap, GwbGroup* __restrict__ groups, int group_cap, GwbUnit* __restrict__ units,
                               int unit_cap, int32_t* __restrict__ counters) {
     const int row = blockIdx.x;
@@ -200,15 +225,26 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
             const int pos = s_base + written + before + __popc(m & ((1u << lane) - 1));
             const int col = iw[(long long)row * ldv + w];
             float zr = 0.f, zi = 0.f;
-            for (int c = 0; c < Kp; ++c) {
-                const float zc = ld_as_float(Z, (long long)c * ldz + col, form) +
-                                 (form == 2 ? ld_as_float(Zlo, (long long)c * ldz + col, 2) : 0.f);
-                const float ar = ld_as_float(Are, (long long)row * lda + c, form) +
-                                 (form == 2 ? ld_as_float(Are_lo, (long long)row * lda + c, 2) : 0.f);
-                const float ai = ld_as_float(Aim, (long long)row * lda + c, form) +
-                                 (form == 2 ? ld_as_float(Aim_lo, (long long)row * lda + c, 2) : 0.f);
-                zr = fmaf(ar, zc, zr);
-                zi = fmaf(ai, zc, zi);
+            auto ldz_ = [&](long long c) {
+                return ld_as_float(Z, c * ldz + col, form) + (form == 2 ? ld_as_float(Zlo, c * ldz + col, 2) : 0.f);
+            };
+            auto lda_ = [&](const void* hi, const void* lo, long long c) {
+                return ld_as_float(hi, (long long)row * lda + c, form) +
+                       (form == 2 ? ld_as_float(lo, (long long)row * lda + c, 2) : 0.f);
+            };
+            if (kh > 0) {       // compact operands: A = [ReA | ImA], Z = [ReZ ; ImZ]
+                for (int c = 0; c < kh; ++c) {
+                    const float ar = lda_(Are, Are_lo, c), ai = lda_(Are, Are_lo, kh + c);
+                    const float zc = ldz_(c), zs = ldz_(kh + c);
+                    zr = fmaf(ar, zc, fmaf(-ai, zs, zr));
+                    zi = fmaf(ai, zc, fmaf(ar, zs, zi));
+                }
+            } else {
+                for (int c = 0; c < Kp; ++c) {
+                    const float zc = ldz_(c);
+                    zr = fmaf(lda_(Are, Are_lo, c), zc, zr);
+                    zi = fmaf(lda_(Aim, Aim_lo, c), zc, zi);
+                }
             }
             GwbCand cd;
             cd.row = row0 + row;
@@ -260,57 +296,60 @@ int gwb_basis_scale(const float* zb, long long ldz, int rows, long long a0, long
     return GWB_OK;
 }
 
-int gwb_basis_pack(const float* zb, long long ldzb, int rows, int r, int row0, long long a0, long long Tn,
+int gwb_basis_pack(const float* zb, long long ldzb, int rows, int im_off, int row0, long long a0, long long Tn,
                    const float* scale, int form, void* Z, void* Zlo, long long ldz, void* stream) {
     using namespace gwb;
     GWB_CHECK_ARG(zb && scale && Z && (form != 2 || Zlo), GWB_ERR_ARG, "basis_pack: null pointer");
-    GWB_CHECK_ARG(form >= 0 && form <= 2, GWB_ERR_ARG, "basis_pack: form %d", form);
-    GWB_CHECK_ARG(rows > 0 && row0 >= 0 && row0 + rows <= r && Tn > 0 && a0 >= 0 && a0 + Tn <= ldzb && ldz >= Tn,
-                  GWB_ERR_SHAPE, "basis_pack: rows=%d row0=%d r=%d a0=%lld Tn=%lld", rows, row0, r, a0, Tn);
+    GWB_CHECK_ARG(form >= 0 && form <= 3, GWB_ERR_ARG, "basis_pack: form %d", form);
+    GWB_CHECK_ARG(rows > 0 && row0 >= 0 && row0 + rows <= im_off && Tn > 0 && a0 >= 0 && a0 + Tn <= ldzb && ldz >= Tn,
+                  GWB_ERR_SHAPE, "basis_pack: rows=%d row0=%d im_off=%d a0=%lld Tn=%lld", rows, row0, im_off, a0, Tn);
     const int gx = (int)std::min<long long>(cdiv(Tn, kThreads), 1024);
     dim3 grid(gx, rows);
     const float2* src = reinterpret_cast<const float2*>(zb);
     cudaStream_t s = (cudaStream_t)stream;
-    if (form == 0) pack_kernel<0><<<grid, kThreads, 0, s>>>(src, ldzb, rows, r, row0, a0, Tn, scale, Z, Zlo, ldz);
-    else if (form == 1) pack_kernel<1><<<grid, kThreads, 0, s>>>(src, ldzb, rows, r, row0, a0, Tn, scale, Z, Zlo, ldz);
-    else pack_kernel<2><<<grid, kThreads, 0, s>>>(src, ldzb, rows, r, row0, a0, Tn, scale, Z, Zlo, ldz);
+    if (form == 0) pack_kernel<0><<<grid, kThreads, 0, s>>>(src, ldzb, rows, im_off, row0, a0, Tn, scale, Z, Zlo, ldz);
+    else if (form == 1) pack_kernel<1><<<grid, kThreads, 0, s>>>(src, ldzb, rows, im_off, row0, a0, Tn, scale, Z, Zlo, ldz);
+    else if (form == 2) pack_kernel<2><<<grid, kThreads, 0, s>>>(src, ldzb, rows, im_off, row0, a0, Tn, scale, Z, Zlo, ldz);
+    else pack_kernel<3><<<grid, kThreads, 0, s>>>(src, ldzb, rows, im_off, row0, a0, Tn, scale, Z, Zlo, ldz);
     GWB_LAUNCH_CHECK("pack_kernel");
     return GWB_OK;
 }
 
 int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride, double df4,
-                  const float* scale, int Kp, int form, void* Are, void* Aim, void* Are_lo, void* Aim_lo,
+                  const float* scale, int Kp, int kh, int form, void* Are, void* Aim, void* Are_lo, void* Aim_lo,
                   long long ldo, void* stream) {
     using namespace gwb;
-    GWB_CHECK_ARG(A && nrm && scale && Are && Aim && (form != 2 || (Are_lo && Aim_lo)), GWB_ERR_ARG,
-                  "stacked_a: null pointer");
-    GWB_CHECK_ARG(form >= 0 && form <= 2, GWB_ERR_ARG, "stacked_a: form %d", form);
-    GWB_CHECK_ARG(n > 0 && r > 0 && Kp >= 2 * r && lda >= r && ldo >= Kp, GWB_ERR_SHAPE,
-                  "stacked_a: n=%d r=%d Kp=%d", n, r, Kp);
+    GWB_CHECK_ARG(A && nrm && scale && Are && (kh > 0 || Aim) &&
+                  (form != 2 || (Are_lo && (kh > 0 || Aim_lo))), GWB_ERR_ARG, "stacked_a: null pointer");
+    GWB_CHECK_ARG(form >= 0 && form <= 3, GWB_ERR_ARG, "stacked_a: form %d", form);
+    GWB_CHECK_ARG(n > 0 && r > 0 && lda >= r && ldo >= Kp && (kh > 0 ? (kh >= r && Kp == 2 * kh) : Kp >= 2 * r),
+                  GWB_ERR_SHAPE, "stacked_a: n=%d r=%d Kp=%d kh=%d", n, r, Kp, kh);
     cudaStream_t s = (cudaStream_t)stream;
     const float2* a = reinterpret_cast<const float2*>(A);
-    if (form == 0) stacked_a_kernel<0><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
-    else if (form == 1) stacked_a_kernel<1><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
-    else stacked_a_kernel<2><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, Are, Aim, Are_lo, Aim_lo, ldo);
+    if (form == 0) stacked_a_kernel<0><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
+    else if (form == 1) stacked_a_kernel<1><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
+    else if (form == 2) stacked_a_kernel<2><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
+    else stacked_a_kernel<3><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
     GWB_LAUNCH_CHECK("stacked_a_kernel");
     return GWB_OK;
 }
 
 int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2, long long a0,
                        int row0, int seg, const void* Are, const void* Aim, const void* Are_lo, const void* Aim_lo,
-                       long long lda, const void* Z, const void* Zlo, long long ldz, int Kp, int form, GwbCand* cands,
-                       int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units, int unit_cap, int32_t* counters,
-                       void* stream) {
+                       long long lda, const void* Z, const void* Zlo, long long ldz, int Kp, int kh, int form,
+                       GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units, int unit_cap,
+                       int32_t* counters, void* stream) {
     using namespace gwb;
-    GWB_CHECK_ARG(vw && iw && Are && Aim && Z && cands && groups && units && counters, GWB_ERR_ARG,
+    GWB_CHECK_ARG(vw && iw && Are && (kh > 0 || Aim) && Z && cands && groups && units && counters, GWB_ERR_ARG,
                   "select_windows: null pointer");
-    GWB_CHECK_ARG(form >= 0 && form <= 2 && (form != 2 || (Are_lo && Aim_lo && Zlo)), GWB_ERR_ARG,
+    GWB_CHECK_ARG(form >= 0 && form <= 3 && (form != 2 || (Are_lo && (kh > 0 || Aim_lo) && Zlo)), GWB_ERR_ARG,
                   "select_windows: form %d", form);
+    GWB_CHECK_ARG(kh == 0 || Kp == 2 * kh, GWB_ERR_SHAPE, "select_windows: Kp=%d with kh=%d", Kp, kh);
     GWB_CHECK_ARG(n > 0 && nw >= 0 && ldv >= nw && Kp > 0 && lda >= Kp, GWB_ERR_SHAPE, "select_windows: n=%d nw=%d", n,
                   nw);
     if (nw == 0) return GWB_OK;
     select_kernel<<<n, kThreads, 0, (cudaStream_t)stream>>>(vw, iw, ldv, n, nw, thr2, a0, row0, seg, Are, Aim, Are_lo,
-                                                            Aim_lo, lda, Z, Zlo, ldz, Kp, form, cands, cand_cap, groups,
+                                                            Aim_lo, lda, Z, Zlo, ldz, Kp, kh, form, cands, cand_cap, groups,
                                                             group_cap, units, unit_cap, counters);
     GWB_LAUNCH_CHECK("select_kernel");
     return GWB_OK;

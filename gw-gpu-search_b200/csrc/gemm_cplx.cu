@@ -1,0 +1,389 @@
+// Complex reconstruction GEMM with fused |z|^2 and windowed argmax, compact operand layout, tcgen05 (sm_100a).
+//
+// Same result as the reference's stacked GEMM (pipeline/fp_filter.py:615-621, pipeline/fp_gemm.py:14-33) but with
+// the complex structure used instead of stored: the reference stacks Are = [Re As, -Im As] and Aim = [Im As, Re As]
+// against Z = [Re zb; Im zb]; here A = [Re As | Im As] (each half Kh columns, Kh a multiple of 16, zero-padded past
+// r) and Z = [Re zb; Im zb] (each half Kh rows), and the four products are issued as
+//     z_re = ReA . ReZ - ImA . ImZ      (the minus is the MMA's A-negate bit)
+//     z_im = ImA . ReZ + ReA . ImZ
+// so A takes half the shared memory of Are + Aim and stays resident for any r up to 192 (fp16 / bf16) or 128 (split
+// bf16), while Z streams through a ring of K-chunks by TMA. Work item = (128-sample time tile, 128-row M block); the
+// re and im accumulators of an item sit in 256 TMEM columns, double buffered. Epilogue as the stacked kernel: warps
+// 2-9 read TMEM, form |z|^2 and keep max and first index per row over `group` tiles.
+// Forms: 0 fp16 (one product), 1 bf16 (one product), 2 split bf16 (hi.hi + hi.lo + lo.hi, about 16 bits).
+#include "common.cuh"
+
+namespace gwb {
+namespace {
+
+constexpr int kTile = 128;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;
+constexpr int kATile = 128 * 128;      // 128 rows x 64 two-byte columns
+constexpr int kTmemCols = 512;
+
+struct __align__(64) CplxArgs {
+    CUtensorMap tA[2];   // A hi, A lo: (n, 2 Kh), K-major
+    CUtensorMap tZ[2];   // Z hi, Z lo: (2 Kh, Tn), sample-major
+    float* V;
+    int32_t* I;
+    long long ldv;
+    long long Tn;
+    int M, Kh, ntiles, group, nout, stages, MB, KC;
+    DeviceError* err;
+};
+
+template <int FORM>
+struct Cfg {
+    static constexpr int NH = FORM == 2 ? 2 : 1;          // hi (and lo) copies of each operand
+    static constexpr int NPROD = FORM == 2 ? 3 : 1;
+    static constexpr uint32_t FMT = FORM == 0 ? 0u : 1u;   // f16 or bf16
+};
+
+struct Layout {
+    uint32_t a_tiles, a_bytes, z_off, stage_bytes, x_off, bar_off, total;
+};
+
+__host__ __device__ inline Layout layout_of(int nh, int MB, int Kh, int KC, int stages) {
+    Layout L;
+    L.a_tiles = (uint32_t)((2 * Kh + 63) / 64);
+    L.a_bytes = (uint32_t)MB * nh * L.a_tiles * kATile;
+    L.z_off = L.a_bytes;
+    L.stage_bytes = 2u * nh * 2u * (uint32_t)KC * 128u;   // (re, im) x (hi, lo) x two 64-sample halves
+    L.x_off = L.z_off + (uint32_t)stages * L.stage_bytes;
+    L.bar_off = L.x_off + 2048u;
+    L.total = L.bar_off + (uint32_t)(2 * stages + 6) * 8u + 16u;
+    return L;
+}
+
+template <int FORM>
+__global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_constant__ CplxArgs args) {
+    using C = Cfg<FORM>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+    const int Kh = args.Kh, KC = args.KC, S = args.stages, MB = args.MB;
+    const Layout L = layout_of(C::NH, MB, Kh, KC, S);
+    const int nkc = (Kh + KC - 1) / KC;
+    uint8_t* sA = smem;
+    uint8_t* sZ = smem + L.z_off;
+    float* xv = reinterpret_cast<float*>(smem + L.x_off);
+    int* xi = reinterpret_cast<int*>(smem + L.x_off + 1024);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + S;
+    uint64_t* tfull = bars + 2 * S;
+    uint64_t* tempty = tfull + 2;
+    uint64_t* barA = tempty + 2;
+    uint64_t* done = barA + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * 128 * MB;
+    const int MBe = min(MB, (args.M - m0 + 127) / 128);
+    const long long o0 = (long long)blockIdx.x * args.nout / gridDim.x;
+    const long long o1 = (long long)(blockIdx.x + 1) * args.nout / gridDim.x;
+    const int t_begin = (int)(o0 * args.group);
+    const int t_end = (int)min(o1 * (long long)args.group, (long long)args.ntiles);
+    const int ntl = t_end - t_begin;
+    if (ntl <= 0 || MBe <= 0) return;
+    const int nfill = ntl * nkc;   // Z stages consumed by this CTA
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kEpiWarps);
+        }
+        mbar_init(barA, 1);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, kTmemCols);
+        tmem_relinquish();
+        tc_fence_before();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            for (int h = 0; h < C::NH; ++h) {
+                prefetch_tmap(&args.tA[h]);
+                prefetch_tmap(&args.tZ[h]);
+            }
+            mbar_arrive_expect_tx(barA, (uint32_t)(MBe * C::NH * L.a_tiles * kATile));
+            for (int mb = 0; mb < MBe; ++mb)
+                for (int h = 0; h < C::NH; ++h)
+                    for (int a = 0; a < (int)L.a_tiles; ++a)
+                        tma_load_2d(sA + ((mb * C::NH + h) * L.a_tiles + a) * kATile, &args.tA[h], barA, a * 64,
+                                    m0 + mb * 128);
+            for (int f = 0; f < nfill; ++f) {
+                const int s = f % S;
+                const uint32_t n = (uint32_t)(f / S);
+                const int i = f / nkc, kc = f % nkc;
+                if (*abort_flag) break;
+                if (!mbar_wait_bounded(&empty[s], (n & 1) ^ 1)) {
+                    record_error(args.err, GWB_ERR_TIMEOUT, 201, blockIdx.x, f);
+                    *abort_flag = 1;
+                    break;
+                }
+                mbar_arrive_expect_tx(&full[s], L.stage_bytes);
+                const int x = (t_begin + i) * kTile;
+                uint8_t* st = sZ + s * L.stage_bytes;
+                for (int ri = 0; ri < 2; ++ri)
+                    for (int h = 0; h < C::NH; ++h)
+                        for (int half = 0; half < 2; ++half)
+                            tma_load_2d(st + ((ri * C::NH + h) * 2 + half) * KC * 128, &args.tZ[h], &full[s],
+                                        x + 64 * half, ri * Kh + kc * KC);
+            }
+            mbar_wait_bounded(barA, 0);
+            for (int s = 0; s < S && s < nfill; ++s) {
+                const int nf = (nfill - s + S - 1) / S;
+                mbar_wait_bounded(&full[s], (uint32_t)((nf - 1) & 1));
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc(128, 128, C::FMT, C::FMT, 0, 1);
+            const uint32_t idesc_neg = idesc | (1u << 13);     // negate A
+            const uint32_t a_base = smem_u32(sA), z_base = smem_u32(sZ);
+            bool ok = mbar_wait_bounded(barA, 0);
+            if (!ok) {
+                record_error(args.err, GWB_ERR_TIMEOUT, 202, blockIdx.x, 0);
+                *abort_flag = 1;
+            }
+            tc_fence_after();
+            int f = 0;
+            for (int i = 0; i < ntl && ok; ++i) {
+                for (int kc = 0; kc < nkc && ok; ++kc, ++f) {
+                    const int s = f % S;
+                    if (*abort_flag || !mbar_wait_bounded(&full[s], (uint32_t)((f / S) & 1))) {
+                        record_error(args.err, GWB_ERR_TIMEOUT, 203, blockIdx.x, f);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = z_base + s * L.stage_bytes;
+                    for (int mb = 0; mb < MBe && ok; ++mb) {
+                        const int j = i * MBe + mb, b = j & 1;
+                        if (kc == 0) {
+                            // this item's accumulators must have been read out by the epilogue
+                            const uint32_t u = (uint32_t)(j >> 1);
+                            if (!mbar_wait_bounded(&tempty[b], (u & 1) ^ 1)) {
+                                record_error(args.err, GWB_ERR_TIMEOUT, 204, blockIdx.x, i);
+                                *abort_flag = 1;
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                        }
+                        const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
+                        const int nsteps = min(KC, Kh - kc * KC) / 16;
+                        for (int sk = 0; sk < nsteps; ++sk) {
+                            const int k = kc * KC + sk * 16;
+                            for (int pr = 0; pr < C::NPROD; ++pr) {
+                                const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
+                                const uint32_t abase = a_base + (mb * C::NH + ha) * L.a_tiles * kATile;
+                                const uint32_t are = abase + (k >> 6) * kATile + (k & 63) * 2;
+                                const uint32_t aim = abase + ((Kh + k) >> 6) * kATile + ((Kh + k) & 63) * 2;
+                                const uint32_t zre = st + ((0 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
+                                const uint32_t zim = st + ((1 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
+                                const uint64_t dAre = smem_desc(are, 16, 1024, 2), dAim = smem_desc(aim, 16, 1024, 2);
+                                const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
+                                const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                                const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
+                                umma_f16(dre, dAre, dZre, idesc, acc);
+                                umma_f16(dre, dAim, dZim, idesc_neg, 1u);
+                                umma_f16(dim, dAim, dZre, idesc, acc);
+                                umma_f16(dim, dAre, dZim, idesc, 1u);
+                            }
+                        }
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (ok)
+                    for (int mb = 0; mb < MBe; ++mb) umma_commit(&tfull[(i * MBe + mb) & 1]);
+            }
+            umma_commit(done);
+            mbar_wait_bounded(done, 0);
+        }
+        __syncwarp();
+    } else {
+        const int ew = warp - 2, q = warp & 3, hh = ew >> 2;
+        const int rl = 32 * q + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * q) << 16);
+        float wb0 = -1.f, wb1 = -1.f;
+        int wi0 = 0, wi1 = 0;
+        for (int i = 0; i < ntl; ++i) {
+            const int t = t_begin + i;
+            const long long col0 = (long long)t * kTile;
+            const bool full_tile = col0 + kTile <= args.Tn;
+#pragma unroll
+            for (int mb = 0; mb < 2; ++mb) {
+                if (mb >= MBe) break;
+                const int j = i * MBe + mb, b = j & 1;
+                const uint32_t u = (uint32_t)(j >> 1);
+                float best = -1.f;
+                int bi = 0;
+                if (*abort_flag || !mbar_wait_bounded(&tfull[b], u & 1)) {
+                    record_error(args.err, GWB_ERR_TIMEOUT, 205, blockIdx.x, i);
+                    *abort_flag = 1;
+                } else {
+                    tc_fence_after();
+#pragma unroll
+                    for (int c = 0; c < 64; c += 32) {
+                        uint32_t re[32], im[32];
+                        tmem_ld_32x32b_x32(lane_base + (uint32_t)(b * 256 + hh * 64 + c), re);
+                        tmem_ld_32x32b_x32(lane_base + (uint32_t)(b * 256 + 128 + hh * 64 + c), im);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int jj = 0; jj < 32; ++jj) asm volatile("" : "+r"(re[jj]), "+r"(im[jj]));
+                        const int cb = hh * 64 + c;
+#pragma unroll
+                        for (int jj = 0; jj < 32; ++jj) {
+                            const float xr = __uint_as_float(re[jj]), xm = __uint_as_float(im[jj]);
+                            float p = fmaf(xr, xr, xm * xm);
+                            if (!full_tile && col0 + cb + jj >= args.Tn) p = -1.f;
+                            if (p > best) {
+                                best = p;
+                                bi = cb + jj;
+                            }
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[b]);
+                if (hh == 1) {
+                    xv[(j & 1) * 128 + rl] = best;
+                    xi[(j & 1) * 128 + rl] = bi;
+                }
+                named_bar_sync(1, 32 * kEpiWarps);
+                if (hh == 0) {
+                    const float ob = xv[(j & 1) * 128 + rl];
+                    const int oi = xi[(j & 1) * 128 + rl];
+                    if (ob > best) {
+                        best = ob;
+                        bi = oi;
+                    }
+                    const int gi = (int)(col0 + bi);
+                    const bool first = (t % args.group) == 0;
+                    const bool last = ((t + 1) % args.group) == 0 || t == args.ntiles - 1;
+                    float& wb = (mb == 0) ? wb0 : wb1;
+                    int& wi = (mb == 0) ? wi0 : wi1;
+                    if (first || best > wb) {
+                        wb = best;
+                        wi = gi;
+                    }
+                    if (last) {
+                        const int row = m0 + mb * 128 + rl;
+                        if (row < args.M) {
+                            const long long o = t / args.group;
+                            args.V[(long long)row * args.ldv + o] = wb;
+                            args.I[(long long)row * args.ldv + o] = wi;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+template <int FORM>
+int launch_cplx(const uint16_t* const* A, const uint16_t* const* Zp, long long lda, long long ldz, int M, int Kh,
+                long long Tn, int group, float* V, int32_t* I, long long ldv, cudaStream_t stream) {
+    using C = Cfg<FORM>;
+    GWB_CHECK_ARG(M > 0 && Tn > 0 && group > 0, GWB_ERR_SHAPE, "fused_peaks_cplx: M=%d Tn=%lld group=%d", M, Tn, group);
+    GWB_CHECK_ARG(Kh > 0 && Kh % 16 == 0, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d must be a positive multiple of 16", Kh);
+    GWB_CHECK_ARG(lda >= 2 * Kh && ldz >= Tn, GWB_ERR_SHAPE, "fused_peaks_cplx: lda=%lld < 2 Kh or ldz=%lld < Tn", lda,
+                  ldz);
+    GWB_CHECK_ARG(lda % 8 == 0 && ldz % 8 == 0, GWB_ERR_ALIGN,
+                  "fused_peaks_cplx: lda=%lld and ldz=%lld must be multiples of 8", lda, ldz);
+    for (int h = 0; h < C::NH; ++h) {
+        GWB_CHECK_ARG(A[h] && aligned(A[h], 16), GWB_ERR_ALIGN, "fused_peaks_cplx: A operand %d misaligned", h);
+        GWB_CHECK_ARG(Zp[h] && aligned(Zp[h], 16), GWB_ERR_ALIGN, "fused_peaks_cplx: Z operand %d misaligned", h);
+    }
+    GWB_CHECK_ARG(V && I, GWB_ERR_ARG, "fused_peaks_cplx: null output");
+    const long long ntiles = cdiv(Tn, kTile);
+    GWB_CHECK_ARG(ntiles * kTile < (1ll << 31), GWB_ERR_SHAPE, "fused_peaks_cplx: Tn too large for int32 indices");
+    const long long nout = cdiv(ntiles, group);
+    GWB_CHECK_ARG(ldv >= nout, GWB_ERR_SHAPE, "fused_peaks_cplx: ldv=%lld < outputs per row %lld", ldv, nout);
+    const uint32_t max_smem = 227 * 1024;
+    const int KC = FORM == 2 ? 32 : 64;
+    auto fits = [&](int mb, int st) { return layout_of(C::NH, mb, Kh, KC, st).total + 1024 <= max_smem; };
+    auto most_stages = [&](int mb) {
+        int st = 6;
+        while (st > 0 && !fits(mb, st)) --st;
+        return st;
+    };
+    // two M blocks per CTA (Z read once for both) when that still leaves a 3-deep Z ring, else one
+    int MB = (M > 128 && most_stages(2) >= 3) ? 2 : 1;
+    const int stages = most_stages(MB);
+    GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE,
+                  "fused_peaks_cplx: Kh=%d does not fit in shared memory for this form (at most %d)", Kh,
+                  FORM == 2 ? 128 : 192);
+    CplxArgs args;
+    memset(&args, 0, sizeof(args));
+    const CUtensorMapDataType dt = FORM == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    for (int h = 0; h < C::NH; ++h) {
+        int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)lda * 2, 64, 128,
+                               CU_TENSOR_MAP_SWIZZLE_128B);
+        if (r) return r;
+        r = encode_tmap_2d(&args.tZ[h], dt, Zp[h], (uint64_t)Tn, (uint64_t)(2 * Kh), (uint64_t)ldz * 2, 64, (uint32_t)KC,
+                           CU_TENSOR_MAP_SWIZZLE_128B);
+        if (r) return r;
+    }
+    args.V = V;
+    args.I = I;
+    args.ldv = ldv;
+    args.Tn = Tn;
+    args.M = M;
+    args.Kh = Kh;
+    args.ntiles = (int)ntiles;
+    args.group = group;
+    args.nout = (int)nout;
+    args.stages = stages;
+    args.MB = MB;
+    args.KC = KC;
+    args.err = device_error_ptr();
+    const uint32_t smem = layout_of(C::NH, MB, Kh, KC, stages).total + 1024;
+    auto kern = umma_cplx_kernel<FORM>;
+    GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int mgroups = (M + 128 * MB - 1) / (128 * MB);
+    const int gx = (int)std::max(1ll, std::min(nout, (long long)std::max(1, num_sms() / mgroups)));
+    kern<<<dim3(gx, mgroups), kThreads, smem, stream>>>(args);
+    GWB_LAUNCH_CHECK("umma_cplx_kernel");
+    return GWB_OK;
+}
+
+}  // namespace
+}  // namespace gwb
+
+extern "C" int gwb_fused_peaks_cplx(int form, const uint16_t* A_hi, const uint16_t* A_lo, long long lda,
+                                    const uint16_t* Z_hi, const uint16_t* Z_lo, long long ldz, int M, int Kh,
+                                    long long Tn, int group, float* V, int32_t* I, long long ldv, void* stream) {
+    const uint16_t* A[2] = {A_hi, A_lo};
+    const uint16_t* Z[2] = {Z_hi, Z_lo};
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (form) {
+        case 0: return gwb::launch_cplx<0>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, s);
+        case 1: return gwb::launch_cplx<1>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, s);
+        case 2: return gwb::launch_cplx<2>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, s);
+        default:
+            gwb::set_error("fused_peaks_cplx: form %d (0 fp16, 1 bf16, 2 split bf16)", form);
+            return GWB_ERR_ARG;
+    }
+}

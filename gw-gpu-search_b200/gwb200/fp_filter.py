@@ -15,7 +15,7 @@ from . import _lib
 
 CH = 1 << 16       # fp_filter.py:42 (kept for reference; the kernels do not chunk)
 RB = 64            # basis rows per inverse-FFT batch (fp_filter.py:43)
-FORMS = {'f16': 0, 'f32': 1, 'bf16x3': 2}
+FORMS = {'f16': 0, 'f32': 1, 'bf16x3': 2, 'bf16': 3}     # operand encodings of the pack / stacked-A kernels
 
 
 def _s():
@@ -100,11 +100,18 @@ class BasisWorkspace:
         self.ones = torch.ones(flen, dtype=torch.float32, device=device)
 
 
-def basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16'):
+def kh_of(r):
+    """Half width of the compact operands: r rounded up to the MMA's K step of 16."""
+    return ((r + 15) // 16) * 16
+
+
+def basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16', im_off=None):
     """Z rows: real parts of the r basis series over [a0, a0+Tn) divided by the first batch's rms, then the imaginary
-    parts (fp_filter.py:597-613), written into a preallocated Z (Kp, >= Tn) (rows >= 2r left as they are). D: one
-    segment's data (flen,) complex64; isw: 1/sw (or None when D is already divided by sw). Returns the device scale."""
+    parts from row im_off (r by default, the reference's layout; kh_of(r) for the compact one) (fp_filter.py:597-613),
+    written into a preallocated Z (rows not written are left as they are). D: one segment's data (flen,) complex64;
+    isw: 1/sw (or None when D is already divided by sw). Returns the device scale."""
     r, flen = Vh.shape
+    im_off = r if im_off is None else im_off
     assert flen == ws.flen and Tn <= ws.tlen - a0
     f = FORMS[form]
     iw = ws.ones if isw is None else isw
@@ -116,22 +123,22 @@ def basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16'):
         if c0 == 0:
             _lib.call('gwb_basis_scale', _lib.ptr(ws.zb), ws.tlen, nb, int(a0), int(Tn), _lib.ptr(ws.partials),
                       ws.partials.numel(), _lib.ptr(ws.ticket), _lib.ptr(ws.scale), _s())
-        _lib.call('gwb_basis_pack', _lib.ptr(ws.zb), ws.tlen, nb, r, c0, int(a0), int(Tn), _lib.ptr(ws.scale), f,
+        _lib.call('gwb_basis_pack', _lib.ptr(ws.zb), ws.tlen, nb, im_off, c0, int(a0), int(Tn), _lib.ptr(ws.scale), f,
                   _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0), _s())
     return ws.scale
 
 
 def _z_dtype(form):
-    return {'f16': torch.float16, 'f32': torch.float32, 'bf16x3': torch.bfloat16}[form]
+    return {'f16': torch.float16, 'f32': torch.float32, 'bf16x3': torch.bfloat16, 'bf16': torch.bfloat16}[form]
 
 
-def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='f16', df4=0.0):
-    """As = A (norm scale); Are = [Re As, -Im As], Aim = [Im As, Re As], zero-padded to Kp (fp_filter.py:615-621).
-    nrm: float64 CUDA vector (a strided view is fine), the norms, or sigma^2 when df4 = 4 df is given; scale: device
-    float32 scalar."""
+def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='f16', df4=0.0, kh=0):
+    """As = A (norm scale); Are = [Re As, -Im As], Aim = [Im As, Re As], zero-padded to Kp (fp_filter.py:615-621), or
+    with kh > 0 the compact Are = [Re As | Im As] (Kp = 2 kh, Aim unused). nrm: float64 CUDA vector (a strided view is
+    fine), the norms, or sigma^2 when df4 = 4 df is given; scale: device float32 scalar."""
     n, r = A.shape
     _lib.call('gwb_stacked_a', _lib.ptr(A), A.stride(0), n, r, _lib.ptr(nrm), nrm.stride(0), float(df4),
-              _lib.ptr(scale), Kp,
+              _lib.ptr(scale), Kp, int(kh),
               FORMS[form], _lib.ptr(Are), _lib.ptr(Aim), _lib.ptr(Are_lo), _lib.ptr(Aim_lo), Are.stride(0), _s())
 
 

@@ -66,7 +66,7 @@ class Bank:
         for t, ids in enumerate(self.tiles):
             Ht = self.H[self.row0[t]:self.row0[t] + len(ids)]
             r, A, Vh, worst = fp_filter.svd_tile(Ht, sw, self.kmin, cfg.eps)
-            self.svd.append(dict(r=r, A=A, Vh=Vh, worst=worst, Kp=fp_filter.kp_of(r)))
+            self.svd.append(dict(r=r, A=A, Vh=Vh, worst=worst, Kp=fp_filter.kp_of(r), Kh=fp_filter.kh_of(r)))
 
     @property
     def r_over_n(self):
@@ -85,17 +85,24 @@ class MatchedFilter:
         self.nw = Tn // cw
         self.Tn = self.nw * cw
         self.form = cfg.form
+        # fp16 / bf16 / split bf16 use the compact complex operands on the tensor cores (A = [ReA | ImA], Z = [ReZ ;
+        # ImZ], halves of Kh rows); the plain fp32 form uses the reference's stacked layout on the fp32 pipe
+        self.compact = self.form != 'f32'
         self.ws = fp_filter.BasisWorkspace(tlen, bank.flen, fp_filter.RB, device)
-        Kp = max(s['Kp'] for s in bank.svd)
+        if self.compact:
+            K = 2 * max(s['Kh'] for s in bank.svd)
+        else:
+            K = max(s['Kp'] for s in bank.svd)
         nmax = max(len(t) for t in bank.tiles)
         dt = fp_filter._z_dtype(self.form)
         ldz = -(-self.Tn // 8) * 8
-        self.Z = torch.zeros((Kp, ldz), dtype=dt, device=device)
+        self.Z = torch.zeros((K, ldz), dtype=dt, device=device)
         self.Zlo = torch.zeros_like(self.Z) if self.form == 'bf16x3' else None
-        self.Are = torch.zeros((nmax, Kp), dtype=dt, device=device)
-        self.Aim = torch.zeros_like(self.Are)
+        lda = -(-K // 8) * 8
+        self.Are = torch.zeros((nmax, lda), dtype=dt, device=device)
+        self.Aim = None if self.compact else torch.zeros_like(self.Are)
         self.Are_lo = torch.zeros_like(self.Are) if self.form == 'bf16x3' else None
-        self.Aim_lo = torch.zeros_like(self.Are) if self.form == 'bf16x3' else None
+        self.Aim_lo = None
         self.V = torch.empty((nmax, self.nw), dtype=torch.float32, device=device)
         self.I = torch.empty((nmax, self.nw), dtype=torch.int32, device=device)
         cap = cfg.cand_cap
@@ -115,47 +122,47 @@ class MatchedFilter:
         self.fft_launches = 0
         self.profile = None      # set to {} to record CUDA events around the GEMM and the basis series
 
-    def _gemm(self, n, Kp):
+    def _gemm(self, n, K, Kh):
         s = _lib.stream_ptr()
-        Zs = self.Z[:Kp]
-        if self.form == 'f16':
-            _lib.call('gwb_fused_peaks_f16', _lib.ptr(self.Are), _lib.ptr(self.Aim), self.Are.stride(0), _lib.ptr(Zs),
-                      Zs.stride(0), n, Kp, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
-        elif self.form == 'f32':
-            _lib.call('gwb_fused_peaks_f32', _lib.ptr(self.Are), _lib.ptr(self.Aim), self.Are.stride(0), _lib.ptr(Zs),
-                      Zs.stride(0), n, Kp, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
+        if self.compact:
+            code = {'f16': 0, 'bf16': 1, 'bf16x3': 2}[self.form]
+            _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(self.Are), _lib.ptr(self.Are_lo), self.Are.stride(0),
+                      _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), n, Kh, self.Tn, self.group,
+                      _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
         else:
-            _lib.call('gwb_fused_peaks_bf16x3', _lib.ptr(self.Are), _lib.ptr(self.Are_lo), _lib.ptr(self.Aim),
-                      _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(Zs), _lib.ptr(self.Zlo[:Kp]), Zs.stride(0), n,
-                      Kp, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
+            _lib.call('gwb_fused_peaks_f32', _lib.ptr(self.Are), _lib.ptr(self.Aim), self.Are.stride(0),
+                      _lib.ptr(self.Z), self.Z.stride(0), n, K, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I),
+                      self.V.stride(0), s)
 
     def tile_segment(self, t, D, isw, sig, seg):
         """Basis series, stacked A, fused GEMM and window selection of tile t against segment seg (row of D)."""
         b = self.bank
         sv = b.svd[t]
         n = len(b.tiles[t])
-        r, Kp = sv['r'], sv['Kp']
+        r = sv['r']
+        Kh = sv['Kh'] if self.compact else 0
+        K = 2 * Kh if self.compact else sv['Kp']
         prof = self.profile
         if prof is not None:
             e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
             e[0].record()
         scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
-                                            self.Zlo, self.form)
+                                            self.Zlo, self.form, im_off=Kh if self.compact else r)
         nrm = sig[b.row0[t]:b.row0[t] + n, seg]
-        fp_filter.stacked_A_into(sv['A'], nrm, scale, Kp, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
-                                 df4=4.0 * b.df)
+        fp_filter.stacked_A_into(sv['A'], nrm, scale, K, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
+                                 df4=4.0 * b.df, kh=Kh)
         if prof is not None:
             e[1].record()
-        self._gemm(n, Kp)
+        self._gemm(n, K, Kh)
         if prof is not None:
             e[2].record()
-            prof.setdefault('launches', []).append((e, n, r, Kp))
+            prof.setdefault('launches', []).append((e, n, r, K))
         f = fp_filter.FORMS[self.form]
         cap = self.cfg.cand_cap
         _lib.call('gwb_select_windows', _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), n, self.nw, self.thr2,
                   self.a0, b.row0[t], seg, _lib.ptr(self.Are), _lib.ptr(self.Aim), _lib.ptr(self.Are_lo),
-                  _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), Kp,
-                  f, _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
+                  _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), K,
+                  Kh, f, _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
                   _lib.ptr(self.counters), _lib.stream_ptr())
         nb = -(-r // fp_filter.RB)
         self.kernel_launches += 2 * nb + 4      # premul and pack per batch; scale, stacked A, GEMM, selection

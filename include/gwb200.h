@@ -109,6 +109,15 @@ GWB_API int gwb_fused_peaks_bf16x3(const uint16_t* Are_hi, const uint16_t* Are_l
 GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long lda, const float* Z, long long ldz, int M,
                         int K, long long Tn, int group, float* V, int32_t* I, long long ldv, void* stream);
 
+/* Compact complex form (same outputs): A = [Re As | Im As] (M, 2 Kh), Z = [Re zb ; Im zb] (2 Kh, Tn), each half Kh
+ * wide (Kh a multiple of 16, halves zero-padded past r). z_re = ReA.ReZ - ImA.ImZ and z_im = ImA.ReZ + ReA.ImZ are
+ * issued as four products per K step (the minus by the MMA's A negation), so A takes half the space of the
+ * reference's stacked Are/Aim (pipeline/fp_filter.py:615-621) and stays in shared memory. form 0: fp16 A_hi, Z_hi;
+ * 1: bf16; 2: split bf16 with A_lo, Z_lo (hi.hi + hi.lo + lo.hi). Kh <= 192 (forms 0, 1) or 128 (form 2). */
+GWB_API int gwb_fused_peaks_cplx(int form, const uint16_t* A_hi, const uint16_t* A_lo, long long lda,
+                                 const uint16_t* Z_hi, const uint16_t* Z_lo, long long ldz, int M, int Kh, long long Tn,
+                                 int group, float* V, int32_t* I, long long ldv, void* stream);
+
 /* ---- handle and transforms (cuFFT) ----------------------------------------------------------------------------- */
 /* The handle caches cuFFT plans per (kind, n, batch, strides); plans are made on first use of a shape. Transforms are
  * unnormalised (cuFFT convention), as the reference's norm='forward' inverse transforms and its explicit dt / df
@@ -200,28 +209,30 @@ GWB_API int gwb_basis_premul(const float* Vh, long long ldvh, int rows, const fl
  * npartials doubles; ticket: one uint32, zero on entry (left zero). */
 GWB_API int gwb_basis_scale(const float* zb, long long ldz, int rows, long long a0, long long Tn, double* partials,
                             int npartials, uint32_t* ticket, float* scale_out, void* stream);
-/* Z rows row0+j (real) and r+row0+j (imaginary) = zb[j, a0 + t] / scale for t < Tn. form 0 fp16, 1 fp32, 2 bf16 hi
- * in Z and lo in Zlo. */
-GWB_API int gwb_basis_pack(const float* zb, long long ldzb, int rows, int r, int row0, long long a0, long long Tn,
+/* Z rows row0+j (real) and im_off+row0+j (imaginary) = zb[j, a0 + t] / scale for t < Tn; im_off = r gives the
+ * reference's layout, im_off = Kh the compact one. form 0 fp16, 1 fp32, 2 bf16 hi in Z and lo in Zlo, 3 bf16. */
+GWB_API int gwb_basis_pack(const float* zb, long long ldzb, int rows, int im_off, int row0, long long a0, long long Tn,
                            const float* scale, int form, void* Z, void* Zlo, long long ldz, void* stream);
-/* As = A (norm_i scale); Are = [Re As, -Im As, 0...], Aim = [Im As, Re As, 0...] padded to Kp columns. nrm is read
- * at nrm[i * nrm_stride] (float64): the norm itself when df4 <= 0, else sigma^2 with norm = df4 / sqrt(sigma^2)
+/* As = A (norm_i scale); Are = [Re As, -Im As, 0...], Aim = [Im As, Re As, 0...] padded to Kp columns, or with
+ * kh > 0 the compact single operand Are = [Re As (kh) | Im As (kh)] (Kp = 2 kh; Aim unused). nrm is read at
+ * nrm[i * nrm_stride] (float64): the norm itself when df4 <= 0, else sigma^2 with norm = df4 / sqrt(sigma^2)
  * (df4 = 4 df). form as gwb_basis_pack. */
 GWB_API int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
-                          double df4, const float* scale, int Kp, int form, void* Are, void* Aim, void* Are_lo,
-                          void* Aim_lo, long long ldo, void* stream);
+                          double df4, const float* scale, int Kp, int kh, int form, void* Are, void* Aim,
+                          void* Are_lo, void* Aim_lo, long long ldo, void* stream);
 
 /* ---- candidate selection and the exact stage ---------------------------------------------------------------- */
 /* Window candidates of one (tile, segment) (fp_filter.py:745-764): rows i < n whose windowed maximum vw (the fused
  * GEMM output with group = cw/128) exceeds thr2 become GwbCand records (row0 + i, seg, a0 + iw, window, sqrt(vw),
  * rebuilt z), appended per row in window order; each row with candidates becomes one GwbUnit and groups of <= 8
  * candidates become GwbGroup records. counters[0..3]: candidates, groups, units, overflow flag (1 when a capacity was
- * exceeded; the row is then dropped). */
+ * exceeded; the row is then dropped). Operands in the layout the GEMM used: stacked Are/Aim (kh = 0, K = Kp) or
+ * compact A = [ReA | ImA] with Z = [ReZ ; ImZ] (kh > 0, Kp = 2 kh); form as gwb_basis_pack. */
 GWB_API int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2,
                                long long a0, int row0, int seg, const void* Are, const void* Aim, const void* Are_lo,
                                const void* Aim_lo, long long lda, const void* Z, const void* Zlo, long long ldz, int Kp,
-                               int form, GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units,
-                               int unit_cap, int32_t* counters, void* stream);
+                               int kh, int form, GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap,
+                               GwbUnit* units, int unit_cap, int32_t* counters, void* stream);
 /* Chi-squared bin edges per unit (multi_filter.edges_per_template, pipeline/multi_filter.py:264-282; the fused
  * kernel of chisq_edges.py:92-143): E[u, 0..B] int32, B >= max nbins. Unit count = min(*ucount, umax) when ucount is
  * not NULL, else umax. nbins and kmax are indexed by the unit's row. offset_mode 1 reproduces the reference's

@@ -150,3 +150,78 @@ def test_window_peaks_bit_exact():
     assert np.array_equal(p.cpu().numpy(), pr)
     assert np.array_equal(i.cpu().numpy(), ir)
     assert i[5, 0].item() == 10
+
+
+def _compact(rng, M, r, Kh, Tn, dtype):
+    """Random complex As (M, r) and zb (r, Tn) in the compact layout, plus the reference's stacked layout."""
+    As = (rng.standard_normal((M, r)) + 1j * rng.standard_normal((M, r))).astype(np.complex64)
+    zb = (rng.standard_normal((r, Tn)) + 1j * rng.standard_normal((r, Tn))).astype(np.complex64)
+    A = np.zeros((M, 2 * Kh), np.float32)
+    A[:, :r], A[:, Kh:Kh + r] = As.real, As.imag
+    Z = np.zeros((2 * Kh, Tn), np.float32)
+    Z[:r], Z[Kh:Kh + r] = zb.real, zb.imag
+    A, Z = A.astype(dtype).astype(np.float32), Z.astype(dtype).astype(np.float32)   # the values the kernel sees
+    Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
+    Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
+    return A, Z, Are, Aim
+
+
+@pytest.mark.parametrize('M,r,Tn,group', [(256, 60, 2048 * 20, 16), (256, 190, 2048 * 6, 16), (300, 100, 40000, 1),
+                                          (100, 17, 2048 * 3 + 384, 4)])
+def test_cplx_f16_against_oracle(M, r, Tn, group):
+    from gwb200 import _lib
+    rng = np.random.default_rng(r + M)
+    Kh = -(-r // 16) * 16
+    A, Z, Are, Aim = _compact(rng, M, r, Kh, Tn, np.float16)
+    Ad, Zd = _dev(A, torch.float16), _dev(Z, torch.float16)
+    nout = -(-(-(-Tn // 128)) // group)
+    V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
+    I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
+    _lib.call('gwb_fused_peaks_cplx', 0, _lib.ptr(Ad), None, Ad.stride(0), _lib.ptr(Zd), None, Zd.stride(0), M, Kh, Tn,
+              group, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.stream_ptr())
+    Vr, Ir = og.gemm_absmax(Are, Aim, Z, M, Tn)
+    tie = _near_tie_mask(Are, Aim, Z, M, Tn, Ir)
+    if group > 1:
+        Vr, Ir, tie = _grouped(Vr, Ir, tie, group)
+    _check(V.cpu().numpy(), I.cpu().numpy(), Vr, Ir, tie)
+
+
+@pytest.mark.parametrize('form,r', [(1, 120), (2, 120), (2, 40)])
+def test_cplx_bf16_forms_against_oracle(form, r):
+    from gwb200 import _lib
+    rng = np.random.default_rng(form * 100 + r)
+    M, Tn, group = 256, 2048 * 8, 16
+    Kh = -(-r // 16) * 16
+    As = (rng.standard_normal((M, r)) + 1j * rng.standard_normal((M, r))).astype(np.complex64)
+    zb = (rng.standard_normal((r, Tn)) + 1j * rng.standard_normal((r, Tn))).astype(np.complex64)
+    A = np.zeros((M, 2 * Kh), np.float32)
+    A[:, :r], A[:, Kh:Kh + r] = As.real, As.imag
+    Z = np.zeros((2 * Kh, Tn), np.float32)
+    Z[:r], Z[Kh:Kh + r] = zb.real, zb.imag
+    At, Zt = torch.from_numpy(A).cuda(), torch.from_numpy(Z).cuda()
+    Ah, Zh = At.to(torch.bfloat16), Zt.to(torch.bfloat16)
+    Al, Zl = (At - Ah.float()).to(torch.bfloat16), (Zt - Zh.float()).to(torch.bfloat16)
+    nout = -(-(Tn // 128) // group)
+    V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
+    I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
+    _lib.call('gwb_fused_peaks_cplx', form, _lib.ptr(Ah), _lib.ptr(Al if form == 2 else None), Ah.stride(0),
+              _lib.ptr(Zh), _lib.ptr(Zl if form == 2 else None), Zh.stride(0), M, Kh, Tn, group, _lib.ptr(V),
+              _lib.ptr(I), V.stride(0), _lib.stream_ptr())
+    Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
+    Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
+    Vr, Ir = og.group_reduce(*og.gemm_absmax(Are, Aim, Z, M, Tn), group)
+    rel = np.abs(V.cpu().numpy() - Vr) / Vr
+    # split bf16 carries ~16 bits per operand; one bf16 product ~8 bits, averaged over K terms
+    assert rel.max() < (5e-5 if form == 2 else 2e-2), rel.max()
+    assert (I.cpu().numpy() == Ir).mean() > (0.99 if form == 2 else 0.8)
+
+
+def test_cplx_rejects_oversized_kh():
+    from gwb200 import _lib
+    with pytest.raises(_lib.GwbError, match='shared memory'):
+        x = torch.zeros((256, 512), dtype=torch.bfloat16, device='cuda')
+        z = torch.zeros((512, 4096), dtype=torch.bfloat16, device='cuda')
+        V = torch.empty((256, 2), dtype=torch.float32, device='cuda')
+        I = torch.empty((256, 2), dtype=torch.int32, device='cuda')
+        _lib.call('gwb_fused_peaks_cplx', 2, _lib.ptr(x), _lib.ptr(x), 512, _lib.ptr(z), _lib.ptr(z), 4096, 256, 256,
+                  4096, 16, _lib.ptr(V), _lib.ptr(I), 2, _lib.stream_ptr())
