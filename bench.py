@@ -222,7 +222,9 @@ def main():
     ap.add_argument('--chunks', type=int, default=64, help='chunks per detector')
     ap.add_argument('--templates', type=int, default=5880)
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
-    ap.add_argument('--forms', default='bf16x3,f32', help='forms timed (the first gives value)')
+    ap.add_argument('--forms', default='f16,bf16,f32', help='forms timed (the first gives value)')
+    ap.add_argument('--slow-steps', type=int, default=1,
+                    help='timed steps (and warm-up steps) for the plain fp32 form, which is many times slower')
     a = ap.parse_args()
     if a.impl == 'reference':
         run_reference(a)
@@ -272,7 +274,8 @@ def main():
             Dd, IPd = cond(x)
             mf.step(Dd, IPd, isw)
 
-        for _ in range(a.warmup):
+        nsteps, nwarm = (a.slow_steps, a.slow_steps) if form == 'f32' else (a.steps, a.warmup)
+        for _ in range(nwarm):
             step()
         torch.cuda.synchronize()
         res0 = mf.results()
@@ -282,13 +285,13 @@ def main():
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with Clocks(local) as clk:
             ev0.record()
-            for _ in range(a.steps):
+            for _ in range(nsteps):
                 step()
             ev1.record()
             torch.cuda.synchronize()
         barrier()
-        ms = ev0.elapsed_time(ev1) / a.steps
-        launches = (cond.launches - l0c + mf.kernel_launches - l0m) // a.steps
+        ms = ev0.elapsed_time(ev1) / nsteps
+        launches = (cond.launches - l0c + mf.kernel_launches - l0m) // nsteps
         if world > 1:
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -300,7 +303,7 @@ def main():
         e0 = time.perf_counter()
         ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ee0.record()
-        for _ in range(a.steps):
+        for _ in range(nsteps):
             x.copy_(x_host, non_blocking=True)
             step()
             r = mf.results()
@@ -308,7 +311,7 @@ def main():
         ee1.record()
         torch.cuda.synchronize()
         barrier()
-        ms_e2e = ee0.elapsed_time(ee1) / a.steps
+        ms_e2e = ee0.elapsed_time(ee1) / nsteps
         if world > 1:
             t = torch.tensor([ms_e2e], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -321,7 +324,7 @@ def main():
         g_ms = [e[1].elapsed_time(e[2]) for e, n, r, kp in L]
         b_ms = [e[0].elapsed_time(e[1]) for e, n, r, kp in L]
         useful = [8.0 * n * r * mf.Tn for e, n, r, kp in L]
-        nprod = {'bf16x3': 3, 'f16': 1, 'f32': 1}[form]
+        nprod = {'bf16x3': 3, 'f16': 1, 'bf16': 1, 'f32': 1}[form]
         issued = [nprod * 4.0 * n * kp * mf.Tn for e, n, r, kp in L]
         mf.profile = None
         val = world * (analysed / WEEK2) / (ms / 1e3 / 3600.0)
@@ -338,7 +341,7 @@ def main():
     peaks, kind = peaks_file()
     ach = R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
     pk = peaks.get('bf16_tflops', 1590.0) if main_form != 'f32' else None
-    roof = dict(kernel='umma_absmax_kernel<bf16x3>' if main_form == 'bf16x3' else 'fused GEMM (%s)' % main_form,
+    roof = dict(kernel='umma_cplx_kernel (%s)' % main_form if main_form != 'f32' else 'simt_absmax_kernel',
                 bound='tensor', achieved=ach, peak=pk, unit='TFLOP/s', frac=(ach / pk) if pk else None, traffic=None,
                 flops_per_launch_useful=R['useful'], flops_per_launch_issued=R['issued'],
                 issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
@@ -346,17 +349,20 @@ def main():
                 basis_share_of_step=R['basis_total_ms'] / R['ms'], peak_kind='%s burst bf16' % kind)
     line = dict(metric=METRIC, value=R['value'], unit='2-det weeks / GPU-hour', n_gpus=world, steps=a.steps,
                 warmup=a.warmup, ms_per_step=R['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
-                dtype={'bf16x3': 'bf16 hi+lo (fp32 accumulate)', 'f16': 'f16', 'f32': 'f32'}[main_form],
+                dtype={'bf16x3': 'bf16 hi+lo (fp32 accumulate)', 'f16': 'f16 (fp32 accumulate)',
+                       'bf16': 'bf16 (fp32 accumulate)', 'f32': 'f32'}[main_form],
                 data='synthetic (seeded noise, TaylorF2 bank and injections)',
                 config=dict(workload='C2: 2 det x %d chunks x 512 s at 2048 Hz, %d TaylorF2 templates in tiles of 256, '
                                      'eps 1e-3, 16 chi-squared bins' % (a.chunks, len(bank['mass1'])),
                             form=main_form, analysed_s_per_step=analysed, r_over_n=B.r_over_n,
+                            r_per_tile=[s_['r'] for s_ in B.svd],
                             l2='inputs larger than L2 (strain 512 MiB, bank 24.7 GB)', parallelism='dp%d' % world),
                 e2e=dict(value=R['e2e'], unit='2-det weeks / GPU-hour', h2d_bytes_per_step=R['h2d'],
                          d2h_bytes_per_step=R['d2h']),
                 gpu_launches=R['launches'], clocks=R['clocks'], bank_setup_s=bank_setup, roofline=roof,
                 forms={k: dict(value=v['value'], ms_per_step=v['ms'], e2e=v['e2e'], n_candidates=v['n_candidates'],
-                               n_kept=v['n_kept']) for k, v in results.items()},
+                               n_kept=v['n_kept'], gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
+                               basis_share=v['basis_total_ms'] / v['ms']) for k, v in results.items()},
                 peaks_source=kind)
     if rank == 0:
         if not a.no_cpu:
