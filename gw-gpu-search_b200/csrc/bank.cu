@@ -10,11 +10,19 @@
 //   [kmin, kmax_i), phase in float64 to 3.5PN with aligned-spin spin-orbit (1.5PN) and spin-spin (2PN) terms and the
 //   leading eccentric term, reduced to [-pi, pi] in float64 before a float32 sincos.
 #include "common.cuh"
+#include <mutex>
 
 namespace gwb {
 namespace {
 
 constexpr int kRows = 64, kSegs = 32, kK = 32;
+
+// Scratch of gwb_sigma2_noalloc: the split-k partial sums of the template norms, at most kNoAllocPart doubles
+// (4 MiB). It lives in the library's own device image, so every GPU that loads the library holds it until exit.
+constexpr long long kNoAllocPart = 1ll << 19;
+static __device__ __align__(256) double g_sigma2_scratch[kNoAllocPart];
+std::mutex g_scratch_mu;
+double* g_scratch_ptr[64] = {nullptr};
 
 __global__ void __launch_bounds__(256) sigma2_partial_kernel(const float2* __restrict__ H, long long ldh, int n,
                                                              const float* __restrict__ IP, long long ldip, int nseg,
@@ -269,6 +277,33 @@ int gwb_sigma2(const float* H, long long ldh, int n, const float* IP, long long 
     sigma2_reduce_kernel<<<(unsigned)cdiv(ne, 256), 256, 0, s>>>(part, nsplit, n, nseg, 4.0 * df, sig, ldsig);
     GWB_LAUNCH_CHECK("sigma2_reduce_kernel");
     return GWB_OK;
+}
+
+int gwb_sigma2_noalloc(const float* H, long long ldh, int n, const float* IP, long long ldip, int nseg, int kmin,
+                       int flen, double df, double* sig, long long ldsig, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(n > 0 && nseg > 0, GWB_ERR_SHAPE, "sigma2_noalloc: n=%d nseg=%d", n, nseg);
+    GWB_CHECK_ARG((long long)n * nseg <= kNoAllocPart, GWB_ERR_CAPACITY,
+                  "sigma2_noalloc: n * nseg = %lld exceeds the static scratch of %lld partial sums; call gwb_sigma2 "
+                  "with a workspace, or split the rows", (long long)n * nseg, kNoAllocPart);
+    int dev = 0;
+    GWB_CUDA(cudaGetDevice(&dev));
+    GWB_CHECK_ARG(dev >= 0 && dev < 64, GWB_ERR_ARG, "sigma2_noalloc: device %d", dev);
+    double* part = nullptr;
+    {
+        // once per device, with that device current: the device address of the static array (the host-side
+        // symbol is only a stand-in and must never be handed to a kernel)
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        if (g_scratch_ptr[dev] == nullptr) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_sigma2_scratch);
+            if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_sigma2_scratch)");
+            g_scratch_ptr[dev] = static_cast<double*>(p);
+        }
+        part = g_scratch_ptr[dev];
+    }
+    // every partial the reduction reads is written by the partial kernel first: nothing needs clearing
+    return gwb_sigma2(H, ldh, n, IP, ldip, nseg, kmin, flen, df, part, kNoAllocPart, sig, ldsig, stream);
 }
 
 int gwb_gram(const float* H, long long ldh, int n, const float* sw, int kmin, int flen, double* part,

@@ -191,6 +191,19 @@ GWB_API int gwb_taylorf2(const double* m1, const double* m2, const double* chi1,
 GWB_API int gwb_sigma2(const float* H, long long ldh, int n, const float* IP, long long ldip, int nseg, int kmin,
                        int flen, double df, double* part, long long part_elems, double* sig, long long ldsig,
                        void* stream);
+/* Template norms as gwb_sigma2, for callers that must not allocate device memory: no counterpart in the reference.
+ * Some callers cannot let a library call cudaMalloc: a host program (for example a Go or Java service over the C ABI)
+ * whose own pool owns every byte of device memory, code that runs between stream-capture begin and end, where an
+ * allocation would break the capture, or a latency-bound loop where cudaMalloc / cudaFree synchronise the device.
+ * This variant takes no workspace and allocates nothing: its split-k scratch is a static device array of 2^19
+ * doubles (4 MiB) inside the library, held by every GPU that loads the library until the process exits, so
+ * n * nseg must not exceed 524,288 (else GWB_ERR_CAPACITY, nothing queued). The first call on each device looks up
+ * the array's device address (once, with that device current); make that first call before any stream capture.
+ * All calls on a device share the one array: calls that overlap on the GPU (different streams, no ordering between
+ * them) race and must not be issued. Each call overwrites every scratch element it later reads, so nothing carries
+ * over from the previous call. */
+GWB_API int gwb_sigma2_noalloc(const float* H, long long ldh, int n, const float* IP, long long ldip, int nseg,
+                               int kmin, int flen, double df, double* sig, long long ldsig, void* stream);
 /* Tile Gram matrix (svd_tile, fp_filter.py:578-581) in float64: G (n x n complex128, interleaved) =
  * sum_{k >= kmin} (H_k sw_k)(H_k sw_k)^H. part: workspace of part_elems doubles (>= 2 n^2). */
 GWB_API int gwb_gram(const float* H, long long ldh, int n, const float* sw, int kmin, int flen, double* part,
