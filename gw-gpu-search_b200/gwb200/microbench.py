@@ -1,0 +1,117 @@
+"""Micro-benchmarks of single kernels on synthetic operands (used for profiling; prints one JSON line per case).
+
+    python -m gwb200.microbench gemm  [--r 128] [--n 256] [--tn 917504] [--form f16] [--reps 20]
+    python -m gwb200.microbench basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5]
+    python -m gwb200.microbench exact [--groups 512] [--peaks 1] [--tlen 1048576] [--reps 5]
+
+Run from gw-gpu-search_b200/ (or with it on sys.path). Operand sizes default to one (tile, chunk) of the C2
+workload; inputs are larger than L2 where the real ones are."""
+import argparse
+import json
+
+import numpy as np
+import torch
+
+from . import _exact, _lib, fp_filter
+
+
+def _time(fn, reps):
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def gemm(a):
+    n, r, Tn = a.n, a.r, a.tn
+    Kh = fp_filter.kh_of(r)
+    code = {'f16': 0, 'bf16': 1, 'bf16x3': 2}[a.form]
+    dt = torch.float16 if a.form == 'f16' else torch.bfloat16
+    g = torch.Generator(device='cuda').manual_seed(0)
+    A = torch.randn((n, 2 * Kh), generator=g, device='cuda').to(dt)
+    Z = torch.randn((2 * Kh, Tn), generator=g, device='cuda').to(dt)
+    lo = (A.clone(), Z.clone()) if code == 2 else (None, None)
+    nw = Tn // 2048
+    V = torch.empty((n, nw), dtype=torch.float32, device='cuda')
+    I = torch.empty((n, nw), dtype=torch.int32, device='cuda')
+
+    def f():
+        _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(A), _lib.ptr(lo[0]), A.stride(0), _lib.ptr(Z), _lib.ptr(lo[1]),
+                  Z.stride(0), n, Kh, Tn, 16, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.stream_ptr())
+    ms = _time(f, a.reps)
+    useful = 8.0 * n * r * Tn
+    issued = (3 if code == 2 else 1) * 4.0 * n * 2 * Kh * Tn
+    zbytes = 2 * Kh * Tn * 2 * (2 if code == 2 else 1)
+    return dict(kernel='umma_cplx_kernel', form=a.form, n=n, r=r, Kh=Kh, Tn=Tn, ms=ms, useful_tflops=useful / ms / 1e9,
+                issued_tflops=issued / ms / 1e9, z_gbs=zbytes / ms / 1e6)
+
+
+def basis(a):
+    r, tlen = a.r, a.tlen
+    flen = tlen // 2 + 1
+    ws = fp_filter.BasisWorkspace(tlen, flen)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    Vh = torch.randn((r, flen), generator=g, device='cuda', dtype=torch.complex64)
+    D = torch.randn(flen, generator=g, device='cuda', dtype=torch.complex64)
+    isw = torch.rand(flen, generator=g, device='cuda')
+    a0, Tn = tlen * 3 // 32, tlen * 28 // 32
+    Kh = fp_filter.kh_of(r)
+    Z = torch.zeros((2 * Kh, Tn), dtype=fp_filter._z_dtype(a.form), device='cuda')
+    Zlo = torch.zeros_like(Z) if a.form == 'bf16x3' else None
+    ms = _time(lambda: fp_filter.basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
+    return dict(kernel='basis_series', form=a.form, r=r, tlen=tlen, ms=ms, us_per_row=ms * 1e3 / r)
+
+
+def exact(a):
+    tlen = a.tlen
+    flen = tlen // 2 + 1
+    kmin = tlen // 100
+    nrow = 64
+    g = torch.Generator(device='cuda').manual_seed(0)
+    H = torch.randn((nrow, flen), generator=g, device='cuda', dtype=torch.complex64)
+    D = torch.randn((1, flen), generator=g, device='cuda', dtype=torch.complex64)
+    rng = np.random.default_rng(0)
+    rows = np.repeat(rng.integers(0, nrow, a.groups), a.peaks)
+    samples = rng.integers(0, tlen, len(rows))
+    order, rows_u, cands, groups, units = _exact.plan(rows, samples)
+    B = 16
+    edges = np.linspace(kmin, flen - 2, B + 1).astype(np.int32)
+    E = torch.from_numpy(np.tile(edges, (len(units), 1))).cuda()
+    nb = torch.full((nrow,), B, dtype=torch.int32, device='cuda')
+    nchunk = _lib.load().gwb_exact_chunks(flen, kmin)
+    slots = torch.empty((len(cands), nchunk, B, 2), dtype=torch.float32, device='cuda')
+    cd, gd, ud = _exact.to_dev(cands), _exact.to_dev(groups), _exact.to_dev(units)
+
+    def f():
+        _lib.call('gwb_bin_sums', _lib.ptr(gd), None, len(groups), _lib.ptr(ud), _lib.ptr(cd), _lib.ptr(E), B,
+                  _lib.ptr(nb), _lib.ptr(H), H.stride(0), _lib.ptr(D), D.stride(0), kmin, flen, tlen, _lib.ptr(slots),
+                  _lib.stream_ptr())
+    ms = _time(f, a.reps)
+    nbins = int(edges[-1] - edges[0])
+    return dict(kernel='binsum_kernel', groups=len(groups), peaks_per_group=a.peaks, ms=ms,
+                gbs=len(groups) * nbins * 16 / ms / 1e6)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('what', choices=['gemm', 'basis', 'exact'])
+    ap.add_argument('--r', type=int, default=128)
+    ap.add_argument('--n', type=int, default=256)
+    ap.add_argument('--tn', type=int, default=917504)
+    ap.add_argument('--tlen', type=int, default=1 << 20)
+    ap.add_argument('--form', default='f16')
+    ap.add_argument('--groups', type=int, default=512)
+    ap.add_argument('--peaks', type=int, default=1)
+    ap.add_argument('--reps', type=int, default=10)
+    a = ap.parse_args()
+    print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact}[a.what](a)))
+
+
+if __name__ == '__main__':
+    main()
