@@ -224,41 +224,54 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
         if (hit) {
             const int pos = s_base + written + before + __popc(m & ((1u << lane) - 1));
             const int col = iw[(long long)row * ldv + w];
-            float zr = 0.f, zi = 0.f;
-            auto ldz_ = [&](long long c) {
-                return ld_as_float(Z, c * ldz + col, form) + (form == 2 ? ld_as_float(Zlo, c * ldz + col, 2) : 0.f);
-            };
-            auto lda_ = [&](const void* hi, const void* lo, long long c) {
-                return ld_as_float(hi, (long long)row * lda + c, form) +
-                       (form == 2 ? ld_as_float(lo, (long long)row * lda + c, 2) : 0.f);
-            };
-            if (kh > 0) {       // compact operands: A = [ReA | ImA], Z = [ReZ ; ImZ]
-                for (int c = 0; c < kh; ++c) {
-                    const float ar = lda_(Are, Are_lo, c), ai = lda_(Are, Are_lo, kh + c);
-                    const float zc = ldz_(c), zs = ldz_(kh + c);
-                    zr = fmaf(ar, zc, fmaf(-ai, zs, zr));
-                    zi = fmaf(ai, zc, fmaf(ar, zs, zi));
-                }
-            } else {
-                for (int c = 0; c < Kp; ++c) {
-                    const float zc = ldz_(c);
-                    zr = fmaf(lda_(Are, Are_lo, c), zc, zr);
-                    zi = fmaf(lda_(Aim, Aim_lo, c), zc, zi);
-                }
-            }
             GwbCand cd;
             cd.row = row0 + row;
             cd.seg = seg;
             cd.sample = (int)(a0 + col);
             cd.window = w;
             cd.approx = sqrtf(v[w]);
-            cd.zr = zr;
-            cd.zi = zi;
+            cd.zr = 0.f;
+            cd.zi = 0.f;
             cd.unit = s_unit;
             cands[pos] = cd;
         }
         written += chunk_total;
         __syncthreads();
+    }
+    // rebuilt complex SNR of each candidate of this row: one warp per candidate, lanes over K
+    auto ldz_ = [&](long long c, int col) {
+        return ld_as_float(Z, c * ldz + col, form) + (form == 2 ? ld_as_float(Zlo, c * ldz + col, 2) : 0.f);
+    };
+    auto lda_ = [&](const void* hi, const void* lo, long long c) {
+        return ld_as_float(hi, (long long)row * lda + c, form) +
+               (form == 2 ? ld_as_float(lo, (long long)row * lda + c, 2) : 0.f);
+    };
+    for (int i = warp; i < total; i += kThreads / 32) {
+        const int col = cands[s_base + i].sample - (int)a0;
+        float zr = 0.f, zi = 0.f;
+        if (kh > 0) {       // compact operands: A = [ReA | ImA], Z = [ReZ ; ImZ]
+            for (int c = lane; c < kh; c += 32) {
+                const float ar = lda_(Are, Are_lo, c), ai = lda_(Are, Are_lo, kh + c);
+                const float zc = ldz_(c, col), zs = ldz_(kh + c, col);
+                zr = fmaf(ar, zc, fmaf(-ai, zs, zr));
+                zi = fmaf(ai, zc, fmaf(ar, zs, zi));
+            }
+        } else {
+            for (int c = lane; c < Kp; c += 32) {
+                const float zc = ldz_(c, col);
+                zr = fmaf(lda_(Are, Are_lo, c), zc, zr);
+                zi = fmaf(lda_(Aim, Aim_lo, c), zc, zi);
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            zr += __shfl_down_sync(0xffffffffu, zr, off);
+            zi += __shfl_down_sync(0xffffffffu, zi, off);
+        }
+        if (lane == 0) {
+            cands[s_base + i].zr = zr;
+            cands[s_base + i].zi = zi;
+        }
     }
 }
 

@@ -1,0 +1,325 @@
+// Fused basis series: conj(Vh) D isw -> inverse DFT of length N -> Re / scale, Im / scale packed into Z, in two
+// passes over HBM instead of premul + cuFFT (two passes) + pack (fp_filter.basis_series, fp_filter.py:597-613).
+//
+// N = N1 N2 with k = N2 k1 + k2 and t = t1 + N1 t2 (Cooley-Tukey, four-step):
+//   z[t1 + N1 t2] = sum_k2 e^{2 pi i k2 t2 / N2} e^{2 pi i k2 t1 / N} [ sum_k1 q[N2 k1 + k2] e^{2 pi i k1 t1 / N1} ]
+// pass 1, CTA = (8 consecutive k2, one basis row): forms q = conj(Vh) D isw on load (zero above N/2, where the
+//   reference zero-pads), DFT of length N1 over k1 in shared memory, multiplies by e^{2 pi i k2 t1 / N} and writes
+//   W[row][k2][t1] (t1 contiguous). For the first rows it also sums |q|^2 for the scale.
+// pass 2, CTA = (8 consecutive t1, one basis row): DFT of length N2 over k2, then z at t in [a0, a0 + Tn) is divided
+//   by the scale and written to Z as fp16, fp32, bf16 or bf16 hi + lo.
+// The in-CTA DFT is a Stockham radix-4 (plus one radix-2 when log2 L is odd) over 8 interleaved columns, each stage
+// staged through registers so one shared buffer suffices. Twiddles come from one table e^{2 pi i m / N} (float from
+// double), also used with stride N / L for the in-CTA stages.
+// Scale: the reference divides by the rms of the first batch's outputs over the analysed span; here the rms over the
+// whole series is taken from the inputs by Parseval (sum_t |z_t|^2 = N sum_k |q_k|^2), so no pass re-reads the
+// outputs. The scale only normalises Z for its 16-bit range: A is multiplied by the same scale, so the SNR is
+// unchanged (fp_filter.py:617).
+#include "common.cuh"
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace gwb {
+namespace {
+
+constexpr int TB = 8;   // interleaved columns per CTA
+
+__global__ void twiddle_kernel(float2* tw, long long N) {
+    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= N) return;
+    double s, c;
+    sincospi(2.0 * (double)m / (double)N, &s, &c);
+    tw[m] = make_float2((float)c, (float)s);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -(a.y * b.y)), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// In-place inverse DFT of length L over TB interleaved columns: X[p * TB + c] holds element p of column c.
+// tw_s: e^{2 pi i m / L} for m < L in shared memory.
+template <int L, int NT>
+__device__ __forceinline__ void fft_smem(float2* X, const float2* tw_s) {
+    const int tid = threadIdx.x;
+    int Ns = 1;
+    constexpr int LOG = (L == 64) ? 6 : (L == 128) ? 7 : (L == 256) ? 8 : (L == 512) ? 9 : (L == 1024) ? 10 : 11;
+    constexpr int N4 = LOG / 2;                 // radix-4 stages
+    constexpr int Q4 = (L / 4) * TB / NT;       // butterflies per thread in a radix-4 stage
+#pragma unroll 1
+    for (int st = 0; st < N4; ++st) {
+        float2 v[Q4][4];
+#pragma unroll
+        for (int q = 0; q < Q4; ++q) {
+            const int b = tid + NT * q;
+            const int c = b % TB, j = b / TB;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) v[q][r] = X[(j + r * (L / 4)) * TB + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < Q4; ++q) {
+            const int b = tid + NT * q;
+            const int c = b % TB, j = b / TB;
+            const int k = j % Ns;
+            const int step = L / (Ns * 4);
+#pragma unroll
+            for (int r = 1; r < 4; ++r) v[q][r] = cmul(v[q][r], tw_s[k * r * step]);
+            const float2 a = make_float2(v[q][0].x + v[q][2].x, v[q][0].y + v[q][2].y);
+            const float2 bb = make_float2(v[q][0].x - v[q][2].x, v[q][0].y - v[q][2].y);
+            const float2 cc = make_float2(v[q][1].x + v[q][3].x, v[q][1].y + v[q][3].y);
+            const float2 d = make_float2(v[q][1].x - v[q][3].x, v[q][1].y - v[q][3].y);
+            const int idx = (j / Ns) * Ns * 4 + k;
+            X[(idx + 0 * Ns) * TB + c] = make_float2(a.x + cc.x, a.y + cc.y);
+            X[(idx + 1 * Ns) * TB + c] = make_float2(bb.x - d.y, bb.y + d.x);      // b + i d
+            X[(idx + 2 * Ns) * TB + c] = make_float2(a.x - cc.x, a.y - cc.y);
+            X[(idx + 3 * Ns) * TB + c] = make_float2(bb.x + d.y, bb.y - d.x);      // b - i d
+        }
+        __syncthreads();
+        Ns *= 4;
+    }
+    if (LOG & 1) {
+        constexpr int Q2 = (L / 2) * TB / NT;
+        float2 v[Q2][2];
+#pragma unroll
+        for (int q = 0; q < Q2; ++q) {
+            const int b = tid + NT * q;
+            const int c = b % TB, j = b / TB;
+            v[q][0] = X[j * TB + c];
+            v[q][1] = X[(j + L / 2) * TB + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < Q2; ++q) {
+            const int b = tid + NT * q;
+            const int c = b % TB, j = b / TB;
+            const int k = j % Ns;
+            const float2 w = cmul(v[q][1], tw_s[k * (L / (Ns * 2))]);
+            const int idx = (j / Ns) * Ns * 2 + k;
+            X[idx * TB + c] = make_float2(v[q][0].x + w.x, v[q][0].y + w.y);
+            X[(idx + Ns) * TB + c] = make_float2(v[q][0].x - w.x, v[q][0].y - w.y);
+        }
+        __syncthreads();
+    }
+}
+
+template <int L>
+constexpr int threads_for() {
+    return (L * TB / 32) < 64 ? 64 : (L * TB / 32);
+}
+
+// pass 1: rows of the batch in blockIdx.y, 8 consecutive k2 in blockIdx.x
+template <int N1>
+__global__ void __launch_bounds__(threads_for<N1>()) basis_pass1(
+    const float2* __restrict__ Vh, long long ldvh, const float2* __restrict__ D, const float* __restrict__ isw,
+    long long flen, long long N, int N2, const float2* __restrict__ tw, float2* __restrict__ W, int nfirst,
+    double* __restrict__ partials, unsigned int* __restrict__ ticket, float* __restrict__ scale_out) {
+    constexpr int NT = threads_for<N1>();
+    extern __shared__ float2 sm[];
+    float2* X = sm;                  // N1 x TB
+    float2* tw_s = sm + N1 * TB;     // N1
+    const int row = blockIdx.y, k20 = blockIdx.x * TB, tid = threadIdx.x;
+    const long long stride = N / N1;
+    for (int m = tid; m < N1; m += NT) tw_s[m] = tw[(long long)m * stride];
+    const float2* v = Vh + (long long)row * ldvh;
+    double acc = 0.0;
+    const long long half = N / 2;
+    for (int e = tid; e < N1 * TB; e += NT) {
+        const int c = e % TB, k1 = e / TB;
+        const long long k = (long long)N2 * k1 + k20 + c;
+        float2 q = make_float2(0.f, 0.f);
+        if (k <= half && k < flen) {
+            const float2 a = v[k], dk = D[k];
+            const float w = isw[k];
+            const float dr = dk.x * w, di = dk.y * w;
+            q = make_float2(fmaf(a.x, dr, a.y * di), fmaf(a.x, di, -(a.y * dr)));
+            if (row < nfirst) acc += (double)q.x * q.x + (double)q.y * q.y;
+        }
+        X[k1 * TB + c] = q;
+    }
+    __syncthreads();
+    fft_smem<N1, NT>(X, tw_s);
+    // twiddle e^{2 pi i k2 t1 / N} and write W[row][k2][t1], t1 contiguous
+    float2* Wr = W + (long long)row * N;
+    const unsigned long long mask = (unsigned long long)N - 1;
+    for (int e = tid; e < N1 * TB; e += NT) {
+        const int c = e % TB, t1 = e / TB;     // shared reads conflict-free; global writes in 32-byte runs
+        const unsigned long long m = ((unsigned long long)(k20 + c) * (unsigned long long)t1) & mask;
+        Wr[(long long)(k20 + c) * N1 + t1] = cmul(X[t1 * TB + c], tw[m]);
+    }
+    // scale partials: one per CTA of the first rows, summed in a fixed order by the last CTA to finish
+    if (nfirst > 0) {
+        __shared__ double red[32];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if ((tid & 31) == 0) red[tid >> 5] = acc;
+        __syncthreads();
+        __shared__ bool last;
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < NT / 32; ++w) s += red[w];
+            const unsigned nb = gridDim.x * (unsigned)min(nfirst, (int)gridDim.y);
+            if (row < nfirst) partials[(long long)row * gridDim.x + blockIdx.x] = s;
+            __threadfence();
+            last = false;
+            if (row < nfirst) last = atomicAdd(ticket, 1u) == nb - 1;
+        }
+        __syncthreads();
+        if (last && tid == 0) {
+            __threadfence();
+            const int nr = min(nfirst, (int)gridDim.y);
+            double s = 0.0;
+            for (long long b = 0; b < (long long)nr * gridDim.x; ++b) s += ((volatile double*)partials)[b];
+            // mean over t of |z|^2 = sum_k |q|^2 (Parseval); scale = sqrt(mean / 2)
+            *scale_out = (float)sqrt(s / (double)nr / 2.0);
+            *ticket = 0;
+        }
+    }
+}
+
+template <int N2, int FORM>
+__global__ void __launch_bounds__(threads_for<N2>()) basis_pass2(
+    const float2* __restrict__ W, long long N, int N1, const float2* __restrict__ tw, long long a0, long long Tn,
+    const float* __restrict__ scale, void* __restrict__ Z, void* __restrict__ Zlo, long long ldz, int im_off,
+    int row0) {
+    constexpr int NT = threads_for<N2>();
+    extern __shared__ float2 sm[];
+    float2* X = sm;
+    float2* tw_s = sm + N2 * TB;
+    const int row = blockIdx.y, t10 = blockIdx.x * TB, tid = threadIdx.x;
+    const long long stride = N / N2;
+    for (int m = tid; m < N2; m += NT) tw_s[m] = tw[(long long)m * stride];
+    const float2* Wr = W + (long long)row * N;
+    for (int e = tid; e < N2 * TB; e += NT) {
+        const int c = e % TB, k2 = e / TB;
+        X[k2 * TB + c] = Wr[(long long)k2 * N1 + t10 + c];
+    }
+    __syncthreads();
+    fft_smem<N2, NT>(X, tw_s);
+    const float inv = 1.0f / *scale;
+    const long long re_row = row0 + row, im_row = im_off + row0 + row;
+    for (int e = tid; e < N2 * TB; e += NT) {
+        const int c = e % TB, t2 = e / TB;
+        const long long t = (long long)t10 + c + (long long)N1 * t2 - a0;
+        if (t < 0 || t >= Tn) continue;
+        const float2 v = X[t2 * TB + c];
+        const float xr = v.x * inv, xi = v.y * inv;
+        if (FORM == 0) {
+            static_cast<__half*>(Z)[re_row * ldz + t] = __float2half_rn(xr);
+            static_cast<__half*>(Z)[im_row * ldz + t] = __float2half_rn(xi);
+        } else if (FORM == 1) {
+            static_cast<float*>(Z)[re_row * ldz + t] = xr;
+            static_cast<float*>(Z)[im_row * ldz + t] = xi;
+        } else {
+            const __nv_bfloat16 hr = __float2bfloat16_rn(xr), hm = __float2bfloat16_rn(xi);
+            static_cast<__nv_bfloat16*>(Z)[re_row * ldz + t] = hr;
+            static_cast<__nv_bfloat16*>(Z)[im_row * ldz + t] = hm;
+            if (FORM == 2) {
+                static_cast<__nv_bfloat16*>(Zlo)[re_row * ldz + t] = __float2bfloat16_rn(xr - __bfloat162float(hr));
+                static_cast<__nv_bfloat16*>(Zlo)[im_row * ldz + t] = __float2bfloat16_rn(xi - __bfloat162float(hm));
+            }
+        }
+    }
+}
+
+int log2i(long long n) {
+    int l = 0;
+    while ((1ll << l) < n) ++l;
+    return l;
+}
+
+template <int N1>
+int launch_pass1(const float2* Vh, long long ldvh, int rows, const float2* D, const float* isw, long long flen,
+                 long long N, int N2, const float2* tw, float2* W, int nfirst, double* partials, unsigned* ticket,
+                 float* scale_out, cudaStream_t s) {
+    constexpr int NT = threads_for<N1>();
+    const size_t smem = (size_t)(N1 * TB + N1) * sizeof(float2);
+    auto k = basis_pass1<N1>;
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<dim3(N2 / TB, rows), NT, smem, s>>>(Vh, ldvh, D, isw, flen, N, N2, tw, W, nfirst, partials, ticket, scale_out);
+    GWB_LAUNCH_CHECK("basis_pass1");
+    return GWB_OK;
+}
+
+template <int N2, int FORM>
+int launch_pass2_f(const float2* W, long long N, int N1, int rows, const float2* tw, long long a0, long long Tn,
+                   const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
+    constexpr int NT = threads_for<N2>();
+    const size_t smem = (size_t)(N2 * TB + N2) * sizeof(float2);
+    auto k = basis_pass2<N2, FORM>;
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<dim3(N1 / TB, rows), NT, smem, s>>>(W, N, N1, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0);
+    GWB_LAUNCH_CHECK("basis_pass2");
+    return GWB_OK;
+}
+
+template <int N2>
+int launch_pass2(int form, const float2* W, long long N, int N1, int rows, const float2* tw, long long a0,
+                 long long Tn, const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0,
+                 cudaStream_t s) {
+    switch (form) {
+        case 0: return launch_pass2_f<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        case 1: return launch_pass2_f<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        case 2: return launch_pass2_f<N2, 2>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        default: return launch_pass2_f<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+    }
+}
+
+}  // namespace
+}  // namespace gwb
+
+extern "C" {
+
+int gwb_fft_twiddles(long long N, float* tw, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(tw, GWB_ERR_ARG, "fft_twiddles: null pointer");
+    GWB_CHECK_ARG(is_pow2(N) && N >= 64, GWB_ERR_NOT_POW2, "fft_twiddles: N=%lld must be a power of two >= 64", N);
+    twiddle_kernel<<<(unsigned)cdiv(N, 256), 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<float2*>(tw), N);
+    GWB_LAUNCH_CHECK("twiddle_kernel");
+    return GWB_OK;
+}
+
+int gwb_basis_fused(const float* Vh, long long ldvh, int rows, const float* D, const float* isw, long long flen,
+                    long long N, const float* tw, float* W, long long a0, long long Tn, int form, void* Z, void* Zlo,
+                    long long ldz, int im_off, int row0, int nfirst, double* partials, long long npartials,
+                    uint32_t* ticket, float* scale, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(Vh && D && isw && tw && W && Z && scale && (form != 2 || Zlo), GWB_ERR_ARG,
+                  "basis_fused: null pointer");
+    GWB_CHECK_ARG(form >= 0 && form <= 3, GWB_ERR_ARG, "basis_fused: form %d", form);
+    GWB_CHECK_ARG(is_pow2(N) && N >= (1 << 12) && N <= (1 << 22), GWB_ERR_NOT_POW2,
+                  "basis_fused: N=%lld must be a power of two in [2^12, 2^22]", N);
+    GWB_CHECK_ARG(rows > 0 && rows < 65536 && flen <= N / 2 + 1 && ldvh >= flen && a0 >= 0 && Tn > 0 &&
+                  a0 + Tn <= N && ldz >= Tn && row0 >= 0 && row0 + rows <= im_off, GWB_ERR_SHAPE,
+                  "basis_fused: rows=%d flen=%lld N=%lld a0=%lld Tn=%lld", rows, flen, N, a0, Tn);
+    const int p = log2i(N);
+    const int N1 = 1 << ((p + 1) / 2), N2 = (int)(N / N1);
+    GWB_CHECK_ARG(nfirst <= 0 || (partials && ticket && (long long)std::min(nfirst, rows) * (N2 / TB) <= npartials),
+                  GWB_ERR_SHAPE, "basis_fused: scale partials need %lld entries",
+                  (long long)std::min(nfirst, rows) * (N2 / TB));
+    cudaStream_t s = (cudaStream_t)stream;
+    const float2* v = reinterpret_cast<const float2*>(Vh);
+    const float2* d = reinterpret_cast<const float2*>(D);
+    const float2* t = reinterpret_cast<const float2*>(tw);
+    float2* w = reinterpret_cast<float2*>(W);
+    unsigned* tk = reinterpret_cast<unsigned*>(ticket);
+    int st;
+    switch (N1) {
+        case 64: st = launch_pass1<64>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 128: st = launch_pass1<128>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 256: st = launch_pass1<256>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 512: st = launch_pass1<512>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 1024: st = launch_pass1<1024>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        default: st = launch_pass1<2048>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+    }
+    if (st) return st;
+    switch (N2) {
+        case 64: return launch_pass2<64>(form, w, N, N1, rows, t, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        case 128: return launch_pass2<128>(form, w, N, N1, rows, t, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        case 256: return launch_pass2<256>(form, w, N, N1, rows, t, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        case 512: return launch_pass2<512>(form, w, N, N1, rows, t, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        case 1024: return launch_pass2<1024>(form, w, N, N1, rows, t, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        default: return launch_pass2<2048>(form, w, N, N1, rows, t, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+    }
+}
+
+}  // extern "C"

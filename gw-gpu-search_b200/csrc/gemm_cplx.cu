@@ -247,15 +247,35 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
 #pragma unroll
                         for (int jj = 0; jj < 32; ++jj) asm volatile("" : "+r"(re[jj]), "+r"(im[jj]));
                         const int cb = hh * 64 + c;
+                        // best of this 32-column chunk first (index as an immediate), then merged: 2 FMA-pipe and 3
+                        // ALU instructions per element
+                        float lb = -1.f;
+                        int lj = 0;
+                        if (full_tile) {
 #pragma unroll
-                        for (int jj = 0; jj < 32; ++jj) {
-                            const float xr = __uint_as_float(re[jj]), xm = __uint_as_float(im[jj]);
-                            float p = fmaf(xr, xr, xm * xm);
-                            if (!full_tile && col0 + cb + jj >= args.Tn) p = -1.f;
-                            if (p > best) {
-                                best = p;
-                                bi = cb + jj;
+                            for (int jj = 0; jj < 32; ++jj) {
+                                const float xr = __uint_as_float(re[jj]), xm = __uint_as_float(im[jj]);
+                                const float p = fmaf(xr, xr, xm * xm);
+                                if (p > lb) {
+                                    lb = p;
+                                    lj = jj;
+                                }
                             }
+                        } else {
+                            const int valid = (int)min((long long)32, max(0ll, args.Tn - (col0 + cb)));
+#pragma unroll
+                            for (int jj = 0; jj < 32; ++jj) {
+                                const float xr = __uint_as_float(re[jj]), xm = __uint_as_float(im[jj]);
+                                const float p = jj < valid ? fmaf(xr, xr, xm * xm) : -1.f;
+                                if (p > lb) {
+                                    lb = p;
+                                    lj = jj;
+                                }
+                            }
+                        }
+                        if (lb > best) {
+                            best = lb;
+                            bi = cb + lj;
                         }
                     }
                 }

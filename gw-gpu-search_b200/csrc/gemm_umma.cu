@@ -246,19 +246,25 @@ __global__ void __launch_bounds__(kThreads, 1) umma_absmax_kernel(const __grid_c
 #pragma unroll
                         for (int jj = 0; jj < 32; ++jj) asm volatile("" : "+r"(re[jj]), "+r"(im[jj]));
                         const int cb = hh * 64 + c;
+                        float lb = -1.f;
+                        int lj = 0;
                         if (full_tile) {
 #pragma unroll
                             for (int jj = 0; jj < 32; ++jj) {
                                 const float xr = __uint_as_float(re[jj]), xi_ = __uint_as_float(im[jj]);
-                                keep_best(fmaf(xr, xr, xi_ * xi_), cb + jj, best, bi);
+                                keep_best(fmaf(xr, xr, xi_ * xi_), jj, lb, lj);
                             }
                         } else {
+                            const int valid = (int)min((long long)32, max(0ll, args.Tn - (col0 + cb)));
 #pragma unroll
                             for (int jj = 0; jj < 32; ++jj) {
                                 const float xr = __uint_as_float(re[jj]), xi_ = __uint_as_float(im[jj]);
-                                const float p = (col0 + cb + jj < args.Tn) ? fmaf(xr, xr, xi_ * xi_) : -1.f;
-                                keep_best(p, cb + jj, best, bi);
+                                keep_best(jj < valid ? fmaf(xr, xr, xi_ * xi_) : -1.f, jj, lb, lj);
                             }
+                        }
+                        if (lb > best) {
+                            best = lb;
+                            bi = cb + lj;
                         }
                     }
                 }

@@ -86,6 +86,47 @@ def kp_of(r):
     return ((2 * r + 63) // 64) * 64
 
 
+_TWIDDLES = {}
+
+
+def twiddles(N, device='cuda'):
+    """e^{2 pi i m / N}, m < N, complex64 on the device (cached per (N, device))."""
+    key = (int(N), str(torch.device(device)))
+    t = _TWIDDLES.get(key)
+    if t is None:
+        t = torch.empty(N, dtype=torch.complex64, device=device)
+        _lib.call('gwb_fft_twiddles', int(N), _lib.ptr(t), _lib.stream_ptr(t.device))
+        _TWIDDLES[key] = t
+    return t
+
+
+class FusedBasisWorkspace:
+    """Workspace of the fused two-pass basis series: the intermediate W (rows x tlen complex), the twiddle table,
+    the scale partials and ticket."""
+
+    def __init__(self, tlen, flen, rows, device='cuda'):
+        self.tlen, self.flen, self.rows = tlen, flen, rows
+        self.W = torch.empty((rows, tlen), dtype=torch.complex64, device=device)
+        self.tw = twiddles(tlen, device)
+        self.partials = torch.empty(RB * max(1, tlen // 8), dtype=torch.float64, device=device)
+        self.ticket = torch.zeros(1, dtype=torch.int32, device=device)
+        self.scale = torch.empty(1, dtype=torch.float32, device=device)
+
+
+def basis_series_fused(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16', im_off=None):
+    """Same Z as basis_series_into in two fused passes (gwb_basis_fused); the scale is the whole-series rms of the
+    first RB rows by Parseval instead of the analysed-span rms (it cancels between Z and A). Returns the device
+    scale."""
+    r, flen = Vh.shape
+    assert r <= ws.rows and flen == ws.flen
+    im_off = r if im_off is None else im_off
+    _lib.call('gwb_basis_fused', _lib.ptr(Vh), Vh.stride(0), r, _lib.ptr(D), _lib.ptr(isw), flen, ws.tlen,
+              _lib.ptr(ws.tw), _lib.ptr(ws.W), int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0),
+              int(im_off), 0, min(RB, r), _lib.ptr(ws.partials), ws.partials.numel(), _lib.ptr(ws.ticket),
+              _lib.ptr(ws.scale), _lib.stream_ptr())
+    return ws.scale
+
+
 class BasisWorkspace:
     """Device buffers of the basis series for one (tlen, batch) shape: the zero-padded transform input q, the
     transform output, the scale reduction's partials and ticket. q's upper half is zeroed once and never written."""

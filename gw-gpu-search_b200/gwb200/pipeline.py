@@ -88,7 +88,14 @@ class MatchedFilter:
         # fp16 / bf16 / split bf16 use the compact complex operands on the tensor cores (A = [ReA | ImA], Z = [ReZ ;
         # ImZ], halves of Kh rows); the plain fp32 form uses the reference's stacked layout on the fp32 pipe
         self.compact = self.form != 'f32'
-        self.ws = fp_filter.BasisWorkspace(tlen, bank.flen, fp_filter.RB, device)
+        rmax = max(s['r'] for s in bank.svd)
+        # the fused two-pass basis series (premul and pack folded into the transform passes) where the length allows,
+        # else premul + cuFFT + pack
+        self.fused = (1 << 12) <= tlen <= (1 << 22)
+        if self.fused:
+            self.fws = fp_filter.FusedBasisWorkspace(tlen, bank.flen, rmax, device)
+        else:
+            self.ws = fp_filter.BasisWorkspace(tlen, bank.flen, fp_filter.RB, device)
         if self.compact:
             K = 2 * max(s['Kh'] for s in bank.svd)
         else:
@@ -146,8 +153,13 @@ class MatchedFilter:
         if prof is not None:
             e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
             e[0].record()
-        scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
-                                            self.Zlo, self.form, im_off=Kh if self.compact else r)
+        im_off = Kh if self.compact else r
+        if self.fused:
+            scale = fp_filter.basis_series_fused(self.fws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z, self.Zlo,
+                                                 self.form, im_off=im_off)
+        else:
+            scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
+                                                self.Zlo, self.form, im_off=im_off)
         nrm = sig[b.row0[t]:b.row0[t] + n, seg]
         fp_filter.stacked_A_into(sv['A'], nrm, scale, K, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
                                  df4=4.0 * b.df, kh=Kh)
@@ -164,9 +176,12 @@ class MatchedFilter:
                   _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), K,
                   Kh, f, _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
                   _lib.ptr(self.counters), _lib.stream_ptr())
-        nb = -(-r // fp_filter.RB)
-        self.kernel_launches += 2 * nb + 4      # premul and pack per batch; scale, stacked A, GEMM, selection
-        self.fft_launches += nb
+        if self.fused:
+            self.kernel_launches += 5           # two basis passes, stacked A, GEMM, selection
+        else:
+            nb = -(-r // fp_filter.RB)
+            self.kernel_launches += 2 * nb + 4  # premul and pack per batch; scale, stacked A, GEMM, selection
+            self.fft_launches += nb
 
     def norms(self, IP):
         """Template norms for every (row, segment): sig (M, S) float64 = 4 df sum |H|^2 IP (fp_filter.py:710-714)."""

@@ -90,3 +90,28 @@ def test_basis_series_and_gemm_rebuild_the_reference_snr(golden, form):
     np.testing.assert_allclose(V.cpu().numpy(), Vr, rtol=1e-4)
     t = int(float(g['t0']) * 2048) - a0
     assert abs(int(I[3].cpu().numpy()[np.argmax(V[3].cpu().numpy())]) - t) <= 2
+
+
+@pytest.mark.parametrize('tlen', [1 << 12, 1 << 15, 1 << 16, 1 << 20])
+def test_fused_basis_series_matches_float64_transform(tlen):
+    """The fused two-pass basis series (fp32 output) times its scale equals ifft(conj(Vh) D isw) over the span."""
+    from gwb200 import fp_filter
+    rng = np.random.default_rng(tlen % 1000)
+    flen = tlen // 2 + 1
+    r = 70
+    Vh = (rng.standard_normal((r, flen)) + 1j * rng.standard_normal((r, flen))).astype(np.complex64)
+    D = (rng.standard_normal(flen) + 1j * rng.standard_normal(flen)).astype(np.complex64)
+    isw = rng.uniform(0.5, 2, flen).astype(np.float32)
+    a0, Tn = tlen // 16, tlen - tlen // 8
+    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r)
+    Z = torch.zeros((2 * r, Tn), dtype=torch.float32, device='cuda')
+    sc = fp_filter.basis_series_fused(ws, torch.from_numpy(Vh).cuda(), torch.from_numpy(D).cuda(),
+                                      torch.from_numpy(isw).cuda(), a0, Tn, Z, None, 'f32', im_off=r)
+    scale = float(sc.item())
+    zb = of.basis_series_complex(Vh, D * isw, a0, Tn, tlen)
+    got = (Z[:r].double() + 1j * Z[r:].double()).cpu().numpy() * scale
+    err = np.abs(got - zb).max() / np.abs(zb).max()
+    assert err < 2e-5, err
+    # Parseval scale over the first 64 rows
+    q = np.conj(Vh[:64].astype(np.complex128)) * (D * isw)
+    assert abs(scale - np.sqrt((np.abs(q) ** 2).sum() / 64 / 2)) < 1e-5 * scale
