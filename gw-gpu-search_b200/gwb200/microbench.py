@@ -64,8 +64,14 @@ def basis(a):
     Kh = fp_filter.kh_of(r)
     Z = torch.zeros((2 * Kh, Tn), dtype=fp_filter._z_dtype(a.form), device='cuda')
     Zlo = torch.zeros_like(Z) if a.form == 'bf16x3' else None
+    fws = fp_filter.FusedBasisWorkspace(tlen, flen, r)
     ms = _time(lambda: fp_filter.basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
-    return dict(kernel='basis_series', form=a.form, r=r, tlen=tlen, ms=ms, us_per_row=ms * 1e3 / r)
+    msf = _time(lambda: fp_filter.basis_series_fused(fws, Vh, D, isw, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
+    # algorithmic bytes of the fused form: Vh read, W written and read, Z written (D and isw stay in L2)
+    zb = 2 * Tn * (2 if a.form in ('f16', 'bf16') else 4)
+    byts = r * (8 * flen + 16 * tlen + zb)
+    return dict(kernel='basis_series', form=a.form, r=r, tlen=tlen, ms_cufft_path=ms, us_per_row_cufft=ms * 1e3 / r,
+                ms_fused=msf, us_per_row_fused=msf * 1e3 / r, fused_gbs=byts / msf / 1e6)
 
 
 def exact(a):
