@@ -36,69 +36,80 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -(a.y * b.y)), fmaf(a.x, b.y, a.y * b.x));
 }
 
-// In-place inverse DFT of length L over TB interleaved columns: X[p * TB + c] holds element p of column c.
-// tw_s: e^{2 pi i m / L} for m < L in shared memory.
-template <int L, int NT>
-__device__ __forceinline__ void fft_smem(float2* X, const float2* tw_s) {
+// One Stockham stage of an in-place inverse DFT of length L over TB interleaved columns (X[p * TB + c] holds element
+// p of column c); NS = product of the radices already applied, all compile-time so index arithmetic is shifts and
+// masks. Each thread stages its butterflies' inputs in registers, the block syncs, then outputs are stored.
+// tw_s: e^{2 pi i m / L}, m < L.
+template <int L, int NT, int NS>
+__device__ __forceinline__ void radix4_stage(float2* X, const float2* tw_s) {
+    constexpr int Q = (L / 4) * TB / NT;
+    constexpr int STEP = L / (NS * 4);
     const int tid = threadIdx.x;
-    int Ns = 1;
-    constexpr int LOG = (L == 64) ? 6 : (L == 128) ? 7 : (L == 256) ? 8 : (L == 512) ? 9 : (L == 1024) ? 10 : 11;
-    constexpr int N4 = LOG / 2;                 // radix-4 stages
-    constexpr int Q4 = (L / 4) * TB / NT;       // butterflies per thread in a radix-4 stage
-#pragma unroll 1
-    for (int st = 0; st < N4; ++st) {
-        float2 v[Q4][4];
+    float2 v[Q][4];
 #pragma unroll
-        for (int q = 0; q < Q4; ++q) {
-            const int b = tid + NT * q;
-            const int c = b % TB, j = b / TB;
+    for (int q = 0; q < Q; ++q) {
+        const int b = tid + NT * q;
+        const int c = b % TB, j = b / TB;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) v[q][r] = X[(j + r * (L / 4)) * TB + c];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < Q4; ++q) {
-            const int b = tid + NT * q;
-            const int c = b % TB, j = b / TB;
-            const int k = j % Ns;
-            const int step = L / (Ns * 4);
-#pragma unroll
-            for (int r = 1; r < 4; ++r) v[q][r] = cmul(v[q][r], tw_s[k * r * step]);
-            const float2 a = make_float2(v[q][0].x + v[q][2].x, v[q][0].y + v[q][2].y);
-            const float2 bb = make_float2(v[q][0].x - v[q][2].x, v[q][0].y - v[q][2].y);
-            const float2 cc = make_float2(v[q][1].x + v[q][3].x, v[q][1].y + v[q][3].y);
-            const float2 d = make_float2(v[q][1].x - v[q][3].x, v[q][1].y - v[q][3].y);
-            const int idx = (j / Ns) * Ns * 4 + k;
-            X[(idx + 0 * Ns) * TB + c] = make_float2(a.x + cc.x, a.y + cc.y);
-            X[(idx + 1 * Ns) * TB + c] = make_float2(bb.x - d.y, bb.y + d.x);      // b + i d
-            X[(idx + 2 * Ns) * TB + c] = make_float2(a.x - cc.x, a.y - cc.y);
-            X[(idx + 3 * Ns) * TB + c] = make_float2(bb.x + d.y, bb.y - d.x);      // b - i d
-        }
-        __syncthreads();
-        Ns *= 4;
+        for (int r = 0; r < 4; ++r) v[q][r] = X[(j + r * (L / 4)) * TB + c];
     }
-    if (LOG & 1) {
-        constexpr int Q2 = (L / 2) * TB / NT;
-        float2 v[Q2][2];
+    __syncthreads();
 #pragma unroll
-        for (int q = 0; q < Q2; ++q) {
-            const int b = tid + NT * q;
-            const int c = b % TB, j = b / TB;
-            v[q][0] = X[j * TB + c];
-            v[q][1] = X[(j + L / 2) * TB + c];
-        }
-        __syncthreads();
+    for (int q = 0; q < Q; ++q) {
+        const int b = tid + NT * q;
+        const int c = b % TB, j = b / TB;
+        const int k = j % NS;
+        if (NS > 1) {
 #pragma unroll
-        for (int q = 0; q < Q2; ++q) {
-            const int b = tid + NT * q;
-            const int c = b % TB, j = b / TB;
-            const int k = j % Ns;
-            const float2 w = cmul(v[q][1], tw_s[k * (L / (Ns * 2))]);
-            const int idx = (j / Ns) * Ns * 2 + k;
-            X[idx * TB + c] = make_float2(v[q][0].x + w.x, v[q][0].y + w.y);
-            X[(idx + Ns) * TB + c] = make_float2(v[q][0].x - w.x, v[q][0].y - w.y);
+            for (int r = 1; r < 4; ++r) v[q][r] = cmul(v[q][r], tw_s[k * r * STEP]);
         }
-        __syncthreads();
+        const float2 a = make_float2(v[q][0].x + v[q][2].x, v[q][0].y + v[q][2].y);
+        const float2 bb = make_float2(v[q][0].x - v[q][2].x, v[q][0].y - v[q][2].y);
+        const float2 cc = make_float2(v[q][1].x + v[q][3].x, v[q][1].y + v[q][3].y);
+        const float2 d = make_float2(v[q][1].x - v[q][3].x, v[q][1].y - v[q][3].y);
+        const int idx = (j / NS) * NS * 4 + k;
+        X[(idx + 0 * NS) * TB + c] = make_float2(a.x + cc.x, a.y + cc.y);
+        X[(idx + 1 * NS) * TB + c] = make_float2(bb.x - d.y, bb.y + d.x);      // b + i d
+        X[(idx + 2 * NS) * TB + c] = make_float2(a.x - cc.x, a.y - cc.y);
+        X[(idx + 3 * NS) * TB + c] = make_float2(bb.x + d.y, bb.y - d.x);      // b - i d
+    }
+    __syncthreads();
+}
+
+template <int L, int NT, int NS>
+__device__ __forceinline__ void radix2_stage(float2* X, const float2* tw_s) {
+    constexpr int Q = (L / 2) * TB / NT;
+    constexpr int STEP = L / (NS * 2);
+    const int tid = threadIdx.x;
+    float2 v[Q][2];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int b = tid + NT * q;
+        const int c = b % TB, j = b / TB;
+        v[q][0] = X[j * TB + c];
+        v[q][1] = X[(j + L / 2) * TB + c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int b = tid + NT * q;
+        const int c = b % TB, j = b / TB;
+        const int k = j % NS;
+        const float2 w = NS > 1 ? cmul(v[q][1], tw_s[k * STEP]) : v[q][1];
+        const int idx = (j / NS) * NS * 2 + k;
+        X[idx * TB + c] = make_float2(v[q][0].x + w.x, v[q][0].y + w.y);
+        X[(idx + NS) * TB + c] = make_float2(v[q][0].x - w.x, v[q][0].y - w.y);
+    }
+    __syncthreads();
+}
+
+template <int L, int NT, int NS = 1>
+__device__ __forceinline__ void fft_smem(float2* X, const float2* tw_s) {
+    if constexpr (NS * 4 <= L) {
+        radix4_stage<L, NT, NS>(X, tw_s);
+        fft_smem<L, NT, NS * 4>(X, tw_s);
+    } else if constexpr (NS * 2 == L) {
+        radix2_stage<L, NT, NS>(X, tw_s);
     }
 }
 
@@ -120,6 +131,19 @@ __global__ void __launch_bounds__(threads_for<N1>()) basis_pass1(
     const int row = blockIdx.y, k20 = blockIdx.x * TB, tid = threadIdx.x;
     const long long stride = N / N1;
     for (int m = tid; m < N1; m += NT) tw_s[m] = tw[(long long)m * stride];
+    // e^{2 pi i k2 t1 / N} = TH[c][t1 / 32] TL[c][t1 % 32] for this CTA's 8 columns k2 = k20 + c
+    constexpr int NH = (N1 + 31) / 32;
+    float2* TH = tw_s + N1;             // TB x NH
+    float2* TL = TH + TB * NH;          // TB x 32
+    const unsigned long long mask = (unsigned long long)N - 1;
+    for (int e = tid; e < TB * NH; e += NT) {
+        const int c = e / NH, a = e % NH;
+        TH[e] = tw[((unsigned long long)(k20 + c) * (unsigned long long)(32 * a)) & mask];
+    }
+    for (int e = tid; e < TB * 32; e += NT) {
+        const int c = e / 32, b = e % 32;
+        TL[e] = tw[((unsigned long long)(k20 + c) * (unsigned long long)b) & mask];
+    }
     const float2* v = Vh + (long long)row * ldvh;
     double acc = 0.0;
     const long long half = N / 2;
@@ -140,11 +164,10 @@ __global__ void __launch_bounds__(threads_for<N1>()) basis_pass1(
     fft_smem<N1, NT>(X, tw_s);
     // twiddle e^{2 pi i k2 t1 / N} and write W[row][k2][t1], t1 contiguous
     float2* Wr = W + (long long)row * N;
-    const unsigned long long mask = (unsigned long long)N - 1;
     for (int e = tid; e < N1 * TB; e += NT) {
         const int c = e % TB, t1 = e / TB;     // shared reads conflict-free; global writes in 32-byte runs
-        const unsigned long long m = ((unsigned long long)(k20 + c) * (unsigned long long)t1) & mask;
-        Wr[(long long)(k20 + c) * N1 + t1] = cmul(X[t1 * TB + c], tw[m]);
+        const float2 w = cmul(TH[c * NH + (t1 >> 5)], TL[c * 32 + (t1 & 31)]);
+        Wr[(long long)(k20 + c) * N1 + t1] = cmul(X[t1 * TB + c], w);
     }
     // scale partials: one per CTA of the first rows, summed in a fixed order by the last CTA to finish
     if (nfirst > 0) {
@@ -232,7 +255,7 @@ int launch_pass1(const float2* Vh, long long ldvh, int rows, const float2* D, co
                  long long N, int N2, const float2* tw, float2* W, int nfirst, double* partials, unsigned* ticket,
                  float* scale_out, cudaStream_t s) {
     constexpr int NT = threads_for<N1>();
-    const size_t smem = (size_t)(N1 * TB + N1) * sizeof(float2);
+    const size_t smem = (size_t)(N1 * TB + N1 + TB * ((N1 + 31) / 32) + TB * 32) * sizeof(float2);
     auto k = basis_pass1<N1>;
     GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<dim3(N2 / TB, rows), NT, smem, s>>>(Vh, ldvh, D, isw, flen, N, N2, tw, W, nfirst, partials, ticket, scale_out);
