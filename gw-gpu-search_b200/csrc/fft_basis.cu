@@ -115,7 +115,7 @@ __device__ __forceinline__ void fft_smem(float2* X, const float2* tw_s) {
 
 template <int L>
 constexpr int threads_for() {
-    return (L * TB / 32) < 64 ? 64 : (L * TB / 32);
+    return (L * TB / 16) < 64 ? 64 : (L * TB / 16);
 }
 
 // pass 1: rows of the batch in blockIdx.y, 8 consecutive k2 in blockIdx.x
@@ -132,41 +132,55 @@ __global__ void __launch_bounds__(threads_for<N1>()) basis_pass1(
     const long long stride = N / N1;
     for (int m = tid; m < N1; m += NT) tw_s[m] = tw[(long long)m * stride];
     // e^{2 pi i k2 t1 / N} = TH[c][t1 / 32] TL[c][t1 % 32] for this CTA's 8 columns k2 = k20 + c
-    constexpr int NH = (N1 + 31) / 32;
-    float2* TH = tw_s + N1;             // TB x NH
-    float2* TL = TH + TB * NH;          // TB x 32
+    // rows padded by one entry so the 8 columns of a warp fall in different banks
+    constexpr int NH = (N1 + 31) / 32, NHP = NH + 1, NLP = 33;
+    float2* TH = tw_s + N1;             // TB x NHP
+    float2* TL = TH + TB * NHP;         // TB x NLP
     const unsigned long long mask = (unsigned long long)N - 1;
     for (int e = tid; e < TB * NH; e += NT) {
         const int c = e / NH, a = e % NH;
-        TH[e] = tw[((unsigned long long)(k20 + c) * (unsigned long long)(32 * a)) & mask];
+        TH[c * NHP + a] = tw[((unsigned long long)(k20 + c) * (unsigned long long)(32 * a)) & mask];
     }
     for (int e = tid; e < TB * 32; e += NT) {
         const int c = e / 32, b = e % 32;
-        TL[e] = tw[((unsigned long long)(k20 + c) * (unsigned long long)b) & mask];
+        TL[c * NLP + b] = tw[((unsigned long long)(k20 + c) * (unsigned long long)b) & mask];
     }
     const float2* v = Vh + (long long)row * ldvh;
     double acc = 0.0;
-    const long long half = N / 2;
-    for (int e = tid; e < N1 * TB; e += NT) {
-        const int c = e % TB, k1 = e / TB;
-        const long long k = (long long)N2 * k1 + k20 + c;
-        float2 q = make_float2(0.f, 0.f);
-        if (k <= half && k < flen) {
-            const float2 a = v[k], dk = D[k];
-            const float w = isw[k];
-            const float dr = dk.x * w, di = dk.y * w;
-            q = make_float2(fmaf(a.x, dr, a.y * di), fmaf(a.x, di, -(a.y * dr)));
-            if (row < nfirst) acc += (double)q.x * q.x + (double)q.y * q.y;
+    const long long lim = min(N / 2 + 1, flen);     // q is zero from N/2 + 1 on (the reference's zero padding)
+    // all loads of a batch issued before any use, so each thread keeps several requests in flight
+    constexpr int PER = N1 * TB / NT, BATCH = 8;
+    static_assert(PER % BATCH == 0, "loads per thread");
+#pragma unroll
+    for (int i0 = 0; i0 < PER; i0 += BATCH) {
+        float2 av[BATCH], dv[BATCH];
+        float wv[BATCH];
+#pragma unroll
+        for (int i = 0; i < BATCH; ++i) {
+            const int e = tid + NT * (i0 + i);
+            const long long k = (long long)N2 * (e / TB) + k20 + (e % TB);
+            const bool ok = k < lim;
+            av[i] = ok ? v[k] : make_float2(0.f, 0.f);
+            dv[i] = ok ? D[k] : make_float2(0.f, 0.f);
+            wv[i] = ok ? isw[k] : 0.f;
         }
-        X[k1 * TB + c] = q;
+#pragma unroll
+        for (int i = 0; i < BATCH; ++i) {
+            const int e = tid + NT * (i0 + i);
+            const float dr = dv[i].x * wv[i], di = dv[i].y * wv[i];
+            const float2 q = make_float2(fmaf(av[i].x, dr, av[i].y * di), fmaf(av[i].x, di, -(av[i].y * dr)));
+            acc += (double)q.x * q.x + (double)q.y * q.y;
+            X[e] = q;              // e = k1 * TB + c
+        }
     }
+    if (row >= nfirst) acc = 0.0;
     __syncthreads();
     fft_smem<N1, NT>(X, tw_s);
     // twiddle e^{2 pi i k2 t1 / N} and write W[row][k2][t1], t1 contiguous
     float2* Wr = W + (long long)row * N;
     for (int e = tid; e < N1 * TB; e += NT) {
         const int c = e % TB, t1 = e / TB;     // shared reads conflict-free; global writes in 32-byte runs
-        const float2 w = cmul(TH[c * NH + (t1 >> 5)], TL[c * 32 + (t1 & 31)]);
+        const float2 w = cmul(TH[c * NHP + (t1 >> 5)], TL[c * NLP + (t1 & 31)]);
         Wr[(long long)(k20 + c) * N1 + t1] = cmul(X[t1 * TB + c], w);
     }
     // scale partials: one per CTA of the first rows, summed in a fixed order by the last CTA to finish
@@ -212,9 +226,18 @@ __global__ void __launch_bounds__(threads_for<N2>()) basis_pass2(
     const long long stride = N / N2;
     for (int m = tid; m < N2; m += NT) tw_s[m] = tw[(long long)m * stride];
     const float2* Wr = W + (long long)row * N;
-    for (int e = tid; e < N2 * TB; e += NT) {
-        const int c = e % TB, k2 = e / TB;
-        X[k2 * TB + c] = Wr[(long long)k2 * N1 + t10 + c];
+    constexpr int PER = N2 * TB / NT, BATCH = 8;
+    static_assert(PER % BATCH == 0, "loads per thread");
+#pragma unroll
+    for (int i0 = 0; i0 < PER; i0 += BATCH) {
+        float2 wv[BATCH];
+#pragma unroll
+        for (int i = 0; i < BATCH; ++i) {
+            const int e = tid + NT * (i0 + i);
+            wv[i] = Wr[(long long)(e / TB) * N1 + t10 + (e % TB)];
+        }
+#pragma unroll
+        for (int i = 0; i < BATCH; ++i) X[tid + NT * (i0 + i)] = wv[i];
     }
     __syncthreads();
     fft_smem<N2, NT>(X, tw_s);
@@ -255,7 +278,7 @@ int launch_pass1(const float2* Vh, long long ldvh, int rows, const float2* D, co
                  long long N, int N2, const float2* tw, float2* W, int nfirst, double* partials, unsigned* ticket,
                  float* scale_out, cudaStream_t s) {
     constexpr int NT = threads_for<N1>();
-    const size_t smem = (size_t)(N1 * TB + N1 + TB * ((N1 + 31) / 32) + TB * 32) * sizeof(float2);
+    const size_t smem = (size_t)(N1 * TB + N1 + TB * ((N1 + 31) / 32 + 1) + TB * 33) * sizeof(float2);
     auto k = basis_pass1<N1>;
     GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<dim3(N2 / TB, rows), NT, smem, s>>>(Vh, ldvh, D, isw, flen, N, N2, tw, W, nfirst, partials, ticket, scale_out);
