@@ -18,6 +18,8 @@
 #include "common.cuh"
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <utility>
+#include <type_traits>
 
 namespace gwb {
 namespace {
@@ -112,6 +114,97 @@ __device__ __forceinline__ void fft_smem(float2* X, const float2* tw_s) {
         radix2_stage<L, NT, NS>(X, tw_s);
     }
 }
+
+// ---- register two-level DFT (L <= 1024): L = R1 R2, k = R2 a + b, t = u + R1 v ----
+//   X[u + R1 v] = sum_b e^{2 pi i b v / R2} e^{2 pi i b u / L} [ sum_a x[R2 a + b] e^{2 pi i a u / R1} ]
+// step 1: one thread per (b, column) holds x[R2 a + b] for all a in registers, R1-point DFT, twiddle, store to shared
+// step 2: one thread per (u, column) reads the R2 values, R2-point DFT in registers.
+// Shared memory is crossed once per pass (one store, one load per element) instead of once per radix-4 stage.
+
+// sin / cos of 2 pi k / n in double at compile time (argument reduced to [-pi, pi], Taylor series to 30 terms)
+__host__ __device__ constexpr double sin_taylor(double x) {
+    double term = x, sum = x;
+    for (int i = 1; i < 30; ++i) {
+        term *= -x * x / ((2.0 * i) * (2.0 * i + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double cos_taylor(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int i = 1; i < 30; ++i) {
+        term *= -x * x / ((2.0 * i - 1.0) * (2.0 * i));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double turn_angle(int k, int n) {
+    const int m = ((k % n) + n) % n;
+    const int r = 2 * m > n ? m - n : m;
+    return 6.283185307179586476925286766559 * (double)r / (double)n;
+}
+
+template <int I>
+using ic = std::integral_constant<int, I>;
+
+template <typename F, int... I>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
+    (f(ic<I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+    static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+constexpr int brev(int x, int bits) { return bits == 0 ? 0 : ((x & 1) << (bits - 1)) | brev(x >> 1, bits - 1); }
+
+// v * e^{2 pi i J / M}, trivial angles without multiplies
+template <int J, int M>
+__device__ __forceinline__ float2 rot(float2 v) {
+    constexpr int j = ((J % M) + M) % M;
+    if constexpr (j == 0) {
+        return v;
+    } else if constexpr (4 * j == M) {
+        return make_float2(-v.y, v.x);
+    } else if constexpr (2 * j == M) {
+        return make_float2(-v.x, -v.y);
+    } else if constexpr (4 * j == 3 * M) {
+        return make_float2(v.y, -v.x);
+    } else {
+        constexpr float c = (float)cos_taylor(turn_angle(J, M)), s = (float)sin_taylor(turn_angle(J, M));
+        return make_float2(fmaf(v.x, c, -(v.y * s)), fmaf(v.x, s, v.y * c));
+    }
+}
+
+// in-register inverse DFT (e^{+2 pi i}) of size R, decimation in frequency: natural input order, output X[u] in
+// x[brev(u)]
+template <int R>
+__device__ __forceinline__ void dft_reg(float2 (&x)[R]) {
+    static_for<ilog2(R)>([&](auto S) {
+        constexpr int h = R >> (decltype(S)::value + 1);
+        static_for<R / (2 * h)>([&](auto B) {
+            constexpr int base = decltype(B)::value * 2 * h;
+            static_for<h>([&](auto J) {
+                constexpr int j = decltype(J)::value;
+                const float2 a = x[base + j], b = x[base + j + h];
+                x[base + j] = make_float2(a.x + b.x, a.y + b.y);
+                x[base + j + h] = rot<j, 2 * h>(make_float2(a.x - b.x, a.y - b.y));
+            });
+        });
+    });
+}
+
+template <int L>
+struct Split {
+    static constexpr int R1 = 1 << ((ilog2(L) + 1) / 2);
+    static constexpr int R2 = L / R1;
+    static constexpr int NT = TB * R2;                 // step 1: one R1-point DFT per thread
+    static constexpr int P2 = R1 / R2;                 // step 2: R2-point DFTs per thread
+    static constexpr int SB = ((R1 + 15) / 16) * 16 + 1;           // = 1 mod 16 (8-byte words)
+    static constexpr int SC = R2 * SB + ((4 - (R2 * SB) % 16) + 16) % 16;   // = 4 mod 16
+    static_assert(R1 >= R2 && R1 % R2 == 0, "split");
+};
 
 template <int L>
 constexpr int threads_for() {
@@ -267,10 +360,201 @@ __global__ void __launch_bounds__(threads_for<N2>()) basis_pass2(
     }
 }
 
+// pass 1, register form: rows in blockIdx.y, 8 consecutive k2 in blockIdx.x
+template <int N1>
+__global__ void __launch_bounds__(Split<N1>::NT) basis_pass1_reg(
+    const float2* __restrict__ Vh, long long ldvh, const float2* __restrict__ D, const float* __restrict__ isw,
+    long long flen, long long N, int N2, const float2* __restrict__ tw, float2* __restrict__ W, int nfirst,
+    double* __restrict__ partials, unsigned int* __restrict__ ticket, float* __restrict__ scale_out) {
+    using S = Split<N1>;
+    constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC;
+    extern __shared__ float2 sm[];
+    float2* Y = sm;                       // TB x SC
+    float2* twL = Y + TB * SC;            // e^{2 pi i m / N1}, m < N1
+    float2* TL = twL + N1;                // TB x (R1 + 1): e^{2 pi i k2 u / N}
+    float2* TH = TL + TB * (R1 + 1);      // TB x (R2 + 1): e^{2 pi i k2 R1 v / N}
+    const int row = blockIdx.y, k20 = blockIdx.x * TB, tid = threadIdx.x;
+    const unsigned long long mask = (unsigned long long)N - 1;
+    const long long stride = N / N1;
+    for (int m = tid; m < N1; m += NT) twL[m] = tw[(long long)m * stride];
+    for (int e = tid; e < TB * R1; e += NT) {
+        const int c = e / R1, u = e % R1;
+        TL[c * (R1 + 1) + u] = tw[((unsigned long long)(k20 + c) * (unsigned long long)u) & mask];
+    }
+    for (int e = tid; e < TB * R2; e += NT) {
+        const int c = e / R2, v = e % R2;
+        TH[c * (R2 + 1) + v] = tw[((unsigned long long)(k20 + c) * (unsigned long long)(R1 * v)) & mask];
+    }
+    // step 1: thread (b, c) loads q at k1 = R2 a + b, k2 = k20 + c; q is zero from N/2 + 1 on (the reference's zero
+    // padding)
+    const int c = tid % TB, b = tid / TB;
+    const float2* v = Vh + (long long)row * ldvh;
+    const long long lim = min(N / 2 + 1, flen);
+    float2 x[R1];
+    float part = 0.f;
+#pragma unroll
+    for (int a = 0; a < R1; ++a) {
+        const long long k = (long long)N2 * (R2 * a + b) + k20 + c;
+        const bool ok = k < lim;
+        const float2 av = ok ? v[k] : make_float2(0.f, 0.f);
+        const float2 dk = ok ? D[k] : make_float2(0.f, 0.f);
+        const float w = ok ? isw[k] : 0.f;
+        const float dr = dk.x * w, di = dk.y * w;
+        x[a] = make_float2(fmaf(av.x, dr, av.y * di), fmaf(av.x, di, -(av.y * dr)));
+        part = fmaf(x[a].x, x[a].x, fmaf(x[a].y, x[a].y, part));
+    }
+    dft_reg<R1>(x);
+    __syncthreads();                      // tables
+    static_for<R1>([&](auto U) {
+        constexpr int u = decltype(U)::value;
+        Y[c * SC + b * SB + u] = cmul(x[brev(u, ilog2(R1))], twL[b * u]);
+    });
+    __syncthreads();
+    // step 2: thread (u, c), u fastest so the W stores run along t1
+    float2* Wr = W + (long long)row * N;
+#pragma unroll
+    for (int p = 0; p < S::P2; ++p) {
+        const int d = tid + NT * p;
+        const int u = d % R1, c2 = d / R1;
+        float2 y[R2];
+#pragma unroll
+        for (int bb = 0; bb < R2; ++bb) y[bb] = Y[c2 * SC + bb * SB + u];
+        dft_reg<R2>(y);
+        const float2 tl = TL[c2 * (R1 + 1) + u];
+        float2* wc = Wr + (long long)(k20 + c2) * N1 + u;
+        static_for<R2>([&](auto V) {
+            constexpr int vv = decltype(V)::value;
+            wc[R1 * vv] = cmul(y[brev(vv, ilog2(R2))], cmul(tl, TH[c2 * (R2 + 1) + vv]));
+        });
+    }
+    // scale partials: one per CTA of the first rows, summed in a fixed order by the last CTA to finish
+    if (nfirst > 0) {
+        __shared__ double red[32];
+        double acc = row < nfirst ? (double)part : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if ((tid & 31) == 0) red[tid >> 5] = acc;
+        __syncthreads();
+        __shared__ bool last;
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < NT / 32; ++w) s += red[w];
+            const unsigned nb = gridDim.x * (unsigned)min(nfirst, (int)gridDim.y);
+            if (row < nfirst) partials[(long long)row * gridDim.x + blockIdx.x] = s;
+            __threadfence();
+            last = false;
+            if (row < nfirst) last = atomicAdd(ticket, 1u) == nb - 1;
+        }
+        __syncthreads();
+        if (last && tid == 0) {
+            __threadfence();
+            const int nr = min(nfirst, (int)gridDim.y);
+            double s = 0.0;
+            for (long long i = 0; i < (long long)nr * gridDim.x; ++i) s += ((volatile double*)partials)[i];
+            *scale_out = (float)sqrt(s / (double)nr / 2.0);
+            *ticket = 0;
+        }
+    }
+}
+
+template <int FORM>
+__device__ __forceinline__ void store_z(void* Z, void* Zlo, long long re, long long im, float xr, float xi) {
+    if constexpr (FORM == 0) {
+        static_cast<__half*>(Z)[re] = __float2half_rn(xr);
+        static_cast<__half*>(Z)[im] = __float2half_rn(xi);
+    } else if constexpr (FORM == 1) {
+        static_cast<float*>(Z)[re] = xr;
+        static_cast<float*>(Z)[im] = xi;
+    } else {
+        const __nv_bfloat16 hr = __float2bfloat16_rn(xr), hm = __float2bfloat16_rn(xi);
+        static_cast<__nv_bfloat16*>(Z)[re] = hr;
+        static_cast<__nv_bfloat16*>(Z)[im] = hm;
+        if constexpr (FORM == 2) {
+            static_cast<__nv_bfloat16*>(Zlo)[re] = __float2bfloat16_rn(xr - __bfloat162float(hr));
+            static_cast<__nv_bfloat16*>(Zlo)[im] = __float2bfloat16_rn(xi - __bfloat162float(hm));
+        }
+    }
+}
+
+// pass 2, register form: rows in blockIdx.y, 8 consecutive t1 in blockIdx.x
+template <int N2, int FORM>
+__global__ void __launch_bounds__(Split<N2>::NT) basis_pass2_reg(
+    const float2* __restrict__ W, long long N, int N1, const float2* __restrict__ tw, long long a0, long long Tn,
+    const float* __restrict__ scale, void* __restrict__ Z, void* __restrict__ Zlo, long long ldz, int im_off,
+    int row0) {
+    using S = Split<N2>;
+    constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC;
+    extern __shared__ float2 sm[];
+    float2* Y = sm;
+    float2* twL = Y + TB * SC;
+    const int row = blockIdx.y, t10 = blockIdx.x * TB, tid = threadIdx.x;
+    const long long stride = N / N2;
+    for (int m = tid; m < N2; m += NT) twL[m] = tw[(long long)m * stride];
+    const int c = tid % TB, b = tid / TB;
+    const float2* wc = W + (long long)row * N + t10 + c;
+    float2 x[R1];
+#pragma unroll
+    for (int a = 0; a < R1; ++a) x[a] = wc[(long long)(R2 * a + b) * N1];
+    dft_reg<R1>(x);
+    __syncthreads();
+    static_for<R1>([&](auto U) {
+        constexpr int u = decltype(U)::value;
+        Y[c * SC + b * SB + u] = cmul(x[brev(u, ilog2(R1))], twL[b * u]);
+    });
+    __syncthreads();
+    // step 2: thread (c, u), c fastest so the Z stores run along t
+    const float inv = 1.0f / *scale;
+    const long long re_base = (long long)(row0 + row) * ldz, im_base = (long long)(im_off + row0 + row) * ldz;
+#pragma unroll
+    for (int p = 0; p < S::P2; ++p) {
+        const int d = tid + NT * p;
+        const int c2 = d % TB, u = d / TB;
+        float2 y[R2];
+#pragma unroll
+        for (int bb = 0; bb < R2; ++bb) y[bb] = Y[c2 * SC + bb * SB + u];
+        dft_reg<R2>(y);
+        const long long t0 = (long long)t10 + c2 + (long long)N1 * u - a0;
+        static_for<R2>([&](auto V) {
+            constexpr int vv = decltype(V)::value;
+            const long long t = t0 + (long long)N1 * (R1 * vv);
+            if (t >= 0 && t < Tn) {
+                const float2 z = y[brev(vv, ilog2(R2))];
+                store_z<FORM>(Z, Zlo, re_base + t, im_base + t, z.x * inv, z.y * inv);
+            }
+        });
+    }
+}
+
 int log2i(long long n) {
     int l = 0;
     while ((1ll << l) < n) ++l;
     return l;
+}
+
+template <int N1>
+int launch_pass1_reg(const float2* Vh, long long ldvh, int rows, const float2* D, const float* isw, long long flen,
+                     long long N, int N2, const float2* tw, float2* W, int nfirst, double* partials, unsigned* ticket,
+                     float* scale_out, cudaStream_t s) {
+    using S = Split<N1>;
+    const size_t smem = (size_t)(TB * S::SC + N1 + TB * (S::R1 + 1) + TB * (S::R2 + 1)) * sizeof(float2);
+    auto k = basis_pass1_reg<N1>;
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<dim3(N2 / TB, rows), S::NT, smem, s>>>(Vh, ldvh, D, isw, flen, N, N2, tw, W, nfirst, partials, ticket,
+                                              scale_out);
+    GWB_LAUNCH_CHECK("basis_pass1_reg");
+    return GWB_OK;
+}
+
+template <int N2, int FORM>
+int launch_pass2_reg(const float2* W, long long N, int N1, int rows, const float2* tw, long long a0, long long Tn,
+                     const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
+    using S = Split<N2>;
+    const size_t smem = (size_t)(TB * S::SC + N2) * sizeof(float2);
+    auto k = basis_pass2_reg<N2, FORM>;
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<dim3(N1 / TB, rows), S::NT, smem, s>>>(W, N, N1, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0);
+    GWB_LAUNCH_CHECK("basis_pass2_reg");
+    return GWB_OK;
 }
 
 template <int N1>
@@ -302,11 +586,20 @@ template <int N2>
 int launch_pass2(int form, const float2* W, long long N, int N1, int rows, const float2* tw, long long a0,
                  long long Tn, const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0,
                  cudaStream_t s) {
-    switch (form) {
-        case 0: return launch_pass2_f<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
-        case 1: return launch_pass2_f<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
-        case 2: return launch_pass2_f<N2, 2>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
-        default: return launch_pass2_f<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+    if constexpr (N2 <= 1024) {
+        switch (form) {
+            case 0: return launch_pass2_reg<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            case 1: return launch_pass2_reg<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            case 2: return launch_pass2_reg<N2, 2>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            default: return launch_pass2_reg<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        }
+    } else {
+        switch (form) {
+            case 0: return launch_pass2_f<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            case 1: return launch_pass2_f<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            case 2: return launch_pass2_f<N2, 2>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            default: return launch_pass2_f<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        }
     }
 }
 
@@ -350,11 +643,11 @@ int gwb_basis_fused(const float* Vh, long long ldvh, int rows, const float* D, c
     unsigned* tk = reinterpret_cast<unsigned*>(ticket);
     int st;
     switch (N1) {
-        case 64: st = launch_pass1<64>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
-        case 128: st = launch_pass1<128>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
-        case 256: st = launch_pass1<256>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
-        case 512: st = launch_pass1<512>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
-        case 1024: st = launch_pass1<1024>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 64: st = launch_pass1_reg<64>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 128: st = launch_pass1_reg<128>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 256: st = launch_pass1_reg<256>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 512: st = launch_pass1_reg<512>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
+        case 1024: st = launch_pass1_reg<1024>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
         default: st = launch_pass1<2048>(v, ldvh, rows, d, isw, flen, N, N2, t, w, nfirst, partials, tk, scale, s); break;
     }
     if (st) return st;
