@@ -100,28 +100,48 @@ def twiddles(N, device='cuda'):
     return t
 
 
-class FusedBasisWorkspace:
-    """Workspace of the fused two-pass basis series: the intermediate W (rows x tlen complex), the twiddle table,
-    the scale partials and ticket."""
+FUSED_MIN, FUSED_MAX = 1 << 12, 1 << 20     # transform lengths of the fused basis series
 
-    def __init__(self, tlen, flen, rows, device='cuda'):
+
+def fourstep_order(X, N, isw=None, out=None):
+    """Rows of a half spectrum (rows, flen) complex64 in the four-step order of a length-N transform: P[j, k2 (N1/2) +
+    k1] = X[j, N2 k1 + k2] (times isw), P[j, N/2] = X[j, N/2] (gwb_fourstep_order); the input layout of the fused
+    basis series."""
+    _lib.require_cuda(X)
+    X2 = X if X.dim() == 2 else X[None]
+    rows, flen = X2.shape
+    if out is None:
+        out = torch.empty((rows, N // 2 + 1), dtype=torch.complex64, device=X.device)
+    _lib.call('gwb_fourstep_order', _lib.ptr(X2), X2.stride(0), rows, _lib.ptr(isw), flen, int(N), _lib.ptr(out),
+              out.stride(0), _lib.stream_ptr(X.device))
+    return out if X.dim() == 2 else out[0]
+
+
+class FusedBasisWorkspace:
+    """Workspace of the fused two-pass basis series: the intermediate W (wrows x tlen complex; the rows go through it
+    in batches of wrows), the twiddle table, the scale partials and ticket."""
+
+    def __init__(self, tlen, flen, rows, device='cuda', wrows=None):
+        assert FUSED_MIN <= tlen <= FUSED_MAX and flen <= tlen // 2 + 1
         self.tlen, self.flen, self.rows = tlen, flen, rows
-        self.W = torch.empty((rows, tlen), dtype=torch.complex64, device=device)
+        self.wrows = rows if wrows is None else max(1, min(int(wrows), rows))
+        self.W = torch.empty((self.wrows, tlen), dtype=torch.complex64, device=device)
         self.tw = twiddles(tlen, device)
-        self.partials = torch.empty(RB * max(1, tlen // 8), dtype=torch.float64, device=device)
+        self.partials = torch.empty(RB * max(1, tlen // 64), dtype=torch.float64, device=device)
         self.ticket = torch.zeros(1, dtype=torch.int32, device=device)
         self.scale = torch.empty(1, dtype=torch.float32, device=device)
 
 
-def basis_series_fused(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16', im_off=None):
-    """Same Z as basis_series_into in two fused passes (gwb_basis_fused); the scale is the whole-series rms of the
-    first RB rows by Parseval instead of the analysed-span rms (it cancels between Z and A). Returns the device
-    scale."""
-    r, flen = Vh.shape
-    assert r <= ws.rows and flen == ws.flen
+def basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo=None, form='f16', im_off=None):
+    """Same Z as basis_series_into in two fused passes (gwb_basis_fused), from the basis filters Vp (r, tlen/2 + 1) and
+    one segment's D isw Dp (tlen/2 + 1,), both in four-step order (fourstep_order). The scale is the whole-series rms
+    of the first min(RB, wrows) rows by Parseval instead of the analysed-span rms (it cancels between Z and A).
+    Returns the device scale."""
+    r = Vp.shape[0]
+    assert r <= ws.rows and Vp.shape[1] >= ws.tlen // 2 + 1 and Dp.numel() >= ws.tlen // 2 + 1
     im_off = r if im_off is None else im_off
-    _lib.call('gwb_basis_fused', _lib.ptr(Vh), Vh.stride(0), r, _lib.ptr(D), _lib.ptr(isw), flen, ws.tlen,
-              _lib.ptr(ws.tw), _lib.ptr(ws.W), int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0),
+    _lib.call('gwb_basis_fused', _lib.ptr(Vp), Vp.stride(0), r, _lib.ptr(Dp), ws.tlen, _lib.ptr(ws.tw),
+              _lib.ptr(ws.W), ws.wrows, int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0),
               int(im_off), 0, min(RB, r), _lib.ptr(ws.partials), ws.partials.numel(), _lib.ptr(ws.ticket),
               _lib.ptr(ws.scale), _lib.stream_ptr())
     return ws.scale

@@ -1,7 +1,7 @@
 """Micro-benchmarks of single kernels on synthetic operands (used for profiling; prints one JSON line per case).
 
     python -m gwb200.microbench gemm  [--r 128] [--n 256] [--tn 917504] [--form f16] [--reps 20]
-    python -m gwb200.microbench basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5]
+    python -m gwb200.microbench basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5] [--wrows 0,4,8]
     python -m gwb200.microbench exact [--groups 512] [--peaks 1] [--tlen 1048576] [--reps 5]
 
 Run from gw-gpu-search_b200/ (or with it on sys.path). Operand sizes default to one (tile, chunk) of the C2
@@ -64,14 +64,18 @@ def basis(a):
     Kh = fp_filter.kh_of(r)
     Z = torch.zeros((2 * Kh, Tn), dtype=fp_filter._z_dtype(a.form), device='cuda')
     Zlo = torch.zeros_like(Z) if a.form == 'bf16x3' else None
-    fws = fp_filter.FusedBasisWorkspace(tlen, flen, r)
+    Dp = fp_filter.fourstep_order(D, tlen, isw)
+    Vp = fp_filter.fourstep_order(Vh, tlen)
     ms = _time(lambda: fp_filter.basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
-    msf = _time(lambda: fp_filter.basis_series_fused(fws, Vh, D, isw, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
-    # algorithmic bytes of the fused form: Vh read, W written and read, Z written (D and isw stay in L2)
+    out = dict(kernel='basis_series', form=a.form, r=r, tlen=tlen, ms_cufft_path=ms, us_per_row_cufft=ms * 1e3 / r)
     zb = 2 * Tn * (2 if a.form in ('f16', 'bf16') else 4)
-    byts = r * (8 * flen + 16 * tlen + zb)
-    return dict(kernel='basis_series', form=a.form, r=r, tlen=tlen, ms_cufft_path=ms, us_per_row_cufft=ms * 1e3 / r,
-                ms_fused=msf, us_per_row_fused=msf * 1e3 / r, fused_gbs=byts / msf / 1e6)
+    for wr in [int(x) for x in a.wrows.split(',')]:
+        fws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wr or None)
+        msf = _time(lambda: fp_filter.basis_series_fused(fws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
+        # HBM bytes of the fused form when W stays in L2: Vh read and Z written (D isw stays in L2)
+        out[f'us_per_row_fused_w{fws.wrows}'] = msf * 1e3 / r
+        out[f'hbm_gbs_w{fws.wrows}'] = r * (8 * flen + zb) / msf / 1e6
+    return out
 
 
 def exact(a):
@@ -115,6 +119,7 @@ def main():
     ap.add_argument('--groups', type=int, default=512)
     ap.add_argument('--peaks', type=int, default=1)
     ap.add_argument('--reps', type=int, default=10)
+    ap.add_argument('--wrows', default='0', help='basis: comma list of W row batches (0: all rows at once)')
     a = ap.parse_args()
     print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact}[a.what](a)))
 

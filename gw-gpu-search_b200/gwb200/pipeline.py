@@ -4,7 +4,9 @@ loop (pipeline/fp_filter.py:700-888).
 Layout in HBM (all resident for a run):
   H      (M, flen) complex64   every template of the bank, tile after tile (rows sorted by chirp time); read by the
                                Gram/Vh setup and by the exact stage
-  Vh_t   (r_t, flen) complex64 per tile basis filters; A_t (n_t, r_t) complex64 mixing matrices
+  Vh_t   (r_t, flen) complex64 per tile basis filters (and Vp_t, the same in four-step order for the fused basis
+                               series); A_t (n_t, r_t) complex64 mixing matrices
+  Dp     (S, tlen/2 + 1)       D isw of every segment in four-step order
   D, IP  (S, flen)             over-whitened data and inverse PSD of every segment
   sig    (M, S) float64        template norms
   Z      (Kp, Tn)              basis series of the current (tile, segment), fp16 / fp32 / bf16 hi+lo
@@ -91,9 +93,12 @@ class MatchedFilter:
         rmax = max(s['r'] for s in bank.svd)
         # the fused two-pass basis series (premul and pack folded into the transform passes) where the length allows,
         # else premul + cuFFT + pack
-        self.fused = (1 << 12) <= tlen <= (1 << 22)
+        self.fused = fp_filter.FUSED_MIN <= tlen <= fp_filter.FUSED_MAX
         if self.fused:
             self.fws = fp_filter.FusedBasisWorkspace(tlen, bank.flen, rmax, device)
+            # basis filters in the four-step order of the transform, once per tile; D isw per step (self.Dp)
+            self.vp = [fp_filter.fourstep_order(s['Vh'], tlen) for s in bank.svd]
+            self.Dp = None
         else:
             self.ws = fp_filter.BasisWorkspace(tlen, bank.flen, fp_filter.RB, device)
         if self.compact:
@@ -155,8 +160,8 @@ class MatchedFilter:
             e[0].record()
         im_off = Kh if self.compact else r
         if self.fused:
-            scale = fp_filter.basis_series_fused(self.fws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z, self.Zlo,
-                                                 self.form, im_off=im_off)
+            scale = fp_filter.basis_series_fused(self.fws, self.vp[t], self.Dp[seg], self.a0, self.Tn, self.Z,
+                                                 self.Zlo, self.form, im_off=im_off)
         else:
             scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
                                                 self.Zlo, self.form, im_off=im_off)
@@ -177,7 +182,8 @@ class MatchedFilter:
                   Kh, f, _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
                   _lib.ptr(self.counters), _lib.stream_ptr())
         if self.fused:
-            self.kernel_launches += 5           # two basis passes, stacked A, GEMM, selection
+            nb = -(-r // self.fws.wrows)
+            self.kernel_launches += 2 * nb + 3  # two basis passes per row batch, stacked A, GEMM, selection
         else:
             nb = -(-r // fp_filter.RB)
             self.kernel_launches += 2 * nb + 4  # premul and pack per batch; scale, stacked A, GEMM, selection
@@ -219,6 +225,12 @@ class MatchedFilter:
         Nothing is copied back; call results() after the stream is synchronised."""
         self.counters.zero_()
         sig = self.norms(IP)
+        if self.fused:
+            # every segment's D isw in four-step order, shared by all tiles
+            if self.Dp is None or self.Dp.shape[0] != D.shape[0]:
+                self.Dp = torch.empty((D.shape[0], self.tlen // 2 + 1), dtype=torch.complex64, device=D.device)
+            fp_filter.fourstep_order(D, self.tlen, isw, out=self.Dp)
+            self.kernel_launches += 1
         segs = range(D.shape[0]) if seg_ids is None else seg_ids
         for t in range(len(self.bank.tiles)):
             for s in segs:

@@ -234,18 +234,25 @@ GWB_API int gwb_stacked_a(const float* A, long long lda, int n, int r, const dou
                           double df4, const float* scale, int Kp, int kh, int form, void* Are, void* Aim,
                           void* Are_lo, void* Aim_lo, long long ldo, void* stream);
 
-/* Fused basis series in two passes over HBM (replaces premul + C2C inverse transform + pack, fp_filter.py:597-613):
- * pass 1 forms q = conj(Vh) D isw (zero above N/2) on load and transforms over k1 (N = N1 N2), pass 2 transforms
- * over k2 and packs z[a0 .. a0+Tn) / scale into Z (rows row0+j and im_off+row0+j; form as gwb_basis_pack).
- * tw: e^{2 pi i m / N}, m < N (gwb_fft_twiddles). W: workspace of rows x N complex. The scale is computed from the
- * inputs of the first nfirst rows by Parseval (rms over the whole series; the reference takes the rms of the outputs
- * over the analysed span; the scale cancels between Z and A). partials: >= min(nfirst, rows) * N2 / 8 doubles;
- * ticket: one uint32, zero on entry. N a power of two in [2^12, 2^22]. */
+/* Fused basis series in two passes over HBM (replaces premul + C2C inverse transform + pack, fp_filter.py:597-613).
+ * N = N1 N2 (N1 = 2^ceil(log2(N) / 2)), k = N2 k1 + k2; only k <= N/2 enters (the reference zero-pads the half
+ * spectrum). Inputs in four-step order (gwb_fourstep_order): Vp (rows x ldvp, the basis filters) and Dp (D isw of one
+ * segment, the product the reference passes at fp_filter.py:741). Pass 1 forms q = conj(Vp) Dp and transforms over k1;
+ * pass 2 transforms over k2 and packs z[a0 .. a0+Tn) / scale into Z (rows row0+j and im_off+row0+j; form as
+ * gwb_basis_pack). tw: e^{2 pi i m / N}, m < N (gwb_fft_twiddles). W: workspace of wrows x N complex; rows are
+ * transformed in batches of wrows through it. The scale is computed from the inputs of the first min(nfirst, wrows)
+ * rows by Parseval (rms over the whole series; the reference takes the rms of the outputs over the analysed span of
+ * its first batch; the scale cancels between Z and A). partials: >= that many rows x N2 / 8 doubles; ticket: one
+ * uint32, zero on entry. N a power of two in [2^12, 2^20]. */
 GWB_API int gwb_fft_twiddles(long long N, float* tw, void* stream);
-GWB_API int gwb_basis_fused(const float* Vh, long long ldvh, int rows, const float* D, const float* isw, long long flen,
-                            long long N, const float* tw, float* W, long long a0, long long Tn, int form, void* Z,
-                            void* Zlo, long long ldz, int im_off, int row0, int nfirst, double* partials,
-                            long long npartials, uint32_t* ticket, float* scale, void* stream);
+/* Four-step order of rows of a half spectrum: P[j][k2 (N1/2) + k1] = X[j][N2 k1 + k2] isw[k] for k1 < N1/2, k2 < N2,
+ * P[j][N/2] = X[j][N/2] isw[N/2], zero where k >= flen (isw NULL: no weight). ldp >= N/2 + 1. */
+GWB_API int gwb_fourstep_order(const float* X, long long ldx, int rows, const float* isw, long long flen, long long N,
+                               float* P, long long ldp, void* stream);
+GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const float* Dp, long long N, const float* tw,
+                            float* W, int wrows, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz,
+                            int im_off, int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket,
+                            float* scale, void* stream);
 
 /* ---- candidate selection and the exact stage ---------------------------------------------------------------- */
 /* Window candidates of one (tile, segment) (fp_filter.py:745-764): rows i < n whose windowed maximum vw (the fused

@@ -92,9 +92,30 @@ def test_basis_series_and_gemm_rebuild_the_reference_snr(golden, form):
     assert abs(int(I[3].cpu().numpy()[np.argmax(V[3].cpu().numpy())]) - t) <= 2
 
 
-@pytest.mark.parametrize('tlen', [1 << 12, 1 << 15, 1 << 16, 1 << 20])
-def test_fused_basis_series_matches_float64_transform(tlen):
-    """The fused two-pass basis series (fp32 output) times its scale equals ifft(conj(Vh) D isw) over the span."""
+@pytest.mark.parametrize('tlen,flen', [(1 << 12, None), (1 << 13, 3000), (1 << 15, None), (1 << 20, None)])
+def test_fourstep_order(tlen, flen):
+    """P[k2 (N1/2) + k1] = X[N2 k1 + k2] isw for k1 < N1/2, P[N/2] = X[N/2] isw, zero from flen on."""
+    from gwb200 import fp_filter
+    rng = np.random.default_rng(7)
+    flen = tlen // 2 + 1 if flen is None else flen
+    X = (rng.standard_normal((3, flen)) + 1j * rng.standard_normal((3, flen))).astype(np.complex64)
+    isw = rng.uniform(0.5, 2, flen).astype(np.float32)
+    P = fp_filter.fourstep_order(torch.from_numpy(X).cuda(), tlen, torch.from_numpy(isw).cuda()).cpu().numpy()
+    p = (tlen.bit_length() - 1 + 1) // 2
+    N1, N2 = 1 << p, tlen >> p
+    full = np.zeros((3, tlen // 2 + 1), np.complex64)
+    full[:, :flen] = X * isw
+    ref = np.empty_like(full)
+    ref[:, :tlen // 2] = full[:, :tlen // 2].reshape(3, N1 // 2, N2).transpose(0, 2, 1).reshape(3, -1)
+    ref[:, tlen // 2] = full[:, tlen // 2]
+    assert np.array_equal(P, ref)
+
+
+@pytest.mark.parametrize('tlen,wrows', [(1 << 12, None), (1 << 13, 32), (1 << 15, None), (1 << 16, 32), (1 << 20, 8),
+                                        (1 << 20, None)])
+def test_fused_basis_series_matches_float64_transform(tlen, wrows):
+    """The fused two-pass basis series (fp32 output) times its scale equals ifft(conj(Vh) D isw) over the span, with the
+    rows in batches of wrows through W."""
     from gwb200 import fp_filter
     rng = np.random.default_rng(tlen % 1000)
     flen = tlen // 2 + 1
@@ -102,16 +123,19 @@ def test_fused_basis_series_matches_float64_transform(tlen):
     Vh = (rng.standard_normal((r, flen)) + 1j * rng.standard_normal((r, flen))).astype(np.complex64)
     D = (rng.standard_normal(flen) + 1j * rng.standard_normal(flen)).astype(np.complex64)
     isw = rng.uniform(0.5, 2, flen).astype(np.float32)
+    Dw = D * isw
     a0, Tn = tlen // 16, tlen - tlen // 8
-    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r)
+    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wrows)
     Z = torch.zeros((2 * r, Tn), dtype=torch.float32, device='cuda')
-    sc = fp_filter.basis_series_fused(ws, torch.from_numpy(Vh).cuda(), torch.from_numpy(D).cuda(),
-                                      torch.from_numpy(isw).cuda(), a0, Tn, Z, None, 'f32', im_off=r)
+    Vp = fp_filter.fourstep_order(torch.from_numpy(Vh).cuda(), tlen)
+    Dp = fp_filter.fourstep_order(torch.from_numpy(D).cuda(), tlen, torch.from_numpy(isw).cuda())
+    sc = fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, None, 'f32', im_off=r)
     scale = float(sc.item())
-    zb = of.basis_series_complex(Vh, D * isw, a0, Tn, tlen)
+    zb = of.basis_series_complex(Vh, Dw, a0, Tn, tlen)
     got = (Z[:r].double() + 1j * Z[r:].double()).cpu().numpy() * scale
     err = np.abs(got - zb).max() / np.abs(zb).max()
     assert err < 2e-5, err
-    # Parseval scale over the first 64 rows
-    q = np.conj(Vh[:64].astype(np.complex128)) * (D * isw)
-    assert abs(scale - np.sqrt((np.abs(q) ** 2).sum() / 64 / 2)) < 1e-5 * scale
+    # Parseval scale over the first min(64, wrows) rows
+    nf = min(64, ws.wrows)
+    q = np.conj(Vh[:nf].astype(np.complex128)) * Dw
+    assert abs(scale - np.sqrt((np.abs(q) ** 2).sum() / nf / 2)) < 1e-5 * scale
