@@ -171,6 +171,157 @@ struct Split {
     static_assert(R1 >= R2 && R1 % R2 == 0 && R1 % 8 == 0, "split");
 };
 
+// Scale partials of a pass-1 CTA: sum of |q|^2 over the CTA (one double per CTA of the first nfirst rows), summed in
+// a fixed order by the last CTA to finish, which writes scale = sqrt(mean / 2) and resets the ticket.
+template <int NT>
+__device__ __forceinline__ void scale_partials(float part, int row, int nfirst, double* __restrict__ partials,
+                                               unsigned int* __restrict__ ticket, float* __restrict__ scale_out) {
+    __shared__ double red[32];
+    __shared__ bool last;
+    const int tid = threadIdx.x;
+    double acc = row < nfirst ? (double)part : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((tid & 31) == 0) red[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0.0;
+        for (int w = 0; w < NT / 32; ++w) s += red[w];
+        const unsigned nb = gridDim.x * (unsigned)min(nfirst, (int)gridDim.y);
+        if (row < nfirst) partials[(long long)row * gridDim.x + blockIdx.x] = s;
+        __threadfence();
+        last = false;
+        if (row < nfirst) last = atomicAdd(ticket, 1u) == nb - 1;
+    }
+    __syncthreads();
+    if (last && tid == 0) {
+        __threadfence();
+        const int nr = min(nfirst, (int)gridDim.y);
+        double s = 0.0;
+        for (long long i = 0; i < (long long)nr * gridDim.x; ++i) s += ((volatile double*)partials)[i];
+        // mean over t of |z|^2 = sum_k |q|^2 (Parseval); scale = sqrt(mean / 2)
+        *scale_out = (float)sqrt(s / (double)nr / 2.0);
+        *ticket = 0;
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+constexpr int RC = 8;   // rows per pass-1 CTA of the warp-per-column form
+
+// pass 1 for N1 = 1024: one warp per column k2 (8 columns per CTA), RC consecutive rows per CTA. 32 x 32 split: lane
+// b holds q at k1 = 32 a + b (a < 16), 32-point DFT, twiddle, exchange through the warp's own shared tile, lane u
+// then holds the 32 values of t1 = u + 32 v. Per column, D isw and the twiddles stay in registers / shared memory
+// across the rows, and the next row's basis-filter segment (4 KB, contiguous in four-step order) is copied into
+// shared memory (cp.async) while the current row is transformed. No CTA barrier after the set-up, so the warps of a
+// CTA drift apart and one warp's copies overlap another's arithmetic. Scale partials: one per (row chunk, column),
+// summed in a fixed order by the last warp to finish.
+__global__ void __launch_bounds__(256, 2) basis_pass1_w(
+    const float2* __restrict__ Vp, long long ldvp, int rows, const float2* __restrict__ Dp, int N, int N2,
+    const float2* __restrict__ tw, float2* __restrict__ W, int nfirst, double* __restrict__ partials,
+    unsigned int* __restrict__ ticket, float* __restrict__ scale_out) {
+    constexpr int N1 = 1024, R = 32, H = N1 / 2, NW = 8, YS = R * (R + 1);
+    constexpr int WS = YS + R + H;                          // per warp: Y tile, TH, basis-filter segment
+    extern __shared__ float2 sm[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float2* twL = sm;                                       // e^{2 pi i m / N1} at m + m / 16
+    float2* Yw = sm + N1 + N1 / 16 + warp * WS;             // this warp's 32 x 33 tile
+    float2* THw = Yw + YS;                                  // e^{2 pi i k2 32 v / N}, v < 32
+    float2* Vs = THw + R;                                   // Vp[row][k2 H .. k2 H + H)
+    const int k2 = blockIdx.x * NW + warp;
+    const int j0 = blockIdx.y * RC, j1 = min(j0 + RC, rows);
+    const int mask = N - 1;
+    auto fetch = [&](int j) {                               // 4 KB: 8 x 16 bytes per lane
+        const char* g = reinterpret_cast<const char*>(Vp + (long long)j * ldvp + k2 * H);
+        char* d = reinterpret_cast<char*>(Vs);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) cp_async16(d + i * 512 + lane * 16, g + i * 512 + lane * 16);
+        cp_async_commit();
+    };
+    fetch(j0);
+    float2 dk[R / 2];
+#pragma unroll
+    for (int a = 0; a < R / 2; ++a) dk[a] = __ldg(Dp + k2 * H + R * a + lane);
+    const float2 dN = Dp[N / 2];
+    for (int m = threadIdx.x; m < N1; m += NW * 32) twL[m + (m >> 4)] = tw[m * (N / N1)];
+    THw[lane] = tw[(k2 * (R * lane)) & mask];
+    const float2 tl = tw[(k2 * lane) & mask];               // e^{2 pi i k2 u / N}, u = lane
+    __syncthreads();
+    const int nf = min(nfirst, rows);
+    double acc = 0.0;
+    for (int j = j0; j < j1; ++j) {
+        cp_async_wait_all();
+        __syncwarp();
+        float2 x[R];
+#pragma unroll
+        for (int a = 0; a < R / 2; ++a) x[a] = Vs[R * a + lane];
+        __syncwarp();
+        if (j + 1 < j1) fetch(j + 1);
+        float part = 0.f;
+#pragma unroll
+        for (int a = 0; a < R / 2; ++a) {
+            const float2 av = x[a];
+            x[a] = make_float2(fmaf(av.x, dk[a].x, av.y * dk[a].y), fmaf(av.x, dk[a].y, -(av.y * dk[a].x)));
+            part = fmaf(x[a].x, x[a].x, fmaf(x[a].y, x[a].y, part));
+        }
+        x[R / 2] = make_float2(0.f, 0.f);
+        if (k2 == 0 && lane == 0) {                         // the bin N / 2
+            const float2 av = Vp[(long long)j * ldvp + N / 2];
+            x[R / 2] = make_float2(fmaf(av.x, dN.x, av.y * dN.y), fmaf(av.x, dN.y, -(av.y * dN.x)));
+            part = fmaf(x[R / 2].x, x[R / 2].x, fmaf(x[R / 2].y, x[R / 2].y, part));
+        }
+#pragma unroll
+        for (int a = R / 2 + 1; a < R; ++a) x[a] = make_float2(0.f, 0.f);
+        if (j < nf) acc += (double)part;
+        dft_reg<R>(x);
+        static_for<R>([&](auto U) {
+            constexpr int u = decltype(U)::value;
+            const int m = lane * u;
+            Yw[lane * (R + 1) + u] = cmul(x[brev(u, ilog2(R))], twL[m + (m >> 4)]);
+        });
+        __syncwarp();
+#pragma unroll
+        for (int bb = 0; bb < R; ++bb) x[bb] = Yw[bb * (R + 1) + lane];
+        __syncwarp();
+        dft_reg<R>(x);
+        // t1 = lane + 32 v: W block t1 / 8 = 4 v + lane / 8, position lane % 8
+        float2* wc = W + (long long)j * N + (lane >> 3) * (N2 * 8) + k2 * 8 + (lane & 7);
+        static_for<R>([&](auto V) {
+            constexpr int vv = decltype(V)::value;
+            wc[4 * vv * (N2 * 8)] = cmul(x[brev(vv, ilog2(R))], cmul(tl, THw[vv]));
+        });
+    }
+    if (nf <= 0 || j0 >= nf) return;
+    // scale: partials[chunk * N2 + k2]; the last of the ceil(nf / RC) * N2 warps sums them in a fixed order
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    const unsigned total = (unsigned)(((nf + RC - 1) / RC) * N2);
+    unsigned last = 0;
+    if (lane == 0) {
+        partials[(long long)blockIdx.y * N2 + k2] = acc;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == total - 1;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    double s = 0.0;
+    for (unsigned i = lane; i < total; i += 32) s += ((volatile double*)partials)[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) {
+        // mean over t of |z|^2 = sum_k |q|^2 (Parseval); scale = sqrt(mean / 2)
+        *scale_out = (float)sqrt(s / (double)nf / 2.0);
+        *ticket = 0;
+    }
+}
+
 // pass 1: rows in blockIdx.y, TB consecutive k2 in blockIdx.x. Vp, Dp in four-step order (Dp already D isw).
 template <int N1>
 __global__ void __launch_bounds__(Split<N1, 8>::NT) basis_pass1(
@@ -242,34 +393,7 @@ __global__ void __launch_bounds__(Split<N1, 8>::NT) basis_pass1(
             wc[(R1 / 8) * vv * (N2 * 8)] = cmul(y[brev(vv, ilog2(R2))], cmul(tl, TH[c2 * (R2 + 1) + vv]));
         });
     }
-    // scale partials: one per CTA of the first rows, summed in a fixed order by the last CTA to finish
-    if (nfirst > 0) {
-        __shared__ double red[32];
-        double acc = row < nfirst ? (double)part : 0.0;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
-        if ((tid & 31) == 0) red[tid >> 5] = acc;
-        __syncthreads();
-        __shared__ bool last;
-        if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < NT / 32; ++w) s += red[w];
-            const unsigned nb = gridDim.x * (unsigned)min(nfirst, (int)gridDim.y);
-            if (row < nfirst) partials[(long long)row * gridDim.x + blockIdx.x] = s;
-            __threadfence();
-            last = false;
-            if (row < nfirst) last = atomicAdd(ticket, 1u) == nb - 1;
-        }
-        __syncthreads();
-        if (last && tid == 0) {
-            __threadfence();
-            const int nr = min(nfirst, (int)gridDim.y);
-            double s = 0.0;
-            for (long long i = 0; i < (long long)nr * gridDim.x; ++i) s += ((volatile double*)partials)[i];
-            *scale_out = (float)sqrt(s / (double)nr / 2.0);
-            *ticket = 0;
-        }
-    }
+    if (nfirst > 0) scale_partials<NT>(part, row, nfirst, partials, ticket, scale_out);
 }
 
 template <int FORM>
@@ -354,6 +478,16 @@ int log2i(long long n) {
     return l;
 }
 
+int launch_pass1_w(const float2* Vp, long long ldvp, int rows, const float2* Dp, int N, int N2, const float2* tw,
+                   float2* W, int nfirst, double* partials, unsigned* ticket, float* scale_out, cudaStream_t s) {
+    const size_t smem = (size_t)(1024 + 64 + 8 * (32 * 33 + 32 + 512)) * sizeof(float2);
+    GWB_CUDA(cudaFuncSetAttribute(basis_pass1_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    basis_pass1_w<<<dim3(N2 / 8, (rows + RC - 1) / RC), 256, smem, s>>>(Vp, ldvp, rows, Dp, N, N2, tw, W, nfirst,
+                                                                         partials, ticket, scale_out);
+    GWB_LAUNCH_CHECK("basis_pass1_w");
+    return GWB_OK;
+}
+
 template <int N1>
 int launch_pass1(const float2* Vp, long long ldvp, int rows, const float2* Dp, int N, int N2, const float2* tw,
                  float2* W, int nfirst, double* partials, unsigned* ticket, float* scale_out, cudaStream_t s) {
@@ -434,8 +568,11 @@ int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const float* Dp, 
     const int p = log2i(N);
     const int N1 = 1 << ((p + 1) / 2), N2 = (int)(N / N1);
     const int nf = std::min(nfirst, std::min(rows, wrows));
-    GWB_CHECK_ARG(nf <= 0 || (partials && ticket && (long long)nf * (N2 / TB) <= npartials), GWB_ERR_SHAPE,
-                  "basis_fused: scale partials need %lld entries", (long long)nf * (N2 / TB));
+    const long long need = N1 == 1024 ? (long long)(nf + RC - 1) / RC * N2 : (long long)nf * (N2 / TB);
+    GWB_CHECK_ARG(nf <= 0 || (partials && ticket && need <= npartials), GWB_ERR_SHAPE,
+                  "basis_fused: scale partials need %lld entries", need);
+    GWB_CHECK_ARG(N1 != 1024 || ((uintptr_t)Vp % 16 == 0 && ldvp % 2 == 0), GWB_ERR_ALIGN,
+                  "basis_fused: Vp and its row stride must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
     const float2* d = reinterpret_cast<const float2*>(Dp);
     const float2* t = reinterpret_cast<const float2*>(tw);
@@ -454,7 +591,7 @@ int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const float* Dp, 
             case 128: st = launch_pass1<128>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
             case 256: st = launch_pass1<256>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
             case 512: st = launch_pass1<512>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
-            default: st = launch_pass1<1024>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
+            default: st = launch_pass1_w(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
         }
         if (st) return st;
         const int r0 = row0 + j0;

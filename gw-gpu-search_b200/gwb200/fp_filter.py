@@ -111,7 +111,8 @@ def fourstep_order(X, N, isw=None, out=None):
     X2 = X if X.dim() == 2 else X[None]
     rows, flen = X2.shape
     if out is None:
-        out = torch.empty((rows, N // 2 + 1), dtype=torch.complex64, device=X.device)
+        # rows padded to an even length: 16-byte aligned rows for the fused pass's asynchronous copies
+        out = torch.empty((rows, N // 2 + 2), dtype=torch.complex64, device=X.device)[:, :N // 2 + 1]
     _lib.call('gwb_fourstep_order', _lib.ptr(X2), X2.stride(0), rows, _lib.ptr(isw), flen, int(N), _lib.ptr(out),
               out.stride(0), _lib.stream_ptr(X.device))
     return out if X.dim() == 2 else out[0]

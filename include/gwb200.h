@@ -243,7 +243,8 @@ GWB_API int gwb_stacked_a(const float* A, long long lda, int n, int r, const dou
  * transformed in batches of wrows through it. The scale is computed from the inputs of the first min(nfirst, wrows)
  * rows by Parseval (rms over the whole series; the reference takes the rms of the outputs over the analysed span of
  * its first batch; the scale cancels between Z and A). partials: >= that many rows x N2 / 8 doubles; ticket: one
- * uint32, zero on entry. N a power of two in [2^12, 2^20]. */
+ * uint32, zero on entry. N a power of two in [2^12, 2^20]; for N1 = 1024 (N = 2^19, 2^20) Vp and ldvp must be
+ * 16-byte aligned (an even ldvp; fourstep_order pads its rows to N/2 + 2). */
 GWB_API int gwb_fft_twiddles(long long N, float* tw, void* stream);
 /* Four-step order of rows of a half spectrum: P[j][k2 (N1/2) + k1] = X[j][N2 k1 + k2] isw[k] for k1 < N1/2, k2 < N2,
  * P[j][N/2] = X[j][N/2] isw[N/2], zero where k >= flen (isw NULL: no weight). ldp >= N/2 + 1. */
