@@ -230,8 +230,8 @@ __global__ void __launch_bounds__(256, 2) basis_pass1_w(
     constexpr int WS = YS + R + H;                          // per warp: Y tile, TH, basis-filter segment
     extern __shared__ float2 sm[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float2* twL = sm;                                       // e^{2 pi i m / N1} at m + m / 16
-    float2* Yw = sm + N1 + N1 / 16 + warp * WS;             // this warp's 32 x 33 tile
+    float2* tw2 = sm;                                       // tw2[u 32 + b] = e^{2 pi i b u / N1}
+    float2* Yw = sm + N1 + warp * WS;                       // this warp's 32 x 33 tile
     float2* THw = Yw + YS;                                  // e^{2 pi i k2 32 v / N}, v < 32
     float2* Vs = THw + R;                                   // Vp[row][k2 H .. k2 H + H)
     const int k2 = blockIdx.x * NW + warp;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256, 2) basis_pass1_w(
 #pragma unroll
     for (int a = 0; a < R / 2; ++a) dk[a] = __ldg(Dp + k2 * H + R * a + lane);
     const float2 dN = Dp[N / 2];
-    for (int m = threadIdx.x; m < N1; m += NW * 32) twL[m + (m >> 4)] = tw[m * (N / N1)];
+    for (int e = threadIdx.x; e < N1; e += NW * 32) tw2[e] = tw[(e % R) * (e / R) * (N / N1)];
     THw[lane] = tw[(k2 * (R * lane)) & mask];
     const float2 tl = tw[(k2 * lane) & mask];               // e^{2 pi i k2 u / N}, u = lane
     __syncthreads();
@@ -282,8 +282,7 @@ __global__ void __launch_bounds__(256, 2) basis_pass1_w(
         dft_reg<R>(x);
         static_for<R>([&](auto U) {
             constexpr int u = decltype(U)::value;
-            const int m = lane * u;
-            Yw[lane * (R + 1) + u] = cmul(x[brev(u, ilog2(R))], twL[m + (m >> 4)]);
+            Yw[lane * (R + 1) + u] = cmul(x[brev(u, ilog2(R))], tw2[u * R + lane]);
         });
         __syncwarp();
 #pragma unroll
@@ -406,11 +405,11 @@ __device__ __forceinline__ void store_z(void* Zr, void* Zi, void* Zlr, void* Zli
         __stcs(static_cast<float*>(Zi) + t, xi);
     } else {
         const __nv_bfloat16 hr = __float2bfloat16_rn(xr), hm = __float2bfloat16_rn(xi);
-        static_cast<__nv_bfloat16*>(Zr)[t] = hr;
-        static_cast<__nv_bfloat16*>(Zi)[t] = hm;
+        __stcs(static_cast<__nv_bfloat16*>(Zr) + t, hr);
+        __stcs(static_cast<__nv_bfloat16*>(Zi) + t, hm);
         if constexpr (FORM == 2) {
-            static_cast<__nv_bfloat16*>(Zlr)[t] = __float2bfloat16_rn(xr - __bfloat162float(hr));
-            static_cast<__nv_bfloat16*>(Zli)[t] = __float2bfloat16_rn(xi - __bfloat162float(hm));
+            __stcs(static_cast<__nv_bfloat16*>(Zlr) + t, __float2bfloat16_rn(xr - __bfloat162float(hr)));
+            __stcs(static_cast<__nv_bfloat16*>(Zli) + t, __float2bfloat16_rn(xi - __bfloat162float(hm)));
         }
     }
 }
@@ -472,6 +471,84 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT) basis_pass2(
     }
 }
 
+// pass 2 over row chunks: CTA = (TB consecutive t1, RC consecutive rows). One shared buffer holds the W tile of a row
+// (TB x N2, contiguous in the blocked layout, copied with cp.async) and then, once every thread has its inputs in
+// registers, the exchange tile; the next row's copy is issued as soon as the exchange tile has been read, and runs
+// under the second DFT and the Z stores (and under the other CTA on the SM).
+template <int N2, int FORM>
+__global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
+    const float2* __restrict__ W, int rows, int N, int N1, const float2* __restrict__ tw, int a0, int Tn,
+    const float* __restrict__ scale, void* __restrict__ Z, void* __restrict__ Zlo, long long ldz, int im_off,
+    int row0) {
+    using S = Split<N2, 2>;
+    constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC, P2 = S::P2;
+    constexpr int ES = FORM == 1 ? 4 : 2;        // bytes per Z element
+    constexpr int CP = TB * N2 * 8 / 16 / NT;    // 16-byte copies per thread per tile
+    static_assert(SC >= N2, "the exchange tile covers the W tile");
+    extern __shared__ float2 sm[];
+    float2* Bt = sm;                              // W tile Bt[k2 TB + c], then the exchange tile Bt[c SC + b SB + u]
+    float2* tw2 = Bt + TB * SC;                   // tw2[u R2 + b] = e^{2 pi i b u / N2}
+    const int tid = threadIdx.x, t10 = blockIdx.x * TB;
+    const int j0 = blockIdx.y * RC, j1 = min(j0 + RC, rows);
+    auto fetch = [&](int j) {
+        const char* g = reinterpret_cast<const char*>(W + (long long)j * N + (long long)blockIdx.x * (N2 * TB));
+        char* d = reinterpret_cast<char*>(Bt);
+#pragma unroll
+        for (int i = 0; i < CP; ++i) cp_async16(d + (i * NT + tid) * 16, g + (i * NT + tid) * 16);
+        cp_async_commit();
+    };
+    fetch(j0);
+    for (int e = tid; e < N2; e += NT) tw2[e] = tw[(e % R2) * (e / R2) * (N / N2)];
+    const float inv = 1.0f / *scale;
+    const int c = tid % TB, b = tid / TB;
+    char* zb = static_cast<char*>(Z);
+    char* zl = static_cast<char*>(Zlo);
+    for (int j = j0; j < j1; ++j) {
+        cp_async_wait_all();
+        __syncthreads();
+        float2 x[R1];
+#pragma unroll
+        for (int a = 0; a < R1; ++a) x[a] = Bt[(R2 * a + b) * TB + c];
+        __syncthreads();
+        dft_reg<R1>(x);
+        static_for<R1>([&](auto U) {
+            constexpr int u = decltype(U)::value;
+            Bt[c * SC + b * SB + u] = cmul(x[brev(u, ilog2(R1))], tw2[u * R2 + b]);
+        });
+        __syncthreads();
+        float2 y[P2][R2];
+#pragma unroll
+        for (int p = 0; p < P2; ++p) {
+            const int d = tid + NT * p;
+            const int c2 = d % TB, u = d / TB;
+#pragma unroll
+            for (int bb = 0; bb < R2; ++bb) y[p][bb] = Bt[c2 * SC + bb * SB + u];
+        }
+        __syncthreads();
+        if (j + 1 < j1) fetch(j + 1);
+        const long long re_off = (long long)(row0 + j) * ldz * ES, im_off_b = (long long)(im_off + row0 + j) * ldz * ES;
+        void* Zr = zb + re_off;
+        void* Zi = zb + im_off_b;
+        void* Zlr = FORM == 2 ? (void*)(zl + re_off) : nullptr;
+        void* Zli = FORM == 2 ? (void*)(zl + im_off_b) : nullptr;
+#pragma unroll
+        for (int p = 0; p < P2; ++p) {
+            const int d = tid + NT * p;
+            const int c2 = d % TB, u = d / TB;
+            dft_reg<R2>(y[p]);
+            const int t0 = t10 + c2 + N1 * u - a0;
+            static_for<R2>([&](auto V) {
+                constexpr int vv = decltype(V)::value;
+                const int t = t0 + N1 * (R1 * vv);
+                if (t >= 0 && t < Tn) {
+                    const float2 z = y[p][brev(vv, ilog2(R2))];
+                    store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * inv, z.y * inv);
+                }
+            });
+        }
+    }
+}
+
 int log2i(long long n) {
     int l = 0;
     while ((1ll << l) < n) ++l;
@@ -480,7 +557,7 @@ int log2i(long long n) {
 
 int launch_pass1_w(const float2* Vp, long long ldvp, int rows, const float2* Dp, int N, int N2, const float2* tw,
                    float2* W, int nfirst, double* partials, unsigned* ticket, float* scale_out, cudaStream_t s) {
-    const size_t smem = (size_t)(1024 + 64 + 8 * (32 * 33 + 32 + 512)) * sizeof(float2);
+    const size_t smem = (size_t)(1024 + 8 * (32 * 33 + 32 + 512)) * sizeof(float2);
     GWB_CUDA(cudaFuncSetAttribute(basis_pass1_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     basis_pass1_w<<<dim3(N2 / 8, (rows + RC - 1) / RC), 256, smem, s>>>(Vp, ldvp, rows, Dp, N, N2, tw, W, nfirst,
                                                                          partials, ticket, scale_out);
@@ -512,9 +589,31 @@ int launch_pass2_f(const float2* W, int N, int N1, int rows, const float2* tw, i
     return GWB_OK;
 }
 
+template <int N2, int FORM>
+int launch_pass2_p(const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn, const float* scale,
+                   void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
+    using S = Split<N2, 2>;
+    const size_t smem = (size_t)(TB * S::SC + N2) * sizeof(float2);
+    auto k = basis_pass2_p<N2, FORM>;
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<dim3(N1 / TB, (rows + RC - 1) / RC), S::NT, smem, s>>>(W, rows, N, N1, tw, a0, Tn, scale, Z, Zlo, ldz,
+                                                               im_off, row0);
+    GWB_LAUNCH_CHECK("basis_pass2_p");
+    return GWB_OK;
+}
+
 template <int N2>
 int launch_pass2(int form, const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn,
                  const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
+    // row-chunk form for the long transforms; the split bf16 form (four Z planes) runs faster on the per-row kernel
+    if constexpr (N2 >= 512) {
+        switch (form) {
+            case 0: return launch_pass2_p<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            case 1: return launch_pass2_p<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            case 3: return launch_pass2_p<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            default: break;
+        }
+    }
     switch (form) {
         case 0: return launch_pass2_f<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
         case 1: return launch_pass2_f<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
