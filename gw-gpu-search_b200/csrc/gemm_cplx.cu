@@ -160,57 +160,81 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                 *abort_flag = 1;
             }
             tc_fence_after();
-            int f = 0;
-            for (int i = 0; i < ntl && ok; ++i) {
-                for (int kc = 0; kc < nkc && ok; ++kc, ++f) {
-                    const int s = f % S;
-                    if (*abort_flag || !mbar_wait_bounded(&full[s], (uint32_t)((f / S) & 1))) {
-                        record_error(args.err, GWB_ERR_TIMEOUT, 203, blockIdx.x, f);
-                        *abort_flag = 1;
-                        ok = false;
-                        break;
+            // the MMAs of one item (M block mb) on one Z chunk
+            auto issue = [&](int kc, int mb, int b, uint32_t st) {
+                const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
+                const int nsteps = min(KC, Kh - kc * KC) / 16;
+                for (int sk = 0; sk < nsteps; ++sk) {
+                    const int k = kc * KC + sk * 16;
+                    for (int pr = 0; pr < C::NPROD; ++pr) {
+                        const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
+                        const uint32_t abase = a_base + (mb * C::NH + ha) * L.a_tiles * kATile;
+                        const uint32_t are = abase + (k >> 6) * kATile + (k & 63) * 2;
+                        const uint32_t aim = abase + ((Kh + k) >> 6) * kATile + ((Kh + k) & 63) * 2;
+                        const uint32_t zre = st + ((0 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
+                        const uint32_t zim = st + ((1 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
+                        const uint64_t dAre = smem_desc(are, 16, 1024, 2), dAim = smem_desc(aim, 16, 1024, 2);
+                        const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
+                        const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                        const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
+                        umma_f16(dre, dAre, dZre, idesc, acc);
+                        umma_f16(dre, dAim, dZim, idesc_neg, 1u);
+                        umma_f16(dim, dAim, dZre, idesc, acc);
+                        umma_f16(dim, dAre, dZim, idesc, 1u);
                     }
-                    tc_fence_after();
-                    const uint32_t st = z_base + s * L.stage_bytes;
-                    for (int mb = 0; mb < MBe && ok; ++mb) {
-                        const int j = i * MBe + mb, b = j & 1;
-                        if (kc == 0) {
-                            // this item's accumulators must have been read out by the epilogue
-                            const uint32_t u = (uint32_t)(j >> 1);
-                            if (!mbar_wait_bounded(&tempty[b], (u & 1) ^ 1)) {
-                                record_error(args.err, GWB_ERR_TIMEOUT, 204, blockIdx.x, i);
-                                *abort_flag = 1;
-                                ok = false;
-                                break;
-                            }
-                            tc_fence_after();
-                        }
-                        const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
-                        const int nsteps = min(KC, Kh - kc * KC) / 16;
-                        for (int sk = 0; sk < nsteps; ++sk) {
-                            const int k = kc * KC + sk * 16;
-                            for (int pr = 0; pr < C::NPROD; ++pr) {
-                                const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
-                                const uint32_t abase = a_base + (mb * C::NH + ha) * L.a_tiles * kATile;
-                                const uint32_t are = abase + (k >> 6) * kATile + (k & 63) * 2;
-                                const uint32_t aim = abase + ((Kh + k) >> 6) * kATile + ((Kh + k) & 63) * 2;
-                                const uint32_t zre = st + ((0 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
-                                const uint32_t zim = st + ((1 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
-                                const uint64_t dAre = smem_desc(are, 16, 1024, 2), dAim = smem_desc(aim, 16, 1024, 2);
-                                const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
-                                const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
-                                const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
-                                umma_f16(dre, dAre, dZre, idesc, acc);
-                                umma_f16(dre, dAim, dZim, idesc_neg, 1u);
-                                umma_f16(dim, dAim, dZre, idesc, acc);
-                                umma_f16(dim, dAre, dZim, idesc, 1u);
-                            }
-                        }
-                    }
-                    umma_commit(&empty[s]);
                 }
-                if (ok)
-                    for (int mb = 0; mb < MBe; ++mb) umma_commit(&tfull[(i * MBe + mb) & 1]);
+            };
+            // this item's accumulators must have been read out by the epilogue
+            auto wait_tempty = [&](int i, int j) {
+                const uint32_t u = (uint32_t)(j >> 1);
+                if (!mbar_wait_bounded(&tempty[j & 1], (u & 1) ^ 1)) {
+                    record_error(args.err, GWB_ERR_TIMEOUT, 204, blockIdx.x, i);
+                    *abort_flag = 1;
+                    return false;
+                }
+                tc_fence_after();
+                return true;
+            };
+            auto wait_full = [&](int f) {
+                if (*abort_flag || !mbar_wait_bounded(&full[f % S], (uint32_t)((f / S) & 1))) {
+                    record_error(args.err, GWB_ERR_TIMEOUT, 203, blockIdx.x, f);
+                    *abort_flag = 1;
+                    return false;
+                }
+                tc_fence_after();
+                return true;
+            };
+            // Two M blocks: when the Z ring holds a whole tile, M block 0 runs through all chunks before M block 1,
+            // so block 0's MMAs overlap the epilogue of the previous tile's block 1 and block 1's the epilogue of
+            // this tile's block 0. Otherwise both blocks go chunk by chunk.
+            const bool mb_outer = MBe == 2 && S >= nkc;
+            for (int i = 0; i < ntl && ok; ++i) {
+                if (mb_outer) {
+                    for (int mb = 0; mb < MBe && ok; ++mb) {
+                        const int j = i * MBe + mb;
+                        for (int kc = 0; kc < nkc && ok; ++kc) {
+                            const int f = i * nkc + kc;
+                            if (mb == 0 && !(ok = wait_full(f))) break;
+                            if (kc == 0 && !(ok = wait_tempty(i, j))) break;
+                            issue(kc, mb, j & 1, z_base + (f % S) * L.stage_bytes);
+                            if (mb == MBe - 1) umma_commit(&empty[f % S]);
+                        }
+                        if (ok) umma_commit(&tfull[j & 1]);
+                    }
+                } else {
+                    for (int kc = 0; kc < nkc && ok; ++kc) {
+                        const int f = i * nkc + kc;
+                        if (!(ok = wait_full(f))) break;
+                        for (int mb = 0; mb < MBe && ok; ++mb) {
+                            const int j = i * MBe + mb;
+                            if (kc == 0 && !(ok = wait_tempty(i, j))) break;
+                            issue(kc, mb, j & 1, z_base + (f % S) * L.stage_bytes);
+                        }
+                        umma_commit(&empty[f % S]);
+                    }
+                    if (ok)
+                        for (int mb = 0; mb < MBe; ++mb) umma_commit(&tfull[(i * MBe + mb) & 1]);
+                }
             }
             umma_commit(done);
             mbar_wait_bounded(done, 0);
