@@ -373,8 +373,10 @@ int launch_cplx(const uint16_t* const* A, const uint16_t* const* Zp, long long l
         while (st > 0 && !fits(mb, st)) --st;
         return st;
     };
-    // two M blocks per CTA (Z read once for both) when that still leaves a 3-deep Z ring, else one
-    int MB = (M > 128 && most_stages(2) >= 3) ? 2 : 1;
+    // one M block per CTA: measured faster than two per CTA sharing each Z tile (0.285 vs 0.292 ms at n = 256, Kh =
+    // 128, Tn = 917,504; the second M group's Z reads hit L2), with the TMEM double buffer spanning tiles. The kernel
+    // also runs two M blocks per CTA (each Z tile read once for both) when MB = 2.
+    const int MB = 1;
     const int stages = most_stages(MB);
     GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE,
                   "fused_peaks_cplx: Kh=%d does not fit in shared memory for this form (at most %d)", Kh,
