@@ -212,6 +212,19 @@ def run_reference(a):
                           e2e=dict(value=val, unit='2-det weeks / hour', h2d_bytes_per_step=0, d2h_bytes_per_step=0))))
 
 
+def traffic_ratios():
+    """Measured DRAM bytes over algorithmic bytes, from the committed ncu summaries (lines 'traffic_ratio: X')."""
+    out = {}
+    for key, name in (('basis', 'basis_passes_c2_r128.md'), ('gemm', 'umma_cplx_kernel_c2_r128.md')):
+        try:
+            for ln in open(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'profiles', name)):
+                if ln.startswith('traffic_ratio:'):
+                    out[key] = float(ln.split(':')[1])
+        except OSError:
+            pass
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -322,7 +335,11 @@ def main():
         torch.cuda.synchronize()
         L = mf.profile['launches']
         g_ms = [e[1].elapsed_time(e[2]) for e, n, r, kp in L]
-        b_ms = [e[0].elapsed_time(e[1]) for e, n, r, kp in L]
+        b_ms = [e[0].elapsed_time(e[3]) for e, n, r, kp in L]
+        # algorithmic HBM bytes of one basis-series call (both passes): Vp read (tlen/2 + 1 complex per row), W
+        # written and read back (tlen complex per row), Z written (re + im over Tn, one or two 16-bit planes or fp32)
+        zb = {'bf16x3': 8, 'f16': 4, 'bf16': 4, 'f32': 8}[form]
+        b_bytes = [r * (8 * (mf.tlen // 2 + 1) + 16 * mf.tlen + zb * mf.Tn) for e, n, r, kp in L]
         useful = [8.0 * n * r * mf.Tn for e, n, r, kp in L]
         nprod = {'bf16x3': 3, 'f16': 1, 'bf16': 1, 'f32': 1}[form]
         issued = [nprod * 4.0 * n * kp * mf.Tn for e, n, r, kp in L]
@@ -333,20 +350,35 @@ def main():
                              n_candidates=res0['n_candidates'], n_kept=int(res0['keep'].sum()),
                              h2d=x.numel() * 4, d2h=res_bytes, gemm_ms=float(np.mean(g_ms)),
                              gemm_total_ms=float(np.sum(g_ms)), basis_total_ms=float(np.sum(b_ms)),
+                             basis_ms=float(np.mean(b_ms)), basis_bytes=float(np.mean(b_bytes)),
+                             z_bytes=float(np.mean([2 * kp * mf.Tn * (2 if form != 'f32' else 4) *
+                                                    (2 if form == 'bf16x3' else 1) for e, n, r, kp in L])),
                              useful=float(np.mean(useful)), issued=float(np.mean(issued)), n_gemm=len(L))
         del mf
         torch.cuda.empty_cache()
     main_form = forms[0]
     R = results[main_form]
     peaks, kind = peaks_file()
+    ratios = traffic_ratios()
+    # dominant kernel: the fused basis series (basis_pass1_w + basis_pass2_p, one call per (tile, segment)), HBM-bound
+    hbm = peaks.get('hbm_gbs', 6650.0)
+    b_ach = R['basis_bytes'] / (R['basis_ms'] / 1e3) / 1e9
+    b_tr = ratios.get('basis') and ratios['basis'] * R['basis_bytes']
+    roof = dict(kernel='basis series: basis_pass1_w + basis_pass2_p (%s)' % main_form, bound='hbm', achieved=b_ach,
+                peak=hbm, unit='GB/s', frac=b_ach / hbm, traffic=b_tr, bytes_per_call=R['basis_bytes'],
+                avg_call_ms=R['basis_ms'], calls=R['n_gemm'], share_of_step=R['basis_total_ms'] / R['ms'],
+                peak_kind='%s hbm copy' % kind,
+                traffic_source='profiles/basis_passes_c2_r128.md (dram bytes / algorithmic bytes, scaled)')
     ach = R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
     pk = peaks.get('bf16_tflops', 1590.0) if main_form != 'f32' else None
-    roof = dict(kernel='umma_cplx_kernel (%s)' % main_form if main_form != 'f32' else 'simt_absmax_kernel',
-                bound='tensor', achieved=ach, peak=pk, unit='TFLOP/s', frac=(ach / pk) if pk else None, traffic=None,
-                flops_per_launch_useful=R['useful'], flops_per_launch_issued=R['issued'],
-                issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
-                launches=R['n_gemm'], gemm_share_of_step=R['gemm_total_ms'] / R['ms'],
-                basis_share_of_step=R['basis_total_ms'] / R['ms'], peak_kind='%s burst bf16' % kind)
+    g_tr = ratios.get('gemm') and ratios['gemm'] * R['z_bytes']
+    roof_gemm = dict(kernel='umma_cplx_kernel (%s)' % main_form if main_form != 'f32' else 'simt_absmax_kernel',
+                     bound='tensor', achieved=ach, peak=pk, unit='TFLOP/s', frac=(ach / pk) if pk else None,
+                     traffic=g_tr, flops_per_launch_useful=R['useful'], flops_per_launch_issued=R['issued'],
+                     issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
+                     launches=R['n_gemm'], share_of_step=R['gemm_total_ms'] / R['ms'],
+                     peak_kind='%s burst bf16' % kind,
+                     traffic_source='profiles/umma_cplx_kernel_c2_r128.md (dram bytes / Z bytes, scaled)')
     line = dict(metric=METRIC, value=R['value'], unit='2-det weeks / GPU-hour', n_gpus=world, steps=a.steps,
                 warmup=a.warmup, ms_per_step=R['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
                 dtype={'bf16x3': 'bf16 hi+lo (fp32 accumulate)', 'f16': 'f16 (fp32 accumulate)',
@@ -360,6 +392,7 @@ def main():
                 e2e=dict(value=R['e2e'], unit='2-det weeks / GPU-hour', h2d_bytes_per_step=R['h2d'],
                          d2h_bytes_per_step=R['d2h']),
                 gpu_launches=R['launches'], clocks=R['clocks'], bank_setup_s=bank_setup, roofline=roof,
+                roofline_gemm=roof_gemm,
                 forms={k: dict(value=v['value'], ms_per_step=v['ms'], e2e=v['e2e'], n_candidates=v['n_candidates'],
                                n_kept=v['n_kept'], gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
                                basis_share=v['basis_total_ms'] / v['ms']) for k, v in results.items()},

@@ -132,7 +132,8 @@ class MatchedFilter:
         self.thr2 = float((cfg.snr_threshold * (1 - cfg.margin)) ** 2)
         self.kernel_launches = 0
         self.fft_launches = 0
-        self.profile = None      # set to {} to record CUDA events around the GEMM and the basis series
+        # set to {} to record CUDA events per (tile, segment): e0 basis series e3 stacked A e1 GEMM e2
+        self.profile = None
 
     def _gemm(self, n, K, Kh):
         s = _lib.stream_ptr()
@@ -156,7 +157,7 @@ class MatchedFilter:
         K = 2 * Kh if self.compact else sv['Kp']
         prof = self.profile
         if prof is not None:
-            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             e[0].record()
         im_off = Kh if self.compact else r
         if self.fused:
@@ -165,6 +166,8 @@ class MatchedFilter:
         else:
             scale = fp_filter.basis_series_into(self.ws, sv['Vh'], D[seg], isw, self.a0, self.Tn, self.Z,
                                                 self.Zlo, self.form, im_off=im_off)
+        if prof is not None:
+            e[3].record()
         nrm = sig[b.row0[t]:b.row0[t] + n, seg]
         fp_filter.stacked_A_into(sv['A'], nrm, scale, K, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
                                  df4=4.0 * b.df, kh=Kh)
