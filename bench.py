@@ -235,6 +235,7 @@ def main():
     ap.add_argument('--chunks', type=int, default=64, help='chunks per detector')
     ap.add_argument('--templates', type=int, default=5880)
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    ap.add_argument('--no-precision', action='store_true', help='skip the float64 precision comparison')
     ap.add_argument('--forms', default='f16,bf16,f32', help='forms timed (the first gives value)')
     ap.add_argument('--slow-steps', type=int, default=1,
                     help='timed steps (and warm-up steps) for the plain fp32 form, which is many times slower')
@@ -356,6 +357,29 @@ def main():
                              useful=float(np.mean(useful)), issued=float(np.mean(issued)), n_gemm=len(L))
         del mf
         torch.cuda.empty_cache()
+    # precision of every form against float64 on one (tile, chunk) (after the timed regions; the split bf16 form
+    # needs r <= 128, so the tile is the one with the largest such rank)
+    precision_rep = None
+    if not a.no_precision and rank == 0:
+        from gwb200 import precision
+        t_p = max((i for i, s_ in enumerate(B.svd) if s_['r'] <= 128), key=lambda i: B.svd[i]['r'])
+        seg_p = 0
+        Dd, IPd = cond(x)
+        precision_rep = dict(tile=t_p, r=B.svd[t_p]['r'], segment=seg_p,
+                             reference='float64 transform and product (gwb200.precision)')
+        ref = None
+        for form in ('f32', 'bf16x3', 'f16', 'bf16'):
+            cfg = pipeline.FilterConfig(form=form)
+            mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg, device=dev)
+            sig = mf.norms(IPd)
+            if ref is None:
+                r0, n = B.row0[t_p], len(B.tiles[t_p])
+                ref = precision.fp64_window_snr(B.svd[t_p], Dd[seg_p], isw, sig[r0:r0 + n, seg_p], DF, TLEN, A0,
+                                                mf.Tn, mf.cw)
+            v, i = precision.form_window_snr(mf, t_p, Dd, isw, sig, seg_p)
+            precision_rep[form] = precision.compare(v, i, ref[0], ref[1], cfg.snr_threshold)
+            del mf
+            torch.cuda.empty_cache()
     main_form = forms[0]
     R = results[main_form]
     peaks, kind = peaks_file()
@@ -392,7 +416,7 @@ def main():
                 e2e=dict(value=R['e2e'], unit='2-det weeks / GPU-hour', h2d_bytes_per_step=R['h2d'],
                          d2h_bytes_per_step=R['d2h']),
                 gpu_launches=R['launches'], clocks=R['clocks'], bank_setup_s=bank_setup, roofline=roof,
-                roofline_gemm=roof_gemm,
+                roofline_gemm=roof_gemm, precision=precision_rep,
                 forms={k: dict(value=v['value'], ms_per_step=v['ms'], e2e=v['e2e'], n_candidates=v['n_candidates'],
                                n_kept=v['n_kept'], gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
                                basis_share=v['basis_total_ms'] / v['ms']) for k, v in results.items()},
