@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 
 namespace gwb {
 namespace {
@@ -161,9 +162,43 @@ __global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, in
     }
 }
 
+// fp8 screening form, compact A: row i of [Re As' | Im As'] with As'_ij = A_ij norm_i rowscale_z[j] (the basis-row
+// scales of Z folded in), quantised to e4m3 with the row's own scale sa_i = max_j |As'_ij| / 448 (written to sa).
+__global__ void stacked_a8_kernel(const float2* __restrict__ A, long long lda, int n, int r,
+                                  const double* __restrict__ nrm, long long nrm_stride, double df4,
+                                  const float* __restrict__ zscale, int kh, __nv_fp8_storage_t* __restrict__ A8,
+                                  long long ldo, float* __restrict__ sa) {
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    const double v = nrm[(long long)i * nrm_stride];
+    const float f = (float)(df4 > 0.0 ? df4 / sqrt(v) : v);
+    auto value = [&](int c) {
+        const int cc = c < kh ? c : c - kh;
+        if (cc >= r) return 0.f;
+        const float2 a = A[(long long)i * lda + cc];
+        return (c < kh ? a.x : a.y) * f * zscale[cc];
+    };
+    float m = 0.f;
+    for (int c = threadIdx.x; c < 2 * kh; c += blockDim.x) m = fmaxf(m, fabsf(value(c)));
+    __shared__ float red[32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    float mx = 0.f;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) mx = fmaxf(mx, red[w]);
+    const float s = mx > 0.f ? mx / 448.f : 1.f;
+    if (threadIdx.x == 0) sa[i] = s;
+    const float inv = 1.f / s;
+    for (int c = threadIdx.x; c < 2 * kh; c += blockDim.x)
+        A8[(long long)i * ldo + c] = __nv_cvt_float_to_fp8(value(c) * inv, __NV_SATFINITE, __NV_E4M3);
+}
+
 __device__ __forceinline__ float ld_as_float(const void* p, long long i, int form) {
     if (form == 0) return __half2float(static_cast<const __half*>(p)[i]);
     if (form == 1) return static_cast<const float*>(p)[i];
+    if (form == 4)
+        return __half2float(__half(__nv_cvt_fp8_to_halfraw(static_cast<const __nv_fp8_storage_t*>(p)[i], __NV_E4M3)));
     return __bfloat162float(static_cast<const __nv_bfloat16*>(p)[i]);    // forms 2 (hi or lo) and 3
 }
 
@@ -177,7 +212,7 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
                               const void* __restrict__ Aim, const void* __restrict__ Are_lo,
                               const void* __restrict__ Aim_lo, long long lda, const void* __restrict__ Z,
                               const void* __restrict__ Zlo, long long ldz, int Kp, int kh, int form,
-                              GwbCand* __restrict__ cands,
+                              const float* __restrict__ rowscale, GwbCand* __restrict__ cands,
                               int cand_cap, GwbGroup* __restrict__ groups, int group_cap, GwbUnit* __restrict__ units,
                               int unit_cap, int32_t* __restrict__ counters) {
     const int row = blockIdx.x;
@@ -269,8 +304,9 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
             zi += __shfl_down_sync(0xffffffffu, zi, off);
         }
         if (lane == 0) {
-            cands[s_base + i].zr = zr;
-            cands[s_base + i].zi = zi;
+            const float rs = rowscale ? rowscale[row] : 1.f;     // fp8: the row scale of A
+            cands[s_base + i].zr = zr * rs;
+            cands[s_base + i].zi = zi * rs;
         }
     }
 }
@@ -347,22 +383,36 @@ int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm
     return GWB_OK;
 }
 
+int gwb_stacked_a8(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride, double df4,
+                   const float* zscale, int kh, void* A8, long long ldo, float* sa, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(A && nrm && zscale && A8 && sa, GWB_ERR_ARG, "stacked_a8: null pointer");
+    GWB_CHECK_ARG(n > 0 && r > 0 && kh >= r && kh % 32 == 0 && lda >= r && ldo >= 2 * kh, GWB_ERR_SHAPE,
+                  "stacked_a8: n=%d r=%d kh=%d (a multiple of 32, >= r) ldo=%lld", n, r, kh, ldo);
+    stacked_a8_kernel<<<n, 128, 0, (cudaStream_t)stream>>>(reinterpret_cast<const float2*>(A), lda, n, r, nrm,
+                                                            nrm_stride, df4, zscale, kh,
+                                                            static_cast<__nv_fp8_storage_t*>(A8), ldo, sa);
+    GWB_LAUNCH_CHECK("stacked_a8_kernel");
+    return GWB_OK;
+}
+
 int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2, long long a0,
                        int row0, int seg, const void* Are, const void* Aim, const void* Are_lo, const void* Aim_lo,
                        long long lda, const void* Z, const void* Zlo, long long ldz, int Kp, int kh, int form,
-                       GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units, int unit_cap,
-                       int32_t* counters, void* stream) {
+                       const float* rowscale, GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap,
+                       GwbUnit* units, int unit_cap, int32_t* counters, void* stream) {
     using namespace gwb;
     GWB_CHECK_ARG(vw && iw && Are && (kh > 0 || Aim) && Z && cands && groups && units && counters, GWB_ERR_ARG,
                   "select_windows: null pointer");
-    GWB_CHECK_ARG(form >= 0 && form <= 3 && (form != 2 || (Are_lo && (kh > 0 || Aim_lo) && Zlo)), GWB_ERR_ARG,
-                  "select_windows: form %d", form);
+    GWB_CHECK_ARG(form >= 0 && form <= 4 && (form != 2 || (Are_lo && (kh > 0 || Aim_lo) && Zlo)) &&
+                      (form != 4 || (kh > 0 && rowscale)), GWB_ERR_ARG, "select_windows: form %d", form);
     GWB_CHECK_ARG(kh == 0 || Kp == 2 * kh, GWB_ERR_SHAPE, "select_windows: Kp=%d with kh=%d", Kp, kh);
     GWB_CHECK_ARG(n > 0 && nw >= 0 && ldv >= nw && Kp > 0 && lda >= Kp, GWB_ERR_SHAPE, "select_windows: n=%d nw=%d", n,
                   nw);
     if (nw == 0) return GWB_OK;
     select_kernel<<<n, kThreads, 0, (cudaStream_t)stream>>>(vw, iw, ldv, n, nw, thr2, a0, row0, seg, Are, Aim, Are_lo,
-                                                            Aim_lo, lda, Z, Zlo, ldz, Kp, kh, form, cands, cand_cap, groups,
+                                                            Aim_lo, lda, Z, Zlo, ldz, Kp, kh, form,
+                                                            form == 4 ? rowscale : nullptr, cands, cand_cap, groups,
                                                             group_cap, units, unit_cap, counters);
     GWB_LAUNCH_CHECK("select_kernel");
     return GWB_OK;

@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <type_traits>
 #include <utility>
 
@@ -225,7 +226,7 @@ constexpr int RC = 8;   // rows per pass-1 CTA of the warp-per-column form
 __global__ void __launch_bounds__(256, 2) basis_pass1_w(
     const float2* __restrict__ Vp, long long ldvp, int rows, const float2* __restrict__ Dp, int N, int N2,
     const float2* __restrict__ tw, float2* __restrict__ W, int nfirst, double* __restrict__ partials,
-    unsigned int* __restrict__ ticket, float* __restrict__ scale_out) {
+    unsigned int* __restrict__ ticket, float* __restrict__ scale_out, float* __restrict__ rowpart) {
     constexpr int N1 = 1024, R = 32, H = N1 / 2, NW = 8, YS = R * (R + 1);
     constexpr int WS = YS + R + H;                          // per warp: Y tile, TH, basis-filter segment
     extern __shared__ float2 sm[];
@@ -279,6 +280,12 @@ __global__ void __launch_bounds__(256, 2) basis_pass1_w(
 #pragma unroll
         for (int a = R / 2 + 1; a < R; ++a) x[a] = make_float2(0.f, 0.f);
         if (j < nf) acc += (double)part;
+        if (rowpart) {                                      // per-row sums of |q|^2: rowpart[j][k2]
+            float ps = part;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, off);
+            if (lane == 0) rowpart[(long long)j * N2 + k2] = ps;
+        }
         dft_reg<R>(x);
         static_for<R>([&](auto U) {
             constexpr int u = decltype(U)::value;
@@ -326,7 +333,7 @@ template <int N1>
 __global__ void __launch_bounds__(Split<N1, 8>::NT) basis_pass1(
     const float2* __restrict__ Vp, long long ldvp, const float2* __restrict__ Dp, int N, int N2,
     const float2* __restrict__ tw, float2* __restrict__ W, int nfirst, double* __restrict__ partials,
-    unsigned int* __restrict__ ticket, float* __restrict__ scale_out) {
+    unsigned int* __restrict__ ticket, float* __restrict__ scale_out, float* __restrict__ rowpart) {
     using S = Split<N1, 8>;
     constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC, H = N1 / 2;
     extern __shared__ float2 sm[];
@@ -392,7 +399,39 @@ __global__ void __launch_bounds__(Split<N1, 8>::NT) basis_pass1(
             wc[(R1 / 8) * vv * (N2 * 8)] = cmul(y[brev(vv, ilog2(R2))], cmul(tl, TH[c2 * (R2 + 1) + vv]));
         });
     }
+    if (rowpart) {                                          // per-row sums of |q|^2: rowpart[row][blockIdx.x]
+        __shared__ float rred[NT / 32];
+        float ps = part;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, off);
+        if ((tid & 31) == 0) rred[tid >> 5] = ps;
+        __syncthreads();
+        if (tid == 0) {
+            float sum = 0.f;
+            for (int w = 0; w < NT / 32; ++w) sum += rred[w];
+            rowpart[(long long)row * gridDim.x + blockIdx.x] = sum;
+        }
+    }
     if (nfirst > 0) scale_partials<NT>(part, row, nfirst, partials, ticket, scale_out);
+}
+
+// Per-row scale of the fp8 form: rowscale[j] = (rms of one component of basis series j) / 16, from the row's |q|^2
+// sums (Parseval: mean_t |z_t|^2 = sum_k |q_k|^2), summed in a fixed order in float64. Z_j / rowscale[j] then has a
+// per-component rms of 16: far inside e4m3's range (448) for the peaks, above its subnormals for the bulk.
+__global__ void rowscale_kernel(const float* __restrict__ rowpart, int P, float* __restrict__ rowscale) {
+    __shared__ double red[256 / 32];
+    const int j = blockIdx.x, tid = threadIdx.x;
+    double s = 0.0;
+    for (int i = tid; i < P; i += 256) s += (double)rowpart[(long long)j * P + i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((tid & 31) == 0) red[tid >> 5] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += red[w];
+        rowscale[j] = t > 0.0 ? (float)(sqrt(t / 2.0) / 16.0) : 1.f;
+    }
 }
 
 template <int FORM>
@@ -403,6 +442,9 @@ __device__ __forceinline__ void store_z(void* Zr, void* Zi, void* Zlr, void* Zli
     } else if constexpr (FORM == 1) {
         __stcs(static_cast<float*>(Zr) + t, xr);
         __stcs(static_cast<float*>(Zi) + t, xi);
+    } else if constexpr (FORM == 4) {
+        static_cast<__nv_fp8_storage_t*>(Zr)[t] = __nv_cvt_float_to_fp8(xr, __NV_SATFINITE, __NV_E4M3);
+        static_cast<__nv_fp8_storage_t*>(Zi)[t] = __nv_cvt_float_to_fp8(xi, __NV_SATFINITE, __NV_E4M3);
     } else {
         const __nv_bfloat16 hr = __float2bfloat16_rn(xr), hm = __float2bfloat16_rn(xi);
         __stcs(static_cast<__nv_bfloat16*>(Zr) + t, hr);
@@ -422,7 +464,7 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT) basis_pass2(
     int row0) {
     using S = Split<N2, 2>;
     constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC;
-    constexpr int ES = FORM == 1 ? 4 : 2;        // bytes per Z element
+    constexpr int ES = FORM == 1 ? 4 : (FORM == 4 ? 1 : 2);   // bytes per Z element
     extern __shared__ float2 sm[];
     float2* Y = sm;
     float2* twL = Y + TB * SC;
@@ -442,8 +484,8 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT) basis_pass2(
         Y[c * SC + b * SB + u] = cmul(x[brev(u, ilog2(R1))], twL[b * u]);
     });
     __syncthreads();
-    // step 2: thread (c, u), c fastest so the Z stores run along t
-    const float inv = 1.0f / *scale;
+    // step 2: thread (c, u), c fastest so the Z stores run along t. fp8: scale holds one scale per row
+    const float inv = 1.0f / (FORM == 4 ? scale[row] : *scale);
     char* zb = static_cast<char*>(Z);
     char* zl = static_cast<char*>(Zlo);
     const long long re_off = (long long)(row0 + row) * ldz * ES, im_off_b = (long long)(im_off + row0 + row) * ldz * ES;
@@ -482,7 +524,7 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
     int row0) {
     using S = Split<N2, 2>;
     constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC, P2 = S::P2;
-    constexpr int ES = FORM == 1 ? 4 : 2;        // bytes per Z element
+    constexpr int ES = FORM == 1 ? 4 : (FORM == 4 ? 1 : 2);   // bytes per Z element
     constexpr int CP = TB * N2 * 8 / 16 / NT;    // 16-byte copies per thread per tile
     static_assert(SC >= N2, "the exchange tile covers the W tile");
     extern __shared__ float2 sm[];
@@ -499,11 +541,12 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
     };
     fetch(j0);
     for (int e = tid; e < N2; e += NT) tw2[e] = tw[(e % R2) * (e / R2) * (N / N2)];
-    const float inv = 1.0f / *scale;
+    const float inv0 = FORM == 4 ? 0.f : 1.0f / *scale;    // fp8: scale holds one scale per row
     const int c = tid % TB, b = tid / TB;
     char* zb = static_cast<char*>(Z);
     char* zl = static_cast<char*>(Zlo);
     for (int j = j0; j < j1; ++j) {
+        const float inv = FORM == 4 ? 1.0f / scale[j] : inv0;
         cp_async_wait_all();
         __syncthreads();
         float2 x[R1];
@@ -556,23 +599,26 @@ int log2i(long long n) {
 }
 
 int launch_pass1_w(const float2* Vp, long long ldvp, int rows, const float2* Dp, int N, int N2, const float2* tw,
-                   float2* W, int nfirst, double* partials, unsigned* ticket, float* scale_out, cudaStream_t s) {
+                   float2* W, int nfirst, double* partials, unsigned* ticket, float* scale_out, float* rowpart,
+                   cudaStream_t s) {
     const size_t smem = (size_t)(1024 + 8 * (32 * 33 + 32 + 512)) * sizeof(float2);
     GWB_CUDA(cudaFuncSetAttribute(basis_pass1_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     basis_pass1_w<<<dim3(N2 / 8, (rows + RC - 1) / RC), 256, smem, s>>>(Vp, ldvp, rows, Dp, N, N2, tw, W, nfirst,
-                                                                         partials, ticket, scale_out);
+                                                                         partials, ticket, scale_out, rowpart);
     GWB_LAUNCH_CHECK("basis_pass1_w");
     return GWB_OK;
 }
 
 template <int N1>
 int launch_pass1(const float2* Vp, long long ldvp, int rows, const float2* Dp, int N, int N2, const float2* tw,
-                 float2* W, int nfirst, double* partials, unsigned* ticket, float* scale_out, cudaStream_t s) {
+                 float2* W, int nfirst, double* partials, unsigned* ticket, float* scale_out, float* rowpart,
+                 cudaStream_t s) {
     using S = Split<N1, 8>;
     const size_t smem = (size_t)(TB * S::SC + N1 + N1 / 16 + TB * (S::R1 + 1) + TB * (S::R2 + 1)) * sizeof(float2);
     auto k = basis_pass1<N1>;
     GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<dim3(N2 / TB, rows), S::NT, smem, s>>>(Vp, ldvp, Dp, N, N2, tw, W, nfirst, partials, ticket, scale_out);
+    k<<<dim3(N2 / TB, rows), S::NT, smem, s>>>(Vp, ldvp, Dp, N, N2, tw, W, nfirst, partials, ticket, scale_out,
+                                              rowpart);
     GWB_LAUNCH_CHECK("basis_pass1");
     return GWB_OK;
 }
@@ -611,6 +657,7 @@ int launch_pass2(int form, const float2* W, int N, int N1, int rows, const float
             case 0: return launch_pass2_p<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
             case 1: return launch_pass2_p<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
             case 3: return launch_pass2_p<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            case 4: return launch_pass2_p<N2, 4>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
             default: break;
         }
     }
@@ -618,6 +665,7 @@ int launch_pass2(int form, const float2* W, int N, int N1, int rows, const float
         case 0: return launch_pass2_f<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
         case 1: return launch_pass2_f<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
         case 2: return launch_pass2_f<N2, 2>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+        case 4: return launch_pass2_f<N2, 4>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
         default: return launch_pass2_f<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
     }
 }
@@ -655,10 +703,10 @@ int gwb_fourstep_order(const float* X, long long ldx, int rows, const float* isw
 int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const float* Dp, long long N, const float* tw, float* W,
                     int wrows, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz, int im_off,
                     int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket, float* scale,
-                    void* stream) {
+                    float* rowscale, float* rowpart, long long rowpart_elems, void* stream) {
     using namespace gwb;
     GWB_CHECK_ARG(Vp && Dp && tw && W && Z && scale && (form != 2 || Zlo), GWB_ERR_ARG, "basis_fused: null pointer");
-    GWB_CHECK_ARG(form >= 0 && form <= 3, GWB_ERR_ARG, "basis_fused: form %d", form);
+    GWB_CHECK_ARG(form >= 0 && form <= 4, GWB_ERR_ARG, "basis_fused: form %d", form);
     GWB_CHECK_ARG(is_pow2(N) && N >= (1 << 12) && N <= (1 << 20), GWB_ERR_NOT_POW2,
                   "basis_fused: N=%lld must be a power of two in [2^12, 2^20]", N);
     GWB_CHECK_ARG(rows > 0 && rows < 65536 && wrows > 0 && ldvp >= N / 2 + 1 && a0 >= 0 && Tn > 0 && a0 + Tn <= N &&
@@ -672,34 +720,46 @@ int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const float* Dp, 
                   "basis_fused: scale partials need %lld entries", need);
     GWB_CHECK_ARG(N1 != 1024 || ((uintptr_t)Vp % 16 == 0 && ldvp % 2 == 0), GWB_ERR_ALIGN,
                   "basis_fused: Vp and its row stride must be 16-byte aligned");
+    // fp8: per-row partial sums of |q|^2 (P per row) and one scale per row
+    const int P = N1 == 1024 ? N2 : N2 / TB;
+    const long long pneed = (long long)std::min(rows, wrows) * P;
+    GWB_CHECK_ARG(form != 4 || (rowscale && rowpart && rowpart_elems >= pneed), GWB_ERR_SHAPE,
+                  "basis_fused: the fp8 form needs rowscale (rows floats) and rowpart (%lld floats)", pneed);
     cudaStream_t s = (cudaStream_t)stream;
     const float2* d = reinterpret_cast<const float2*>(Dp);
     const float2* t = reinterpret_cast<const float2*>(tw);
     float2* w = reinterpret_cast<float2*>(W);
     unsigned* tk = reinterpret_cast<unsigned*>(ticket);
+    float* rp = form == 4 ? rowpart : nullptr;
     const int n = (int)N, ia0 = (int)a0, iTn = (int)Tn;
     // batches of wrows rows through the same W (W can then stay in L2 between the passes); the scale comes from the
-    // first batch and every batch's pass 2 reads it
+    // first batch and every batch's pass 2 reads it (fp8: each batch's rows get their own scales between the passes)
     for (int j0 = 0; j0 < rows; j0 += wrows) {
         const int nr = std::min(wrows, rows - j0);
         const int nfb = j0 == 0 ? nf : 0;
         const float2* v = reinterpret_cast<const float2*>(Vp) + (long long)j0 * ldvp;
         int st;
         switch (N1) {
-            case 64: st = launch_pass1<64>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
-            case 128: st = launch_pass1<128>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
-            case 256: st = launch_pass1<256>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
-            case 512: st = launch_pass1<512>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
-            default: st = launch_pass1_w(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, s); break;
+            case 64: st = launch_pass1<64>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, rp, s); break;
+            case 128: st = launch_pass1<128>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, rp, s); break;
+            case 256: st = launch_pass1<256>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, rp, s); break;
+            case 512: st = launch_pass1<512>(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, rp, s); break;
+            default: st = launch_pass1_w(v, ldvp, nr, d, n, N2, t, w, nfb, partials, tk, scale, rp, s); break;
         }
         if (st) return st;
+        const float* sc = scale;
+        if (form == 4) {
+            rowscale_kernel<<<nr, 256, 0, s>>>(rowpart, P, rowscale + j0);
+            GWB_LAUNCH_CHECK("rowscale_kernel");
+            sc = rowscale + j0;
+        }
         const int r0 = row0 + j0;
         switch (N2) {
-            case 64: st = launch_pass2<64>(form, w, n, N1, nr, t, ia0, iTn, scale, Z, Zlo, ldz, im_off, r0, s); break;
-            case 128: st = launch_pass2<128>(form, w, n, N1, nr, t, ia0, iTn, scale, Z, Zlo, ldz, im_off, r0, s); break;
-            case 256: st = launch_pass2<256>(form, w, n, N1, nr, t, ia0, iTn, scale, Z, Zlo, ldz, im_off, r0, s); break;
-            case 512: st = launch_pass2<512>(form, w, n, N1, nr, t, ia0, iTn, scale, Z, Zlo, ldz, im_off, r0, s); break;
-            default: st = launch_pass2<1024>(form, w, n, N1, nr, t, ia0, iTn, scale, Z, Zlo, ldz, im_off, r0, s); break;
+            case 64: st = launch_pass2<64>(form, w, n, N1, nr, t, ia0, iTn, sc, Z, Zlo, ldz, im_off, r0, s); break;
+            case 128: st = launch_pass2<128>(form, w, n, N1, nr, t, ia0, iTn, sc, Z, Zlo, ldz, im_off, r0, s); break;
+            case 256: st = launch_pass2<256>(form, w, n, N1, nr, t, ia0, iTn, sc, Z, Zlo, ldz, im_off, r0, s); break;
+            case 512: st = launch_pass2<512>(form, w, n, N1, nr, t, ia0, iTn, sc, Z, Zlo, ldz, im_off, r0, s); break;
+            default: st = launch_pass2<1024>(form, w, n, N1, nr, t, ia0, iTn, sc, Z, Zlo, ldz, im_off, r0, s); break;
         }
         if (st) return st;
     }

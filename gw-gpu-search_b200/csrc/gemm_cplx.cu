@@ -10,7 +10,9 @@
 // bf16), while Z streams through a ring of K-chunks by TMA. Work item = (128-sample time tile, 128-row M block); the
 // re and im accumulators of an item sit in 256 TMEM columns, double buffered. Epilogue as the stacked kernel: warps
 // 2-9 read TMEM, form |z|^2 and keep max and first index per row over `group` tiles.
-// Forms: 0 fp16 (one product), 1 bf16 (one product), 2 split bf16 (hi.hi + hi.lo + lo.hi, about 16 bits).
+// Forms: 0 fp16 (one product), 1 bf16 (one product), 2 split bf16 (hi.hi + hi.lo + lo.hi, about 16 bits), 3 fp8 e4m3
+// (kind::f8f6f4, K = 32 per MMA, 128-byte rows hold 128 elements; the screening form: A rows carry a per-row scale
+// that the epilogue applies, V = rowscale^2 max |z|^2).
 #include "common.cuh"
 
 namespace gwb {
@@ -27,6 +29,7 @@ struct __align__(64) CplxArgs {
     CUtensorMap tZ[2];   // Z hi, Z lo: (2 Kh, Tn), sample-major
     float* V;
     int32_t* I;
+    const float* rowscale;   // form 3: per-row scale of A (V is multiplied by its square); else null
     long long ldv;
     long long Tn;
     int M, Kh, ntiles, group, nout, stages, MB, KC;
@@ -37,19 +40,25 @@ template <int FORM>
 struct Cfg {
     static constexpr int NH = FORM == 2 ? 2 : 1;          // hi (and lo) copies of each operand
     static constexpr int NPROD = FORM == 2 ? 3 : 1;
-    static constexpr uint32_t FMT = FORM == 0 ? 0u : 1u;   // f16 or bf16
+    static constexpr uint32_t FMT = FORM == 1 || FORM == 2 ? 1u : 0u;   // kind::f16: 0 f16, 1 bf16; kind::f8f6f4: 0 e4m3
+    static constexpr bool F8 = FORM == 3;
+    static constexpr int ES = F8 ? 1 : 2;                 // bytes per element
+    static constexpr int KSTEP = F8 ? 32 : 16;            // K per MMA
+    static constexpr int ROWEL = 128 / ES;                // elements per 128-byte swizzle row
+    static constexpr int HALVES = 128 / ROWEL;            // 128-sample tile = HALVES boxes of ROWEL samples
 };
 
 struct Layout {
     uint32_t a_tiles, a_bytes, z_off, stage_bytes, x_off, bar_off, total;
 };
 
-__host__ __device__ inline Layout layout_of(int nh, int MB, int Kh, int KC, int stages) {
+__host__ __device__ inline Layout layout_of(int nh, int MB, int Kh, int KC, int stages, int rowel = 64) {
     Layout L;
-    L.a_tiles = (uint32_t)((2 * Kh + 63) / 64);
+    L.a_tiles = (uint32_t)((2 * Kh + rowel - 1) / rowel);
     L.a_bytes = (uint32_t)MB * nh * L.a_tiles * kATile;
     L.z_off = L.a_bytes;
-    L.stage_bytes = 2u * nh * 2u * (uint32_t)KC * 128u;   // (re, im) x (hi, lo) x two 64-sample halves
+    // (re, im) x (hi, lo) x the 128-sample tile as 128-byte rows (two 64-sample halves for 16-bit, one for 8-bit)
+    L.stage_bytes = 2u * nh * (uint32_t)(128 / rowel) * (uint32_t)KC * 128u;
     L.x_off = L.z_off + (uint32_t)stages * L.stage_bytes;
     L.bar_off = L.x_off + 2048u;
     L.total = L.bar_off + (uint32_t)(2 * stages + 6) * 8u + 16u;
@@ -62,7 +71,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int Kh = args.Kh, KC = args.KC, S = args.stages, MB = args.MB;
-    const Layout L = layout_of(C::NH, MB, Kh, KC, S);
+    const Layout L = layout_of(C::NH, MB, Kh, KC, S, C::ROWEL);
     const int nkc = (Kh + KC - 1) / KC;
     uint8_t* sA = smem;
     uint8_t* sZ = smem + L.z_off;
@@ -122,8 +131,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
             for (int mb = 0; mb < MBe; ++mb)
                 for (int h = 0; h < C::NH; ++h)
                     for (int a = 0; a < (int)L.a_tiles; ++a)
-                        tma_load_2d(sA + ((mb * C::NH + h) * L.a_tiles + a) * kATile, &args.tA[h], barA, a * 64,
-                                    m0 + mb * 128);
+                        tma_load_2d(sA + ((mb * C::NH + h) * L.a_tiles + a) * kATile, &args.tA[h], barA,
+                                    a * C::ROWEL, m0 + mb * 128);
             for (int f = 0; f < nfill; ++f) {
                 const int s = f % S;
                 const uint32_t n = (uint32_t)(f / S);
@@ -139,9 +148,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                 uint8_t* st = sZ + s * L.stage_bytes;
                 for (int ri = 0; ri < 2; ++ri)
                     for (int h = 0; h < C::NH; ++h)
-                        for (int half = 0; half < 2; ++half)
-                            tma_load_2d(st + ((ri * C::NH + h) * 2 + half) * KC * 128, &args.tZ[h], &full[s],
-                                        x + 64 * half, ri * Kh + kc * KC);
+                        for (int half = 0; half < C::HALVES; ++half)
+                            tma_load_2d(st + ((ri * C::NH + h) * C::HALVES + half) * KC * 128, &args.tZ[h],
+                                        &full[s], x + C::ROWEL * half, ri * Kh + kc * KC);
             }
             mbar_wait_bounded(barA, 0);
             for (int s = 0; s < S && s < nfill; ++s) {
@@ -163,24 +172,32 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
             // the MMAs of one item (M block mb) on one Z chunk
             auto issue = [&](int kc, int mb, int b, uint32_t st) {
                 const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
-                const int nsteps = min(KC, Kh - kc * KC) / 16;
+                const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
                 for (int sk = 0; sk < nsteps; ++sk) {
-                    const int k = kc * KC + sk * 16;
+                    const int k = kc * KC + sk * C::KSTEP;
                     for (int pr = 0; pr < C::NPROD; ++pr) {
                         const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
                         const uint32_t abase = a_base + (mb * C::NH + ha) * L.a_tiles * kATile;
-                        const uint32_t are = abase + (k >> 6) * kATile + (k & 63) * 2;
-                        const uint32_t aim = abase + ((Kh + k) >> 6) * kATile + ((Kh + k) & 63) * 2;
-                        const uint32_t zre = st + ((0 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
-                        const uint32_t zim = st + ((1 * C::NH + hz) * 2) * KC * 128 + sk * 2048;
+                        const uint32_t are = abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
+                        const uint32_t aim = abase + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
+                        // K step = KSTEP rows of 128 bytes (2048 bytes for 16-bit, 4096 for 8-bit)
+                        const uint32_t zre = st + ((0 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
+                        const uint32_t zim = st + ((1 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
                         const uint64_t dAre = smem_desc(are, 16, 1024, 2), dAim = smem_desc(aim, 16, 1024, 2);
                         const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
                         const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
                         const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
-                        umma_f16(dre, dAre, dZre, idesc, acc);
-                        umma_f16(dre, dAim, dZim, idesc_neg, 1u);
-                        umma_f16(dim, dAim, dZre, idesc, acc);
-                        umma_f16(dim, dAre, dZim, idesc, 1u);
+                        if constexpr (C::F8) {
+                            umma_f8(dre, dAre, dZre, idesc, acc);
+                            umma_f8(dre, dAim, dZim, idesc_neg, 1u);
+                            umma_f8(dim, dAim, dZre, idesc, acc);
+                            umma_f8(dim, dAre, dZim, idesc, 1u);
+                        } else {
+                            umma_f16(dre, dAre, dZre, idesc, acc);
+                            umma_f16(dre, dAim, dZim, idesc_neg, 1u);
+                            umma_f16(dim, dAim, dZre, idesc, acc);
+                            umma_f16(dim, dAre, dZim, idesc, 1u);
+                        }
                     }
                 }
             };
@@ -331,7 +348,12 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                         const int row = m0 + mb * 128 + rl;
                         if (row < args.M) {
                             const long long o = t / args.group;
-                            args.V[(long long)row * args.ldv + o] = wb;
+                            float vo = wb;
+                            if (args.rowscale) {
+                                const float rs = args.rowscale[row];
+                                vo = wb * rs * rs;
+                            }
+                            args.V[(long long)row * args.ldv + o] = vo;
                             args.I[(long long)row * args.ldv + o] = wi;
                         }
                     }
@@ -347,15 +369,18 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
 }
 
 template <int FORM>
-int launch_cplx(const uint16_t* const* A, const uint16_t* const* Zp, long long lda, long long ldz, int M, int Kh,
-                long long Tn, int group, float* V, int32_t* I, long long ldv, cudaStream_t stream) {
+int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long long ldz, int M, int Kh,
+                long long Tn, int group, float* V, int32_t* I, long long ldv, const float* rowscale,
+                cudaStream_t stream) {
     using C = Cfg<FORM>;
     GWB_CHECK_ARG(M > 0 && Tn > 0 && group > 0, GWB_ERR_SHAPE, "fused_peaks_cplx: M=%d Tn=%lld group=%d", M, Tn, group);
-    GWB_CHECK_ARG(Kh > 0 && Kh % 16 == 0, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d must be a positive multiple of 16", Kh);
+    GWB_CHECK_ARG(Kh > 0 && Kh % C::KSTEP == 0, GWB_ERR_SHAPE,
+                  "fused_peaks_cplx: Kh=%d must be a positive multiple of %d", Kh, C::KSTEP);
     GWB_CHECK_ARG(lda >= 2 * Kh && ldz >= Tn, GWB_ERR_SHAPE, "fused_peaks_cplx: lda=%lld < 2 Kh or ldz=%lld < Tn", lda,
                   ldz);
-    GWB_CHECK_ARG(lda % 8 == 0 && ldz % 8 == 0, GWB_ERR_ALIGN,
-                  "fused_peaks_cplx: lda=%lld and ldz=%lld must be multiples of 8", lda, ldz);
+    GWB_CHECK_ARG((lda * C::ES) % 16 == 0 && (ldz * C::ES) % 16 == 0, GWB_ERR_ALIGN,
+                  "fused_peaks_cplx: lda=%lld and ldz=%lld must be multiples of 16 bytes", lda, ldz);
+    GWB_CHECK_ARG(!C::F8 || rowscale, GWB_ERR_ARG, "fused_peaks_cplx: the fp8 form needs the row scales of A");
     for (int h = 0; h < C::NH; ++h) {
         GWB_CHECK_ARG(A[h] && aligned(A[h], 16), GWB_ERR_ALIGN, "fused_peaks_cplx: A operand %d misaligned", h);
         GWB_CHECK_ARG(Zp[h] && aligned(Zp[h], 16), GWB_ERR_ALIGN, "fused_peaks_cplx: Z operand %d misaligned", h);
@@ -366,8 +391,8 @@ int launch_cplx(const uint16_t* const* A, const uint16_t* const* Zp, long long l
     const long long nout = cdiv(ntiles, group);
     GWB_CHECK_ARG(ldv >= nout, GWB_ERR_SHAPE, "fused_peaks_cplx: ldv=%lld < outputs per row %lld", ldv, nout);
     const uint32_t max_smem = 227 * 1024;
-    const int KC = FORM == 2 ? 32 : 64;
-    auto fits = [&](int mb, int st) { return layout_of(C::NH, mb, Kh, KC, st).total + 1024 <= max_smem; };
+    const int KC = FORM == 2 ? 32 : (C::F8 ? 128 : 64);    // K rows per Z stage (32 KB per stage in every form)
+    auto fits = [&](int mb, int st) { return layout_of(C::NH, mb, Kh, KC, st, C::ROWEL).total + 1024 <= max_smem; };
     auto most_stages = [&](int mb) {
         int st = 6;
         while (st > 0 && !fits(mb, st)) --st;
@@ -383,16 +408,18 @@ int launch_cplx(const uint16_t* const* A, const uint16_t* const* Zp, long long l
                   FORM == 2 ? 128 : 192);
     CplxArgs args;
     memset(&args, 0, sizeof(args));
-    const CUtensorMapDataType dt = FORM == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const CUtensorMapDataType dt = C::F8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                   : FORM == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     for (int h = 0; h < C::NH; ++h) {
-        int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)lda * 2, 64, 128,
-                               CU_TENSOR_MAP_SWIZZLE_128B);
+        int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)(lda * C::ES),
+                               C::ROWEL, 128, CU_TENSOR_MAP_SWIZZLE_128B);
         if (r) return r;
-        r = encode_tmap_2d(&args.tZ[h], dt, Zp[h], (uint64_t)Tn, (uint64_t)(2 * Kh), (uint64_t)ldz * 2, 64, (uint32_t)KC,
-                           CU_TENSOR_MAP_SWIZZLE_128B);
+        r = encode_tmap_2d(&args.tZ[h], dt, Zp[h], (uint64_t)Tn, (uint64_t)(2 * Kh), (uint64_t)(ldz * C::ES), C::ROWEL,
+                           (uint32_t)KC, CU_TENSOR_MAP_SWIZZLE_128B);
         if (r) return r;
     }
     args.V = V;
+    args.rowscale = C::F8 ? rowscale : nullptr;
     args.I = I;
     args.ldv = ldv;
     args.Tn = Tn;
@@ -405,7 +432,7 @@ int launch_cplx(const uint16_t* const* A, const uint16_t* const* Zp, long long l
     args.MB = MB;
     args.KC = KC;
     args.err = device_error_ptr();
-    const uint32_t smem = layout_of(C::NH, MB, Kh, KC, stages).total + 1024;
+    const uint32_t smem = layout_of(C::NH, MB, Kh, KC, stages, C::ROWEL).total + 1024;
     auto kern = umma_cplx_kernel<FORM>;
     GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int mgroups = (M + 128 * MB - 1) / (128 * MB);
@@ -418,18 +445,19 @@ int launch_cplx(const uint16_t* const* A, const uint16_t* const* Zp, long long l
 }  // namespace
 }  // namespace gwb
 
-extern "C" int gwb_fused_peaks_cplx(int form, const uint16_t* A_hi, const uint16_t* A_lo, long long lda,
-                                    const uint16_t* Z_hi, const uint16_t* Z_lo, long long ldz, int M, int Kh,
-                                    long long Tn, int group, float* V, int32_t* I, long long ldv, void* stream) {
-    const uint16_t* A[2] = {A_hi, A_lo};
-    const uint16_t* Z[2] = {Z_hi, Z_lo};
+extern "C" int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
+                                    const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,
+                                    int32_t* I, long long ldv, const float* rowscale, void* stream) {
+    const void* A[2] = {A_hi, A_lo};
+    const void* Z[2] = {Z_hi, Z_lo};
     cudaStream_t s = (cudaStream_t)stream;
     switch (form) {
-        case 0: return gwb::launch_cplx<0>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, s);
-        case 1: return gwb::launch_cplx<1>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, s);
-        case 2: return gwb::launch_cplx<2>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, s);
+        case 0: return gwb::launch_cplx<0>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
+        case 1: return gwb::launch_cplx<1>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
+        case 2: return gwb::launch_cplx<2>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
+        case 3: return gwb::launch_cplx<3>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
         default:
-            gwb::set_error("fused_peaks_cplx: form %d (0 fp16, 1 bf16, 2 split bf16)", form);
+            gwb::set_error("fused_peaks_cplx: form %d (0 fp16, 1 bf16, 2 split bf16, 3 fp8 e4m3)", form);
             return GWB_ERR_ARG;
     }
 }

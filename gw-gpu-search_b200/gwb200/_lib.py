@@ -41,16 +41,18 @@ SIGNATURES = {
     'gwb_fused_peaks_f16': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_bf16x3': [_P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_f32': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
-    'gwb_fused_peaks_cplx': [_I, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
+    'gwb_fused_peaks_cplx': [_I, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P, _P],
     'gwb_basis_premul': [_P, _LL, _I, _P, _LL, _I, _P, _LL, _P, _LL, _P],
     'gwb_basis_scale': [_P, _LL, _I, _LL, _LL, _P, _I, _P, _P, _P],
     'gwb_fft_twiddles': [_LL, _P, _P],
     'gwb_fourstep_order': [_P, _LL, _I, _P, _LL, _LL, _P, _LL, _P],
-    'gwb_basis_fused': [_P, _LL, _I, _P, _LL, _P, _P, _I, _LL, _LL, _I, _P, _P, _LL, _I, _I, _I, _P, _LL, _P, _P, _P],
+    'gwb_basis_fused': [_P, _LL, _I, _P, _LL, _P, _P, _I, _LL, _LL, _I, _P, _P, _LL, _I, _I, _I, _P, _LL, _P, _P, _P,
+                        _P, _LL, _P],
     'gwb_basis_pack': [_P, _LL, _I, _I, _I, _LL, _LL, _P, _I, _P, _P, _LL, _P],
     'gwb_stacked_a': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _I, _I, _P, _P, _P, _P, _LL, _P],
+    'gwb_stacked_a8': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _P, _LL, _P, _P],
     'gwb_select_windows': [_P, _P, _LL, _I, _I, _F, _LL, _I, _I, _P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _I, _P,
-                           _I, _P, _I, _P, _I, _P, _P],
+                           _P, _I, _P, _I, _P, _I, _P, _P],
     'gwb_edges': [_P, _P, _I, _P, _LL, _P, _LL, _P, _P, _I, _I, _I, _P, _P],
     'gwb_bin_sums': [_P, _P, _I, _P, _P, _P, _I, _P, _P, _LL, _P, _LL, _I, _I, _LL, _P, _P],
     'gwb_exact_finalize': [_P, _P, _I, _P, _P, _I, _P, _I, _I, _P, _P, _LL, _D, _P, _P],

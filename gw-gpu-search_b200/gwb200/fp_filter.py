@@ -15,7 +15,9 @@ from . import _lib
 
 CH = 1 << 16       # fp_filter.py:42 (kept for reference; the kernels do not chunk)
 RB = 64            # basis rows per inverse-FFT batch (fp_filter.py:43)
-FORMS = {'f16': 0, 'f32': 1, 'bf16x3': 2, 'bf16': 3}     # operand encodings of the pack / stacked-A kernels
+# operand encodings of the pack / stacked-A / selection kernels; fp8 (e4m3 with per-row scales, the screening form)
+# exists in the fused basis series and the compact GEMM only
+FORMS = {'f16': 0, 'f32': 1, 'bf16x3': 2, 'bf16': 3, 'fp8': 4}
 
 
 def _s():
@@ -131,20 +133,25 @@ class FusedBasisWorkspace:
         self.partials = torch.empty(RB * max(1, tlen // 64), dtype=torch.float64, device=device)
         self.ticket = torch.zeros(1, dtype=torch.int32, device=device)
         self.scale = torch.empty(1, dtype=torch.float32, device=device)
+        # fp8 form: one scale per basis row, and the per-row |q|^2 partial sums behind it (at most N2 per row)
+        self.rowscale = torch.empty(rows, dtype=torch.float32, device=device)
+        n2 = tlen >> ((tlen.bit_length() - 1 + 1) // 2)
+        self.rowpart = torch.empty(self.wrows * n2, dtype=torch.float32, device=device)
 
 
 def basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo=None, form='f16', im_off=None):
     """Same Z as basis_series_into in two fused passes (gwb_basis_fused), from the basis filters Vp (r, tlen/2 + 1) and
     one segment's D isw Dp (tlen/2 + 1,), both in four-step order (fourstep_order). The scale is the whole-series rms
     of the first min(RB, wrows) rows by Parseval instead of the analysed-span rms (it cancels between Z and A).
-    Returns the device scale."""
+    Returns the device scale; for form 'fp8' Z row j holds z_j / ws.rowscale[j] in e4m3 instead."""
     r = Vp.shape[0]
     assert r <= ws.rows and Vp.shape[1] >= ws.tlen // 2 + 1 and Dp.numel() >= ws.tlen // 2 + 1
     im_off = r if im_off is None else im_off
     _lib.call('gwb_basis_fused', _lib.ptr(Vp), Vp.stride(0), r, _lib.ptr(Dp), ws.tlen, _lib.ptr(ws.tw),
               _lib.ptr(ws.W), ws.wrows, int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0),
               int(im_off), 0, min(RB, r), _lib.ptr(ws.partials), ws.partials.numel(), _lib.ptr(ws.ticket),
-              _lib.ptr(ws.scale), _lib.stream_ptr())
+              _lib.ptr(ws.scale), _lib.ptr(ws.rowscale), _lib.ptr(ws.rowpart), ws.rowpart.numel(),
+              _lib.stream_ptr())
     return ws.scale
 
 
@@ -162,9 +169,10 @@ class BasisWorkspace:
         self.ones = torch.ones(flen, dtype=torch.float32, device=device)
 
 
-def kh_of(r):
-    """Half width of the compact operands: r rounded up to the MMA's K step of 16."""
-    return ((r + 15) // 16) * 16
+def kh_of(r, form='f16'):
+    """Half width of the compact operands: r rounded up to the MMA's K step (16; 32 for fp8)."""
+    k = 32 if form == 'fp8' else 16
+    return ((r + k - 1) // k) * k
 
 
 def basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16', im_off=None):
@@ -191,7 +199,8 @@ def basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16', im_off=No
 
 
 def _z_dtype(form):
-    return {'f16': torch.float16, 'f32': torch.float32, 'bf16x3': torch.bfloat16, 'bf16': torch.bfloat16}[form]
+    return {'f16': torch.float16, 'f32': torch.float32, 'bf16x3': torch.bfloat16, 'bf16': torch.bfloat16,
+            'fp8': torch.uint8}[form]
 
 
 def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='f16', df4=0.0, kh=0):
@@ -202,6 +211,14 @@ def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='
     _lib.call('gwb_stacked_a', _lib.ptr(A), A.stride(0), n, r, _lib.ptr(nrm), nrm.stride(0), float(df4),
               _lib.ptr(scale), Kp, int(kh),
               FORMS[form], _lib.ptr(Are), _lib.ptr(Aim), _lib.ptr(Are_lo), _lib.ptr(Aim_lo), Are.stride(0), _s())
+
+
+def stacked_A8_into(A, nrm, zscale, kh, A8, sa, df4):
+    """fp8 screening form of the compact A: A8 row i = e4m3([Re As' | Im As'] / sa[i]) with As'_ij = A_ij norm_i
+    zscale[j] (gwb_stacked_a8); sa (n,) float32 receives the row scales."""
+    n, r = A.shape
+    _lib.call('gwb_stacked_a8', _lib.ptr(A), A.stride(0), n, r, _lib.ptr(nrm), nrm.stride(0), float(df4),
+              _lib.ptr(zscale), int(kh), _lib.ptr(A8), A8.stride(0), _lib.ptr(sa), _s())
 
 
 def make_closures(kmin, flen, tlen, sw, eps_b, dev='cuda', form='f16'):

@@ -30,12 +30,17 @@ def _time(fn, reps):
 
 def gemm(a):
     n, r, Tn = a.n, a.r, a.tn
-    Kh = fp_filter.kh_of(r)
-    code = {'f16': 0, 'bf16': 1, 'bf16x3': 2}[a.form]
-    dt = torch.float16 if a.form == 'f16' else torch.bfloat16
+    code = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}[a.form]
+    Kh = fp_filter.kh_of(r, a.form)
     g = torch.Generator(device='cuda').manual_seed(0)
-    A = torch.randn((n, 2 * Kh), generator=g, device='cuda').to(dt)
-    Z = torch.randn((2 * Kh, Tn), generator=g, device='cuda').to(dt)
+    A = torch.randn((n, 2 * Kh), generator=g, device='cuda')
+    Z = torch.randn((2 * Kh, Tn), generator=g, device='cuda')
+    if code == 3:
+        A, Z = A.to(torch.float8_e4m3fn).view(torch.uint8), Z.to(torch.float8_e4m3fn).view(torch.uint8)
+    else:
+        dt = torch.float16 if a.form == 'f16' else torch.bfloat16
+        A, Z = A.to(dt), Z.to(dt)
+    rs = torch.ones(n, device='cuda')
     lo = (A.clone(), Z.clone()) if code == 2 else (None, None)
     nw = Tn // 2048
     V = torch.empty((n, nw), dtype=torch.float32, device='cuda')
@@ -43,11 +48,11 @@ def gemm(a):
 
     def f():
         _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(A), _lib.ptr(lo[0]), A.stride(0), _lib.ptr(Z), _lib.ptr(lo[1]),
-                  Z.stride(0), n, Kh, Tn, 16, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.stream_ptr())
+                  Z.stride(0), n, Kh, Tn, 16, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rs), _lib.stream_ptr())
     ms = _time(f, a.reps)
     useful = 8.0 * n * r * Tn
     issued = (3 if code == 2 else 1) * 4.0 * n * 2 * Kh * Tn
-    zbytes = 2 * Kh * Tn * 2 * (2 if code == 2 else 1)
+    zbytes = 2 * Kh * Tn * (1 if code == 3 else 2) * (2 if code == 2 else 1)
     return dict(kernel='umma_cplx_kernel', form=a.form, n=n, r=r, Kh=Kh, Tn=Tn, ms=ms, useful_tflops=useful / ms / 1e9,
                 issued_tflops=issued / ms / 1e9, z_gbs=zbytes / ms / 1e6)
 

@@ -36,6 +36,7 @@ class FilterConfig:
     cluster_window: float = 1.0
     snr_threshold: float = 5.5
     margin: float = 0.04
+    screen_margin: float = 0.15   # fp8 form: candidates down to thr (1 - screen_margin); the exact stage decides
     form: str = 'bf16x3'
     cand_cap: int = 1 << 20
     seg_batch: int = 16
@@ -87,9 +88,11 @@ class MatchedFilter:
         self.nw = Tn // cw
         self.Tn = self.nw * cw
         self.form = cfg.form
-        # fp16 / bf16 / split bf16 use the compact complex operands on the tensor cores (A = [ReA | ImA], Z = [ReZ ;
-        # ImZ], halves of Kh rows); the plain fp32 form uses the reference's stacked layout on the fp32 pipe
+        # fp16 / bf16 / split bf16 / fp8 use the compact complex operands on the tensor cores (A = [ReA | ImA], Z =
+        # [ReZ ; ImZ], halves of Kh rows); the plain fp32 form uses the reference's stacked layout on the fp32 pipe.
+        # fp8 (e4m3, per-row scales) is a screening form: its candidates go to the exact stage with a wider margin
         self.compact = self.form != 'f32'
+        self.fp8 = self.form == 'fp8'
         rmax = max(s['r'] for s in bank.svd)
         # the fused two-pass basis series (premul and pack folded into the transform passes) where the length allows,
         # else premul + cuFFT + pack
@@ -101,20 +104,23 @@ class MatchedFilter:
             self.Dp = None
         else:
             self.ws = fp_filter.BasisWorkspace(tlen, bank.flen, fp_filter.RB, device)
+        assert self.fused or not self.fp8, 'the fp8 form needs the fused basis series (tlen in [2^12, 2^20])'
+        self.khs = [fp_filter.kh_of(s['r'], self.form) if self.compact else 0 for s in bank.svd]
         if self.compact:
-            K = 2 * max(s['Kh'] for s in bank.svd)
+            K = 2 * max(self.khs)
         else:
             K = max(s['Kp'] for s in bank.svd)
         nmax = max(len(t) for t in bank.tiles)
         dt = fp_filter._z_dtype(self.form)
-        ldz = -(-self.Tn // 8) * 8
+        ldz = -(-self.Tn // 16) * 16          # rows on 16-byte boundaries (TMA) for every element size
         self.Z = torch.zeros((K, ldz), dtype=dt, device=device)
         self.Zlo = torch.zeros_like(self.Z) if self.form == 'bf16x3' else None
-        lda = -(-K // 8) * 8
+        lda = -(-K // 16) * 16
         self.Are = torch.zeros((nmax, lda), dtype=dt, device=device)
         self.Aim = None if self.compact else torch.zeros_like(self.Are)
         self.Are_lo = torch.zeros_like(self.Are) if self.form == 'bf16x3' else None
         self.Aim_lo = None
+        self.sa = torch.empty(nmax, dtype=torch.float32, device=device) if self.fp8 else None   # A row scales
         self.V = torch.empty((nmax, self.nw), dtype=torch.float32, device=device)
         self.I = torch.empty((nmax, self.nw), dtype=torch.int32, device=device)
         cap = cfg.cand_cap
@@ -129,7 +135,8 @@ class MatchedFilter:
         assert cap <= 1 << 22
         self.slots = None
         self.peaks = torch.empty(cap * _exact.PEAK.itemsize, dtype=torch.uint8, device=device)
-        self.thr2 = float((cfg.snr_threshold * (1 - cfg.margin)) ** 2)
+        margin = max(cfg.margin, cfg.screen_margin) if self.fp8 else cfg.margin
+        self.thr2 = float((cfg.snr_threshold * (1 - margin)) ** 2)
         self.kernel_launches = 0
         self.fft_launches = 0
         # set to {} to record CUDA events per (tile, segment): e0 basis series e3 stacked A e1 GEMM e2
@@ -138,10 +145,10 @@ class MatchedFilter:
     def _gemm(self, n, K, Kh):
         s = _lib.stream_ptr()
         if self.compact:
-            code = {'f16': 0, 'bf16': 1, 'bf16x3': 2}[self.form]
+            code = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}[self.form]
             _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(self.Are), _lib.ptr(self.Are_lo), self.Are.stride(0),
                       _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), n, Kh, self.Tn, self.group,
-                      _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), s)
+                      _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), _lib.ptr(self.sa), s)
         else:
             _lib.call('gwb_fused_peaks_f32', _lib.ptr(self.Are), _lib.ptr(self.Aim), self.Are.stride(0),
                       _lib.ptr(self.Z), self.Z.stride(0), n, K, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I),
@@ -153,7 +160,7 @@ class MatchedFilter:
         sv = b.svd[t]
         n = len(b.tiles[t])
         r = sv['r']
-        Kh = sv['Kh'] if self.compact else 0
+        Kh = self.khs[t]
         K = 2 * Kh if self.compact else sv['Kp']
         prof = self.profile
         if prof is not None:
@@ -169,8 +176,11 @@ class MatchedFilter:
         if prof is not None:
             e[3].record()
         nrm = sig[b.row0[t]:b.row0[t] + n, seg]
-        fp_filter.stacked_A_into(sv['A'], nrm, scale, K, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
-                                 df4=4.0 * b.df, kh=Kh)
+        if self.fp8:
+            fp_filter.stacked_A8_into(sv['A'], nrm, self.fws.rowscale, Kh, self.Are, self.sa, df4=4.0 * b.df)
+        else:
+            fp_filter.stacked_A_into(sv['A'], nrm, scale, K, self.Are, self.Aim, self.Are_lo, self.Aim_lo, self.form,
+                                     df4=4.0 * b.df, kh=Kh)
         if prof is not None:
             e[1].record()
         self._gemm(n, K, Kh)
@@ -182,7 +192,7 @@ class MatchedFilter:
         _lib.call('gwb_select_windows', _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), n, self.nw, self.thr2,
                   self.a0, b.row0[t], seg, _lib.ptr(self.Are), _lib.ptr(self.Aim), _lib.ptr(self.Are_lo),
                   _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), K,
-                  Kh, f, _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
+                  Kh, f, _lib.ptr(self.sa), _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
                   _lib.ptr(self.counters), _lib.stream_ptr())
         if self.fused:
             nb = -(-r // self.fws.wrows)

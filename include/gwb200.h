@@ -113,10 +113,13 @@ GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long ld
  * wide (Kh a multiple of 16, halves zero-padded past r). z_re = ReA.ReZ - ImA.ImZ and z_im = ImA.ReZ + ReA.ImZ are
  * issued as four products per K step (the minus by the MMA's A negation), so A takes half the space of the
  * reference's stacked Are/Aim (pipeline/fp_filter.py:615-621) and stays in shared memory. form 0: fp16 A_hi, Z_hi;
- * 1: bf16; 2: split bf16 with A_lo, Z_lo (hi.hi + hi.lo + lo.hi). Kh <= 192 (forms 0, 1) or 128 (form 2). */
-GWB_API int gwb_fused_peaks_cplx(int form, const uint16_t* A_hi, const uint16_t* A_lo, long long lda,
-                                 const uint16_t* Z_hi, const uint16_t* Z_lo, long long ldz, int M, int Kh, long long Tn,
-                                 int group, float* V, int32_t* I, long long ldv, void* stream);
+ * 1: bf16; 2: split bf16 with A_lo, Z_lo (hi.hi + hi.lo + lo.hi); 3: fp8 e4m3 (the screening form, no reference
+ * counterpart; Kh a multiple of 32), V = rowscale[i]^2 max |z|^2 with rowscale the per-row scale of A
+ * (gwb_stacked_a8); rowscale is ignored by the other forms (may be NULL). Kh <= 192 (forms 0, 1, 3) or 128 (form 2).
+ * lda, ldz in elements, multiples of 16 bytes. */
+GWB_API int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
+                                 const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,
+                                 int32_t* I, long long ldv, const float* rowscale, void* stream);
 
 /* ---- handle and transforms (cuFFT) ----------------------------------------------------------------------------- */
 /* The handle caches cuFFT plans per (kind, n, batch, strides); plans are made on first use of a shape. Transforms are
@@ -233,6 +236,12 @@ GWB_API int gwb_basis_pack(const float* zb, long long ldzb, int rows, int im_off
 GWB_API int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
                           double df4, const float* scale, int Kp, int kh, int form, void* Are, void* Aim,
                           void* Are_lo, void* Aim_lo, long long ldo, void* stream);
+/* fp8 screening form of stacked A (no reference counterpart): compact row i = [Re As' | Im As'] with As'_ij = A_ij
+ * norm_i zscale[j] (norm as gwb_stacked_a from nrm and df4; zscale the basis-row scales of Z from gwb_basis_fused
+ * form 4), in e4m3 divided by the row's scale sa[i] = max_j |As'_ij| / 448 (out, n floats; the GEMM's and the
+ * selection's rowscale). kh a multiple of 32, >= r; columns r..kh-1 of each half are zero. */
+GWB_API int gwb_stacked_a8(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
+                           double df4, const float* zscale, int kh, void* A8, long long ldo, float* sa, void* stream);
 
 /* Fused basis series in two passes over HBM (replaces premul + C2C inverse transform + pack, fp_filter.py:597-613).
  * N = N1 N2 (N1 = 2^ceil(log2(N) / 2)), k = N2 k1 + k2; only k <= N/2 enters (the reference zero-pads the half
@@ -250,10 +259,14 @@ GWB_API int gwb_fft_twiddles(long long N, float* tw, void* stream);
  * P[j][N/2] = X[j][N/2] isw[N/2], zero where k >= flen (isw NULL: no weight). ldp >= N/2 + 1. */
 GWB_API int gwb_fourstep_order(const float* X, long long ldx, int rows, const float* isw, long long flen, long long N,
                                float* P, long long ldp, void* stream);
+/* form 4 (fp8 e4m3, the screening form; no reference counterpart): each basis row j gets its own scale,
+ * rowscale[j] = (rms of one component of its series) / 16 from the row's |q|^2 sums (Parseval), and Z rows hold
+ * z_j / rowscale[j] in e4m3 (saturating). rowscale: rows floats (out); rowpart: workspace of min(rows, wrows) x P
+ * floats, P = N2 for N1 = 1024 else N2 / 8. Other forms ignore both (may be NULL). */
 GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const float* Dp, long long N, const float* tw,
                             float* W, int wrows, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz,
                             int im_off, int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket,
-                            float* scale, void* stream);
+                            float* scale, float* rowscale, float* rowpart, long long rowpart_elems, void* stream);
 
 /* ---- candidate selection and the exact stage ---------------------------------------------------------------- */
 /* Window candidates of one (tile, segment) (fp_filter.py:745-764): rows i < n whose windowed maximum vw (the fused
@@ -261,12 +274,13 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
  * rebuilt z), appended per row in window order; each row with candidates becomes one GwbUnit and groups of <= 8
  * candidates become GwbGroup records. counters[0..3]: candidates, groups, units, overflow flag (1 when a capacity was
  * exceeded; the row is then dropped). Operands in the layout the GEMM used: stacked Are/Aim (kh = 0, K = Kp) or
- * compact A = [ReA | ImA] with Z = [ReZ ; ImZ] (kh > 0, Kp = 2 kh); form as gwb_basis_pack. */
+ * compact A = [ReA | ImA] with Z = [ReZ ; ImZ] (kh > 0, Kp = 2 kh); form as gwb_basis_pack, plus 4 = fp8 e4m3
+ * (compact only), whose rebuilt z is multiplied by rowscale[i] (gwb_stacked_a8's sa; NULL for the other forms). */
 GWB_API int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2,
                                long long a0, int row0, int seg, const void* Are, const void* Aim, const void* Are_lo,
                                const void* Aim_lo, long long lda, const void* Z, const void* Zlo, long long ldz, int Kp,
-                               int kh, int form, GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap,
-                               GwbUnit* units, int unit_cap, int32_t* counters, void* stream);
+                               int kh, int form, const float* rowscale, GwbCand* cands, int cand_cap, GwbGroup* groups,
+                               int group_cap, GwbUnit* units, int unit_cap, int32_t* counters, void* stream);
 /* Chi-squared bin edges per unit (multi_filter.edges_per_template, pipeline/multi_filter.py:264-282; the fused
  * kernel of chisq_edges.py:92-143): E[u, 0..B] int32, B >= max nbins. Unit count = min(*ucount, umax) when ucount is
  * not NULL, else umax. nbins and kmax are indexed by the unit's row. offset_mode 1 reproduces the reference's

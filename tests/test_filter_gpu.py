@@ -139,3 +139,38 @@ def test_fused_basis_series_matches_float64_transform(tlen, wrows):
     nf = min(64, ws.wrows)
     q = np.conj(Vh[:nf].astype(np.complex128)) * Dw
     assert abs(scale - np.sqrt((np.abs(q) ** 2).sum() / nf / 2)) < 1e-5 * scale
+
+
+@pytest.mark.parametrize('tlen,wrows', [(1 << 13, None), (1 << 16, 32), (1 << 20, 8)])
+def test_fused_basis_series_fp8_rows(tlen, wrows):
+    """fp8 form: rowscale[j] = sqrt(sum_k |q_jk|^2 / 2) / 16 (Parseval), and Z row j holds z_j / rowscale[j] rounded to
+    e4m3 (3 mantissa bits: within 2^-4 relative, or half the smallest subnormal step for the smallest values), plus
+    the float32 transform's own error (which can move a value across a rounding midpoint)."""
+    from gwb200 import fp_filter
+    rng = np.random.default_rng(tlen % 997)
+    flen = tlen // 2 + 1
+    r = 40
+    Vh = (rng.standard_normal((r, flen)) + 1j * rng.standard_normal((r, flen))).astype(np.complex64)
+    Vh *= np.linspace(0.2, 3.0, r, dtype=np.float32)[:, None]      # rows of different power
+    D = (rng.standard_normal(flen) + 1j * rng.standard_normal(flen)).astype(np.complex64)
+    isw = rng.uniform(0.5, 2, flen).astype(np.float32)
+    Dw = D * isw
+    a0, Tn = tlen // 16, tlen - tlen // 8
+    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wrows)
+    Kh = fp_filter.kh_of(r, 'fp8')
+    Z = torch.zeros((2 * Kh, -(-Tn // 16) * 16), dtype=torch.uint8, device='cuda')
+    Vp = fp_filter.fourstep_order(torch.from_numpy(Vh).cuda(), tlen)
+    Dp = fp_filter.fourstep_order(torch.from_numpy(D).cuda(), tlen, torch.from_numpy(isw).cuda())
+    fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, None, 'fp8', im_off=Kh)
+    rs = ws.rowscale[:r].double().cpu().numpy()
+    q = np.conj(Vh.astype(np.complex128)) * Dw
+    rs_ref = np.sqrt((np.abs(q) ** 2).sum(1) / 2) / 16
+    np.testing.assert_allclose(rs, rs_ref, rtol=1e-5)
+    dec = Z.view(torch.float8_e4m3fn).float().double().cpu().numpy()
+    got = (dec[:r, :Tn] + 1j * dec[Kh:Kh + r, :Tn])
+    ref = of.basis_series_complex(Vh, Dw, a0, Tn, tlen) / rs[:, None]
+    for part_got, part_ref in ((got.real, ref.real), (got.imag, ref.imag)):
+        err = np.abs(part_got - part_ref)
+        bound = np.maximum(2.0 ** -4 * np.abs(part_ref), 2.0 ** -10) + 1e-5 * np.abs(ref).max()
+        assert (err <= bound).all(), (err - bound).max()
+    assert np.abs(ref).max() < 448                                   # no saturation at this scale

@@ -178,7 +178,7 @@ def test_cplx_f16_against_oracle(M, r, Tn, group):
     V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
     I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
     _lib.call('gwb_fused_peaks_cplx', 0, _lib.ptr(Ad), None, Ad.stride(0), _lib.ptr(Zd), None, Zd.stride(0), M, Kh, Tn,
-              group, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.stream_ptr())
+              group, _lib.ptr(V), _lib.ptr(I), V.stride(0), None, _lib.stream_ptr())
     Vr, Ir = og.gemm_absmax(Are, Aim, Z, M, Tn)
     tie = _near_tie_mask(Are, Aim, Z, M, Tn, Ir)
     if group > 1:
@@ -206,7 +206,7 @@ def test_cplx_bf16_forms_against_oracle(form, r):
     I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
     _lib.call('gwb_fused_peaks_cplx', form, _lib.ptr(Ah), _lib.ptr(Al if form == 2 else None), Ah.stride(0),
               _lib.ptr(Zh), _lib.ptr(Zl if form == 2 else None), Zh.stride(0), M, Kh, Tn, group, _lib.ptr(V),
-              _lib.ptr(I), V.stride(0), _lib.stream_ptr())
+              _lib.ptr(I), V.stride(0), None, _lib.stream_ptr())
     Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
     Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
     Vr, Ir = og.group_reduce(*og.gemm_absmax(Are, Aim, Z, M, Tn), group)
@@ -224,4 +224,34 @@ def test_cplx_rejects_oversized_kh():
         V = torch.empty((256, 2), dtype=torch.float32, device='cuda')
         I = torch.empty((256, 2), dtype=torch.int32, device='cuda')
         _lib.call('gwb_fused_peaks_cplx', 2, _lib.ptr(x), _lib.ptr(x), 512, _lib.ptr(z), _lib.ptr(z), 4096, 256, 256,
-                  4096, 16, _lib.ptr(V), _lib.ptr(I), 2, _lib.stream_ptr())
+                  4096, 16, _lib.ptr(V), _lib.ptr(I), 2, None, _lib.stream_ptr())
+
+
+@pytest.mark.parametrize('r', [96, 150])
+def test_cplx_fp8_integer_operands_exact(r):
+    """fp8 e4m3 form: integer operands in [-4, 4] are exact in e4m3 and every sum is exact in fp32, so V (times the
+    per-row scale squared) and the first-index argmax equal the float64 reference exactly."""
+    from gwb200 import _lib
+    rng = np.random.default_rng(r)
+    M, Tn, group = 256, 2048 * 8, 16
+    Kh = -(-r // 32) * 32
+    A = np.zeros((M, 2 * Kh), np.float32)
+    A[:, :r] = rng.integers(-4, 5, (M, r))
+    A[:, Kh:Kh + r] = rng.integers(-4, 5, (M, r))
+    Z = np.zeros((2 * Kh, Tn), np.float32)
+    Z[:r] = rng.integers(-4, 5, (r, Tn))
+    Z[Kh:Kh + r] = rng.integers(-4, 5, (r, Tn))
+    rs = (1 + np.arange(M) % 3).astype(np.float32)
+    A8 = torch.from_numpy(A).to(torch.float8_e4m3fn).view(torch.uint8).cuda()
+    Z8 = torch.from_numpy(Z).to(torch.float8_e4m3fn).view(torch.uint8).cuda()
+    rsd = torch.from_numpy(rs).cuda()
+    nout = -(-(Tn // 128) // group)
+    V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
+    I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
+    _lib.call('gwb_fused_peaks_cplx', 3, _lib.ptr(A8), None, A8.stride(0), _lib.ptr(Z8), None, Z8.stride(0), M, Kh, Tn,
+              group, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rsd), _lib.stream_ptr())
+    Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
+    Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
+    Vr, Ir = og.group_reduce(*og.gemm_absmax(Are, Aim, Z, M, Tn), group)
+    assert np.array_equal(V.cpu().numpy(), (Vr * rs[:, None] ** 2).astype(np.float32))
+    assert np.array_equal(I.cpu().numpy(), Ir)

@@ -101,3 +101,33 @@ def test_pipeline_matches_oracle(form):
     assert cands['row'][best] == inj_row and kept[best]
     assert abs(cands['sample'][best] - round(inj['t0'] * SR)) <= 2
     assert abs(peaks['snr'][best] - inj['snr']) < 3.0
+
+
+def test_fp8_screen_keeps_the_fp32_peaks():
+    """The fp8 screening form (e4m3 operands, per-row scales, wider candidate margin) followed by the exact stage keeps
+    the same windows as the plain fp32 form, away from the threshold, with the exact SNR of the screened sample within
+    2% of fp32's (the two forms may pick neighbouring samples of a window's peak)."""
+    from gwb200 import fp_filter, pipeline
+    bank, D, IP, kmin, inj = _case()
+    Dd, IPd = torch.from_numpy(D).cuda(), torch.from_numpy(IP).cuda()
+    sw, isw = fp_filter.derive_sw(IPd)
+    out = {}
+    for form in ('f32', 'fp8'):
+        cfg = pipeline.FilterConfig(tile=24, eps=1e-3, nbins=16, snr_threshold=5.0, margin=0.04, form=form,
+                                    cand_cap=1 << 16)
+        B = pipeline.Bank(bank, FLEN, DF, sw, cfg)
+        mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg)
+        mf.step(Dd, IPd, isw)
+        torch.cuda.synchronize()
+        res = mf.results()
+        c, p = res['cands'], res['peaks']
+        out[form] = {(int(a['row']), int(a['seg']), int(a['window'])): float(b['snr']) for a, b in zip(c, p)}
+    thr = 5.0
+    for a, b in (('f32', 'fp8'), ('fp8', 'f32')):
+        for k, v in out[a].items():
+            if v > 1.03 * thr:
+                assert k in out[b] and out[b][k] > thr, (a, b, k, v)
+                assert abs(out[b][k] - v) <= 2e-2 * v, (k, v, out[b][k])
+    inj_row = int(np.flatnonzero(B.order == inj['index'])[0])
+    best = max((v, k) for k, v in out['fp8'].items() if k[0] == inj_row and k[1] == inj['seg'])
+    assert abs(best[0] - inj['snr']) < 3.0
