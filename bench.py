@@ -212,6 +212,23 @@ def run_reference(a):
                           e2e=dict(value=val, unit='2-det weeks / hour', h2d_bytes_per_step=0, d2h_bytes_per_step=0))))
 
 
+def top_peak_sets(kept, thr):
+    """Each form's kept peaks (exact stage) against the plain fp32 form's: windows kept by both, by one only, and by
+    one only with an exact SNR more than 3% above the threshold (a real disagreement, not a threshold straddle)."""
+    if 'f32' not in kept:
+        return None
+    ref = kept['f32']
+    out = {}
+    for f, k in kept.items():
+        if f == 'f32':
+            continue
+        only, only_ref = k.keys() - ref.keys(), ref.keys() - k.keys()
+        out[f] = dict(kept=len(k), kept_f32=len(ref), both=len(k.keys() & ref.keys()), only_this=len(only),
+                      only_f32=len(only_ref), only_this_away=sum(k[x] > 1.03 * thr for x in only),
+                      only_f32_away=sum(ref[x] > 1.03 * thr for x in only_ref))
+    return out
+
+
 def traffic_ratios():
     """Measured DRAM bytes over algorithmic bytes, from the committed ncu summaries (lines 'traffic_ratio: X')."""
     out = {}
@@ -236,7 +253,7 @@ def main():
     ap.add_argument('--templates', type=int, default=5880)
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-precision', action='store_true', help='skip the float64 precision comparison')
-    ap.add_argument('--forms', default='f16,bf16,f32', help='forms timed (the first gives value)')
+    ap.add_argument('--forms', default='f16,bf16,fp8,f32', help='forms timed (the first gives value)')
     ap.add_argument('--slow-steps', type=int, default=1,
                     help='timed steps (and warm-up steps) for the plain fp32 form, which is many times slower')
     a = ap.parse_args()
@@ -273,6 +290,7 @@ def main():
     sw, isw = sw.clone(), isw.clone()
     forms = a.forms.split(',')
     results = {}
+    kept_sets = {}
     torch.cuda.synchronize()
     t_b = time.perf_counter()
     cfg0 = pipeline.FilterConfig(form=forms[0])
@@ -293,6 +311,10 @@ def main():
             step()
         torch.cuda.synchronize()
         res0 = mf.results()
+        # kept peaks of the step after the exact stage: (row, segment, window) -> exact SNR
+        kc, kp = res0['cands'][res0['keep']], res0['peaks'][res0['keep']]
+        kept_sets[form] = dict(zip(zip(kc['row'].tolist(), kc['seg'].tolist(), kc['window'].tolist()),
+                                   kp['snr'].tolist()))
         l0c, l0m = cond.launches, mf.kernel_launches
         barrier()
         torch.cuda.synchronize()
@@ -339,10 +361,10 @@ def main():
         b_ms = [e[0].elapsed_time(e[3]) for e, n, r, kp in L]
         # algorithmic HBM bytes of one basis-series call (both passes): Vp read (tlen/2 + 1 complex per row), W
         # written and read back (tlen complex per row), Z written (re + im over Tn, one or two 16-bit planes or fp32)
-        zb = {'bf16x3': 8, 'f16': 4, 'bf16': 4, 'f32': 8}[form]
+        zb = {'bf16x3': 8, 'f16': 4, 'bf16': 4, 'f32': 8, 'fp8': 2}[form]
         b_bytes = [r * (8 * (mf.tlen // 2 + 1) + 16 * mf.tlen + zb * mf.Tn) for e, n, r, kp in L]
         useful = [8.0 * n * r * mf.Tn for e, n, r, kp in L]
-        nprod = {'bf16x3': 3, 'f16': 1, 'bf16': 1, 'f32': 1}[form]
+        nprod = {'bf16x3': 3, 'f16': 1, 'bf16': 1, 'f32': 1, 'fp8': 1}[form]
         issued = [nprod * 4.0 * n * kp * mf.Tn for e, n, r, kp in L]
         mf.profile = None
         val = world * (analysed / WEEK2) / (ms / 1e3 / 3600.0)
@@ -352,7 +374,7 @@ def main():
                              h2d=x.numel() * 4, d2h=res_bytes, gemm_ms=float(np.mean(g_ms)),
                              gemm_total_ms=float(np.sum(g_ms)), basis_total_ms=float(np.sum(b_ms)),
                              basis_ms=float(np.mean(b_ms)), basis_bytes=float(np.mean(b_bytes)),
-                             z_bytes=float(np.mean([2 * kp * mf.Tn * (2 if form != 'f32' else 4) *
+                             z_bytes=float(np.mean([2 * kp * mf.Tn * {'f32': 4, 'fp8': 1}.get(form, 2) *
                                                     (2 if form == 'bf16x3' else 1) for e, n, r, kp in L])),
                              useful=float(np.mean(useful)), issued=float(np.mean(issued)), n_gemm=len(L))
         del mf
@@ -368,7 +390,7 @@ def main():
         precision_rep = dict(tile=t_p, r=B.svd[t_p]['r'], segment=seg_p,
                              reference='float64 transform and product (gwb200.precision)')
         ref = None
-        for form in ('f32', 'bf16x3', 'f16', 'bf16'):
+        for form in ('f32', 'bf16x3', 'f16', 'bf16', 'fp8'):
             cfg = pipeline.FilterConfig(form=form)
             mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg, device=dev)
             sig = mf.norms(IPd)
@@ -406,7 +428,8 @@ def main():
     line = dict(metric=METRIC, value=R['value'], unit='2-det weeks / GPU-hour', n_gpus=world, steps=a.steps,
                 warmup=a.warmup, ms_per_step=R['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
                 dtype={'bf16x3': 'bf16 hi+lo (fp32 accumulate)', 'f16': 'f16 (fp32 accumulate)',
-                       'bf16': 'bf16 (fp32 accumulate)', 'f32': 'f32'}[main_form],
+                       'bf16': 'bf16 (fp32 accumulate)', 'f32': 'f32',
+                       'fp8': 'fp8 e4m3 screen (fp32 accumulate) + float64 exact stage'}[main_form],
                 data='synthetic (seeded noise, TaylorF2 bank and injections)',
                 config=dict(workload='C2: 2 det x %d chunks x 512 s at 2048 Hz, %d TaylorF2 templates in tiles of 256, '
                                      'eps 1e-3, 16 chi-squared bins' % (a.chunks, len(bank['mass1'])),
@@ -416,7 +439,7 @@ def main():
                 e2e=dict(value=R['e2e'], unit='2-det weeks / GPU-hour', h2d_bytes_per_step=R['h2d'],
                          d2h_bytes_per_step=R['d2h']),
                 gpu_launches=R['launches'], clocks=R['clocks'], bank_setup_s=bank_setup, roofline=roof,
-                roofline_gemm=roof_gemm, precision=precision_rep,
+                roofline_gemm=roof_gemm, precision=precision_rep, top_peak_sets=top_peak_sets(kept_sets, 5.5),
                 forms={k: dict(value=v['value'], ms_per_step=v['ms'], e2e=v['e2e'], n_candidates=v['n_candidates'],
                                n_kept=v['n_kept'], gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
                                basis_share=v['basis_total_ms'] / v['ms']) for k, v in results.items()},

@@ -66,14 +66,16 @@ def basis(a):
     D = torch.randn(flen, generator=g, device='cuda', dtype=torch.complex64)
     isw = torch.rand(flen, generator=g, device='cuda')
     a0, Tn = tlen * 3 // 32, tlen * 28 // 32
-    Kh = fp_filter.kh_of(r)
+    Kh = fp_filter.kh_of(r, a.form)
     Z = torch.zeros((2 * Kh, Tn), dtype=fp_filter._z_dtype(a.form), device='cuda')
     Zlo = torch.zeros_like(Z) if a.form == 'bf16x3' else None
     Dp = fp_filter.fourstep_order(D, tlen, isw)
     Vp = fp_filter.fourstep_order(Vh, tlen)
-    ms = _time(lambda: fp_filter.basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
-    out = dict(kernel='basis_series', form=a.form, r=r, tlen=tlen, ms_cufft_path=ms, us_per_row_cufft=ms * 1e3 / r)
-    zb = 2 * Tn * (2 if a.form in ('f16', 'bf16') else 4)
+    out = dict(kernel='basis_series', form=a.form, r=r, tlen=tlen)
+    if a.form != 'fp8':            # the cuFFT path has no fp8 pack
+        ms = _time(lambda: fp_filter.basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
+        out.update(ms_cufft_path=ms, us_per_row_cufft=ms * 1e3 / r)
+    zb = 2 * Tn * {'f16': 2, 'bf16': 2, 'fp8': 1}.get(a.form, 4)
     for wr in [int(x) for x in a.wrows.split(',')]:
         fws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wr or None)
         msf = _time(lambda: fp_filter.basis_series_fused(fws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)

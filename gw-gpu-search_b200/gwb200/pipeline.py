@@ -36,9 +36,9 @@ class FilterConfig:
     cluster_window: float = 1.0
     snr_threshold: float = 5.5
     margin: float = 0.04
-    screen_margin: float = 0.15   # fp8 form: candidates down to thr (1 - screen_margin); the exact stage decides
+    screen_margin: float = 0.10   # fp8 form: candidates down to thr (1 - screen_margin); the exact stage decides
     form: str = 'bf16x3'
-    cand_cap: int = 1 << 20
+    cand_cap: int = 1 << 21
     seg_batch: int = 16
 
 
