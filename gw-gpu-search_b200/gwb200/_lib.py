@@ -53,6 +53,9 @@ SIGNATURES = {
     'gwb_stacked_a8': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _P, _LL, _P, _P],
     'gwb_select_windows': [_P, _P, _LL, _I, _I, _F, _LL, _I, _I, _P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _I, _P,
                            _P, _I, _P, _I, _P, _I, _P, _P],
+    'gwb_snr_grad': [_P, _I, _P, _LL, _P, _LL, _I, _D, _I, _D, _I, _I, _P, _LL, _P],
+    'gwb_phase_metric': [_P, _I, _P, _LL, _I, _D, _I, _D, _P, _P],
+    'gwb_refine_step': [_P, _P, _LL, _P, _P, _I, _P, _P],
     'gwb_edges': [_P, _P, _I, _P, _LL, _P, _LL, _P, _P, _I, _I, _I, _P, _P],
     'gwb_bin_sums': [_P, _P, _I, _P, _P, _P, _I, _P, _P, _LL, _P, _LL, _I, _I, _LL, _P, _P],
     'gwb_exact_finalize': [_P, _P, _I, _P, _P, _I, _P, _I, _I, _P, _P, _LL, _D, _P, _P],

@@ -268,6 +268,28 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
                             int im_off, int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket,
                             float* scale, float* rowscale, float* rowpart, long long rowpart_elems, void* stream);
 
+/* ---- differentiation (the adjoint form; no reference counterpart: the reference has no gradients) ------------- */
+/* Per trigger i, parameters params[i * 7 + (0..6)] = (Mc [M_sun], q = m2/m1 <= 1, chi1z, chi2z, e0 at f_ecc, t_c [s],
+ * phi_c), the library's TaylorF2 template (gwb_taylorf2's phase) h = f^-7/6 exp(-i (Psi - pi/4 + 2 pi f t_c - phi_c))
+ * on kmin <= k < kmax (the ISCO bin) against the trigger's over-whitened data D (row i, ldd) and inverse PSD IP (row i,
+ * ldip; 0 shares one row): z = 4 df sum conj(h) D, sigma^2 = 4 df sum |h|^2 IP, snr = |z| / sigma, chisq over nbins
+ * equal-power bins (the pipeline's edges, held fixed; dof 2 nbins - 2), newsnr (coinc_rank.py:39-46), and their
+ * derivatives with respect to the 7 parameters (forward-mode dual numbers through the phase in float64; sums in
+ * float32 (fp64 = 0) or float64). out row (ldout >= 28 doubles): snr, newsnr, chisq, sigma^2, z re, z im, kmax,
+ * dsnr[7], dnewsnr[7], dchisq[7]. */
+GWB_API int gwb_snr_grad(const double* params, int n, const float* D, long long ldd, const float* IP, long long ldip,
+                         int flen, double df, int kmin, double f_ecc, int nbins, int fp64, double* out,
+                         long long ldout, void* stream);
+/* Phase metric per bank point (n x 7 x 7 doubles): g_ij = Cov_w(dPhi/dtheta_i, dPhi/dtheta_j) with w = |h|^2 IP, the
+ * quadratic form of the phase-maximised match (1 - match ~ dtheta^T g dtheta / 2); the phi_c row and column are 0. */
+GWB_API int gwb_phase_metric(const double* params, int n, const float* IP, long long ldip, int flen, double df,
+                             int kmin, double f_ecc, double* g, void* stream);
+/* One Levenberg-Marquardt step of the SNR ascent per trigger over the 6 parameters other than phi_c: out = params +
+ * (g + lam[i] diag g)^-1 (dsnr / snr), from gwb_snr_grad's rows (res) and gwb_phase_metric (g), clamped to Mc > 0,
+ * q in [0.05, 1], |chi| <= 0.99, e0 in [0, 0.5]; the caller adapts lam[i] per trigger. */
+GWB_API int gwb_refine_step(const double* params, const double* res, long long ldres, const double* g,
+                            const double* lam, int n, double* out, void* stream);
+
 /* ---- candidate selection and the exact stage ---------------------------------------------------------------- */
 /* Window candidates of one (tile, segment) (fp_filter.py:745-764): rows i < n whose windowed maximum vw (the fused
  * GEMM output with group = cw/128) exceeds thr2 become GwbCand records (row0 + i, seg, a0 + iw, window, sqrt(vw),
