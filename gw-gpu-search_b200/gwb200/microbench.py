@@ -3,6 +3,7 @@
     python -m gwb200.microbench gemm  [--r 128] [--n 256] [--tn 917504] [--form f16] [--reps 20]
     python -m gwb200.microbench basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5] [--wrows 0,4,8]
     python -m gwb200.microbench exact [--groups 512] [--peaks 1] [--tlen 1048576] [--reps 5]
+    python -m gwb200.microbench adjoint [--triggers 4096] [--reps 5]
 
 Run from gw-gpu-search_b200/ (or with it on sys.path). Operand sizes default to one (tile, chunk) of the C2
 workload; inputs are larger than L2 where the real ones are."""
@@ -115,9 +116,43 @@ def exact(a):
                 gbs=len(groups) * nbins * 16 / ms / 1e6)
 
 
+def adjoint(a):
+    """C5: n triggers of 16 s (flen 16,385) with random C2-like parameters against synthetic whitened data: gradient of
+    SNR / newSNR (fp32 and fp64 sums), the 7 x 7 phase metric of 10,000 bank points, and 20 refinement steps."""
+    from . import adjoint as adj
+    n, tlen = a.triggers, 1 << 15
+    flen, df = tlen // 2 + 1, 2048.0 / tlen
+    kmin = int(20.0 / df)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    th = torch.empty((n, 7), dtype=torch.float64, device='cuda')
+    th[:, 0] = 5.0 + 30.0 * torch.rand(n, generator=g, device='cuda', dtype=torch.float64)
+    th[:, 1] = 0.3 + 0.7 * torch.rand(n, generator=g, device='cuda', dtype=torch.float64)
+    th[:, 2:4] = 1.8 * torch.rand((n, 2), generator=g, device='cuda', dtype=torch.float64) - 0.9
+    th[:, 4] = 0.3 * torch.rand(n, generator=g, device='cuda', dtype=torch.float64)
+    th[:, 5] = 0.0
+    th[:, 6] = 0.0
+    D = torch.randn((n, flen), generator=g, device='cuda', dtype=torch.complex64)
+    f = torch.arange(flen, device='cuda', dtype=torch.float64) * df
+    IP = torch.where(f >= 20.0, (f / 200.0) ** 4.0 / (1 + (f / 200.0) ** 4), torch.zeros_like(f)).float()
+    out = {}
+    for fp64 in (False, True):
+        out['ms_grad_fp64' if fp64 else 'ms_grad_fp32'] = _time(lambda: adj.snr_grad(th, D, IP, df, kmin, fp64=fp64),
+                                                                a.reps)
+    bank = th[:min(n, 10000)]
+    if n < 10000:
+        bank = th.repeat(-(-10000 // n), 1)[:10000].contiguous()
+    out['ms_metric_10000'] = _time(lambda: adj.phase_metric(bank, IP, flen, df, kmin), a.reps)
+    out['ms_refine_20_steps'] = _time(lambda: adj.refine(th, D, IP, df, kmin, steps=20), 1)
+    bins = float((adj.snr_grad(th, D, IP, df, kmin)['kmax'] - kmin).clamp_min(0).sum())   # bins below each ISCO
+    return dict(kernel='snr_grad_kernel / phase_metric_kernel / refine', triggers=n, flen=flen,
+                triggers_per_s_fp32=n / out['ms_grad_fp32'] * 1e3, bins=bins, bins_per_ns_fp32=bins / out['ms_grad_fp32'] / 1e6,
+                **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('what', choices=['gemm', 'basis', 'exact'])
+    ap.add_argument('what', choices=['gemm', 'basis', 'exact', 'adjoint'])
+    ap.add_argument('--triggers', type=int, default=4096)
     ap.add_argument('--r', type=int, default=128)
     ap.add_argument('--n', type=int, default=256)
     ap.add_argument('--tn', type=int, default=917504)
@@ -128,7 +163,7 @@ def main():
     ap.add_argument('--reps', type=int, default=10)
     ap.add_argument('--wrows', default='0', help='basis: comma list of W row batches (0: all rows at once)')
     a = ap.parse_args()
-    print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact}[a.what](a)))
+    print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact, 'adjoint': adjoint}[a.what](a)))
 
 
 if __name__ == '__main__':
