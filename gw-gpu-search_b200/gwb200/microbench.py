@@ -4,6 +4,7 @@
     python -m gwb200.microbench basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5] [--wrows 0,4,8]
     python -m gwb200.microbench exact [--groups 512] [--peaks 1] [--tlen 1048576] [--reps 5]
     python -m gwb200.microbench adjoint [--triggers 4096] [--reps 5]
+    python -m gwb200.microbench c4 [--segments 300] [--batch 32] [--form f16] [--no-graph]
 
 Run from gw-gpu-search_b200/ (or with it on sys.path). Operand sizes default to one (tile, chunk) of the C2
 workload; inputs are larger than L2 where the real ones are."""
@@ -149,9 +150,122 @@ def adjoint(a):
                 **out)
 
 
+def c4(a):
+    """C4: science segments with lengths log-uniform in [64, 4096] s at 2048 Hz over two detectors, coloured noise
+    (the analytic PSD with 60/120/180 Hz lines), TaylorF2 injections (SNR 6-30, about one per 290 s), sine-Gaussian
+    glitches (Q = 10, f0 30-300 Hz, SNR 20-200) in 2% of the segments; the C2 bank of 5,880 templates in 512 s chunks.
+    Times filter_segments (autogating, chunking, graph-replayed batches, results) end to end on the device."""
+    import time
+    import numpy as np
+    from . import fp_filter, pipeline, segments as sg, templates
+    sr, L = 2048.0, 512.0
+    tlen = int(L * sr)
+    flen, df = tlen // 2 + 1, 1.0 / L
+    rng = np.random.default_rng(a.seed)
+    lens = np.floor(np.exp(rng.uniform(np.log(64.0), np.log(4096.0), a.segments))).astype(int)
+    dyn = 5.9029581035870565e+20
+
+    def psd(f):
+        x = np.maximum(f, 15.0) / 215.0
+        p_ = 1e-49 * (x ** -4.14 - 5.0 * x ** -2 + 111.0 * (1.0 - x ** 2 + 0.5 * x ** 4) / (1.0 + 0.5 * x ** 2))
+        p_ = np.where(f < 15.0, 1e4 * p_, p_)
+        for f0, h, w in ((60.0, 1e3, 0.02), (120.0, 1e3, 0.02), (180.0, 1e3, 0.02)):
+            p_ = p_ * (1.0 + h / (1.0 + ((f - f0) / w) ** 2))
+        return p_ * dyn ** 2
+
+    rb = np.random.default_rng(0)
+    m = rb.uniform(3.0, 100.0, (4612, 2))
+    mt, q, e0 = rb.uniform(45.0, 100.0, 1268), rb.uniform(1.0, 3.0, 1268), rb.uniform(0.0, 0.3, 1268)
+    bank = dict(mass1=np.r_[m.max(1), mt * q / (1 + q)], mass2=np.r_[m.min(1), mt / (1 + q)],
+                spin1z=np.r_[rb.uniform(-0.9, 0.9, 4612), np.zeros(1268)],
+                spin2z=np.r_[rb.uniform(-0.9, 0.9, 4612), np.zeros(1268)], ecc=np.r_[np.zeros(4612), e0])
+    segs, inj, glitches = [], [], []
+    gps = 1000000000
+    for i, n_s in enumerate(lens):
+        n = int(n_s * sr)
+        fl = n // 2 + 1
+        f = np.arange(fl) * (sr / n)
+        g = torch.Generator(device='cuda').manual_seed(a.seed * 7919 + i)
+        X = torch.fft.rfft(torch.randn(n, generator=g, device='cuda', dtype=torch.float64))
+        X *= torch.from_numpy(np.sqrt(psd(f) * sr / 2.0)).cuda()
+        X[0] = 0
+        ps = torch.from_numpy(psd(f)).cuda()
+        fk = torch.from_numpy(f).cuda()
+        kmin = int(20.0 * n / sr)
+        for _ in range(rng.poisson(n_s / 290.0)):
+            row, t0, snr = int(rng.integers(0, 5880)), rng.uniform(48.0, n_s - 16.0), rng.uniform(6.0, 30.0)
+            h, _ = templates.generate(bank, [row], fl, sr / n, 20.0, device='cuda')
+            h = h[0].to(torch.complex128)
+            h = h * (snr / torch.sqrt(4 * (sr / n) * (h[kmin:].abs() ** 2 / ps[kmin:]).sum()))
+            X += h * torch.exp(-2j * np.pi * fk * t0) * sr
+            inj.append((i, t0, row, snr))
+        x = torch.fft.irfft(X, n)
+        if rng.uniform() < 0.02:
+            f0, snr, tg = rng.uniform(30.0, 300.0), rng.uniform(20.0, 200.0), rng.uniform(20.0, n_s - 20.0)
+            tau = 10.0 / (np.sqrt(2.0) * np.pi * f0)
+            t = torch.arange(n, device='cuda', dtype=torch.float64) / sr - tg
+            sgx = torch.exp(-(t / tau) ** 2) * torch.sin(2 * np.pi * f0 * t)
+            G = torch.fft.rfft(sgx) / sr
+            rho = torch.sqrt(4 * (sr / n) * (G[kmin:].abs() ** 2 / ps[kmin:]).sum())
+            x += sgx * (snr / rho)
+            glitches.append((i, tg, f0, snr))
+        segs.append(dict(x=x.to(torch.float32).contiguous(), start_gps=gps, det=i % 2))
+        gps += int(n_s) + 100
+    cfg = pipeline.FilterConfig(form=a.form)
+    # SVD metric of the run from a first batch of chunks, then the bank (as bench.py builds it)
+    from . import gpu_prep
+    first = [s for s in segs if s['x'].shape[0] >= tlen][:a.batch]
+    Xb = torch.stack([s['x'][:tlen] for s in first] + [first[0]['x'][:tlen]] * (a.batch - len(first)))
+    cond = gpu_prep.BatchConditioner(a.batch, tlen, sr, 20.0, 16.0, 8.0, 63, 16.0)
+    _, IPb = cond(Xb.contiguous())
+    sw, isw = fp_filter.derive_sw(IPb)
+    sw, isw = sw.clone(), isw.clone()
+    del cond
+    torch.cuda.synchronize()
+    t_b = time.perf_counter()
+    B = pipeline.Bank(bank, flen, df, sw, cfg)
+    torch.cuda.synchronize()
+    bank_s = time.perf_counter() - t_b
+    F = sg.SegmentFilter(B, cfg, batch=a.batch, isw=isw, graph=not a.no_graph)
+    F.run(segs[:2], gate=False)            # warm-up (captures the graph)
+    torch.cuda.synchronize()
+    e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0_.record()
+    res = F.run(segs)
+    e1_.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = e0_.elapsed_time(e1_)
+    # injections in analysed time recovered: a kept peak within 0.1 s of the injection in its segment
+    kept = res['keep']
+    c, segi, ch = res['cands'][kept], res['segment'][kept], res['chunk'][kept]
+    t_peak = (np.array([res['plan'][k][1][0] for k in ch]) + c['sample']) / sr if len(c) else np.zeros(0)
+    n_inj_an, found = 0, 0
+    for (i, t_inj, row, snr) in inj:
+        if lens[i] < L or snr < 8.0:
+            continue
+        n_inj_an += 1
+        found += int(np.any((segi == i) & (np.abs(t_peak - t_inj) < 0.1)))
+    gated = sum(1 for (i, *_rest) in glitches if res['gates'][i])
+    weeks = res['analysed_s'] / (2 * 604800.0)
+    return dict(workload='C4: %d segments, log-uniform 64-4096 s, 2 detectors, %d injections, %d glitches; 5880 '
+                         'templates, %s' % (a.segments, len(inj), len(glitches), a.form),
+                value=weeks / (ms / 1e3 / 3600.0), unit='2-det weeks / GPU-hour', ms=ms, wall_s=wall,
+                analysed_s=res['analysed_s'], skipped_s=res['skipped_s'], skipped_segments=len(res['skipped']),
+                total_s=float(lens.sum()), chunks=res['n_chunks'], batches=res['batches'], graph=not a.no_graph,
+                kept=int(kept.sum()), candidates=len(res['cands']), glitches=len(glitches), glitches_gated=gated,
+                injections_snr8_in_analysed=n_inj_an, injections_found=found,
+                gates=sum(len(g) for g in res['gates']), bank_setup_s=bank_s)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('what', choices=['gemm', 'basis', 'exact', 'adjoint'])
+    ap.add_argument('what', choices=['gemm', 'basis', 'exact', 'adjoint', 'c4'])
+    ap.add_argument('--segments', type=int, default=300)
+    ap.add_argument('--batch', type=int, default=32)
+    ap.add_argument('--seed', type=int, default=4)
+    ap.add_argument('--no-graph', action='store_true')
     ap.add_argument('--triggers', type=int, default=4096)
     ap.add_argument('--r', type=int, default=128)
     ap.add_argument('--n', type=int, default=256)
@@ -163,7 +277,7 @@ def main():
     ap.add_argument('--reps', type=int, default=10)
     ap.add_argument('--wrows', default='0', help='basis: comma list of W row batches (0: all rows at once)')
     a = ap.parse_args()
-    print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact, 'adjoint': adjoint}[a.what](a)))
+    print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact, 'adjoint': adjoint, 'c4': c4}[a.what](a)))
 
 
 if __name__ == '__main__':

@@ -1,0 +1,146 @@
+"""Batched filtering of many science segments of different lengths (the batched form): the library's replacement of
+the reference's per-dataset loop over segments (fp_filter.py:700-888 driven once per dataset, with gpu_prep stage 1
+and stage 2 per dataset, gpu_prep.py:362-454).
+
+Each segment is autogated over its whole length (detect_loud_glitches + gate_taper, gpu_prep.py:175-231), then cut
+into chunks of seg_len seconds by the reference's StrainSegments arithmetic (segment_slices, gpu_prep.py:234-271:
+chunks at a fixed stride, the last one shifted back to end at the segment's end, its analysed part starting where the
+previous chunk's ended). Segments shorter than seg_len hold no chunk, as in the reference, and are reported as
+skipped. Chunks go through the device in batches of `batch`: one conditioning (BatchConditioner) and one filter step
+(MatchedFilter) per batch, captured once as a CUDA graph and replayed for every batch. Candidates outside a chunk's
+analysed part are dropped when the results are mapped back to segments.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import gpu_prep, pipeline
+
+
+@dataclass
+class Gating:
+    threshold: float = 8.0      # whitened |x| (the reference's argv uses 50, for glitches far louder than SNR 200)
+    cluster: float = 0.5
+    width: float = 0.25
+    taper: float = 0.25
+    pad: float = 16.0
+    f_low: float = 15.0
+    max_iterations: int = 1
+
+
+def plan_chunks(lengths, sr, start_gps, seg_len, start_pad, end_pad):
+    """Chunks of segments of the given lengths (samples): list of (segment index, (s0, s1) samples, (a0, a1) analysed
+    samples relative to s0), by segment_slices; and the indices of the segments shorter than seg_len (skipped)."""
+    tlen = int(seg_len * sr)
+    chunks, skipped = [], []
+    for i, n in enumerate(lengths):
+        if n < tlen:
+            skipped.append(i)
+            continue
+        for sl, an in gpu_prep.segment_slices(int(n), sr, start_gps[i], seg_len, start_pad, end_pad, None, None):
+            chunks.append((i, sl, an))
+    return chunks, skipped
+
+
+class SegmentFilter:
+    """Filters lists of segments against one bank. segments: list of dict(x = float32 CUDA strain in DYN_RANGE_FAC
+    units, start_gps, det). The bank's templates must have been generated for chunks of seg_len seconds."""
+
+    def __init__(self, bank, cfg, seg_len=512.0, start_pad=48.0, end_pad=16.0, batch=32, gating=Gating(),
+                 psd=(16.0, 8.0, 63, 16.0), isw=None, graph=True, device='cuda'):
+        self.bank, self.cfg, self.gating = bank, cfg, gating
+        self.sr = cfg.sr
+        self.seg_len, self.start_pad, self.end_pad = seg_len, start_pad, end_pad
+        self.tlen = int(seg_len * self.sr)
+        assert self.tlen // 2 + 1 == bank.flen, 'the bank was generated for another chunk length'
+        self.batch = batch
+        self.device = device
+        seg_l, seg_s, nseg, inv_len = psd
+        self.cond = gpu_prep.BatchConditioner(batch, self.tlen, self.sr, cfg.f_low, seg_l, seg_s, nseg, inv_len,
+                                              device=device)
+        a0, a1 = int(start_pad * self.sr), int((seg_len - end_pad) * self.sr)
+        self.mf = pipeline.MatchedFilter(bank, self.tlen, a0, a1 - a0, cfg, device=device)
+        self.X = torch.zeros((batch, self.tlen), dtype=torch.float32, device=device)
+        self.isw = isw
+        self.use_graph = graph
+        self.graph = None
+
+    def gate(self, x, start_gps):
+        """Autogating of one segment in place (gpu_prep.gpu_stage1's loop); returns the gates (gps, width, taper)."""
+        g = self.gating
+        gates = []
+        for _ in range(g.max_iterations):
+            gt = gpu_prep.detect_loud_glitches(torch, x, self.sr, start_gps, g.threshold, g.cluster, g.f_low, g.pad)
+            gp = [(t, g.width, g.taper) for t in gt]
+            gates += gp
+            gpu_prep.gate_taper(torch, x, self.sr, start_gps, gp)
+            if not gt:
+                break
+        return [(float(t), w, tp) for t, w, tp in gates]
+
+    def plan(self, segments):
+        """Chunks of every segment: list of (segment index, (s0, s1) samples, (a0, a1) analysed samples in the chunk),
+        and the skipped segments (shorter than seg_len)."""
+        return plan_chunks([s['x'].shape[0] for s in segments], self.sr, [s['start_gps'] for s in segments],
+                           self.seg_len, self.start_pad, self.end_pad)
+
+    def _step(self):
+        D, IP = self.cond(self.X)
+        self.mf.step(D, IP, self.isw)
+
+    def _capture(self):
+        self._step()                           # warm-up: plans, workspaces and cached tables outside the capture
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._step()
+        torch.cuda.synchronize()
+
+    def run(self, segments, gate=True):
+        """Gates, plans and filters every segment. Returns dict(cands, peaks, keep (the kept peaks after the exact
+        stage), segment and chunk index of each candidate, gates per segment, analysed_s, skipped_s, batches)."""
+        gates = [self.gate(s['x'], s['start_gps']) if gate else [] for s in segments]
+        chunks, skipped = self.plan(segments)
+        if self.isw is None:
+            # the SVD metric of the run (fp_filter.py:354-370) from the first batch, as the bank was built
+            raise ValueError('isw (the bank\'s 1 / sw) must be given')
+        out_c, out_p, seg_i, chunk_i = [], [], [], []
+        analysed = 0.0
+        for b0 in range(0, len(chunks), self.batch):
+            part = chunks[b0:b0 + self.batch]
+            for r in range(self.batch):
+                i, (s0, s1), _ = part[min(r, len(part) - 1)]     # unused rows repeat a real chunk (dropped below)
+                self.X[r].copy_(segments[i]['x'][s0:s1])
+            if self.use_graph:
+                if self.graph is None:
+                    self._capture()
+                self.graph.replay()
+            else:
+                self._step()
+            torch.cuda.synchronize()
+            res = self.mf.results()
+            c, p = res['cands'], res['peaks']
+            row = c['seg'].astype(np.int64)
+            ok = row < len(part)
+            a_lo = np.array([an[0] for _, _, an in part] + [0] * (self.batch - len(part)))
+            a_hi = np.array([an[1] for _, _, an in part] + [0] * (self.batch - len(part)))
+            ok &= (c['sample'] >= a_lo[row]) & (c['sample'] < a_hi[row])
+            out_c.append(c[ok])
+            out_p.append(p[ok])
+            seg_i.append(np.array([part[r][0] for r in row[ok]], np.int64))
+            chunk_i.append(b0 + row[ok])
+            analysed += sum((an[1] - an[0]) for _, _, an in part) / self.sr
+        cands = np.concatenate(out_c) if out_c else np.zeros(0)
+        peaks = np.concatenate(out_p) if out_p else np.zeros(0)
+        keep = peaks['snr'] > self.cfg.snr_threshold if len(peaks) else np.zeros(0, bool)
+        skipped_s = sum(segments[i]['x'].shape[0] for i in skipped) / self.sr
+        return dict(cands=cands, peaks=peaks, keep=keep, segment=np.concatenate(seg_i) if seg_i else np.zeros(0),
+                    chunk=np.concatenate(chunk_i) if chunk_i else np.zeros(0), gates=gates, analysed_s=analysed,
+                    skipped_s=skipped_s, skipped=skipped, n_chunks=len(chunks), batches=-(-len(chunks) // self.batch),
+                    plan=chunks)
+
+
+def filter_segments(segments, bank, cfg, isw, **kw):
+    """Batched filter of a list of segments (see SegmentFilter)."""
+    return SegmentFilter(bank, cfg, isw=isw, **kw).run(segments)

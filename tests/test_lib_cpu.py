@@ -72,3 +72,25 @@ def test_window_peaks_rejects_windows_past_the_row():
 def test_call_raises_with_message():
     with pytest.raises(_lib.GwbError, match='multiple of 64'):
         _lib.call('gwb_fused_peaks_f16', _p(16), _p(16), 48, _p(16), 1024, 64, 48, 1024, 1, _p(16), _p(16), 8, None)
+
+
+def test_segment_chunks_cover_the_analysable_time_once():
+    """Batched form: the chunks of segments of any length cover each segment's [start_pad, len - end_pad) exactly
+    once (the shifted last chunk's analysed part starts where the previous one ended); shorter segments are skipped."""
+    import numpy as np
+    from gwb200 import segments
+    sr, L, sp, ep = 2048.0, 512.0, 48.0, 16.0
+    lens = [512, 700, 1023, 1536, 4096, 300, 3333]
+    chunks, skipped = segments.plan_chunks([int(x * sr) for x in lens], sr, [1000000000 + 10000 * i for i in
+                                                                              range(len(lens))], L, sp, ep)
+    assert skipped == [5]
+    for i, n_s in enumerate(lens):
+        if n_s < L:
+            continue
+        cover = np.zeros(int(n_s * sr), np.int8)
+        for j, (s0, s1), (a0, a1) in chunks:
+            if j == i:
+                assert s1 - s0 == int(L * sr) and 0 <= s0 and s1 <= n_s * sr
+                cover[s0 + a0:s0 + a1] += 1
+        assert cover[int(sp * sr):int((n_s - ep) * sr)].min() == 1 and cover.max() == 1
+        assert cover[:int(sp * sr)].max() == 0 and cover[int((n_s - ep) * sr):].max() == 0
