@@ -71,6 +71,51 @@ __global__ void welch_avg_kernel(const float2* __restrict__ X, long long ldx, in
     psd[(long long)r * ldp + k] = __fmul_rn(q, fac);
 }
 
+// Median Welch average for many frames (more than 256, e.g. the 4 s estimate over a long segment in the autogating):
+// one CTA per (row, bin), the frames' powers sorted in shared memory (bitonic, padded to a power of two with +inf),
+// then the same median, bias and scale arithmetic as welch_avg_kernel.
+__global__ void welch_median_big_kernel(const float2* __restrict__ X, long long ldx, int rows, int nfr, int nbin,
+                                        float dt, float bias32, double bias64, int wide, float fac, int p2,
+                                        float* __restrict__ psd, long long ldp) {
+    extern __shared__ float v[];
+    const int r = blockIdx.x / nbin, k = blockIdx.x % nbin;
+    for (int s = threadIdx.x; s < p2; s += blockDim.x) {
+        float p = __int_as_float(0x7f800000);      // +inf pads past nfr
+        if (s < nfr) {
+            const float2 c = X[((long long)r * nfr + s) * ldx + k];
+            const float a = c.x * dt, b = c.y * dt;
+            p = __fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b));
+            if (k == 0 || k == nbin - 1) p = p / 2.f;
+        }
+        v[s] = p;
+    }
+    __syncthreads();
+    for (int size = 2; size <= p2; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const float a = v[i], b = v[j];
+                    if ((a > b) == up) {
+                        v[i] = b;
+                        v[j] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    if (threadIdx.x == 0) {
+        float q = (nfr & 1) ? v[nfr / 2] : __fdiv_rn(__fadd_rn(v[nfr / 2 - 1], v[nfr / 2]), 2.f);
+        if (wide) {
+            psd[(long long)r * ldp + k] = (float)(((double)q / bias64) * (double)fac);
+            return;
+        }
+        q = __fdiv_rn(q, bias32);
+        psd[(long long)r * ldp + k] = __fmul_rn(q, fac);
+    }
+}
+
 __global__ void interp_kernel(const float* __restrict__ psd, long long ldp, int rows, int nold, double df_old,
                               double df_new, int nnew, float* __restrict__ out, long long ldo) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -243,12 +288,22 @@ int gwb_welch_avg(const float* X, long long ldx, int rows, int nfr, int nbin, fl
                   float fac, float* psd, long long ldp, void* stream) {
     using namespace gwb;
     GWB_CHECK_ARG(X && psd, GWB_ERR_ARG, "welch_avg: null pointer");
-    GWB_CHECK_ARG(rows > 0 && nfr > 0 && nfr <= 256 && nbin > 0 && ldx >= nbin && ldp >= nbin, GWB_ERR_SHAPE,
-                  "welch_avg: rows=%d frames=%d (at most 256) nbin=%d", rows, nfr, nbin);
+    GWB_CHECK_ARG(rows > 0 && nfr > 0 && nbin > 0 && ldx >= nbin && ldp >= nbin && (nfr <= 256 || (median &&
+                  nfr <= 8192)), GWB_ERR_SHAPE, "welch_avg: rows=%d frames=%d (at most 256, or 8192 for the median) "
+                  "nbin=%d", rows, nfr, nbin);
     const long long n = (long long)rows * nbin;
     const int wide = nfr >= 1000;
     cudaStream_t s = (cudaStream_t)stream;
     const float2* x2 = reinterpret_cast<const float2*>(X);
+    if (nfr > 256) {
+        int p2 = 1;
+        while (p2 < nfr) p2 <<= 1;
+        GWB_CHECK_ARG(n < (1ll << 31), GWB_ERR_SHAPE, "welch_avg: rows x nbin = %lld", n);
+        welch_median_big_kernel<<<(unsigned)n, kT, (size_t)p2 * sizeof(float), s>>>(
+            x2, ldx, rows, nfr, nbin, dt, (float)bias, bias, wide, fac, p2, psd, ldp);
+        GWB_LAUNCH_CHECK("welch_median_big_kernel");
+        return GWB_OK;
+    }
     if (nfr <= 64)
         welch_avg_kernel<64><<<blocks_for(n), kT, 0, s>>>(x2, ldx, rows, nfr, nbin, dt, median, (float)bias, bias, wide,
                                                           fac, psd, ldp);

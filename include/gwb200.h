@@ -142,7 +142,7 @@ GWB_API int gwb_frames(const float* x, long long ldx, int rows, long long start,
                        const long long* starts, int nfr, int L, const float* w, float* out, long long ldo, void* stream);
 /* Welch average over nfr frames of each row's rFFT X (complex, row stride ldx): p = |X dt|^2 in float32, bins 0 and
  * nbin-1 halved, then the median (mean of the two middle values for an even count) divided by bias, or the mean;
- * times fac. Replaces welch's per-row loop (gpu_prep.py:107-124). nfr <= 256. */
+ * times fac. Replaces welch's per-row loop (gpu_prep.py:107-124). nfr <= 256 (mean), <= 8192 (median). */
 GWB_API int gwb_welch_avg(const float* X, long long ldx, int rows, int nfr, int nbin, float dt, int median,
                           double bias, float fac, float* psd, long long ldp, void* stream);
 /* np.interp of each PSD row (float64) from k df_old onto k df_new, k < nnew; replaces gpu_prep.interpolate

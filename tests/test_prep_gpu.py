@@ -45,6 +45,13 @@ def test_welch_interp_truncation_against_oracle():
     p, _ = gpu_prep.welch(None, torch.from_numpy(x).cuda(), 4096, 2048, 1 / 2048., num_segments=16)
     pr, _ = op.welch(x, 4096, 2048, 1 / 2048., num_segments=16)
     assert np.abs(p.cpu().numpy() / pr - 1).max() < 2e-5
+    # many frames (the 4 s estimate over a long segment): the shared-memory sort, series bias and log 2 bias
+    for nfr, even in ((601, False), (1200, True)):
+        n = 2048 * (nfr + 1)
+        y = rng.standard_normal((2, n)).astype(np.float32)
+        pb, _ = gpu_prep.welch(None, torch.from_numpy(y).cuda(), 4096, 2048, 1 / 2048., num_segments=nfr)
+        pbr, _ = op.welch(y, 4096, 2048, 1 / 2048., num_segments=nfr)
+        assert np.abs(pb.cpu().numpy() / pbr - 1).max() < 2e-5, (nfr, even)
     q = gpu_prep.interpolate(None, torch.from_numpy(pr).cuda(), 0.5, 1 / 64., 4097 * 8)
     qr = op.interpolate(pr, 0.5, 1 / 64., 4097 * 8)
     assert np.array_equal(q.cpu().numpy(), qr)
