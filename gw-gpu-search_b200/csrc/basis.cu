@@ -206,72 +206,110 @@ __device__ __forceinline__ float ld_as_float(const void* p, long long i, int for
 // windowed output) exceeds thr2 become candidates, written contiguously in window order at an offset taken with one
 // atomic per row; the row's candidates are cut into groups of at most 8 (one group = one exact-stage work unit) and
 // the row is registered once as an edges unit. The rebuilt complex SNR Are[row].Z[:, col] + i Aim[row].Z[:, col]
-// (fp_filter.py:760-764) is computed for each candidate; for the split form the hi and lo parts are summed.
+// (fp_filter.py:760-764) is computed for each candidate; for the split form the hi and lo parts are summed. With
+// ecut > 0 the reference's split (fp_filter.py:769-770) divides the windows: rebuilt SNR >= ecut go to the exact
+// stage as above, the others above rthr become rebuilt peaks (their own list, counters[4], unit -1), which keep the
+// rebuilt SNR and phase.
 __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __restrict__ iw, long long ldv, int n,
-                              int nw, float thr2, long long a0, int row0, int seg, const void* __restrict__ Are,
-                              const void* __restrict__ Aim, const void* __restrict__ Are_lo,
-                              const void* __restrict__ Aim_lo, long long lda, const void* __restrict__ Z,
-                              const void* __restrict__ Zlo, long long ldz, int Kp, int kh, int form,
-                              const float* __restrict__ rowscale, GwbCand* __restrict__ cands,
+                              int nw, float thr2, float ecut, float rthr, long long a0, int row0, int seg,
+                              const void* __restrict__ Are, const void* __restrict__ Aim,
+                              const void* __restrict__ Are_lo, const void* __restrict__ Aim_lo, long long lda,
+                              const void* __restrict__ Z, const void* __restrict__ Zlo, long long ldz, int Kp, int kh,
+                              int form, const float* __restrict__ rowscale, GwbCand* __restrict__ cands,
                               int cand_cap, GwbGroup* __restrict__ groups, int group_cap, GwbUnit* __restrict__ units,
-                              int unit_cap, int32_t* __restrict__ counters) {
+                              int unit_cap, GwbCand* __restrict__ rebuilt, int rebuilt_cap,
+                              int32_t* __restrict__ counters) {
     const int row = blockIdx.x;
     if (row >= n) return;
     const float* v = vw + (long long)row * ldv;
-    __shared__ int s_cnt, s_base, s_unit, s_gbase;
+    // class of a window: 1 = exact-stage candidate (rebuilt SNR >= ecut), 2 = rebuilt peak (below ecut, above rthr)
+    auto cls = [&](int w) -> int {
+        const float x = v[w];
+        if (!(x > thr2)) return 0;
+        const float a = sqrtf(x);
+        return a >= ecut ? 1 : (a > rthr ? 2 : 0);
+    };
+    __shared__ int s_cnt[2], s_base, s_unit, s_gbase, s_rbase, s_ok;
     __shared__ int s_warp[kThreads / 32];
-    if (threadIdx.x == 0) s_cnt = 0;
+    if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
     __syncthreads();
-    // count
-    int cnt = 0;
-    for (int w = threadIdx.x; w < nw; w += blockDim.x) cnt += v[w] > thr2;
+    int ce = 0, cr = 0;
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+        const int c = cls(w);
+        ce += c == 1;
+        cr += c == 2;
+    }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&s_cnt, cnt);
-    __syncthreads();
-    const int total = s_cnt;
-    if (total == 0) return;
-    const int ng = (total + 7) / 8;
-    if (threadIdx.x == 0) {
-        s_base = atomicAdd(&counters[0], total);
-        s_gbase = atomicAdd(&counters[1], ng);
-        s_unit = atomicAdd(&counters[2], 1);
-        if (s_base + total > cand_cap || s_gbase + ng > group_cap || s_unit >= unit_cap) atomicOr(&counters[3], 1);
-        else units[s_unit] = GwbUnit{row0 + row, seg, s_base, total};
+    for (int off = 16; off > 0; off >>= 1) {
+        ce += __shfl_down_sync(0xffffffffu, ce, off);
+        cr += __shfl_down_sync(0xffffffffu, cr, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&s_cnt[0], ce);
+        atomicAdd(&s_cnt[1], cr);
     }
     __syncthreads();
-    if (s_base + total > cand_cap || s_gbase + ng > group_cap || s_unit >= unit_cap) return;
-    for (int g = threadIdx.x; g < ng; g += blockDim.x)
-        groups[s_gbase + g] = GwbGroup{s_unit, s_base + 8 * g, min(8, total - 8 * g), 0};
-    // ordered write: chunks of blockDim windows, prefix over warps
-    int written = 0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int w0 = 0; w0 < nw; w0 += blockDim.x) {
-        const int w = w0 + threadIdx.x;
-        const bool hit = w < nw && v[w] > thr2;
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (lane == 0) s_warp[warp] = __popc(m);
-        __syncthreads();
-        int before = 0;
-        for (int k = 0; k < warp; ++k) before += s_warp[k];
-        int chunk_total = 0;
-        for (int k = 0; k < kThreads / 32; ++k) chunk_total += s_warp[k];
-        if (hit) {
-            const int pos = s_base + written + before + __popc(m & ((1u << lane) - 1));
-            const int col = iw[(long long)row * ldv + w];
-            GwbCand cd;
-            cd.row = row0 + row;
-            cd.seg = seg;
-            cd.sample = (int)(a0 + col);
-            cd.window = w;
-            cd.approx = sqrtf(v[w]);
-            cd.zr = 0.f;
-            cd.zi = 0.f;
-            cd.unit = s_unit;
-            cands[pos] = cd;
+    const int total = s_cnt[0], rtotal = s_cnt[1];
+    if (total == 0 && rtotal == 0) return;
+    const int ng = (total + 7) / 8;
+    if (threadIdx.x == 0) {
+        int ok = 0;
+        if (total > 0) {
+            s_base = atomicAdd(&counters[0], total);
+            s_gbase = atomicAdd(&counters[1], ng);
+            s_unit = atomicAdd(&counters[2], 1);
+            if (s_base + total > cand_cap || s_gbase + ng > group_cap || s_unit >= unit_cap) atomicOr(&counters[3], 1);
+            else {
+                units[s_unit] = GwbUnit{row0 + row, seg, s_base, total};
+                ok |= 1;
+            }
         }
-        written += chunk_total;
-        __syncthreads();
+        if (rtotal > 0) {
+            s_rbase = atomicAdd(&counters[4], rtotal);
+            if (rebuilt == nullptr || s_rbase + rtotal > rebuilt_cap) atomicOr(&counters[3], 1);
+            else ok |= 2;
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    const int okf = s_ok;
+    if (okf & 1)
+        for (int g = threadIdx.x; g < ng; g += blockDim.x)
+            groups[s_gbase + g] = GwbGroup{s_unit, s_base + 8 * g, min(8, total - 8 * g), 0};
+    // ordered writes (window order within the row): chunks of blockDim windows, prefix over warps
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int want = 1; want <= 2; ++want) {
+        if (!(okf & want)) continue;
+        GwbCand* out = want == 1 ? cands + s_base : rebuilt + s_rbase;
+        const int unit = want == 1 ? s_unit : -1;
+        int written = 0;
+        for (int w0 = 0; w0 < nw; w0 += blockDim.x) {
+            const int w = w0 + threadIdx.x;
+            const bool hit = w < nw && cls(w) == want;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) s_warp[warp] = __popc(m);
+            __syncthreads();
+            int before = 0;
+            for (int k = 0; k < warp; ++k) before += s_warp[k];
+            int chunk_total = 0;
+            for (int k = 0; k < kThreads / 32; ++k) chunk_total += s_warp[k];
+            if (hit) {
+                const int pos = written + before + __popc(m & ((1u << lane) - 1));
+                const int col = iw[(long long)row * ldv + w];
+                GwbCand cd;
+                cd.row = row0 + row;
+                cd.seg = seg;
+                cd.sample = (int)(a0 + col);
+                cd.window = w;
+                cd.approx = sqrtf(v[w]);
+                cd.zr = 0.f;
+                cd.zi = 0.f;
+                cd.unit = unit;
+                out[pos] = cd;
+            }
+            written += chunk_total;
+            __syncthreads();
+        }
     }
     // rebuilt complex SNR of each candidate of this row: one warp per candidate, lanes over K
     auto ldz_ = [&](long long c, int col) {
@@ -281,8 +319,10 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
         return ld_as_float(hi, (long long)row * lda + c, form) +
                (form == 2 ? ld_as_float(lo, (long long)row * lda + c, 2) : 0.f);
     };
-    for (int i = warp; i < total; i += kThreads / 32) {
-        const int col = cands[s_base + i].sample - (int)a0;
+    const int ne = (okf & 1) ? total : 0, nr = (okf & 2) ? rtotal : 0;
+    for (int i = warp; i < ne + nr; i += kThreads / 32) {
+        GwbCand* cd = i < ne ? cands + s_base + i : rebuilt + s_rbase + (i - ne);
+        const int col = cd->sample - (int)a0;
         float zr = 0.f, zi = 0.f;
         if (kh > 0) {       // compact operands: A = [ReA | ImA], Z = [ReZ ; ImZ]
             for (int c = lane; c < kh; c += 32) {
@@ -305,8 +345,8 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
         }
         if (lane == 0) {
             const float rs = rowscale ? rowscale[row] : 1.f;     // fp8: the row scale of A
-            cands[s_base + i].zr = zr * rs;
-            cands[s_base + i].zi = zi * rs;
+            cd->zr = zr * rs;
+            cd->zi = zi * rs;
         }
     }
 }
@@ -396,11 +436,12 @@ int gwb_stacked_a8(const float* A, long long lda, int n, int r, const double* nr
     return GWB_OK;
 }
 
-int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2, long long a0,
-                       int row0, int seg, const void* Are, const void* Aim, const void* Are_lo, const void* Aim_lo,
-                       long long lda, const void* Z, const void* Zlo, long long ldz, int Kp, int kh, int form,
-                       const float* rowscale, GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap,
-                       GwbUnit* units, int unit_cap, int32_t* counters, void* stream) {
+int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2, float ecut,
+                       float rthr, long long a0, int row0, int seg, const void* Are, const void* Aim,
+                       const void* Are_lo, const void* Aim_lo, long long lda, const void* Z, const void* Zlo,
+                       long long ldz, int Kp, int kh, int form, const float* rowscale, GwbCand* cands, int cand_cap,
+                       GwbGroup* groups, int group_cap, GwbUnit* units, int unit_cap, GwbCand* rebuilt,
+                       int rebuilt_cap, int32_t* counters, void* stream) {
     using namespace gwb;
     GWB_CHECK_ARG(vw && iw && Are && (kh > 0 || Aim) && Z && cands && groups && units && counters, GWB_ERR_ARG,
                   "select_windows: null pointer");
@@ -410,10 +451,12 @@ int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n,
     GWB_CHECK_ARG(n > 0 && nw >= 0 && ldv >= nw && Kp > 0 && lda >= Kp, GWB_ERR_SHAPE, "select_windows: n=%d nw=%d", n,
                   nw);
     if (nw == 0) return GWB_OK;
-    select_kernel<<<n, kThreads, 0, (cudaStream_t)stream>>>(vw, iw, ldv, n, nw, thr2, a0, row0, seg, Are, Aim, Are_lo,
-                                                            Aim_lo, lda, Z, Zlo, ldz, Kp, kh, form,
+    GWB_CHECK_ARG(ecut <= 0.f || (rebuilt && rebuilt_cap > 0), GWB_ERR_ARG, "select_windows: no rebuilt-peak list");
+    select_kernel<<<n, kThreads, 0, (cudaStream_t)stream>>>(vw, iw, ldv, n, nw, thr2, ecut, rthr, a0, row0, seg, Are,
+                                                            Aim, Are_lo, Aim_lo, lda, Z, Zlo, ldz, Kp, kh, form,
                                                             form == 4 ? rowscale : nullptr, cands, cand_cap, groups,
-                                                            group_cap, units, unit_cap, counters);
+                                                            group_cap, units, unit_cap, rebuilt, rebuilt_cap,
+                                                            counters);
     GWB_LAUNCH_CHECK("select_kernel");
     return GWB_OK;
 }

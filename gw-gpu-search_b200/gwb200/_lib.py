@@ -51,8 +51,8 @@ SIGNATURES = {
     'gwb_basis_pack': [_P, _LL, _I, _I, _I, _LL, _LL, _P, _I, _P, _P, _LL, _P],
     'gwb_stacked_a': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _I, _I, _P, _P, _P, _P, _LL, _P],
     'gwb_stacked_a8': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _P, _LL, _P, _P],
-    'gwb_select_windows': [_P, _P, _LL, _I, _I, _F, _LL, _I, _I, _P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _I, _P,
-                           _P, _I, _P, _I, _P, _I, _P, _P],
+    'gwb_select_windows': [_P, _P, _LL, _I, _I, _F, _F, _F, _LL, _I, _I, _P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _I,
+                           _P, _P, _I, _P, _I, _P, _I, _P, _I, _P, _P],
     'gwb_snr_grad': [_P, _I, _P, _LL, _P, _LL, _I, _D, _I, _D, _I, _I, _P, _LL, _P],
     'gwb_phase_metric': [_P, _I, _P, _LL, _I, _D, _I, _D, _P, _P],
     'gwb_refine_step': [_P, _P, _LL, _P, _P, _I, _P, _P],
@@ -77,6 +77,9 @@ SIGNATURES = {
     'gwb_whiten': [_P, _I, _P, _F, _F, _P],
     'gwb_above': [_P, _LL, _LL, _I, _F, _F, _P, _P, _I, _P, _P],
     'gwb_apply_gates': [_P, _LL, _P, _I, _P],
+    'gwb_consolidate': [_I, _I, _P, _P, _P, _P, _P, _I, _D, _D, _F, _F, _D, _I, _F, _P, _I, _D, _I, _P, _I, _P, _I,
+                        _P, _LL, _P, _P, _P],
+    'gwb_consolidate_work_bytes': [_I, _I],
     'gwb_highpass': [],
     'gwb_resample': [],
 }
@@ -108,6 +111,7 @@ def load():
             f = getattr(lib, name)
             f.argtypes = args
             f.restype = ctypes.c_int
+        lib.gwb_consolidate_work_bytes.restype = ctypes.c_longlong
         _lib = lib
     return _lib
 

@@ -40,6 +40,10 @@ class FilterConfig:
     form: str = 'bf16x3'
     cand_cap: int = 1 << 21
     seg_batch: int = 16
+    # the reference's --exact-snr split (fp_filter.py:769-781): windows whose rebuilt SNR is below
+    # exact_snr (1 - margin) skip the exact stage and keep their rebuilt SNR and phase when above snr_threshold;
+    # 0 sends every candidate to the exact stage (PyCBC-equivalent values)
+    exact_snr: float = 0.0
 
 
 class Bank:
@@ -127,7 +131,7 @@ class MatchedFilter:
         self.cands = torch.empty(cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
         self.groups = torch.empty(cap * _exact.GROUP.itemsize, dtype=torch.uint8, device=device)
         self.units = torch.empty(cap * _exact.UNIT.itemsize, dtype=torch.uint8, device=device)
-        self.counters = torch.zeros(4, dtype=torch.int32, device=device)
+        self.counters = torch.zeros(5, dtype=torch.int32, device=device)
         self.B = cfg.nbins
         self.E = torch.empty((cap, self.B + 1), dtype=torch.int32, device=device)
         self.nchunk = _lib.load().gwb_exact_chunks(bank.flen, bank.kmin)
@@ -137,6 +141,11 @@ class MatchedFilter:
         self.peaks = torch.empty(cap * _exact.PEAK.itemsize, dtype=torch.uint8, device=device)
         margin = max(cfg.margin, cfg.screen_margin) if self.fp8 else cfg.margin
         self.thr2 = float((cfg.snr_threshold * (1 - margin)) ** 2)
+        assert not (self.fp8 and cfg.exact_snr > 0), 'the fp8 screen keeps no rebuilt values: use exact_snr = 0'
+        self.ecut = float(np.float32(cfg.exact_snr * (1 - cfg.margin))) if cfg.exact_snr > 0 else 0.0
+        self.rthr = float(np.float32(cfg.snr_threshold))
+        self.rebuilt = (torch.empty(cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
+                        if cfg.exact_snr > 0 else None)
         self.kernel_launches = 0
         self.fft_launches = 0
         # set to {} to record CUDA events per (tile, segment): e0 basis series e3 stacked A e1 GEMM e2
@@ -190,10 +199,11 @@ class MatchedFilter:
         f = fp_filter.FORMS[self.form]
         cap = self.cfg.cand_cap
         _lib.call('gwb_select_windows', _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), n, self.nw, self.thr2,
-                  self.a0, b.row0[t], seg, _lib.ptr(self.Are), _lib.ptr(self.Aim), _lib.ptr(self.Are_lo),
-                  _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), K,
-                  Kh, f, _lib.ptr(self.sa), _lib.ptr(self.cands), cap, _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap,
-                  _lib.ptr(self.counters), _lib.stream_ptr())
+                  self.ecut, self.rthr, self.a0, b.row0[t], seg, _lib.ptr(self.Are), _lib.ptr(self.Aim),
+                  _lib.ptr(self.Are_lo), _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z),
+                  _lib.ptr(self.Zlo), self.Z.stride(0), K, Kh, f, _lib.ptr(self.sa), _lib.ptr(self.cands), cap,
+                  _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap, _lib.ptr(self.rebuilt),
+                  cap if self.rebuilt is not None else 0, _lib.ptr(self.counters), _lib.stream_ptr())
         if self.fused:
             nb = -(-r // self.fws.wrows)
             self.kernel_launches += 2 * nb + 3  # two basis passes per row batch, stacked A, GEMM, selection
@@ -253,7 +263,8 @@ class MatchedFilter:
 
     def results(self, sig=None):
         """Copy the step's candidates and exact values to the host; returns a dict of numpy arrays (all candidates
-        and the kept peaks with exact SNR above the threshold)."""
+        and the kept peaks with exact SNR above the threshold; with exact_snr > 0 also the rebuilt peaks, whose SNR
+        and phase are the rebuilt ones: `rebuilt`, GwbCand records)."""
         c = self.counters.cpu().numpy()
         if c[3]:
             raise _lib.GwbError('select', _lib.GWB_ERR_CAPACITY, 'candidate capacity %d exceeded' % self.cfg.cand_cap)
@@ -261,4 +272,7 @@ class MatchedFilter:
         cands = _exact.from_dev(self.cands, _exact.CAND, n)
         peaks = _exact.from_dev(self.peaks, _exact.PEAK, n)
         keep = peaks['snr'] > self.cfg.snr_threshold
-        return dict(n_candidates=n, n_units=int(c[2]), n_groups=int(c[1]), cands=cands, peaks=peaks, keep=keep)
+        nr = int(c[4])
+        rebuilt = _exact.from_dev(self.rebuilt, _exact.CAND, nr) if self.rebuilt is not None else np.zeros(0, _exact.CAND)
+        return dict(n_candidates=n, n_units=int(c[2]), n_groups=int(c[1]), cands=cands, peaks=peaks, keep=keep,
+                    rebuilt=rebuilt, n_rebuilt=nr)

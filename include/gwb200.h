@@ -294,15 +294,21 @@ GWB_API int gwb_refine_step(const double* params, const double* res, long long l
 /* Window candidates of one (tile, segment) (fp_filter.py:745-764): rows i < n whose windowed maximum vw (the fused
  * GEMM output with group = cw/128) exceeds thr2 become GwbCand records (row0 + i, seg, a0 + iw, window, sqrt(vw),
  * rebuilt z), appended per row in window order; each row with candidates becomes one GwbUnit and groups of <= 8
- * candidates become GwbGroup records. counters[0..3]: candidates, groups, units, overflow flag (1 when a capacity was
- * exceeded; the row is then dropped). Operands in the layout the GEMM used: stacked Are/Aim (kh = 0, K = Kp) or
- * compact A = [ReA | ImA] with Z = [ReZ ; ImZ] (kh > 0, Kp = 2 kh); form as gwb_basis_pack, plus 4 = fp8 e4m3
- * (compact only), whose rebuilt z is multiplied by rowscale[i] (gwb_stacked_a8's sa; NULL for the other forms). */
+ * candidates become GwbGroup records. With ecut > 0, the reference's exact/rebuilt split (fp_filter.py:769-770,
+ * --exact-snr: ecut = exact_snr (1 - margin), rthr = the SNR threshold, both compared in float32 with sqrt(vw)):
+ * only windows with sqrt(vw) >= ecut are exact-stage candidates as above; those below ecut with sqrt(vw) > rthr are
+ * appended to `rebuilt` (unit -1) and keep their rebuilt SNR and z. ecut <= 0: every window above thr2 is a
+ * candidate (rebuilt may be NULL). counters[0..4]: candidates, groups, units, overflow flag (1 when a capacity was
+ * exceeded; the row's list is then dropped), rebuilt peaks. Operands in the layout the GEMM used: stacked Are/Aim
+ * (kh = 0, K = Kp) or compact A = [ReA | ImA] with Z = [ReZ ; ImZ] (kh > 0, Kp = 2 kh); form as gwb_basis_pack,
+ * plus 4 = fp8 e4m3 (compact only), whose rebuilt z is multiplied by rowscale[i] (gwb_stacked_a8's sa; NULL for the
+ * other forms). */
 GWB_API int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2,
-                               long long a0, int row0, int seg, const void* Are, const void* Aim, const void* Are_lo,
-                               const void* Aim_lo, long long lda, const void* Z, const void* Zlo, long long ldz, int Kp,
-                               int kh, int form, const float* rowscale, GwbCand* cands, int cand_cap, GwbGroup* groups,
-                               int group_cap, GwbUnit* units, int unit_cap, int32_t* counters, void* stream);
+                               float ecut, float rthr, long long a0, int row0, int seg, const void* Are,
+                               const void* Aim, const void* Are_lo, const void* Aim_lo, long long lda, const void* Z,
+                               const void* Zlo, long long ldz, int Kp, int kh, int form, const float* rowscale,
+                               GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units,
+                               int unit_cap, GwbCand* rebuilt, int rebuilt_cap, int32_t* counters, void* stream);
 /* Chi-squared bin edges per unit (multi_filter.edges_per_template, pipeline/multi_filter.py:264-282; the fused
  * kernel of chisq_edges.py:92-143): E[u, 0..B] int32, B >= max nbins. Unit count = min(*ucount, umax) when ucount is
  * not NULL, else umax. nbins and kmax are indexed by the unit's row. offset_mode 1 reproduces the reference's
@@ -324,6 +330,31 @@ GWB_API int gwb_exact_chunks(int flen, int kmin);
 GWB_API int gwb_exact_finalize(const GwbCand* cands, const int32_t* ccount, int cmax, const GwbUnit* units,
                                const int32_t* E, int B, const int32_t* nbins, int kmin, int flen, const float* slots,
                                const double* sig, long long ldsig, double df, GwbPeak* out, void* stream);
+
+/* ---- consolidation (downstream of the exact stage) -------------------------------------------------------- */
+/* Workspace bytes of gwb_consolidate for n items and nwin keep-loudest windows. */
+GWB_API long long gwb_consolidate_work_bytes(int n, int nwin);
+/* Keep mask of one dataset's items (device arrays), in one of two modes:
+ *   mode 0, consolidate (pipeline/fp_filter.py:629-661, pycbc's EventManager.consolidate_events over the whole
+ *     bank): stat = PyCBC's newsnr of snr and chisq / max(dof, 1) in float64 (fp_filter.py:250), or snr when
+ *     use_chisq == 0; kept: stat >= newsnr_thr or exempt (has_exempt and snr >= exempt_snr, float32);
+ *   mode 1, pre_keep (fp_filter.py:663-695): items with snr >= exact_cut (float32) are kept; of the rest, those with
+ *     snr > thr pass the same cut with stat = snr, and with floor_in given (nfloor windows) those at or below the
+ *     floor of their window are dropped.
+ * Both: t = gps_start + ti / sr (ti int64 samples since the dataset's start, float64), and the gate veto drops
+ * |t - g| <= w + taper + 0.5 for each of ng gates (device (ng, 3) float64: g, w, taper). With keep_interval > 0 the
+ * non-exempt kept items are ranked in windows trunc(rint((t - gps_start) sr) / (keep_interval sr)) by stat
+ * descending, ties to the smaller order key (position when order is NULL; keys must be distinct), and only the
+ * keep_num first stay. floor_out (nwin doubles, may be NULL): the keep_num-th stat of every window that has at least
+ * keep_num ranked items, -inf elsewhere (the reference's --pre-consolidate floor). keep: n bytes, 1 = kept.
+ * status[0] (device int32, cleared here) becomes 1 when an item's window lies outside [0, nwin): the mask is then not
+ * valid. work: gwb_consolidate_work_bytes(n, nwin) bytes. */
+GWB_API int gwb_consolidate(int mode, int n, const float* snr, const float* chisq, const int32_t* dof,
+                            const long long* ti, const long long* order, int use_chisq, double gps_start, double sr,
+                            float exact_cut, float thr, double newsnr_thr, int has_exempt, float exempt_snr,
+                            const double* gates, int ng, double keep_interval, int keep_num, const double* floor_in,
+                            int nfloor, double* floor_out, int nwin, void* work, long long work_bytes, uint8_t* keep,
+                            int32_t* status, void* stream);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,8 @@ Each fixture holds the inputs and the reference's outputs for one call. The refe
                      prepared namespace, as the reference's tests/test_prekeep.py does), torch on the CPU
   edges_exact.npz    pipeline/multi_filter.py edges_per_template, pipeline/chisq_edges.py edges_blocked (numpy) and
                      pipeline/exact_stage.py ExactStage.evaluate on the dense numpy backend
+  consolidate.npz    pipeline/fp_filter.py closures consolidate and pre_keep (source text run with exec, torch on the
+                     CPU); PyCBC is absent here, so its newsnr is the oracle's restatement (oracle/consolidate.py)
 The tests compare the oracle (oracle/) against these files on the CPU, and the CUDA kernels against the oracle and
 the files on the GPU. Nothing at test time reads the reference."""
 import argparse
@@ -237,7 +239,94 @@ def gen_edges_exact():
     print('edges_exact', E_full.shape, len(prow), 'peaks')
 
 
-GENERATORS = {'fp_gemm': gen_fp_gemm, 'prep': gen_prep, 'filt': gen_filt, 'edges_exact': gen_edges_exact}
+def _closure(name):
+    """Source of one closure of fp_filter.py's main (indentation-delimited), dedented."""
+    import textwrap
+    src = open(os.path.join(_REF['pipeline'], 'fp_filter.py')).read().splitlines()
+    i = next(k for k, l in enumerate(src) if l.strip().startswith('def %s(' % name))
+    ind = len(src[i]) - len(src[i].lstrip())
+    out = [src[i]]
+    for l in src[i + 1:]:
+        if l.strip() and len(l) - len(l.lstrip()) <= ind:
+            break
+        out.append(l)
+    return textwrap.dedent('\n'.join(out))
+
+
+def gen_consolidate():
+    """Seeded cases of the reference's consolidate (keep mask, floor) and pre_keep (mask): SNRs rounded to 0.01 so
+    that ties are frequent, windows crowded (20 s spans) or sparse (800 s), 0-3 gates, exempt SNR 5 or none, keep
+    1-6 or 30 loudest per 1.072 s window or no ranking, with and without chi-squared."""
+    import time
+    import torch
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.consolidate import newsnr
+    src_c, src_p = _closure('consolidate'), _closure('pre_keep')
+    rng = np.random.default_rng(30)
+    sr, gps0 = 2048.0, 1380077576.0
+    seg_start = [0, 1636352]
+    out = {}
+    nc = npk = 0
+    for trial in range(60):
+        interval = None if trial % 7 == 3 else 1.072
+        num = int(rng.choice([1, 2, 3, 5, 6, 30]))
+        exempt = [5.0, None][trial % 2]
+        do_chisq = trial % 11 != 5
+        a = types.SimpleNamespace(pre_consolidate=True, exact_snr=5.5, margin=0.04, consolidate_exempt_snr=exempt)
+        klo = types.SimpleNamespace(newsnr_threshold=4.0, keep_loudest_interval=interval, keep_loudest_num=num,
+                                    keep_loudest_stat='newsnr')
+        g = dict(time=time, a=a, klo=klo, sr=sr, thr=4.0, T={}, dev='cpu', torch=torch, np=np, newsnr=newsnr,
+                 do_chisq=do_chisq)
+        exec(src_c, g)
+        exec(src_p, g)
+        gates = [(gps0 + float(rng.uniform(0, 1500)), 0.25, 0.25) for _ in range(int(rng.integers(0, 4)))]
+        span = float(rng.choice([20.0, 800.0]))
+        # consolidate: peaks of one dataset, rebuilt (dof 0) and exact (dof 30) mixed
+        n = int(rng.choice([0, 1, 7, 300, 3000]))
+        ti = rng.integers(0, int(span * sr), n) + seg_start[int(rng.integers(0, 2))]
+        t = gps0 + ti / sr
+        snr = np.round(rng.uniform(3.84, 9.0, n), 2).astype(np.float32)
+        isex = rng.uniform(size=n) < 0.4
+        chi = np.where(isex, np.round(rng.uniform(0, 80, n), 1), 0).astype(np.float32)
+        dof = np.where(isex, 30, 0).astype(np.int32)
+        m = dict(gps_start=gps0, gates=gates,
+                 out=dict(snr=[snr], chi=[chi], dof=[dof], t=[t], idx=[np.arange(n)]))
+        g['consolidate'](m)
+        kept = np.concatenate(m['out']['idx']) if m['out']['idx'] else np.zeros(0, np.int64)
+        keep = np.zeros(n, bool)
+        keep[kept] = True
+        floor = m['floor'].numpy() if 'floor' in m else np.zeros(0)
+        pre = 'c%d_' % nc
+        nc += 1
+        out.update({pre + 'ti': ti, pre + 'snr': snr, pre + 'chi': chi, pre + 'dof': dof,
+                    pre + 'gates': np.array(gates, np.float64).reshape(-1, 3),
+                    pre + 'par': np.array([interval or 0.0, num, -1.0 if exempt is None else exempt, do_chisq,
+                                           4.0]),
+                    pre + 'keep': keep, pre + 'floor': floor})
+        # pre_keep on a new part of the same dataset, against the floor that consolidate left
+        s = int(rng.integers(0, 2))
+        k = int(rng.choice([0, 5, 500, 3000]))
+        samp = rng.integers(0, int(span * sr), k).astype(np.int32)
+        apx = np.round(rng.uniform(3.84, 7.0, k), 2).astype(np.float32)
+        mp = dict(gps_start=gps0, seg_start=seg_start, gates=gates)
+        if 'floor' in m and trial % 3:
+            mp['floor'] = m['floor']
+        kp = g['pre_keep'](mp, s, torch.from_numpy(samp), torch.from_numpy(apx)).numpy()
+        pre = 'p%d_' % npk
+        npk += 1
+        out.update({pre + 'ti': samp.astype(np.int64) + seg_start[s], pre + 'apx': apx,
+                    pre + 'gates': np.array(gates, np.float64).reshape(-1, 3),
+                    pre + 'par': np.array([interval or 0.0, num, -1.0 if exempt is None else exempt, 5.5, 0.04, 4.0,
+                                           4.0]),
+                    pre + 'floor': mp['floor'].numpy() if 'floor' in mp else np.zeros(0), pre + 'has_floor':
+                    np.array('floor' in mp), pre + 'keep': kp})
+    out.update(n_cons=nc, n_pre=npk, sr=sr, gps0=gps0)
+    np.savez_compressed(os.path.join(HERE, 'consolidate.npz'), **out)
+    print('consolidate', nc, 'consolidate cases,', npk, 'pre_keep cases')
+
+
+GENERATORS = {'fp_gemm': gen_fp_gemm, 'prep': gen_prep, 'filt': gen_filt, 'edges_exact': gen_edges_exact,
+              'consolidate': gen_consolidate}
 
 
 def main():

@@ -131,3 +131,44 @@ def test_fp8_screen_keeps_the_fp32_peaks():
     inj_row = int(np.flatnonzero(B.order == inj['index'])[0])
     best = max((v, k) for k, v in out['fp8'].items() if k[0] == inj_row and k[1] == inj['seg'])
     assert abs(best[0] - inj['snr']) < 3.0
+
+
+@pytest.mark.parametrize('form', ['f16', 'f32'])
+def test_exact_snr_split(form):
+    """The reference's --exact-snr split (fp_filter.py:769-781) at threshold 4 and exact cut 5.5: the exact-stage
+    candidates are the all-exact run's candidates with rebuilt SNR >= 5.5 (1 - margin), with identical exact values;
+    the rebuilt peaks are the others above 4, with the same rebuilt SNR and z."""
+    from gwb200 import fp_filter, pipeline
+    bank, D, IP, kmin, inj = _case()
+    Dd, IPd = torch.from_numpy(D).cuda(), torch.from_numpy(IP).cuda()
+    sw, isw = fp_filter.derive_sw(IPd)
+    out = {}
+    for es in (0.0, 5.5):
+        cfg = pipeline.FilterConfig(tile=24, eps=1e-3, nbins=16, snr_threshold=4.0, margin=0.04, form=form,
+                                    cand_cap=1 << 18, exact_snr=es)
+        B = pipeline.Bank(bank, FLEN, DF, sw, cfg)
+        mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg)
+        mf.step(Dd, IPd, isw)
+        torch.cuda.synchronize()
+        out[es] = mf.results()
+    full, split = out[0.0], out[5.5]
+    cut = np.float32(5.5 * 0.96)
+    key = lambda c: list(zip(c['row'].tolist(), c['seg'].tolist(), c['sample'].tolist()))
+    c0, p0 = full['cands'], full['peaks']
+    ex = c0['approx'] >= cut
+    rb = ~ex & (c0['approx'] > np.float32(4.0))
+    assert split['n_rebuilt'] > 100 and ex.sum() > 0
+    i_full = {k: i for i, k in enumerate(key(c0))}
+    ks = key(split['cands'])
+    assert sorted(ks) == sorted(k for k, e in zip(key(c0), ex) if e)
+    for j, k in enumerate(ks):
+        i = i_full[k]
+        for f in ('zr', 'zi', 'pw', 'snr', 'chisq', 'newsnr', 'dof'):
+            assert split['peaks'][f][j] == p0[f][i], (k, f)
+    kr = key(split['rebuilt'])
+    assert sorted(kr) == sorted(k for k, e in zip(key(c0), rb) if e)
+    for j, k in enumerate(kr):
+        i = i_full[k]
+        for f in ('approx', 'zr', 'zi'):
+            assert split['rebuilt'][f][j] == c0[f][i], (k, f)
+    assert (split['rebuilt']['unit'] == -1).all()
