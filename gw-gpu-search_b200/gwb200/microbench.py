@@ -4,7 +4,7 @@
     python -m gwb200.microbench basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5] [--wrows 0,4,8]
     python -m gwb200.microbench exact [--groups 512] [--peaks 1] [--tlen 1048576] [--reps 5]
     python -m gwb200.microbench adjoint [--triggers 4096] [--reps 5]
-    python -m gwb200.microbench c4 [--segments 300] [--batch 32] [--form f16] [--no-graph]
+    python -m gwb200.microbench c4 [--segments 300] [--batch 32] [--form f16] [--no-graph] [--production]
 
 Run from gw-gpu-search_b200/ (or with it on sys.path). Operand sizes default to one (tile, chunk) of the C2
 workload; inputs are larger than L2 where the real ones are."""
@@ -212,6 +212,12 @@ def c4(a):
         segs.append(dict(x=x.to(torch.float32).contiguous(), start_gps=gps, det=i % 2))
         gps += int(n_s) + 100
     cfg = pipeline.FilterConfig(form=a.form)
+    co = None
+    if a.production:
+        # production's selection (threshold 4, exact stage above 5.5 (1 - margin), the rest rebuilt) and
+        # consolidation (newsnr 4, 30 loudest per 1.072 s, SNR >= 5 exempt): ops/run_prod_o4a.sh's flags
+        cfg = pipeline.FilterConfig(form=a.form, snr_threshold=4.0, exact_snr=5.5, rebuilt_cap=1 << 24)
+        co = sg.Consolidation()
     # SVD metric of the run from a first batch of chunks, then the bank (as bench.py builds it)
     from . import gpu_prep
     first = [s for s in segs if s['x'].shape[0] >= tlen][:a.batch]
@@ -226,8 +232,8 @@ def c4(a):
     B = pipeline.Bank(bank, flen, df, sw, cfg)
     torch.cuda.synchronize()
     bank_s = time.perf_counter() - t_b
-    F = sg.SegmentFilter(B, cfg, batch=a.batch, isw=isw, graph=not a.no_graph)
-    F.run(segs[:2], gate=False)            # warm-up (captures the graph)
+    F = sg.SegmentFilter(B, cfg, batch=a.batch, isw=isw, graph=not a.no_graph, consolidation=co)
+    F.run(first[:1], gate=False)           # warm-up on one chunk (captures the graph outside the timed run)
     torch.cuda.synchronize()
     e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
@@ -249,6 +255,16 @@ def c4(a):
         found += int(np.any((segi == i) & (np.abs(t_peak - t_inj) < 0.1)))
     gated = sum(1 for (i, *_rest) in glitches if res['gates'][i])
     weeks = res['analysed_s'] / (2 * 604800.0)
+    extra = {}
+    if co is not None:
+        found_t = 0
+        for (i, t_inj, row, snr) in inj:
+            if lens[i] < L or snr < 8.0 or i not in res['tables']:
+                continue
+            found_t += int(np.any(np.abs(res['tables'][i]['end_time'] - (segs[i]['start_gps'] + t_inj)) < 0.1))
+        extra = dict(selection='threshold 4, exact above 5.28, rebuilt below; consolidated (newsnr 4, 30 per '
+                               '1.072 s, exempt 5)', peaks_before_consolidation=res['n_peaks_in'],
+                     peaks_after_consolidation=res['n_peaks_out'], injections_found_in_tables=found_t)
     return dict(workload='C4: %d segments, log-uniform 64-4096 s, 2 detectors, %d injections, %d glitches; 5880 '
                          'templates, %s' % (a.segments, len(inj), len(glitches), a.form),
                 value=weeks / (ms / 1e3 / 3600.0), unit='2-det weeks / GPU-hour', ms=ms, wall_s=wall,
@@ -256,7 +272,7 @@ def c4(a):
                 total_s=float(lens.sum()), chunks=res['n_chunks'], batches=res['batches'], graph=not a.no_graph,
                 kept=int(kept.sum()), candidates=len(res['cands']), glitches=len(glitches), glitches_gated=gated,
                 injections_snr8_in_analysed=n_inj_an, injections_found=found,
-                gates=sum(len(g) for g in res['gates']), bank_setup_s=bank_s)
+                gates=sum(len(g) for g in res['gates']), bank_setup_s=bank_s, seed=a.seed, **extra)
 
 
 def main():
@@ -266,6 +282,7 @@ def main():
     ap.add_argument('--batch', type=int, default=32)
     ap.add_argument('--seed', type=int, default=4)
     ap.add_argument('--no-graph', action='store_true')
+    ap.add_argument('--production', action='store_true')
     ap.add_argument('--triggers', type=int, default=4096)
     ap.add_argument('--r', type=int, default=128)
     ap.add_argument('--n', type=int, default=256)

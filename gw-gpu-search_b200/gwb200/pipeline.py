@@ -44,6 +44,7 @@ class FilterConfig:
     # exact_snr (1 - margin) skip the exact stage and keep their rebuilt SNR and phase when above snr_threshold;
     # 0 sends every candidate to the exact stage (PyCBC-equivalent values)
     exact_snr: float = 0.0
+    rebuilt_cap: int = 0          # capacity of the rebuilt-peak list (0: cand_cap)
 
 
 class Bank:
@@ -144,7 +145,8 @@ class MatchedFilter:
         assert not (self.fp8 and cfg.exact_snr > 0), 'the fp8 screen keeps no rebuilt values: use exact_snr = 0'
         self.ecut = float(np.float32(cfg.exact_snr * (1 - cfg.margin))) if cfg.exact_snr > 0 else 0.0
         self.rthr = float(np.float32(cfg.snr_threshold))
-        self.rebuilt = (torch.empty(cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
+        self.rebuilt_cap = cfg.rebuilt_cap or cap
+        self.rebuilt = (torch.empty(self.rebuilt_cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
                         if cfg.exact_snr > 0 else None)
         self.kernel_launches = 0
         self.fft_launches = 0
@@ -203,7 +205,7 @@ class MatchedFilter:
                   _lib.ptr(self.Are_lo), _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z),
                   _lib.ptr(self.Zlo), self.Z.stride(0), K, Kh, f, _lib.ptr(self.sa), _lib.ptr(self.cands), cap,
                   _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap, _lib.ptr(self.rebuilt),
-                  cap if self.rebuilt is not None else 0, _lib.ptr(self.counters), _lib.stream_ptr())
+                  self.rebuilt_cap if self.rebuilt is not None else 0, _lib.ptr(self.counters), _lib.stream_ptr())
         if self.fused:
             nb = -(-r // self.fws.wrows)
             self.kernel_launches += 2 * nb + 3  # two basis passes per row batch, stacked A, GEMM, selection
@@ -261,10 +263,11 @@ class MatchedFilter:
         self.exact(D, IP, sig)
         return sig
 
-    def results(self, sig=None):
+    def results(self, sig=None, rebuilt_on_device=False):
         """Copy the step's candidates and exact values to the host; returns a dict of numpy arrays (all candidates
         and the kept peaks with exact SNR above the threshold; with exact_snr > 0 also the rebuilt peaks, whose SNR
-        and phase are the rebuilt ones: `rebuilt`, GwbCand records)."""
+        and phase are the rebuilt ones: `rebuilt`, GwbCand records, or with rebuilt_on_device `rebuilt_dev`, a view
+        of the device list as an (n, 8) int32 tensor of the GwbCand fields)."""
         c = self.counters.cpu().numpy()
         if c[3]:
             raise _lib.GwbError('select', _lib.GWB_ERR_CAPACITY, 'candidate capacity %d exceeded' % self.cfg.cand_cap)
@@ -273,6 +276,13 @@ class MatchedFilter:
         peaks = _exact.from_dev(self.peaks, _exact.PEAK, n)
         keep = peaks['snr'] > self.cfg.snr_threshold
         nr = int(c[4])
-        rebuilt = _exact.from_dev(self.rebuilt, _exact.CAND, nr) if self.rebuilt is not None else np.zeros(0, _exact.CAND)
-        return dict(n_candidates=n, n_units=int(c[2]), n_groups=int(c[1]), cands=cands, peaks=peaks, keep=keep,
-                    rebuilt=rebuilt, n_rebuilt=nr)
+        out = dict(n_candidates=n, n_units=int(c[2]), n_groups=int(c[1]), cands=cands, peaks=peaks, keep=keep,
+                   n_rebuilt=nr)
+        if rebuilt_on_device:
+            out['rebuilt_dev'] = (self.rebuilt[:nr * _exact.CAND.itemsize].view(torch.int32).view(nr, 8)
+                                  if self.rebuilt is not None else torch.zeros((0, 8), dtype=torch.int32,
+                                                                               device=self.cands.device))
+        else:
+            out['rebuilt'] = (_exact.from_dev(self.rebuilt, _exact.CAND, nr) if self.rebuilt is not None
+                              else np.zeros(0, _exact.CAND))
+        return out

@@ -9,13 +9,18 @@ previous chunk's ended). Segments shorter than seg_len hold no chunk, as in the 
 skipped. Chunks go through the device in batches of `batch`: one conditioning (BatchConditioner) and one filter step
 (MatchedFilter) per batch, captured once as a CUDA graph and replayed for every batch. Candidates outside a chunk's
 analysed part are dropped when the results are mapped back to segments.
+
+With a Consolidation, each segment is one dataset of the reference: its exact and rebuilt peaks (FilterConfig.
+exact_snr) go to a PeakStore after every batch and are consolidated on the device (consolidate.py), with order keys
+that give the reference's append order (tile, chunk, rebuilt before exact, template row, window; fp_filter.py:
+700-888), and the run returns each segment's peak table (write_one's datasets).
 """
 from dataclasses import dataclass
 
 import numpy as np
 import torch
 
-from . import gpu_prep, pipeline
+from . import consolidate as cons_, gpu_prep, pipeline
 
 
 @dataclass
@@ -27,6 +32,24 @@ class Gating:
     pad: float = 16.0
     f_low: float = 15.0
     max_iterations: int = 1
+
+
+@dataclass
+class Consolidation:
+    """The reference's consolidation options (pycbc_inspiral's --newsnr-threshold, --keep-loudest-interval,
+    --keep-loudest-num, and fp_filter's --consolidate-exempt-snr); production uses 4, 1.072, 30 and 5."""
+    newsnr_threshold: float = 4.0
+    keep_loudest_interval: float = 1.072
+    keep_loudest_num: int = 30
+    exempt_snr: float = 5.0
+
+
+def order_keys(tile, chunk, exact, row_in_tile, window):
+    """int64 keys of the reference's append order within one dataset: tile, chunk, rebuilt before exact, template
+    row within the tile, window."""
+    return ((np.asarray(tile, np.int64) << 47) | (np.asarray(chunk, np.int64) << 33) |
+            (np.asarray(exact, np.int64) << 32) | (np.asarray(row_in_tile, np.int64) << 16) |
+            np.asarray(window, np.int64))
 
 
 def plan_chunks(lengths, sr, start_gps, seg_len, start_pad, end_pad):
@@ -48,8 +71,9 @@ class SegmentFilter:
     units, start_gps, det). The bank's templates must have been generated for chunks of seg_len seconds."""
 
     def __init__(self, bank, cfg, seg_len=512.0, start_pad=48.0, end_pad=16.0, batch=32, gating=Gating(),
-                 psd=(16.0, 8.0, 63, 16.0), isw=None, graph=True, device='cuda'):
+                 psd=(16.0, 8.0, 63, 16.0), isw=None, graph=True, consolidation=None, device='cuda'):
         self.bank, self.cfg, self.gating = bank, cfg, gating
+        self.consolidation = consolidation
         self.sr = cfg.sr
         self.seg_len, self.start_pad, self.end_pad = seg_len, start_pad, end_pad
         self.tlen = int(seg_len * self.sr)
@@ -65,6 +89,10 @@ class SegmentFilter:
         self.isw = isw
         self.use_graph = graph
         self.graph = None
+        self.sig = None
+        self.row0 = np.asarray(bank.row0, np.int64)
+        self.row0_d = torch.from_numpy(self.row0).to(device)
+        self.order_d = torch.from_numpy(np.asarray(bank.order, np.int64)).to(device)
 
     def gate(self, x, start_gps):
         """Autogating of one segment in place (gpu_prep.gpu_stage1's loop); returns the gates (gps, width, taper)."""
@@ -87,7 +115,7 @@ class SegmentFilter:
 
     def _step(self):
         D, IP = self.cond(self.X)
-        self.mf.step(D, IP, self.isw)
+        self.sig = self.mf.step(D, IP, self.isw)
 
     def _capture(self):
         self._step()                           # warm-up: plans, workspaces and cached tables outside the capture
@@ -97,14 +125,67 @@ class SegmentFilter:
             self._step()
         torch.cuda.synchronize()
 
-    def run(self, segments, gate=True):
+    def _peaks(self, res, part, pos):
+        """This batch's output peaks per segment, as device tensors in the PeakStore layout: the exact ones above the
+        threshold (fp_filter.py:837-853) and the rebuilt ones (fp_filter.py:772-781, left on the device), inside
+        each chunk's analysed part; pos[r] = the chunk's index within its segment."""
+        dev = self.device
+        i64 = dict(dtype=torch.int64, device=dev)
+        nb = len(part)
+        a_lo = torch.tensor([an[0] for _, _, an in part], **i64)
+        a_hi = torch.tensor([an[1] for _, _, an in part], **i64)
+        s0 = torch.tensor([sl[0] for _, sl, _ in part], **i64)
+        posd = torch.tensor(pos, **i64)
+        segof = torch.tensor([i for i, _, _ in part], **i64)
+        thr = np.float32(self.cfg.snr_threshold)
+        c, p = res['cands'], res['peaks']
+        sel = p['snr'] > thr
+        c, p = c[sel], p[sel]
+        h = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        ex = dict(row=h(c['row']), seg=h(c['seg']), sample=h(c['sample']), window=h(c['window']), snr=h(p['snr']),
+                  zr=h(p['zr']), zi=h(p['zi']), chisq=h(p['chisq']), dof=h(p['dof']))
+        R = res['rebuilt_dev']
+        f32 = R.view(torch.float32)
+        zf = torch.zeros(R.shape[0], dtype=torch.float32, device=dev)
+        rb = dict(row=R[:, 0], seg=R[:, 1], sample=R[:, 2], window=R[:, 3], snr=f32[:, 4], zr=f32[:, 5], zi=f32[:, 6],
+                  chisq=zf, dof=zf.view(torch.int32))
+        parts = []
+        for exact, d in ((0, rb), (1, ex)):
+            r = d['seg'].long()
+            samp = d['sample'].long()
+            rr = r.clamp(max=nb - 1)
+            ok = (r < nb) & (samp >= a_lo[rr]) & (samp < a_hi[rr])
+            row, rr, samp = d['row'].long()[ok], rr[ok], samp[ok]
+            tile = torch.searchsorted(self.row0_d, row, right=True) - 1
+            key = ((tile << 47) | (posd[rr] << 33) | (exact << 32) | ((row - self.row0_d[tile]) << 16) |
+                   d['window'].long()[ok])
+            parts.append((segof[rr], dict(
+                tid=self.order_d[row], ti=s0[rr] + samp, snr=d['snr'][ok].contiguous(),
+                phase=torch.atan2(d['zi'][ok], d['zr'][ok]), peak_sigmasq=self.sig[row, rr],
+                exact=torch.full((int(row.numel()),), bool(exact), dtype=torch.bool, device=dev),
+                chisq=d['chisq'][ok].contiguous(), dof=d['dof'][ok].contiguous(), order=key)))
+        out = {}
+        for i in sorted({i for i, _, _ in part}):
+            out[i] = {f: torch.cat([d[f][si == i] for si, d in parts]) for f in cons_.FIELDS}
+        return out
+
+    def run(self, segments, gate=True, keep_raw=False):
         """Gates, plans and filters every segment. Returns dict(cands, peaks, keep (the kept peaks after the exact
-        stage), segment and chunk index of each candidate, gates per segment, analysed_s, skipped_s, batches)."""
+        stage), segment and chunk index of each candidate, gates per segment, analysed_s, skipped_s, batches); with a
+        Consolidation also tables (segment -> write_one's datasets) and n_peaks_in / n_peaks_out, and with keep_raw
+        the unconsolidated peaks per segment (raw)."""
         gates = [self.gate(s['x'], s['start_gps']) if gate else [] for s in segments]
         chunks, skipped = self.plan(segments)
         if self.isw is None:
             # the SVD metric of the run (fp_filter.py:354-370) from the first batch, as the bank was built
             raise ValueError('isw (the bank\'s 1 / sw) must be given')
+        co = self.consolidation
+        stores, sigmasq, raw = {}, {}, {}
+        n_chunks_of = {}
+        pos_of = []
+        for i, _, _ in chunks:
+            pos_of.append(n_chunks_of.get(i, 0))
+            n_chunks_of[i] = pos_of[-1] + 1
         out_c, out_p, seg_i, chunk_i = [], [], [], []
         analysed = 0.0
         for b0 in range(0, len(chunks), self.batch):
@@ -119,7 +200,7 @@ class SegmentFilter:
             else:
                 self._step()
             torch.cuda.synchronize()
-            res = self.mf.results()
+            res = self.mf.results(rebuilt_on_device=co is not None)
             c, p = res['cands'], res['peaks']
             row = c['seg'].astype(np.int64)
             ok = row < len(part)
@@ -131,14 +212,40 @@ class SegmentFilter:
             seg_i.append(np.array([part[r][0] for r in row[ok]], np.int64))
             chunk_i.append(b0 + row[ok])
             analysed += sum((an[1] - an[0]) for _, _, an in part) / self.sr
+            if co is not None:
+                sig = None
+                for i, d in self._peaks(res, part, pos_of[b0:b0 + len(part)]).items():
+                    if keep_raw:
+                        raw.setdefault(i, []).append({f: v.cpu().numpy() for f, v in d.items()})
+                    st = stores.get(i)
+                    if st is None:
+                        st = stores[i] = cons_.PeakStore(
+                            segments[i]['start_gps'], self.sr, segments[i]['x'].shape[0], gates[i],
+                            co.newsnr_threshold, co.keep_loudest_interval, co.keep_loudest_num, co.exempt_snr,
+                            device=self.device)
+                    st.add(**d)
+                if sig is None:
+                    sig = self.sig.cpu().numpy()
+                for r, (i, _, _) in enumerate(part):      # template norms of every chunk (the files' sigmasq)
+                    sq = sigmasq.setdefault(i, np.zeros((self.bank.M, n_chunks_of[i])))
+                    sq[self.bank.order, pos_of[b0 + r]] = sig[:, r]
         cands = np.concatenate(out_c) if out_c else np.zeros(0)
         peaks = np.concatenate(out_p) if out_p else np.zeros(0)
         keep = peaks['snr'] > self.cfg.snr_threshold if len(peaks) else np.zeros(0, bool)
         skipped_s = sum(segments[i]['x'].shape[0] for i in skipped) / self.sr
-        return dict(cands=cands, peaks=peaks, keep=keep, segment=np.concatenate(seg_i) if seg_i else np.zeros(0),
-                    chunk=np.concatenate(chunk_i) if chunk_i else np.zeros(0), gates=gates, analysed_s=analysed,
-                    skipped_s=skipped_s, skipped=skipped, n_chunks=len(chunks), batches=-(-len(chunks) // self.batch),
-                    plan=chunks)
+        out = dict(cands=cands, peaks=peaks, keep=keep, segment=np.concatenate(seg_i) if seg_i else np.zeros(0),
+                   chunk=np.concatenate(chunk_i) if chunk_i else np.zeros(0), gates=gates, analysed_s=analysed,
+                   skipped_s=skipped_s, skipped=skipped, n_chunks=len(chunks), batches=-(-len(chunks) // self.batch),
+                   plan=chunks)
+        if co is not None:
+            out['tables'] = {i: cons_.peak_table(st.host(), gates[i], segments[i]['start_gps'], self.sr,
+                                                 sigmasq=sigmasq.get(i)) for i, st in stores.items()}
+            out['n_peaks_in'] = sum(st.n_in for st in stores.values())
+            out['n_peaks_out'] = sum(len(t['snr']) for t in out['tables'].values())
+            if keep_raw:
+                out['raw'] = {i: {f: np.concatenate([d[f] for d in ds]) for f in cons_.FIELDS}
+                              for i, ds in raw.items()}
+        return out
 
 
 def filter_segments(segments, bank, cfg, isw, **kw):

@@ -70,3 +70,41 @@ def test_filter_segments_gates_finds_and_replays():
     key = lambda x: sorted(zip(x['segment'].tolist(), x['chunk'].tolist(), x['cands']['sample'].tolist(),
                                np.round(x['peaks']['snr'], 4).tolist()))
     assert key(out[True]) == key(out[False])
+
+
+def test_filter_segments_consolidated_tables():
+    """Production's selection (threshold 4, exact stage above 5.5 (1 - margin), the rest rebuilt) with consolidation
+    (newsnr 4, 3 loudest per 1.072 s, SNR >= 5 exempt): each segment's table equals the oracle's consolidation of
+    the run's raw peaks in the reference's append order, followed by write_one's assembly."""
+    from gwb200 import fp_filter, gpu_prep, pipeline, segments
+    from oracle import consolidate as oc
+    rng = np.random.default_rng(12)
+    bank = synth.random_bank_c1(48, 3)
+    segs = [dict(x=_segment(300, rng, bank, inj=(7, 150.0, 15.0)), start_gps=1000000000, det=0),
+            dict(x=_segment(200, rng, glitch=(100.0, 120.0, 200.0)), start_gps=1000001000, det=1)]
+    cond = gpu_prep.BatchConditioner(4, TLEN, SR, 20.0, 16.0, 8.0, 15, 16.0)
+    _, IP = cond(torch.stack([segs[0]['x'][:TLEN]] * 4).contiguous())
+    sw, isw = fp_filter.derive_sw(IP)
+    cfg = pipeline.FilterConfig(tile=24, form='f16', snr_threshold=4.0, exact_snr=5.5, cand_cap=1 << 18)
+    B = pipeline.Bank(bank, FLEN, DF, sw.clone(), cfg)
+    co = segments.Consolidation(4.0, 1.072, 3, 5.0)
+    F = segments.SegmentFilter(B, cfg, seg_len=L, start_pad=SP, end_pad=EP, batch=4, psd=(16.0, 8.0, 15, 16.0),
+                               isw=isw.clone(), consolidation=co)
+    r = F.run(segs, keep_raw=True)
+    assert r['n_peaks_in'] > r['n_peaks_out'] > 0
+    for i, tab in r['tables'].items():
+        h = r['raw'][i]
+        gps = segs[i]['start_gps']
+        t = gps + h['ti'] / SR
+        keep, _ = oc.consolidate(h['snr'], h['chisq'], h['dof'], t, r['gates'][i], gps, SR, 4.0, 1.072, 3, 5.0,
+                                 order=h['order'])
+        ref = oc.peak_table(h['tid'][keep], t[keep], h['snr'][keep], h['phase'][keep], h['peak_sigmasq'][keep],
+                            h['exact'][keep], h['chisq'][keep], h['dof'][keep], r['gates'][i], tab['sigmasq'])
+        for k, v in ref.items():
+            assert np.array_equal(tab[k], v), (i, k)
+        assert len(np.unique(h['order'])) == len(h['order'])
+        assert tab['exact'].any() and (~tab['exact']).any()
+    # the injection is among the consolidated peaks of its segment
+    t0 = r['tables'][0]
+    near = np.abs(t0['end_time'] - (1000000000 + 150.0)) < 0.1
+    assert near.any() and abs(t0['snr'][near].max() - 15.0) < 3.0
