@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(kThreads) snr_grad_kernel(const double* __rest
     __shared__ int e[kMaxBins + 1];
     __shared__ double tot;
     __shared__ double acc[kMaxBins][2 + 2 * kNP];      // per bin: z_j (re, im), dz_j (re, im) x 7
+    __shared__ double red[kThreads / 32][2 + 2 * kNP];
     const double* th = params + (long long)i * kNP;
     const PhaseCoef P = phase_coef(th, f_ecc);
     const double tc = th[5], phic = th[6];
@@ -238,59 +239,60 @@ __global__ void __launch_bounds__(kThreads) snr_grad_kernel(const double* __rest
     }
     const float* ip = IP + (long long)i * ldip;
     const float2* d = D + (long long)i * ldd;
-    for (int x = threadIdx.x; x < kMaxBins * (2 + 2 * kNP); x += kThreads) (&acc[0][0])[x] = 0.0;
     block_edges(ip, df, kmin, k1, nb, e, &tot, scan);
-    // main pass: contiguous range per thread, per-bin register sums flushed on bin change
-    const int len = k1 - kmin, chunk = (len + kThreads - 1) / kThreads;
-    const int a = kmin + threadIdx.x * chunk, b = min(a + chunk, k1);
-    int bin = 0;
-    while (bin < nb - 1 && e[bin + 1] <= a) ++bin;
-    T s[2 + 2 * kNP];
+    // main pass, bin by bin: threads stride over the bin's range (coalesced D and IP), then a fixed-order block
+    // reduction (warp shuffles, then the warps in order) gives the bin's sums: the result does not depend on timing
+    constexpr int kNS = 2 + 2 * kNP;
+    for (int j = 0; j < nb; ++j) {
+        T s[kNS];
 #pragma unroll
-    for (int x = 0; x < 2 + 2 * kNP; ++x) s[x] = T(0);
-    auto flush = [&]() {
+        for (int x = 0; x < kNS; ++x) s[x] = T(0);
+        for (int k = e[j] + threadIdx.x; k < e[j + 1]; k += kThreads) {
+            const double f = (double)k * df;
+            const Dual ps = psi_at(P, f);
+            double ph = ps.v - 0.25 * kPi + 2.0 * kPi * f * tc - phic;
+            ph -= 2.0 * kPi * rint(ph * (0.5 / kPi));
+            T sn, cs;
+            if constexpr (sizeof(T) == 8) {
+                sincos(ph, &sn, &cs);
+            } else {
+                sincosf((float)ph, &sn, &cs);
+            }
+            const T amp = (T)pow(f, -7.0 / 6.0);
+            const float2 dk = d[k];
+            // q = conj(h) D = amp e^{+i ph} D
+            const T hr = amp * cs, hi = amp * sn;
+            const T qr = hr * (T)dk.x - hi * (T)dk.y, qi = hr * (T)dk.y + hi * (T)dk.x;
+            s[0] += qr;
+            s[1] += qi;
+            // d q / d theta_p = i dPhi_p q
+            T dph[kNP];
 #pragma unroll
-        for (int x = 0; x < 2 + 2 * kNP; ++x) {
-            atomicAdd(&acc[bin][x], (double)s[x]);
-            s[x] = T(0);
-        }
-    };
-    for (int k = a; k < b; ++k) {
-        if (bin < nb - 1 && k >= e[bin + 1]) {
-            flush();
-            while (bin < nb - 1 && k >= e[bin + 1]) ++bin;
-        }
-        const double f = (double)k * df;
-        const Dual ps = psi_at(P, f);
-        double ph = ps.v - 0.25 * kPi + 2.0 * kPi * f * tc - phic;
-        ph -= 2.0 * kPi * rint(ph * (0.5 / kPi));
-        T sn, cs;
-        if constexpr (sizeof(T) == 8) {
-            sincos(ph, &sn, &cs);
-        } else {
-            sincosf((float)ph, &sn, &cs);
-        }
-        const T amp = (T)pow(f, -7.0 / 6.0);
-        const float2 dk = d[k];
-        // q = conj(h) D = amp e^{+i ph} D
-        const T hr = amp * cs, hi = amp * sn;
-        const T qr = hr * (T)dk.x - hi * (T)dk.y, qi = hr * (T)dk.y + hi * (T)dk.x;
-        s[0] += qr;
-        s[1] += qi;
-        // d q / d theta_p = i dPhi_p q
-        T dph[kNP];
+            for (int p = 0; p < kNI; ++p) dph[p] = (T)ps.d[p];
+            dph[5] = (T)(2.0 * kPi * f);
+            dph[6] = T(-1);
 #pragma unroll
-        for (int p = 0; p < kNI; ++p) dph[p] = (T)ps.d[p];
-        dph[5] = (T)(2.0 * kPi * f);
-        dph[6] = T(-1);
-#pragma unroll
-        for (int p = 0; p < kNP; ++p) {
-            s[2 + 2 * p] -= dph[p] * qi;
-            s[3 + 2 * p] += dph[p] * qr;
+            for (int p = 0; p < kNP; ++p) {
+                s[2 + 2 * p] -= dph[p] * qi;
+                s[3 + 2 * p] += dph[p] * qr;
+            }
         }
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int x = 0; x < kNS; ++x) {
+            double v = (double)s[x];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) red[warp][x] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < kNS) {
+            double v = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) v += red[w][threadIdx.x];
+            acc[j][threadIdx.x] = v;
+        }
+        __syncthreads();
     }
-    if (b > a) flush();
-    __syncthreads();
     if (threadIdx.x == 0) {
         const double c4 = 4.0 * df;
         const double sig2 = c4 * tot;

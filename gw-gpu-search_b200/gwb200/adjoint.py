@@ -38,6 +38,30 @@ def snr_grad(params, D, IP, df, kmin, nbins=16, f_ecc=10.0, fp64=False, out=None
                 dchisq=out[:, 21:28], raw=out)
 
 
+class _Stat(torch.autograd.Function):
+    """SNR, newSNR or chi-squared of each trigger as a function of params, with the hand-written gradient of
+    gwb_snr_grad as its backward (first order only)."""
+
+    @staticmethod
+    def forward(ctx, params, D, IP, df, kmin, nbins, f_ecc, fp64, which):
+        r = snr_grad(params.detach().contiguous(), D, IP, df, kmin, nbins, f_ecc, fp64)
+        ctx.save_for_backward(r['d' + which].clone())
+        return r[which].clone()
+
+    @staticmethod
+    @torch.autograd.function.once_differentiable
+    def backward(ctx, g):
+        (d,) = ctx.saved_tensors
+        return (g[:, None] * d,) + (None,) * 8
+
+
+def stat(params, D, IP, df, kmin, nbins=16, f_ecc=10.0, fp64=False, which='snr'):
+    """Differentiable (torch.autograd) SNR ('snr'), newSNR ('newsnr') or chi-squared ('chisq') of each trigger,
+    (n,) float64; params (n, 7) float64 may require grad."""
+    assert which in ('snr', 'newsnr', 'chisq')
+    return _Stat.apply(params, D, IP, df, kmin, nbins, f_ecc, fp64, which)
+
+
 def phase_metric(params, IP, flen, df, kmin, f_ecc=10.0):
     """(n, 7, 7) float64: g_ij = Cov_w(dPhi/dtheta_i, dPhi/dtheta_j), w = |h|^2 IP, so that the phase-maximised match
     of h(theta) and h(theta + d) is 1 - d^T g d / 2 to second order (the phi_c row is zero; project t_c out for the

@@ -180,3 +180,18 @@ def test_refinement_climbs_to_the_signal():
     # a local ascent: it reaches the maximum near the start (0.98 of the SNR at the true parameters, which the noise
     # need not make the global maximum)
     assert np.all(h[-1] >= 0.98 * truth), (h[0], h[-1], truth)
+
+
+def test_autograd_function_carries_the_gradients():
+    """adjoint.stat as a torch.autograd.Function: backward of a scalar loss gives the chain rule through the
+    hand-written gradients, for snr, newsnr and chisq."""
+    from gwb200 import adjoint
+    D, IP = _data(THETA, seed=4)
+    Dd, IPd, thd = _gpu(D, IP, THETA + 0.01)
+    r = adjoint.snr_grad(thd, Dd, IPd, DF, KMIN, NB, fp64=True)
+    for which in ('snr', 'newsnr', 'chisq'):
+        th = thd.clone().requires_grad_(True)
+        y = adjoint.stat(th, Dd, IPd, DF, KMIN, NB, fp64=True, which=which)
+        assert torch.equal(y.detach(), r[which])
+        (y ** 2).sum().backward()
+        assert torch.allclose(th.grad, 2 * r[which][:, None] * r['d' + which], rtol=1e-14, atol=0)
