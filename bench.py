@@ -354,11 +354,27 @@ def main():
             ms_e2e = float(t.item())
         # dominant kernel: the fused reconstruction GEMM, each launch bracketed by events in one extra step
         mf.profile = {}
-        step()
+        ec = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        ec[0].record()
+        Dd, IPd = cond(x)
+        ec[1].record()
+        mf.step(Dd, IPd, isw)
+        ep = torch.cuda.Event(enable_timing=True)
+        ep.record()
         torch.cuda.synchronize()
         L = mf.profile['launches']
         g_ms = [e[1].elapsed_time(e[2]) for e, n, r, kp in L]
         b_ms = [e[0].elapsed_time(e[3]) for e, n, r, kp in L]
+        # where the profiled step goes (CUDA events; the events themselves add a little)
+        split = dict(conditioning=ec[0].elapsed_time(ec[1]), basis_series=float(np.sum(b_ms)),
+                     stacked_a=float(np.sum([e[3].elapsed_time(e[1]) for e, n, r, kp in L])),
+                     gemm=float(np.sum(g_ms)))
+        sel = [L[i][0][2].elapsed_time(L[i + 1][0][0]) for i in range(len(L) - 1)]
+        split['selection'] = float(np.sum(sel))
+        for name, (a_, b_) in mf.profile['parts']:
+            split[name] = a_.elapsed_time(b_)
+        split['total'] = ec[0].elapsed_time(ep)
+        split = {k: round(v, 3) for k, v in split.items()}
         # algorithmic HBM bytes of one basis-series call (both passes): Vp read (tlen/2 + 1 complex per row), W
         # written and read back (tlen complex per row), Z written (re + im over Tn, one or two 16-bit planes or fp32)
         zb = {'bf16x3': 8, 'f16': 4, 'bf16': 4, 'f32': 8, 'fp8': 2}[form]
@@ -376,7 +392,8 @@ def main():
                              basis_ms=float(np.mean(b_ms)), basis_bytes=float(np.mean(b_bytes)),
                              z_bytes=float(np.mean([2 * kp * mf.Tn * {'f32': 4, 'fp8': 1}.get(form, 2) *
                                                     (2 if form == 'bf16x3' else 1) for e, n, r, kp in L])),
-                             useful=float(np.mean(useful)), issued=float(np.mean(issued)), n_gemm=len(L))
+                             useful=float(np.mean(useful)), issued=float(np.mean(issued)), n_gemm=len(L),
+                             split_ms=split)
         del mf
         torch.cuda.empty_cache()
     # precision of every form against float64 on one (tile, chunk) (after the timed regions; the split bf16 form
@@ -442,7 +459,8 @@ def main():
                 roofline_gemm=roof_gemm, precision=precision_rep, top_peak_sets=top_peak_sets(kept_sets, 5.5),
                 forms={k: dict(value=v['value'], ms_per_step=v['ms'], e2e=v['e2e'], n_candidates=v['n_candidates'],
                                n_kept=v['n_kept'], gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
-                               basis_share=v['basis_total_ms'] / v['ms']) for k, v in results.items()},
+                               basis_share=v['basis_total_ms'] / v['ms'], split_ms=v['split_ms'])
+                       for k, v in results.items()},
                 peaks_source=kind)
     if rank == 0:
         if not a.no_cpu:

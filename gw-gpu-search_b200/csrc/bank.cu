@@ -15,7 +15,7 @@
 namespace gwb {
 namespace {
 
-constexpr int kRows = 64, kSegs = 32, kK = 32;
+constexpr int kK = 32;
 
 // Scratch of gwb_sigma2_noalloc: the split-k partial sums of the template norms, at most kNoAllocPart doubles
 // (4 MiB). It lives in the library's own device image, so every GPU that loads the library holds it until exit.
@@ -24,56 +24,69 @@ static __device__ __align__(256) double g_sigma2_scratch[kNoAllocPart];
 std::mutex g_scratch_mu;
 double* g_scratch_ptr[64] = {nullptr};
 
+// Split-k partial sums of sig for a 64-row x 64-segment block: 256 threads, each a 4 x 4 register tile of float64
+// accumulators; per 32-bin step the block's |H|^2 (float64, exact from complex64) and IP tiles go through shared
+// memory (row stride 65 doubles: the transposing stores of 16 consecutive bins hit 16 distinct bank pairs), and the
+// next step's H and IP are loaded into registers while the current one is multiplied.
+constexpr int kSR = 64, kSS = 64, kSK = 32, kSP = kSK * kSR / 256;    // elements of each tile per thread
 __global__ void __launch_bounds__(256) sigma2_partial_kernel(const float2* __restrict__ H, long long ldh, int n,
                                                              const float* __restrict__ IP, long long ldip, int nseg,
                                                              int kmin, int flen, int kper,
                                                              double* __restrict__ part) {
-    __shared__ double Ps[kK][kRows];
-    __shared__ double Is[kK][kSegs];
+    __shared__ double Ps[kSK][kSR + 1];
+    __shared__ double Is[kSK][kSS + 1];
     const int tid = threadIdx.x;
-    const int tr = tid >> 3, ts = tid & 7;          // 32 x 8 threads: 2 rows x 4 segments each
-    const int r0 = blockIdx.x * kRows, s0 = blockIdx.y * kSegs;
+    const int tr = tid >> 4, ts = tid & 15;         // rows 4 tr .. 4 tr + 3, segments 4 ts .. 4 ts + 3
+    const int r0 = blockIdx.x * kSR, s0 = blockIdx.y * kSS;
     const int ka = kmin + blockIdx.z * kper, kb = min(flen, ka + kper);
-    double acc[2][4];
+    double acc[4][4];
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int k0 = ka; k0 < kb; k0 += kK) {
-        for (int e = tid; e < kK * kRows; e += 256) {
-            const int rr = e / kK, kk = e % kK;
-            const int row = r0 + rr, k = k0 + kk;
-            double p = 0.0;
-            if (row < n && k < kb) {
-                const float2 v = H[(long long)row * ldh + k];
-                p = (double)v.x * v.x + (double)v.y * v.y;
-            }
-            Ps[kk][rr] = p;
-        }
-        for (int e = tid; e < kK * kSegs; e += 256) {
-            const int ss = e / kK, kk = e % kK;
-            const int s = s0 + ss, k = k0 + kk;
-            Is[kk][ss] = (s < nseg && k < kb) ? (double)IP[(long long)s * ldip + k] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < kK; ++kk) {
-            const double p0 = Ps[kk][2 * tr], p1 = Ps[kk][2 * tr + 1];
+    // thread's load slots: element e = tid + 256 i, (row or segment) = e / kSK, bin = e % kSK (32 consecutive bins
+    // of one row per warp: coalesced)
+    float2 hv[kSP];
+    float iv[kSP];
+    auto load = [&](int k0) {
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const double w = Is[kk][4 * ts + b];
-                acc[0][b] = fma(p0, w, acc[0][b]);
-                acc[1][b] = fma(p1, w, acc[1][b]);
-            }
+        for (int i = 0; i < kSP; ++i) {
+            const int e = tid + 256 * i, rr = e / kSK, kk = e % kSK;
+            const int row = r0 + rr, sg = s0 + rr, k = k0 + kk;
+            hv[i] = (row < n && k < kb) ? H[(long long)row * ldh + k] : make_float2(0.f, 0.f);
+            iv[i] = (sg < nseg && k < kb) ? IP[(long long)sg * ldip + k] : 0.f;
+        }
+    };
+    load(ka);
+    for (int k0 = ka; k0 < kb; k0 += kSK) {
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kSP; ++i) {
+            const int e = tid + 256 * i, rr = e / kSK, kk = e % kSK;
+            Ps[kk][rr] = (double)hv[i].x * hv[i].x + (double)hv[i].y * hv[i].y;
+            Is[kk][rr] = (double)iv[i];
         }
         __syncthreads();
+        if (k0 + kSK < kb) load(k0 + kSK);
+#pragma unroll 4
+        for (int kk = 0; kk < kSK; ++kk) {
+            double p[4], w[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) p[a] = Ps[kk][4 * tr + a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) w[b] = Is[kk][4 * ts + b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = fma(p[a], w[b], acc[a][b]);
+        }
     }
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            const int row = r0 + 2 * tr + a, s = s0 + 4 * ts + b;
-            if (row < n && s < nseg) part[((long long)blockIdx.z * n + row) * nseg + s] = acc[a][b];
+            const int row = r0 + 4 * tr + a, sg = s0 + 4 * ts + b;
+            if (row < n && sg < nseg) part[((long long)blockIdx.z * n + row) * nseg + sg] = acc[a][b];
         }
 }
 
@@ -263,11 +276,11 @@ int gwb_sigma2(const float* H, long long ldh, int n, const float* IP, long long 
     GWB_CHECK_ARG(H && IP && part && sig, GWB_ERR_ARG, "sigma2: null pointer");
     GWB_CHECK_ARG(n > 0 && nseg > 0 && flen > kmin && kmin >= 0 && ldsig >= nseg, GWB_ERR_SHAPE,
                   "sigma2: n=%d nseg=%d flen=%d kmin=%d", n, nseg, flen, kmin);
-    const int gx = (int)cdiv(n, kRows), gy = (int)cdiv(nseg, kSegs);
-    int nsplit = (int)std::max(1ll, std::min<long long>(64, (2ll * num_sms()) / std::max(1, gx * gy)));
+    const int gx = (int)cdiv(n, kSR), gy = (int)cdiv(nseg, kSS);
+    int nsplit = (int)std::max(1ll, std::min<long long>(64, (4ll * num_sms()) / std::max(1, gx * gy)));
     nsplit = (int)std::min<long long>(nsplit, part_elems / ((long long)n * nseg));
     GWB_CHECK_ARG(nsplit >= 1, GWB_ERR_SHAPE, "sigma2: workspace of %lld doubles is smaller than n*nseg", part_elems);
-    const int kper = (int)(cdiv(cdiv(flen - kmin, nsplit), kK) * kK);
+    const int kper = (int)(cdiv(cdiv(flen - kmin, nsplit), kSK) * kSK);
     nsplit = (int)cdiv(flen - kmin, kper);
     cudaStream_t s = (cudaStream_t)stream;
     sigma2_partial_kernel<<<dim3(gx, gy, nsplit), 256, 0, s>>>(reinterpret_cast<const float2*>(H), ldh, n, IP, ldip, nseg,

@@ -150,7 +150,8 @@ class MatchedFilter:
                         if cfg.exact_snr > 0 else None)
         self.kernel_launches = 0
         self.fft_launches = 0
-        # set to {} to record CUDA events per (tile, segment): e0 basis series e3 stacked A e1 GEMM e2
+        # set to {} to record CUDA events per (tile, segment): e0 basis series e3 stacked A e1 GEMM e2 (then the
+        # selection until the next e0), and ('parts': norms, four-step order of D, exact stage) per step
         self.profile = None
 
     def _gemm(self, n, K, Kh):
@@ -249,18 +250,37 @@ class MatchedFilter:
         """Queue one step on the current stream: every tile against every segment in seg_ids (rows of D / IP).
         Nothing is copied back; call results() after the stream is synchronised."""
         self.counters.zero_()
+        prof = self.profile
+        ev = (lambda: torch.cuda.Event(enable_timing=True)) if prof is not None else None
+        if prof is not None:
+            e_n = (ev(), ev())
+            e_n[0].record()
         sig = self.norms(IP)
+        if prof is not None:
+            e_n[1].record()
+            prof.setdefault('parts', []).append(('norms', e_n))
+            e_f = (ev(), ev())
+            e_f[0].record()
         if self.fused:
             # every segment's D isw in four-step order, shared by all tiles
             if self.Dp is None or self.Dp.shape[0] != D.shape[0]:
                 self.Dp = torch.empty((D.shape[0], self.tlen // 2 + 1), dtype=torch.complex64, device=D.device)
             fp_filter.fourstep_order(D, self.tlen, isw, out=self.Dp)
             self.kernel_launches += 1
+        if prof is not None:
+            e_f[1].record()
+            prof.setdefault('parts', []).append(('fourstep', e_f))
         segs = range(D.shape[0]) if seg_ids is None else seg_ids
         for t in range(len(self.bank.tiles)):
             for s in segs:
                 self.tile_segment(t, D, isw, sig, s)
+        if prof is not None:
+            e_x = (ev(), ev())
+            e_x[0].record()
         self.exact(D, IP, sig)
+        if prof is not None:
+            e_x[1].record()
+            prof.setdefault('parts', []).append(('exact', e_x))
         return sig
 
     def results(self, sig=None, rebuilt_on_device=False):
