@@ -127,13 +127,23 @@ __global__ void __launch_bounds__(kSumThreads) binsum_kernel(const GwbGroup* __r
                                                              const float2* __restrict__ H, long long ldh,
                                                              const float2* __restrict__ D, long long ldd, int kmin,
                                                              int nchunk, unsigned nmask, float inv_half_n,
+                                                             const int32_t* __restrict__ order,
                                                              float2* __restrict__ slots) {
     __shared__ float2 red[kSumThreads / 32][kMaxPeaks];
     const int ng = count_of(gcount, gmax);
     const long long nitems = (long long)ng * nchunk;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const int g = (int)(it / nchunk), c = (int)(it % nchunk);
+        // group-major over the groups as given, or chunk-major over the groups in template-row order (order): the
+        // items in flight then share a few rows' template chunks and every segment's data chunk in L2
+        int g, c;
+        if (order) {
+            c = (int)(it / ng);
+            g = order[(int)(it % ng)];
+        } else {
+            g = (int)(it / nchunk);
+            c = (int)(it % nchunk);
+        }
         const GwbGroup gr = groups[g];
         const GwbUnit un = units[gr.unit];
         const int np = gr.count;
@@ -214,6 +224,56 @@ __global__ void __launch_bounds__(kSumThreads) binsum_kernel(const GwbGroup* __r
             a = b;
             ++j;
         }
+    }
+}
+
+// Counting sort of the groups by template row (units[group.unit].row): counts, a one-block exclusive scan, scatter.
+// The order within a row is whatever the atomics give; no result depends on it.
+__global__ void group_count_kernel(const GwbGroup* __restrict__ groups, const int32_t* gcount, int gmax,
+                                   const GwbUnit* __restrict__ units, int nrows, int32_t* __restrict__ cnt,
+                                   int32_t* __restrict__ status) {
+    const int ng = count_of(gcount, gmax);
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        int row = units[groups[g].unit].row;
+        if (row < 0 || row >= nrows) {           // flagged; sorted last so that the order stays a permutation
+            atomicOr(status, 1);
+            row = nrows - 1;
+        }
+        atomicAdd(&cnt[row], 1);
+    }
+}
+
+__global__ void __launch_bounds__(1024) group_scan_kernel(const int32_t* __restrict__ cnt, int nrows,
+                                                          int32_t* __restrict__ off) {
+    __shared__ int part[1024];
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int per = (nrows + T - 1) / T;
+    const int b = tid * per, e = min(nrows, b + per);
+    int s = 0;
+    for (int k = b; k < e; ++k) s += cnt[k];
+    part[tid] = s;
+    __syncthreads();
+    for (int d = 1; d < T; d <<= 1) {
+        const int v = tid >= d ? part[tid - d] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    int run = tid ? part[tid - 1] : 0;
+    for (int k = b; k < e; ++k) {
+        off[k] = run;
+        run += cnt[k];
+    }
+}
+
+__global__ void group_scatter_kernel(const GwbGroup* __restrict__ groups, const int32_t* gcount, int gmax,
+                                     const GwbUnit* __restrict__ units, int nrows, const int32_t* __restrict__ off,
+                                     int32_t* __restrict__ fill, int32_t* __restrict__ order) {
+    const int ng = count_of(gcount, gmax);
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        int row = units[groups[g].unit].row;
+        if (row < 0 || row >= nrows) row = nrows - 1;
+        order[off[row] + atomicAdd(&fill[row], 1)] = g;
     }
 }
 
@@ -300,7 +360,52 @@ int gwb_bin_sums(const GwbGroup* groups, const int32_t* gcount, int gmax, const 
     binsum_kernel<<<grid, kSumThreads, 0, (cudaStream_t)stream>>>(
         groups, gcount, gmax, units, cands, E, B, nbins, reinterpret_cast<const float2*>(H), ldh,
         reinterpret_cast<const float2*>(D), ldd, kmin, nchunk, (unsigned)(tlen - 1), (float)(2.0 / (double)tlen),
-        reinterpret_cast<float2*>(slots));
+        nullptr, reinterpret_cast<float2*>(slots));
+    GWB_LAUNCH_CHECK("binsum_kernel");
+    return GWB_OK;
+}
+
+long long gwb_bin_sums_work_bytes(int gmax, int nrows) {
+    if (gmax < 0 || nrows <= 0) return -1;
+    return 4ll * (3ll * nrows + (long long)gmax + 4);
+}
+
+int gwb_bin_sums_ordered(const GwbGroup* groups, const int32_t* gcount, int gmax, const GwbUnit* units,
+                         const GwbCand* cands, const int32_t* E, int B, const int32_t* nbins, int nrows,
+                         const float* H, long long ldh, const float* D, long long ldd, int kmin, int flen,
+                         long long tlen, void* work, long long work_bytes, int32_t* status, float* slots,
+                         void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(groups && units && cands && E && nbins && H && D && slots && work && status, GWB_ERR_ARG,
+                  "bin_sums_ordered: null pointer");
+    GWB_CHECK_ARG(is_pow2(tlen) && tlen <= (1ll << 31), GWB_ERR_NOT_POW2,
+                  "bin_sums_ordered: time length %lld is not a power of two", tlen);
+    GWB_CHECK_ARG(gmax >= 0 && B >= 1 && flen > kmin && nrows > 0, GWB_ERR_SHAPE,
+                  "bin_sums_ordered: gmax=%d B=%d flen=%d kmin=%d nrows=%d", gmax, B, flen, kmin, nrows);
+    GWB_CHECK_ARG(work_bytes >= gwb_bin_sums_work_bytes(gmax, nrows), GWB_ERR_SHAPE,
+                  "bin_sums_ordered: work %lld bytes, %lld needed", work_bytes, gwb_bin_sums_work_bytes(gmax, nrows));
+    cudaStream_t s = (cudaStream_t)stream;
+    GWB_CUDA(cudaMemsetAsync(status, 0, sizeof(int32_t), s));
+    if (gmax == 0) return GWB_OK;
+    int32_t* cnt = static_cast<int32_t*>(work);
+    int32_t* fill = cnt + nrows;
+    int32_t* off = fill + nrows;
+    int32_t* order = off + nrows;
+    GWB_CUDA(cudaMemsetAsync(cnt, 0, 8ll * nrows, s));    // cnt and fill
+    const int gs = (int)std::min<long long>(cdiv(gmax, 256), 4ll * num_sms());
+    group_count_kernel<<<gs, 256, 0, s>>>(groups, gcount, gmax, units, nrows, cnt, status);
+    GWB_LAUNCH_CHECK("group_count_kernel");
+    group_scan_kernel<<<1, 1024, 0, s>>>(cnt, nrows, off);
+    GWB_LAUNCH_CHECK("group_scan_kernel");
+    group_scatter_kernel<<<gs, 256, 0, s>>>(groups, gcount, gmax, units, nrows, off, fill, order);
+    GWB_LAUNCH_CHECK("group_scatter_kernel");
+    const int nchunk = (int)cdiv(flen - kmin, kChunk);
+    const long long items = (long long)gmax * nchunk;
+    const int grid = (int)std::min<long long>(items, 16ll * num_sms());
+    binsum_kernel<<<grid, kSumThreads, 0, s>>>(
+        groups, gcount, gmax, units, cands, E, B, nbins, reinterpret_cast<const float2*>(H), ldh,
+        reinterpret_cast<const float2*>(D), ldd, kmin, nchunk, (unsigned)(tlen - 1), (float)(2.0 / (double)tlen),
+        order, reinterpret_cast<float2*>(slots));
     GWB_LAUNCH_CHECK("binsum_kernel");
     return GWB_OK;
 }

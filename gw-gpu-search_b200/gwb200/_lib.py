@@ -60,6 +60,8 @@ SIGNATURES = {
     'gwb_bin_sums': [_P, _P, _I, _P, _P, _P, _I, _P, _P, _LL, _P, _LL, _I, _I, _LL, _P, _P],
     'gwb_exact_finalize': [_P, _P, _I, _P, _P, _I, _P, _I, _I, _P, _P, _LL, _D, _P, _P],
     'gwb_exact_chunks': [_I, _I],
+    'gwb_bin_sums_ordered': [_P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _LL, _P, _LL, _I, _I, _LL, _P, _LL, _P, _P, _P],
+    'gwb_bin_sums_work_bytes': [_I, _I],
     'gwb_sigma2': [_P, _LL, _I, _P, _LL, _I, _I, _I, _D, _P, _LL, _P, _LL, _P],
     'gwb_sigma2_noalloc': [_P, _LL, _I, _P, _LL, _I, _I, _I, _D, _P, _LL, _P],
     'gwb_gram': [_P, _LL, _I, _P, _I, _I, _P, _LL, _P, _P],
@@ -112,6 +114,7 @@ def load():
             f.argtypes = args
             f.restype = ctypes.c_int
         lib.gwb_consolidate_work_bytes.restype = ctypes.c_longlong
+        lib.gwb_bin_sums_work_bytes.restype = ctypes.c_longlong
         _lib = lib
     return _lib
 

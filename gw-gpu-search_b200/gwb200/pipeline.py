@@ -45,6 +45,7 @@ class FilterConfig:
     # 0 sends every candidate to the exact stage (PyCBC-equivalent values)
     exact_snr: float = 0.0
     rebuilt_cap: int = 0          # capacity of the rebuilt-peak list (0: cand_cap)
+    exact_order: bool = True      # exact stage in template-row order, chunk by chunk (gwb_bin_sums_ordered)
 
 
 class Bank:
@@ -139,6 +140,10 @@ class MatchedFilter:
         self.slot_cap = cap
         assert cap <= 1 << 22
         self.slots = None
+        if cfg.exact_order:
+            wb = _lib.load().gwb_bin_sums_work_bytes(cap, bank.M)
+            self.sort_work = torch.empty(wb, dtype=torch.uint8, device=device)
+            self.sort_status = torch.zeros(1, dtype=torch.int32, device=device)
         self.peaks = torch.empty(cap * _exact.PEAK.itemsize, dtype=torch.uint8, device=device)
         margin = max(cfg.margin, cfg.screen_margin) if self.fp8 else cfg.margin
         self.thr2 = float((cfg.snr_threshold * (1 - margin)) ** 2)
@@ -238,9 +243,16 @@ class MatchedFilter:
         if self.slots is None:
             # every slot the finalisation reads is written by the binned sums: no clearing between steps
             self.slots = torch.empty((self.slot_cap, self.nchunk, self.B, 2), dtype=torch.float32, device=D.device)
-        _lib.call('gwb_bin_sums', _lib.ptr(self.groups), _lib.ptr(cnt[1:]), cap, _lib.ptr(self.units),
-                  _lib.ptr(self.cands), _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), _lib.ptr(b.H), b.H.stride(0),
-                  _lib.ptr(D), D.stride(0), b.kmin, b.flen, self.tlen, _lib.ptr(self.slots), s)
+        if self.cfg.exact_order:
+            _lib.call('gwb_bin_sums_ordered', _lib.ptr(self.groups), _lib.ptr(cnt[1:]), cap, _lib.ptr(self.units),
+                      _lib.ptr(self.cands), _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), b.M, _lib.ptr(b.H),
+                      b.H.stride(0), _lib.ptr(D), D.stride(0), b.kmin, b.flen, self.tlen, _lib.ptr(self.sort_work),
+                      self.sort_work.numel(), _lib.ptr(self.sort_status), _lib.ptr(self.slots), s)
+            self.kernel_launches += 3
+        else:
+            _lib.call('gwb_bin_sums', _lib.ptr(self.groups), _lib.ptr(cnt[1:]), cap, _lib.ptr(self.units),
+                      _lib.ptr(self.cands), _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), _lib.ptr(b.H),
+                      b.H.stride(0), _lib.ptr(D), D.stride(0), b.kmin, b.flen, self.tlen, _lib.ptr(self.slots), s)
         _lib.call('gwb_exact_finalize', _lib.ptr(self.cands), _lib.ptr(cnt[0:]), cap, _lib.ptr(self.units),
                   _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), b.kmin, b.flen, _lib.ptr(self.slots), _lib.ptr(sig),
                   sig.stride(0), float(b.df), _lib.ptr(self.peaks), s)
@@ -291,6 +303,8 @@ class MatchedFilter:
         c = self.counters.cpu().numpy()
         if c[3]:
             raise _lib.GwbError('select', _lib.GWB_ERR_CAPACITY, 'candidate capacity %d exceeded' % self.cfg.cand_cap)
+        if self.cfg.exact_order and int(self.sort_status.item()):
+            raise _lib.GwbError('bin_sums_ordered', _lib.GWB_ERR_SHAPE, 'a unit row outside the bank')
         n = int(c[0])
         cands = _exact.from_dev(self.cands, _exact.CAND, n)
         peaks = _exact.from_dev(self.peaks, _exact.PEAK, n)

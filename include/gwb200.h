@@ -323,6 +323,17 @@ GWB_API int gwb_bin_sums(const GwbGroup* groups, const int32_t* gcount, int gmax
                          const GwbCand* cands, const int32_t* E, int B, const int32_t* nbins, const float* H,
                          long long ldh, const float* D, long long ldd, int kmin, int flen, long long tlen, float* slots,
                          void* stream);
+/* The same binned sums (fused mode: D given) with the work in template-row order: the groups are counting-sorted
+ * by their unit's row (nrows rows; a row outside [0, nrows) sets status[0] = 1) and the items run chunk by chunk, so
+ * the groups in flight share a few template chunks and every segment's data chunk in L2 and each template band is
+ * read from HBM about once per call instead of once per segment. Same slots as gwb_bin_sums, bit for bit. work:
+ * gwb_bin_sums_work_bytes(gmax, nrows) bytes; status: one device int32 (cleared here). */
+GWB_API long long gwb_bin_sums_work_bytes(int gmax, int nrows);
+GWB_API int gwb_bin_sums_ordered(const GwbGroup* groups, const int32_t* gcount, int gmax, const GwbUnit* units,
+                                 const GwbCand* cands, const int32_t* E, int B, const int32_t* nbins, int nrows,
+                                 const float* H, long long ldh, const float* D, long long ldd, int kmin, int flen,
+                                 long long tlen, void* work, long long work_bytes, int32_t* status, float* slots,
+                                 void* stream);
 /* Number of band chunks the slots are laid out for. */
 GWB_API int gwb_exact_chunks(int flen, int kmin);
 /* Per candidate: z, pw from the slots (float64 sums), and with sig given (float64, sig[row * ldsig + seg]) snr,

@@ -172,3 +172,27 @@ def test_exact_snr_split(form):
         for f in ('approx', 'zr', 'zi'):
             assert split['rebuilt'][f][j] == c0[f][i], (k, f)
     assert (split['rebuilt']['unit'] == -1).all()
+
+
+def test_exact_stage_order_is_bitwise_neutral():
+    """The exact stage in template-row, chunk-major order (gwb_bin_sums_ordered) gives the same peaks, bit for bit,
+    as the group-major order."""
+    from gwb200 import fp_filter, pipeline
+    bank, D, IP, kmin, inj = _case()
+    Dd, IPd = torch.from_numpy(D).cuda(), torch.from_numpy(IP).cuda()
+    sw, isw = fp_filter.derive_sw(IPd)
+    out = {}
+    for order in (False, True):
+        cfg = pipeline.FilterConfig(tile=24, eps=1e-3, nbins=16, snr_threshold=4.5, margin=0.04, form='f16',
+                                    cand_cap=1 << 18, exact_order=order)
+        B = pipeline.Bank(bank, FLEN, DF, sw, cfg)
+        mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg)
+        mf.step(Dd, IPd, isw)
+        torch.cuda.synchronize()
+        out[order] = mf.results()
+    a, b = out[False], out[True]
+    assert a['n_candidates'] == b['n_candidates'] > 100
+    ka = {(c['row'], c['seg'], c['sample']): p for c, p in zip(a['cands'], a['peaks'])}
+    for c, p in zip(b['cands'], b['peaks']):
+        q = ka[(c['row'], c['seg'], c['sample'])]
+        assert p.tobytes() == q.tobytes()
