@@ -33,6 +33,11 @@ struct __align__(64) CplxArgs {
     long long ldv;
     long long Tn;
     int M, Kh, ntiles, group, nout, stages, MB, KC;
+    // tile-granular CTA ranges (balanced to one tile): windows cut by a range boundary are written as partial
+    // (max, first index) records, pv/pi[(row * gridDim.x + cta) * 2 + slot] (slot 0: the window began before the
+    // CTA's range, 1: it goes on after it), and merged by window_merge_kernel; null: window-aligned ranges
+    float* pv;
+    int32_t* pi;
     DeviceError* err;
 };
 
@@ -90,10 +95,16 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * 128 * MB;
     const int MBe = min(MB, (args.M - m0 + 127) / 128);
-    const long long o0 = (long long)blockIdx.x * args.nout / gridDim.x;
-    const long long o1 = (long long)(blockIdx.x + 1) * args.nout / gridDim.x;
-    const int t_begin = (int)(o0 * args.group);
-    const int t_end = (int)min(o1 * (long long)args.group, (long long)args.ntiles);
+    int t_begin, t_end;
+    if (args.pv) {
+        t_begin = (int)((long long)blockIdx.x * args.ntiles / gridDim.x);
+        t_end = (int)((long long)(blockIdx.x + 1) * args.ntiles / gridDim.x);
+    } else {
+        const long long o0 = (long long)blockIdx.x * args.nout / gridDim.x;
+        const long long o1 = (long long)(blockIdx.x + 1) * args.nout / gridDim.x;
+        t_begin = (int)(o0 * args.group);
+        t_end = (int)min(o1 * (long long)args.group, (long long)args.ntiles);
+    }
     const int ntl = t_end - t_begin;
     if (ntl <= 0 || MBe <= 0) return;
     const int nfill = ntl * nkc;   // Z stages consumed by this CTA
@@ -336,8 +347,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                         bi = oi;
                     }
                     const int gi = (int)(col0 + bi);
-                    const bool first = (t % args.group) == 0;
-                    const bool last = ((t + 1) % args.group) == 0 || t == args.ntiles - 1;
+                    const bool first = (t % args.group) == 0 || t == t_begin;
+                    const bool last = ((t + 1) % args.group) == 0 || t == args.ntiles - 1 || t == t_end - 1;
                     float& wb = (mb == 0) ? wb0 : wb1;
                     int& wi = (mb == 0) ? wi0 : wi1;
                     if (first || best > wb) {
@@ -348,13 +359,22 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                         const int row = m0 + mb * 128 + rl;
                         if (row < args.M) {
                             const long long o = t / args.group;
-                            float vo = wb;
-                            if (args.rowscale) {
-                                const float rs = args.rowscale[row];
-                                vo = wb * rs * rs;
+                            const int w0 = (int)(o * args.group);
+                            const int w1 = (int)min((long long)w0 + args.group, (long long)args.ntiles);
+                            if (args.pv && (t_begin > w0 || t_end < w1)) {
+                                const long long pidx = ((long long)row * gridDim.x + blockIdx.x) * 2 +
+                                                       (t_begin > w0 ? 0 : 1);
+                                args.pv[pidx] = wb;
+                                args.pi[pidx] = wi;
+                            } else {
+                                float vo = wb;
+                                if (args.rowscale) {
+                                    const float rs = args.rowscale[row];
+                                    vo = wb * rs * rs;
+                                }
+                                args.V[(long long)row * args.ldv + o] = vo;
+                                args.I[(long long)row * args.ldv + o] = wi;
                             }
-                            args.V[(long long)row * args.ldv + o] = vo;
-                            args.I[(long long)row * args.ldv + o] = wi;
                         }
                     }
                 }
@@ -368,10 +388,48 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
     }
 }
 
+// Windows cut by the tile-granular CTA ranges: per (row, window) whose first and last tiles lie in different CTAs,
+// the maximum over the CTAs' partial records in CTA order (strictly greater replaces, so the first index wins ties as
+// in one pass), then V (times rowscale^2 for fp8) and I.
+__device__ __forceinline__ int cta_of_tile(int t, int ntiles, int g) {
+    int c = (int)(((long long)t * g) / ntiles);
+    while (c + 1 < g && (long long)(c + 1) * ntiles / g <= t) ++c;
+    while (c > 0 && (long long)c * ntiles / g > t) --c;
+    return c;
+}
+
+__global__ void window_merge_kernel(int M, int ntiles, int group, int nout, int g, const float* __restrict__ pv,
+                                    const int32_t* __restrict__ pi, const float* __restrict__ rowscale,
+                                    float* __restrict__ V, int32_t* __restrict__ I, long long ldv) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)M * nout) return;
+    const int row = (int)(e / nout), o = (int)(e % nout);
+    const int w0 = o * group, w1 = min(w0 + group, ntiles);
+    const int ca = cta_of_tile(w0, ntiles, g), cb = cta_of_tile(w1 - 1, ntiles, g);
+    if (ca == cb) return;
+    float best = -1.f;
+    int bi = 0;
+    for (int c = ca; c <= cb; ++c) {
+        const int tb = (int)((long long)c * ntiles / g);
+        const long long pidx = ((long long)row * g + c) * 2 + (tb > w0 ? 0 : 1);
+        const float v = pv[pidx];
+        if (v > best) {
+            best = v;
+            bi = pi[pidx];
+        }
+    }
+    if (rowscale) {
+        const float rs = rowscale[row];
+        best = best * rs * rs;
+    }
+    V[(long long)row * ldv + o] = best;
+    I[(long long)row * ldv + o] = bi;
+}
+
 template <int FORM>
 int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long long ldz, int M, int Kh,
-                long long Tn, int group, float* V, int32_t* I, long long ldv, const float* rowscale,
-                cudaStream_t stream) {
+                long long Tn, int group, float* V, int32_t* I, long long ldv, const float* rowscale, void* work,
+                long long work_bytes, cudaStream_t stream) {
     using C = Cfg<FORM>;
     GWB_CHECK_ARG(M > 0 && Tn > 0 && group > 0, GWB_ERR_SHAPE, "fused_peaks_cplx: M=%d Tn=%lld group=%d", M, Tn, group);
     GWB_CHECK_ARG(Kh > 0 && Kh % C::KSTEP == 0, GWB_ERR_SHAPE,
@@ -436,26 +494,61 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     auto kern = umma_cplx_kernel<FORM>;
     GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int mgroups = (M + 128 * MB - 1) / (128 * MB);
-    const int gx = (int)std::max(1ll, std::min(nout, (long long)std::max(1, num_sms() / mgroups)));
+    const long long per = (long long)std::max(1, num_sms() / mgroups);
+    // with a workspace the CTA ranges are tile-granular (balanced to one tile; split windows merged afterwards),
+    // without one they are whole windows (up to one window of imbalance)
+    const bool split = work != nullptr;
+    if (split) {
+        GWB_CHECK_ARG(work_bytes >= 16ll * M * per, GWB_ERR_SHAPE,
+                      "fused_peaks_cplx: work %lld bytes, %lld needed", work_bytes, 16ll * M * per);
+        GWB_CHECK_ARG(aligned(work, 16), GWB_ERR_ALIGN, "fused_peaks_cplx: work misaligned");
+    }
+    const int gx = (int)std::max(1ll, std::min(split ? ntiles : nout, per));
+    if (split) {
+        args.pv = static_cast<float*>(work);
+        args.pi = reinterpret_cast<int32_t*>(static_cast<char*>(work) + 8ll * M * gx);
+    }
     kern<<<dim3(gx, mgroups), kThreads, smem, stream>>>(args);
     GWB_LAUNCH_CHECK("umma_cplx_kernel");
+    if (split && gx > 1) {
+        bool any = false;           // a range boundary inside a window
+        for (int c = 1; c < gx && !any; ++c) any = ((long long)c * ntiles / gx) % group != 0;
+        if (any) {
+            const long long ne = (long long)M * nout;
+            window_merge_kernel<<<(unsigned)cdiv(ne, 256), 256, 0, stream>>>(M, (int)ntiles, group, (int)nout, gx,
+                                                                            args.pv, args.pi, args.rowscale, V, I,
+                                                                            ldv);
+            GWB_LAUNCH_CHECK("window_merge_kernel");
+        }
+    }
     return GWB_OK;
 }
 
 }  // namespace
 }  // namespace gwb
 
+extern "C" long long gwb_fused_peaks_cplx_work_bytes(int M) { return 16ll * M * gwb::num_sms(); }
+
 extern "C" int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
                                     const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,
-                                    int32_t* I, long long ldv, const float* rowscale, void* stream) {
+                                    int32_t* I, long long ldv, const float* rowscale, void* work,
+                                    long long work_bytes, void* stream) {
     const void* A[2] = {A_hi, A_lo};
     const void* Z[2] = {Z_hi, Z_lo};
     cudaStream_t s = (cudaStream_t)stream;
     switch (form) {
-        case 0: return gwb::launch_cplx<0>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
-        case 1: return gwb::launch_cplx<1>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
-        case 2: return gwb::launch_cplx<2>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
-        case 3: return gwb::launch_cplx<3>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, s);
+        case 0:
+            return gwb::launch_cplx<0>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, work, work_bytes,
+                                        s);
+        case 1:
+            return gwb::launch_cplx<1>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, work, work_bytes,
+                                        s);
+        case 2:
+            return gwb::launch_cplx<2>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, work, work_bytes,
+                                        s);
+        case 3:
+            return gwb::launch_cplx<3>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, work, work_bytes,
+                                        s);
         default:
             gwb::set_error("fused_peaks_cplx: form %d (0 fp16, 1 bf16, 2 split bf16, 3 fp8 e4m3)", form);
             return GWB_ERR_ARG;

@@ -41,7 +41,8 @@ SIGNATURES = {
     'gwb_fused_peaks_f16': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_bf16x3': [_P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_f32': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
-    'gwb_fused_peaks_cplx': [_I, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P, _P],
+    'gwb_fused_peaks_cplx': [_I, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P, _P, _LL, _P],
+    'gwb_fused_peaks_cplx_work_bytes': [_I],
     'gwb_basis_premul': [_P, _LL, _I, _P, _LL, _I, _P, _LL, _P, _LL, _P],
     'gwb_basis_scale': [_P, _LL, _I, _LL, _LL, _P, _I, _P, _P, _P],
     'gwb_fft_twiddles': [_LL, _P, _P],
@@ -115,6 +116,7 @@ def load():
             f.restype = ctypes.c_int
         lib.gwb_consolidate_work_bytes.restype = ctypes.c_longlong
         lib.gwb_bin_sums_work_bytes.restype = ctypes.c_longlong
+        lib.gwb_fused_peaks_cplx_work_bytes.restype = ctypes.c_longlong
         _lib = lib
     return _lib
 

@@ -47,10 +47,13 @@ def gemm(a):
     nw = Tn // 2048
     V = torch.empty((n, nw), dtype=torch.float32, device='cuda')
     I = torch.empty((n, nw), dtype=torch.int32, device='cuda')
+    work = torch.empty(_lib.load().gwb_fused_peaks_cplx_work_bytes(n), dtype=torch.uint8, device='cuda')
+    wk = None if a.no_split else work
 
     def f():
         _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(A), _lib.ptr(lo[0]), A.stride(0), _lib.ptr(Z), _lib.ptr(lo[1]),
-                  Z.stride(0), n, Kh, Tn, 16, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rs), _lib.stream_ptr())
+                  Z.stride(0), n, Kh, Tn, 16, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rs), _lib.ptr(wk),
+                  0 if wk is None else wk.numel(), _lib.stream_ptr())
     ms = _time(f, a.reps)
     useful = 8.0 * n * r * Tn
     issued = (3 if code == 2 else 1) * 4.0 * n * 2 * Kh * Tn
@@ -283,6 +286,7 @@ def main():
     ap.add_argument('--seed', type=int, default=4)
     ap.add_argument('--no-graph', action='store_true')
     ap.add_argument('--production', action='store_true')
+    ap.add_argument('--no-split', action='store_true', help='gemm: whole windows per CTA (no partial-window merge)')
     ap.add_argument('--triggers', type=int, default=4096)
     ap.add_argument('--r', type=int, default=128)
     ap.add_argument('--n', type=int, default=256)

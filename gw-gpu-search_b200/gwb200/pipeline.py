@@ -128,6 +128,9 @@ class MatchedFilter:
         self.Aim_lo = None
         self.sa = torch.empty(nmax, dtype=torch.float32, device=device) if self.fp8 else None   # A row scales
         self.V = torch.empty((nmax, self.nw), dtype=torch.float32, device=device)
+        # partial window maxima of the GEMM's tile-granular CTA ranges
+        self.gemm_work = torch.empty(_lib.load().gwb_fused_peaks_cplx_work_bytes(nmax), dtype=torch.uint8,
+                                     device=device) if self.compact else None
         self.I = torch.empty((nmax, self.nw), dtype=torch.int32, device=device)
         cap = cfg.cand_cap
         self.cands = torch.empty(cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
@@ -165,7 +168,8 @@ class MatchedFilter:
             code = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}[self.form]
             _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(self.Are), _lib.ptr(self.Are_lo), self.Are.stride(0),
                       _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), n, Kh, self.Tn, self.group,
-                      _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), _lib.ptr(self.sa), s)
+                      _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), _lib.ptr(self.sa),
+                      _lib.ptr(self.gemm_work), self.gemm_work.numel(), s)
         else:
             _lib.call('gwb_fused_peaks_f32', _lib.ptr(self.Are), _lib.ptr(self.Aim), self.Are.stride(0),
                       _lib.ptr(self.Z), self.Z.stride(0), n, K, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I),

@@ -116,10 +116,15 @@ GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long ld
  * 1: bf16; 2: split bf16 with A_lo, Z_lo (hi.hi + hi.lo + lo.hi); 3: fp8 e4m3 (the screening form, no reference
  * counterpart; Kh a multiple of 32), V = rowscale[i]^2 max |z|^2 with rowscale the per-row scale of A
  * (gwb_stacked_a8); rowscale is ignored by the other forms (may be NULL). Kh <= 192 (forms 0, 1, 3) or 128 (form 2).
- * lda, ldz in elements, multiples of 16 bytes. */
+ * lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
+ * be NULL): with it the CTAs take tile-granular ranges of the time axis (balanced to one 128-sample tile) and windows
+ * cut by a range boundary are merged by a second kernel, bit for bit the same V and I; without it every CTA takes
+ * whole windows (up to one window of imbalance between CTAs). */
+GWB_API long long gwb_fused_peaks_cplx_work_bytes(int M);
 GWB_API int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
                                  const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,
-                                 int32_t* I, long long ldv, const float* rowscale, void* stream);
+                                 int32_t* I, long long ldv, const float* rowscale, void* work, long long work_bytes,
+                                 void* stream);
 
 /* ---- handle and transforms (cuFFT) ----------------------------------------------------------------------------- */
 /* The handle caches cuFFT plans per (kind, n, batch, strides); plans are made on first use of a shape. Transforms are

@@ -168,8 +168,11 @@ def _compact(rng, M, r, Kh, Tn, dtype):
 
 @pytest.mark.parametrize('M,r,Tn,group', [(256, 60, 2048 * 20, 16), (256, 190, 2048 * 6, 16), (300, 100, 40000, 1),
                                           (100, 17, 2048 * 3 + 384, 4)])
-def test_cplx_f16_against_oracle(M, r, Tn, group):
+@pytest.mark.parametrize('split', [False, True])
+def test_cplx_f16_against_oracle(M, r, Tn, group, split):
     from gwb200 import _lib
+    work = torch.empty(_lib.load().gwb_fused_peaks_cplx_work_bytes(M), dtype=torch.uint8, device='cuda') if split \
+        else None
     rng = np.random.default_rng(r + M)
     Kh = -(-r // 16) * 16
     A, Z, Are, Aim = _compact(rng, M, r, Kh, Tn, np.float16)
@@ -178,7 +181,8 @@ def test_cplx_f16_against_oracle(M, r, Tn, group):
     V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
     I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
     _lib.call('gwb_fused_peaks_cplx', 0, _lib.ptr(Ad), None, Ad.stride(0), _lib.ptr(Zd), None, Zd.stride(0), M, Kh, Tn,
-              group, _lib.ptr(V), _lib.ptr(I), V.stride(0), None, _lib.stream_ptr())
+              group, _lib.ptr(V), _lib.ptr(I), V.stride(0), None, _lib.ptr(work), 0 if work is None else work.numel(),
+              _lib.stream_ptr())
     Vr, Ir = og.gemm_absmax(Are, Aim, Z, M, Tn)
     tie = _near_tie_mask(Are, Aim, Z, M, Tn, Ir)
     if group > 1:
@@ -206,7 +210,7 @@ def test_cplx_bf16_forms_against_oracle(form, r):
     I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
     _lib.call('gwb_fused_peaks_cplx', form, _lib.ptr(Ah), _lib.ptr(Al if form == 2 else None), Ah.stride(0),
               _lib.ptr(Zh), _lib.ptr(Zl if form == 2 else None), Zh.stride(0), M, Kh, Tn, group, _lib.ptr(V),
-              _lib.ptr(I), V.stride(0), None, _lib.stream_ptr())
+              _lib.ptr(I), V.stride(0), None, None, 0, _lib.stream_ptr())
     Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
     Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
     Vr, Ir = og.group_reduce(*og.gemm_absmax(Are, Aim, Z, M, Tn), group)
@@ -224,7 +228,7 @@ def test_cplx_rejects_oversized_kh():
         V = torch.empty((256, 2), dtype=torch.float32, device='cuda')
         I = torch.empty((256, 2), dtype=torch.int32, device='cuda')
         _lib.call('gwb_fused_peaks_cplx', 2, _lib.ptr(x), _lib.ptr(x), 512, _lib.ptr(z), _lib.ptr(z), 4096, 256, 256,
-                  4096, 16, _lib.ptr(V), _lib.ptr(I), 2, None, _lib.stream_ptr())
+                  4096, 16, _lib.ptr(V), _lib.ptr(I), 2, None, None, 0, _lib.stream_ptr())
 
 
 @pytest.mark.parametrize('r', [96, 150])
@@ -248,10 +252,14 @@ def test_cplx_fp8_integer_operands_exact(r):
     nout = -(-(Tn // 128) // group)
     V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
     I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
-    _lib.call('gwb_fused_peaks_cplx', 3, _lib.ptr(A8), None, A8.stride(0), _lib.ptr(Z8), None, Z8.stride(0), M, Kh, Tn,
-              group, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rsd), _lib.stream_ptr())
     Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
     Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
     Vr, Ir = og.group_reduce(*og.gemm_absmax(Are, Aim, Z, M, Tn), group)
-    assert np.array_equal(V.cpu().numpy(), (Vr * rs[:, None] ** 2).astype(np.float32))
-    assert np.array_equal(I.cpu().numpy(), Ir)
+    work = torch.empty(_lib.load().gwb_fused_peaks_cplx_work_bytes(M), dtype=torch.uint8, device='cuda')
+    for wk in (None, work):          # whole windows per CTA, and tile-granular ranges with merged windows
+        V.fill_(-7.0)
+        _lib.call('gwb_fused_peaks_cplx', 3, _lib.ptr(A8), None, A8.stride(0), _lib.ptr(Z8), None, Z8.stride(0), M, Kh,
+                  Tn, group, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rsd), _lib.ptr(wk),
+                  0 if wk is None else wk.numel(), _lib.stream_ptr())
+        assert np.array_equal(V.cpu().numpy(), (Vr * rs[:, None] ** 2).astype(np.float32))
+        assert np.array_equal(I.cpu().numpy(), Ir)
