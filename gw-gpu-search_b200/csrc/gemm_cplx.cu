@@ -13,6 +13,8 @@
 // Forms: 0 fp16 (one product), 1 bf16 (one product), 2 split bf16 (hi.hi + hi.lo + lo.hi, about 16 bits), 3 fp8 e4m3
 // (kind::f8f6f4, K = 32 per MMA, 128-byte rows hold 128 elements; the screening form: A rows carry a per-row scale
 // that the epilogue applies, V = rowscale^2 max |z|^2).
+#include <stdlib.h>
+#include <string.h>
 #include "common.cuh"
 
 namespace gwb {
@@ -388,6 +390,271 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// The CTA-pair form (fp16 / bf16): a cluster of two CTAs along x, M blocks 2p (rank 0) and 2p + 1 (rank 1) of the
+// same time range (grid y). Each CTA keeps its own 128 rows of A resident and loads its own 64-sample half of every Z tile; rank 0
+// issues tcgen05.mma.cta_group::2 with M = 256 (each SM computes its 128 rows over all 128 samples, the Z halves
+// shared between the SMs), so per SM the MMAs read half the Z bytes from shared memory. Barriers: the loads of both
+// CTAs complete on rank 0's full / barA barriers; MMA commits arrive on the barriers at the same offset in both
+// CTAs (empty, tfull, done); both CTAs' epilogue warps arrive on rank 0's tempty. Every wait is bounded; every path
+// reaches the final cluster barrier.
+// ---------------------------------------------------------------------------------------------------------------------
+// Shared memory of one CTA of a pair: A (128 rows x 2 Kh, 128-byte rows of 64 elements), stages of (re, im) x KC
+// rows x 64 samples (one 128-byte row each), the epilogue's exchange, the barriers.
+__host__ __device__ inline Layout layout_pair(int Kh, int KC, int stages) {
+    Layout L;
+    L.a_tiles = (uint32_t)((2 * Kh + 63) / 64);
+    L.a_bytes = L.a_tiles * kATile;
+    L.z_off = L.a_bytes;
+    L.stage_bytes = 2u * (uint32_t)KC * 128u;
+    L.x_off = L.z_off + (uint32_t)stages * L.stage_bytes;
+    L.bar_off = L.x_off + 2048u;
+    L.total = L.bar_off + (uint32_t)(2 * stages + 6) * 8u + 16u;
+    return L;
+}
+
+template <int FORM>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    umma_cplx2_kernel(const __grid_constant__ CplxArgs args) {
+    using C = Cfg<FORM>;
+    static_assert(C::NH == 1 && !C::F8, "the CTA-pair form takes one 16-bit product");
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
+    const int Kh = args.Kh, KC = args.KC, S = args.stages;
+    const Layout L = layout_pair(Kh, KC, S);
+    const int nkc = (Kh + KC - 1) / KC;
+    uint8_t* sA = smem;
+    uint8_t* sZ = smem + L.z_off;
+    float* xv = reinterpret_cast<float*>(smem + L.x_off);
+    int* xi = reinterpret_cast<int*>(smem + L.x_off + 1024);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + S;
+    uint64_t* tfull = bars + 2 * S;
+    uint64_t* tempty = tfull + 2;
+    uint64_t* barA = tempty + 2;
+    uint64_t* done = barA + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const bool leader = rank == 0;
+    // grid: x = M block (the pair along x: ranks 0, 1 = M blocks 2p, 2p + 1), y = time range
+    const int m0 = blockIdx.x * 128;
+    const int tr = blockIdx.y;
+    const int t_begin = (int)((long long)tr * args.ntiles / gridDim.y);
+    const int t_end = (int)((long long)(tr + 1) * args.ntiles / gridDim.y);
+    const int ntl = t_end - t_begin;                         // the same in both CTAs of the pair
+    const int nfill = ntl * nkc;
+    const uint32_t a_bytes = (uint32_t)(L.a_tiles * kATile);
+    const uint32_t half_stage = L.stage_bytes;               // one CTA's half of a stage
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 2 * kEpiWarps);
+        }
+        mbar_init(barA, 1);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+    }
+    if (warp == 1) {
+        tmem_alloc_pair(tmem_slot, kTmemCols);
+        tmem_relinquish_pair();
+        tc_fence_before();
+    }
+    __syncthreads();
+    cluster_sync_all();                                      // the peer's barriers are initialised before any arrival
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (ntl > 0 && warp == 0) {
+        if (lane == 0) {
+            prefetch_tmap(&args.tA[0]);
+            prefetch_tmap(&args.tZ[0]);
+            const uint32_t barA_l = mapa_shared(smem_u32(barA), 0);
+            if (leader) mbar_arrive_expect_tx(barA, 2u * a_bytes);
+            for (int a = 0; a < (int)L.a_tiles; ++a)
+                tma_load_2d_pair(sA + a * kATile, &args.tA[0], barA_l, a * C::ROWEL, m0);
+            for (int f = 0; f < nfill; ++f) {
+                const int s = f % S;
+                const uint32_t n = (uint32_t)(f / S);
+                const int i = f / nkc, kc = f % nkc;
+                if (*abort_flag) break;
+                if (!mbar_wait_bounded(&empty[s], (n & 1) ^ 1)) {
+                    record_error(args.err, GWB_ERR_TIMEOUT, 211, tr, f);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (leader) mbar_arrive_expect_tx(&full[s], 2u * half_stage);
+                const uint32_t full_l = mapa_shared(smem_u32(&full[s]), 0);
+                const int x = (t_begin + i) * kTile + 64 * (int)rank;
+                uint8_t* st = sZ + s * half_stage;
+                for (int ri = 0; ri < 2; ++ri)
+                    tma_load_2d_pair(st + ri * KC * 128, &args.tZ[0], full_l, x, ri * Kh + kc * KC);
+            }
+        }
+    } else if (ntl > 0 && warp == 1) {
+        if (lane == 0 && leader) {
+            const uint32_t idesc = instr_desc(256, 128, C::FMT, C::FMT, 0, 1);
+            const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
+            const uint32_t a_base = smem_u32(sA), z_base = smem_u32(sZ);
+            bool ok = mbar_wait_bounded(barA, 0);
+            if (!ok) {
+                record_error(args.err, GWB_ERR_TIMEOUT, 212, tr, 0);
+                *abort_flag = 1;
+            }
+            tc_fence_after();
+            for (int i = 0; i < ntl && ok; ++i) {
+                const int b = i & 1;
+                const uint32_t u = (uint32_t)(i >> 1);
+                if (!mbar_wait_bounded(&tempty[b], (u & 1) ^ 1)) {
+                    record_error(args.err, GWB_ERR_TIMEOUT, 214, tr, i);
+                    *abort_flag = 1;
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
+                for (int kc = 0; kc < nkc && ok; ++kc) {
+                    const int f = i * nkc + kc;
+                    if (*abort_flag || !mbar_wait_bounded(&full[f % S], (uint32_t)((f / S) & 1))) {
+                        record_error(args.err, GWB_ERR_TIMEOUT, 213, tr, f);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = z_base + (f % S) * half_stage;
+                    const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
+                    for (int sk = 0; sk < nsteps; ++sk) {
+                        const int k = kc * KC + sk * C::KSTEP;
+                        const uint32_t are = a_base + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
+                        const uint32_t aim = a_base + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
+                        const uint32_t zre = st + sk * C::KSTEP * 128;
+                        const uint32_t zim = st + KC * 128 + sk * C::KSTEP * 128;
+                        const uint64_t dAre = smem_desc(are, 16, 1024, 2), dAim = smem_desc(aim, 16, 1024, 2);
+                        const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
+                        const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                        const uint32_t acc = (kc > 0 || sk > 0) ? 1u : 0u;
+                        umma_f16_pair(dre, dAre, dZre, idesc, acc);
+                        umma_f16_pair(dre, dAim, dZim, idesc_neg, 1u);
+                        umma_f16_pair(dim, dAim, dZre, idesc, acc);
+                        umma_f16_pair(dim, dAre, dZim, idesc, 1u);
+                    }
+                    umma_commit_pair(&empty[f % S]);
+                }
+                if (ok) umma_commit_pair(&tfull[b]);
+            }
+            umma_commit_pair(done);
+        }
+        __syncwarp();
+        if (lane == 0 && !mbar_wait_bounded(done, 0)) {   // every MMA of the pair has completed
+            record_error(args.err, GWB_ERR_TIMEOUT, 216, tr, (int)rank);
+            *abort_flag = 1;
+        }
+        __syncwarp();
+    } else if (ntl > 0) {
+        const int q = warp & 3, hh = (warp - 2) >> 2;
+        const int rl = 32 * q + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * q) << 16);
+        const uint32_t tempty_l0 = mapa_shared(smem_u32(&tempty[0]), 0);
+        const uint32_t tempty_l1 = mapa_shared(smem_u32(&tempty[1]), 0);
+        float wb = -1.f;
+        int wi = 0;
+        for (int i = 0; i < ntl; ++i) {
+            const int t = t_begin + i;
+            const long long col0 = (long long)t * kTile;
+            const bool full_tile = col0 + kTile <= args.Tn;
+            const int b = i & 1;
+            const uint32_t u = (uint32_t)(i >> 1);
+            float best = -1.f;
+            int bi = 0;
+            if (*abort_flag || !mbar_wait_bounded(&tfull[b], u & 1)) {
+                record_error(args.err, GWB_ERR_TIMEOUT, 215, tr, i);
+                *abort_flag = 1;
+            } else {
+                tc_fence_after();
+#pragma unroll
+                for (int c = 0; c < 64; c += 32) {
+                    uint32_t re[32], im[32];
+                    tmem_ld_32x32b_x32(lane_base + (uint32_t)(b * 256 + hh * 64 + c), re);
+                    tmem_ld_32x32b_x32(lane_base + (uint32_t)(b * 256 + 128 + hh * 64 + c), im);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) asm volatile("" : "+r"(re[jj]), "+r"(im[jj]));
+                    const int cb = hh * 64 + c;
+                    const int valid = full_tile ? 32 : (int)min((long long)32, max(0ll, args.Tn - (col0 + cb)));
+                    float lb = -1.f;
+                    int lj = 0;
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) {
+                        const float xr = __uint_as_float(re[jj]), xm = __uint_as_float(im[jj]);
+                        const float p = jj < valid ? fmaf(xr, xr, xm * xm) : -1.f;
+                        if (p > lb) {
+                            lb = p;
+                            lj = jj;
+                        }
+                    }
+                    if (lb > best) {
+                        best = lb;
+                        bi = cb + lj;
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(b ? tempty_l1 : tempty_l0);
+            if (hh == 1) {
+                xv[b * 128 + rl] = best;
+                xi[b * 128 + rl] = bi;
+            }
+            named_bar_sync(1, 32 * kEpiWarps);
+            if (hh == 0) {
+                const float ob = xv[b * 128 + rl];
+                const int oi = xi[b * 128 + rl];
+                if (ob > best) {
+                    best = ob;
+                    bi = oi;
+                }
+                const int gi = (int)(col0 + bi);
+                const bool first = (t % args.group) == 0 || t == t_begin;
+                const bool last = ((t + 1) % args.group) == 0 || t == args.ntiles - 1 || t == t_end - 1;
+                if (first || best > wb) {
+                    wb = best;
+                    wi = gi;
+                }
+                const int row = m0 + rl;
+                if (last && row < args.M) {
+                    const long long o = t / args.group;
+                    const int w0 = (int)(o * args.group);
+                    const int w1 = (int)min((long long)w0 + args.group, (long long)args.ntiles);
+                    if (args.pv && (t_begin > w0 || t_end < w1)) {
+                        const long long pidx = ((long long)row * gridDim.y + tr) * 2 + (t_begin > w0 ? 0 : 1);
+                        args.pv[pidx] = wb;
+                        args.pi[pidx] = wi;
+                    } else {
+                        args.V[(long long)row * args.ldv + o] = wb;
+                        args.I[(long long)row * args.ldv + o] = wi;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    cluster_sync_all();                                      // no CTA leaves while its peer may still signal it
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc_pair(tmem, kTmemCols);
+    }
+}
+
 // Windows cut by the tile-granular CTA ranges: per (row, window) whose first and last tiles lie in different CTAs,
 // the maximum over the CTAs' partial records in CTA order (strictly greater replaces, so the first index wins ties as
 // in one pass), then V (times rowscale^2 for fp8) and I.
@@ -424,6 +691,65 @@ __global__ void window_merge_kernel(int M, int ntiles, int group, int nout, int 
     }
     V[(long long)row * ldv + o] = best;
     I[(long long)row * ldv + o] = bi;
+}
+
+// CTA pairs are the default for fp16 / bf16; GWB_GEMM_PAIR=0 selects the one-CTA kernel (for comparison)
+inline bool pair_mode() {
+    static const bool on = [] {
+        const char* e = getenv("GWB_GEMM_PAIR");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <int FORM>
+int launch_pair(CplxArgs args, int M, long long ntiles, long long nout, int group, float* V, int32_t* I,
+                long long ldv, void* work, long long work_bytes, cudaStream_t stream) {
+    const uint32_t max_smem = 227 * 1024;
+    const int KC = 64;
+    int stages = 8;
+    while (stages > 0 && layout_pair(args.Kh, KC, stages).total + 1024 > max_smem) --stages;
+    GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d does not fit the CTA-pair form", args.Kh);
+    const int npair = (M + 255) / 256;
+    const long long per = (long long)std::max(1, num_sms() / (2 * npair));
+    const int gx = (int)std::max(1ll, std::min(ntiles, per));
+    GWB_CHECK_ARG(work_bytes >= 16ll * M * gx, GWB_ERR_SHAPE, "fused_peaks_cplx: work %lld bytes, %lld needed",
+                  work_bytes, 16ll * M * gx);
+    args.stages = stages;
+    args.KC = KC;
+    args.MB = 1;
+    args.pv = static_cast<float*>(work);
+    args.pi = reinterpret_cast<int32_t*>(static_cast<char*>(work) + 8ll * M * gx);
+    const uint32_t smem = layout_pair(args.Kh, KC, stages).total + 1024;
+    auto kern = umma_cplx2_kernel<FORM>;
+    GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<dim3(2 * npair, gx), kThreads, smem, stream>>>(args);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+        // what the occupancy calculator says about this cluster shape, for the message
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        cfg.gridDim = dim3(2 * npair, gx);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = smem;
+        int nclusters = -1;
+        cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg);
+        cudaGetLastError();
+        set_error("umma_cplx2_kernel launch (grid %d x %d, cluster 2 x 1, %u bytes of shared memory; max active "
+                  "clusters %d): %s", 2 * npair, gx, smem, nclusters, cudaGetErrorString(le));
+        return GWB_ERR_CUDA;
+    }
+    if (gx > 1) {
+        bool any = false;
+        for (int c = 1; c < gx && !any; ++c) any = ((long long)c * ntiles / gx) % group != 0;
+        if (any) {
+            const long long ne = (long long)M * nout;
+            window_merge_kernel<<<(unsigned)cdiv(ne, 256), 256, 0, stream>>>(M, (int)ntiles, group, (int)nout, gx,
+                                                                            args.pv, args.pi, nullptr, V, I, ldv);
+            GWB_LAUNCH_CHECK("window_merge_kernel");
+        }
+    }
+    return GWB_OK;
 }
 
 template <int FORM>
@@ -493,6 +819,10 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     const uint32_t smem = layout_of(C::NH, MB, Kh, KC, stages, C::ROWEL).total + 1024;
     auto kern = umma_cplx_kernel<FORM>;
     GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if constexpr (FORM == 0 || FORM == 1) {
+        if (work != nullptr && pair_mode()) return launch_pair<FORM>(args, M, ntiles, nout, group, V, I, ldv, work,
+                                                                     work_bytes, stream);
+    }
     const int mgroups = (M + 128 * MB - 1) / (128 * MB);
     const long long per = (long long)std::max(1, num_sms() / mgroups);
     // with a workspace the CTA ranges are tile-granular (balanced to one tile; split windows merged afterwards),
