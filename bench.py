@@ -263,6 +263,7 @@ def main():
     import torch
     import torch.distributed as dist
     from gwb200 import _lib, gpu_prep, pipeline, fp_filter
+    from gwb200 import dist as gdist
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
@@ -328,10 +329,7 @@ def main():
         barrier()
         ms = ev0.elapsed_time(ev1) / nsteps
         launches = (cond.launches - l0c + mf.kernel_launches - l0m) // nsteps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = gdist.max_over_ranks(ms, dev)
         # end to end through the public API: strain from pinned host memory, results back to the host
         res_bytes = 0
         torch.cuda.synchronize()
@@ -348,10 +346,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         ms_e2e = ee0.elapsed_time(ee1) / nsteps
-        if world > 1:
-            t = torch.tensor([ms_e2e], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e2e = float(t.item())
+        ms_e2e = gdist.max_over_ranks(ms_e2e, dev)
         # dominant kernel: the fused reconstruction GEMM, each launch bracketed by events in one extra step
         mf.profile = {}
         ec = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
