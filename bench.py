@@ -232,7 +232,7 @@ def top_peak_sets(kept, thr):
 def traffic_ratios():
     """Measured DRAM bytes over algorithmic bytes, from the committed ncu summaries (lines 'traffic_ratio: X')."""
     out = {}
-    for key, name in (('basis', 'basis_passes_c2_r128.md'), ('gemm', 'umma_cplx_kernel_c2_r128.md')):
+    for key, name in (('basis', 'basis_passes_c2_r128.md'), ('gemm', 'umma_cplx2_kernel_c2_r128.md')):
         try:
             for ln in open(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'profiles', name)):
                 if ln.startswith('traffic_ratio:'):
@@ -436,7 +436,7 @@ def main():
                      issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
                      launches=R['n_gemm'], share_of_step=R['gemm_total_ms'] / R['ms'],
                      peak_kind='%s burst bf16' % kind,
-                     traffic_source='profiles/umma_cplx_kernel_c2_r128.md (dram bytes / Z bytes, scaled)')
+                     traffic_source='profiles/umma_cplx2_kernel_c2_r128.md (dram bytes / Z bytes, scaled)')
     line = dict(metric=METRIC, value=R['value'], unit='2-det weeks / GPU-hour', n_gpus=world, steps=a.steps,
                 warmup=a.warmup, ms_per_step=R['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
                 dtype={'bf16x3': 'bf16 hi+lo (fp32 accumulate)', 'f16': 'f16 (fp32 accumulate)',
