@@ -430,7 +430,9 @@ def main():
     ach = R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
     pk = peaks.get('bf16_tflops', 1590.0) if main_form != 'f32' else None
     g_tr = ratios.get('gemm') and ratios['gemm'] * R['z_bytes']
-    roof_gemm = dict(kernel='umma_cplx_kernel (%s)' % main_form if main_form != 'f32' else 'simt_absmax_kernel',
+    gname = {'f16': 'umma_cplx2_kernel (f16, CTA pairs)', 'bf16': 'umma_cplx2_kernel (bf16, CTA pairs)',
+             'f32': 'simt_absmax_kernel'}.get(main_form, 'umma_cplx_kernel (%s)' % main_form)
+    roof_gemm = dict(kernel=gname,
                      bound='tensor', achieved=ach, peak=pk, unit='TFLOP/s', frac=(ach / pk) if pk else None,
                      traffic=g_tr, flops_per_launch_useful=R['useful'], flops_per_launch_issued=R['issued'],
                      issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
