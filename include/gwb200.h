@@ -119,7 +119,9 @@ GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long ld
  * lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
  * be NULL): with it the CTAs take tile-granular ranges of the time axis (balanced to one 128-sample tile) and windows
  * cut by a range boundary are merged by a second kernel, bit for bit the same V and I; without it every CTA takes
- * whole windows (up to one window of imbalance between CTAs). */
+ * whole windows (up to one window of imbalance between CTAs). With work, forms 0 and 1 run on CTA pairs (clusters
+ * of two CTAs, tcgen05.mma.cta_group::2 with M = 256 over two SMs, each SM loading half of every Z tile; the
+ * environment variable GWB_GEMM_PAIR=0 selects the one-CTA kernel). */
 GWB_API long long gwb_fused_peaks_cplx_work_bytes(int M);
 GWB_API int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
                                  const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,
