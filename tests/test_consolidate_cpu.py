@@ -52,3 +52,40 @@ def test_order_keys_replace_positions():
     k0, _ = oc.consolidate(snr, chi, dof, t, [], 1e9, 2048.0, 4.0, 1.072, 3)
     k1, _ = oc.consolidate(snr[perm], chi[perm], dof[perm], t[perm], [], 1e9, 2048.0, 4.0, 1.072, 3, order=perm)
     assert np.array_equal(k1, k0[perm])
+
+
+def test_peak_table_and_file_match_the_oracle(tmp_path):
+    """write_one's datasets (fp_filter.py:910-934) from the library's host assembly equal the oracle's, and the file
+    written without h5py (.npz) holds the same datasets."""
+    from gwb200 import consolidate as gc
+    rng = np.random.default_rng(9)
+    n, gps0, sr = 5000, 1380077576.0, 2048.0
+    h = dict(tid=rng.integers(0, 300, n).astype(np.int64), ti=rng.integers(0, 600 * 2048, n).astype(np.int64),
+             snr=rng.uniform(4, 12, n).astype(np.float32), phase=rng.uniform(-3, 3, n).astype(np.float32),
+             peak_sigmasq=rng.uniform(1, 2, n), exact=rng.uniform(size=n) < 0.4,
+             chisq=rng.uniform(0, 80, n).astype(np.float32))
+    h['dof'] = np.where(h['exact'], 30, 0).astype(np.int32)
+    gates = [(gps0 + 100.0, 0.25, 0.25), (gps0 + 412.5, 0.25, 0.25)]
+    sig = rng.uniform(1, 2, (300, 3))
+    hashes = np.array(['h%04d' % i for i in range(300)])
+    tab = gc.peak_table(h, gates, gps0, sr, sigmasq=sig, hashes=hashes)
+    ref = oc.peak_table(h['tid'], gps0 + h['ti'] / sr, h['snr'], h['phase'], h['peak_sigmasq'], h['exact'], h['chisq'],
+                        h['dof'], gates, sig, hashes=hashes)
+    assert sorted(tab) == sorted(ref)
+    for k, v in ref.items():
+        assert np.array_equal(tab[k], v), k
+    assert len(tab['snr']) < n                              # the gates removed some peaks
+    path = str(tmp_path / 'H1-peaks')
+    gc.write_peaks(path, tab)
+    try:
+        import h5py
+    except ImportError:
+        h5py = None
+    if h5py is None:
+        with np.load(path + '.npz') as z:
+            for k, v in tab.items():
+                assert np.array_equal(z[k], v), k
+    else:
+        with h5py.File(path, 'r') as f:
+            for k, v in tab.items():
+                assert np.array_equal(f[k][()].astype(v.dtype), v), k
