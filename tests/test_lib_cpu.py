@@ -94,3 +94,21 @@ def test_segment_chunks_cover_the_analysable_time_once():
                 cover[s0 + a0:s0 + a1] += 1
         assert cover[int(sp * sr):int((n_s - ep) * sr)].min() == 1 and cover.max() == 1
         assert cover[:int(sp * sr)].max() == 0 and cover[int((n_s - ep) * sr):].max() == 0
+
+
+def test_order_keys_follow_the_reference_append_order():
+    """Consolidation ties go to the earlier peak in the reference's append order (fp_filter.py:700-888: tile, then
+    chunk, then the rebuilt peaks before the exact ones, each in template-row then window order); the int64 keys sort
+    exactly that way, up to the field limits (16-bit rows and windows, 14-bit chunks)."""
+    import numpy as np
+    from gwb200 import segments
+    rng = np.random.default_rng(2)
+    n = 20000
+    f = dict(tile=rng.integers(0, 1 << 12, n), chunk=rng.integers(0, 1 << 14, n), exact=rng.integers(0, 2, n),
+             row=rng.integers(0, 1 << 16, n), window=rng.integers(0, 1 << 16, n))
+    keys = segments.order_keys(f['tile'], f['chunk'], f['exact'], f['row'], f['window'])
+    assert len(np.unique(keys)) == np.unique(np.stack(list(f.values())), axis=1).shape[1]
+    by_key = np.argsort(keys, kind='stable')
+    by_fields = np.lexsort((f['window'], f['row'], f['exact'], f['chunk'], f['tile']))
+    assert np.array_equal(keys[by_key], keys[by_fields])
+    assert (keys >= 0).all()
