@@ -1,6 +1,6 @@
 """Throughput of the B200 matched-filter hot path on the two-detector production workload.
 
-Workload (name: "C2"): two detectors (H, L) with independent noise, 64 chunks of 512 s at 2048 Hz each (2^20
+Workload c2 (the default): two detectors (H, L) with independent noise, 64 chunks of 512 s at 2048 Hz each (2^20
 samples, one analysis segment per chunk with 48 s / 16 s pads, so 448 s analysed per chunk), Gaussian noise coloured
 by the analytic broadband PSD with narrow lines at 60/120/180 Hz, 200 TaylorF2 injections at SNR 6-30; bank of 5,880
 templates (4,612 aligned-spin TaylorF2, 1,268 eccentric), SVD-compressed per tile of 256 with eps = 1e-3; 16
@@ -11,9 +11,18 @@ One step = the whole hot path over all 128 chunks: conditioning (segment FFT, me
 inverse spectrum truncation, D and IP), template norms, then for every (tile, chunk): basis series, stacked A, the
 fused reconstruction GEMM with |z|^2 and windowed argmax, and candidate selection; then the exact stage over every
 candidate (edges, binned sums, snr / chisq / newsnr). The bank (templates and tile SVDs) is built once before timing
-and reported as bank_setup_s. Metric: two-detector weeks of data filtered per GPU-hour.
+and reported as bank_setup_s. Metric: two-detector weeks of data filtered per hour of the job (per GPU-hour at one
+GPU). The first form of --forms gives the line's value; every other form is timed too (fewer steps) and reported
+under `forms`, with the precision of each against float64 over every tile of one chunk.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form bf16x3|f16|f32] [--impl reference]
+Workload c4: the batched form (300 science segments of uneven length, gating, graph-replayed batches); c5: the
+differentiation form (SNR gradients of 4,096 triggers, the 7 x 7 match metric, 20-step refinement).
+
+The reference arm (--impl reference) times the CPU arm (oracle/cpu_arm.py: the reference's numpy conditioning and
+exact stage as restated by the oracle, its tile pass in its own float32 precision with scipy.fft and BLAS over all
+host cores) on the same workload, one step = one chunk's conditioning plus one tile of 256 templates against it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c4|c5] [--forms f16,...] [--impl reference]
 """
 import argparse
 import json
@@ -38,9 +47,16 @@ START_PAD, END_PAD = 48, 16
 A0, A1 = int(START_PAD * SR), int((CHUNK_S - END_PAD) * SR)
 F_LOW = 20.0
 WEEK2 = 2 * 604800.0
+N_TEMPLATES = 5880
 METRIC = "2-det weeks filtered per GPU-hour, 5,880 templates, SNR err<=1e-3: FP32 vs BF16"
+UNIT = '2-det weeks / hour'
 DYN = 5.9029581035870565e+20
 LINES = ((60.0, 1e3, 0.02), (120.0, 1e3, 0.02), (180.0, 1e3, 0.02))
+CW = 2048
+THR, MARGIN = 5.5, 0.04
+DTYPES = {'bf16x3': 'bf16 hi+lo, 3 products (fp32 accumulate)', 'f16': 'f16 (fp32 accumulate)',
+          'bf16': 'bf16 (fp32 accumulate)', 'f32': 'f32',
+          'fp8': 'fp8 e4m3 screen (fp32 accumulate) + float64 exact stage'}
 
 
 def psd_model(f):
@@ -153,68 +169,94 @@ def peaks_file():
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f), 'measured'
-    return dict(hbm_gbs=6650.0, bf16_tflops=1590.0), 'fallback'
+    return dict(hbm_gbs=6650.0, bf16_tflops=1590.0, bf16_tflops_sustained=1400.0), 'fallback'
 
 
-def cpu_reference(bank, n_tiles_sample=1, seed=5):
-    """The CPU (numpy) arm: conditioning of one chunk and the full per-(tile, segment) pass with exact stage for
-    `n_tiles_sample` tiles of 256, timed with all host threads; returns seconds per chunk for the full bank."""
-    from oracle import prep as op, search as osr, filt as of, synth
+# ---------------------------------------------------------------------------------------------------------------------
+# CPU arm: one (chunk, tile) sample per step, on every host core
+# ---------------------------------------------------------------------------------------------------------------------
+CPU_TILES = (0, 11, 22)          # shortest, middle and longest templates of the chirp-time-sorted bank
+
+
+def cpu_setup(bank, tiles=CPU_TILES, seed=5):
+    """The sample tiles (templates, ISCO cut, SVD; bank set-up, not timed) and one chunk of strain."""
+    from oracle import cpu_arm, filt, synth
     rng = np.random.default_rng(seed)
     x = np.fft.irfft(synth.coloured_noise(TLEN, SR, rng, synth.LINES_C2), TLEN).astype(np.float32)
-    t0 = time.perf_counter()
-    out = op.stage2(x, SR, 0, CHUNK_S, START_PAD, END_PAD, F_LOW, 16, 8, 63, 16)
-    t_cond = time.perf_counter() - t0
-    D, IP = out['D'][0], out['IP'][0]
-    sw, isw = of.derive_sw(out['IP'])
-    order = np.argsort(synth.tau0(bank['mass1'], bank['mass2']), kind='stable')
-    tiles = [order[b:b + 256] for b in range(0, len(order), 256)]
+    D, IP = cpu_arm.condition(x, SR, CHUNK_S, START_PAD, END_PAD, F_LOW, 16, 8, 63, 16)
+    sw, isw = filt.derive_sw(IP[None])
     kmin = int(F_LOW / DF)
-    t_tiles = 0.0
-    for t in np.linspace(0, len(tiles) - 1, n_tiles_sample).astype(int):
-        ids = tiles[t]
+    order = np.argsort(synth.tau0(bank['mass1'], bank['mass2']), kind='stable')
+    prepared = []
+    for t in tiles:
+        ids = order[t * 256:(t + 1) * 256]
         H = np.stack([synth.taylorf2(FLEN, DF, bank['mass1'][i], bank['mass2'][i], bank['spin1z'][i],
                                      bank['spin2z'][i], bank['ecc'][i]) for i in ids]).astype(np.complex64)
         kmax = np.array([min(int(np.floor(synth.f_isco(bank['mass1'][i], bank['mass2'][i]) / DF)) + 1, FLEN - 1)
                          for i in ids])
         for j, k in enumerate(kmax):
             H[j, k:] = 0
-        t1 = time.perf_counter()
-        sig, _ = of.sigma2(H, IP[None], DF)
-        r, A, Vh, worst, _, _ = of.svd_tile(H, sw, kmin, 1e-3)
-        osr.tile_segment_lean(H, np.full(len(ids), 16), kmin, kmax, r, A, Vh, D, IP, isw, sig[:, 0], DF, TLEN, A0,
-                              (A1 - A0) // 2048 * 2048, 2048, 5.5, 0.04)
-        t_tiles += time.perf_counter() - t1
-    per_chunk = t_cond + t_tiles / n_tiles_sample * len(tiles)
-    return per_chunk, dict(cond_s=t_cond, tile_s=t_tiles / n_tiles_sample, n_tiles=len(tiles))
+        r, A, Vh, worst, _, _ = filt.svd_tile(H, sw, kmin, 1e-3)
+        prepared.append(dict(tile=t, H=H, kmax=kmax, r=r, A=A, Vh=Vh, n=len(ids)))
+    return dict(x=x, isw=isw, kmin=kmin, tiles=prepared, workers=cpu_arm.cores())
+
+
+def cpu_step(S, i):
+    """Step i of the CPU arm: conditioning of the chunk, then sample tile i mod 3 against it (norms, basis series,
+    rebuilt SNR window maxima, candidates, float64 exact stage). Returns (seconds, templates filtered)."""
+    from oracle import cpu_arm
+    T = S['tiles'][i % len(S['tiles'])]
+    t0 = time.perf_counter()
+    D, IP = cpu_arm.condition(S['x'], SR, CHUNK_S, START_PAD, END_PAD, F_LOW, 16, 8, 63, 16)
+    cpu_arm.tile_pass(T['H'], np.full(T['n'], 16), S['kmin'], T['kmax'], T['A'], T['Vh'], D, IP, S['isw'], DF, TLEN,
+                      A0, (A1 - A0) // CW * CW, CW, THR, MARGIN, S['workers'])
+    return time.perf_counter() - t0, T['n']
+
+
+def cpu_rate(times, templates):
+    """2-det weeks per hour of the CPU samples: each step filtered (A1 - A0) / SR analysed seconds of one chunk
+    against `templates` of the N_TEMPLATES-template bank."""
+    weeks = sum((A1 - A0) / SR / WEEK2 * (n / N_TEMPLATES) for n in templates)
+    return weeks / (sum(times) / 3600.0)
+
+
+def cpu_sample_desc(S, k):
+    return ('%d steps; each: conditioning of one 512 s chunk + one tile of 256 templates (tiles %s of 23 in turn, '
+            'r = %s) against it (norms, basis series, rebuilt-SNR window maxima, float64 exact stage); throughput '
+            'weighted by the tile\'s share of the %d-template bank' %
+            (k, ', '.join(str(t['tile']) for t in S['tiles']), ', '.join(str(t['r']) for t in S['tiles']),
+             N_TEMPLATES))
 
 
 def run_reference(a):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
-    bank = make_bank()
-    cores = os.cpu_count()
-    per = []
-    info = None
-    for _ in range(max(1, a.steps)):
-        s, info = cpu_reference(bank)
-        per.append(s)
-    per_chunk = float(np.median(per))
-    val = ((A1 - A0) / SR / WEEK2) / (per_chunk / 3600.0)
-    print(json.dumps(dict(metric=METRIC, impl='reference', value=val, unit='2-det weeks / hour', n_gpus=a.gpus,
-                          steps=a.steps, warmup=a.warmup, ms_per_step=per_chunk * 1e3, higher_is_better=True,
-                          scaling='weak', vs_baseline=None, dtype='f32/f64', data='synthetic',
-                          config=dict(workload='C2 sample: 1 chunk x 1 of 23 tiles, extrapolated to the bank'),
-                          cpu_baseline=dict(value=val, unit='2-det weeks / hour', cores=cores, kind='port',
-                                            sample='one 512 s chunk: conditioning + one tile of 256 templates '
-                                                   '(tile pass incl. SVD, exact stage), scaled to 23 tiles', **info),
-                          e2e=dict(value=val, unit='2-det weeks / hour', h2d_bytes_per_step=0, d2h_bytes_per_step=0))))
+    S = cpu_setup(make_bank())
+    for i in range(a.warmup):
+        cpu_step(S, i)
+    times, tmpl = [], []
+    for i in range(a.steps):
+        t, n = cpu_step(S, i)
+        times.append(t)
+        tmpl.append(n)
+    val = cpu_rate(times, tmpl)
+    desc = cpu_sample_desc(S, a.steps)
+    print(json.dumps(dict(metric=METRIC, impl='reference', value=val, unit=UNIT, n_gpus=a.gpus, steps=a.steps,
+                          warmup=a.warmup, ms_per_step=float(np.mean(times)) * 1e3, higher_is_better=True,
+                          scaling='weak', vs_baseline=None, dtype='f32 (complex64 transforms and products), '
+                          'f64 norms and exact stage', data='synthetic (seeded noise, TaylorF2 bank)',
+                          config=dict(workload='C2 per-(chunk, tile) sample on the host cores', sample=desc),
+                          cpu_baseline=dict(value=val, unit=UNIT, cores=S['workers'], kind='port', sample=desc),
+                          e2e=dict(value=val, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------------------------------
+# C2 on the GPU
+# ---------------------------------------------------------------------------------------------------------------------
 def top_peak_sets(kept, thr):
-    """Each form's kept peaks (exact stage) against the plain fp32 form's: windows kept by both, by one only, and by
-    one only with an exact SNR more than 3% above the threshold (a real disagreement, not a threshold straddle)."""
+    """Each form's kept peaks (exact stage) over the whole step against the plain fp32 form's: windows kept by both,
+    by one only, and by one only with an exact SNR more than 3% above the threshold."""
     if 'f32' not in kept:
         return None
     ref = kept['f32']
@@ -234,7 +276,7 @@ def traffic_ratios():
     out = {}
     for key, name in (('basis', 'basis_passes_c2_r128.md'), ('gemm', 'umma_cplx2_kernel_c2_r128.md')):
         try:
-            for ln in open(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'profiles', name)):
+            for ln in open(os.path.join(ROOT, 'profiles', name)):
                 if ln.startswith('traffic_ratio:'):
                     out[key] = float(ln.split(':')[1])
         except OSError:
@@ -242,27 +284,10 @@ def traffic_ratios():
     return out
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=3)
-    ap.add_argument('--warmup', type=int, default=3)
-    ap.add_argument('--impl', default='gwb')
-    ap.add_argument('--form', default='bf16x3', choices=['bf16x3', 'f16', 'f32'])
-    ap.add_argument('--chunks', type=int, default=64, help='chunks per detector')
-    ap.add_argument('--templates', type=int, default=5880)
-    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
-    ap.add_argument('--no-precision', action='store_true', help='skip the float64 precision comparison')
-    ap.add_argument('--forms', default='f16,bf16,fp8,f32', help='forms timed (the first gives value)')
-    ap.add_argument('--slow-steps', type=int, default=1,
-                    help='timed steps (and warm-up steps) for the plain fp32 form, which is many times slower')
-    a = ap.parse_args()
-    if a.impl == 'reference':
-        run_reference(a)
-        return
+def run_c2(a):
     import torch
     import torch.distributed as dist
-    from gwb200 import _lib, gpu_prep, pipeline, fp_filter
+    from gwb200 import gpu_prep, pipeline, fp_filter
     from gwb200 import dist as gdist
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -294,12 +319,11 @@ def main():
     kept_sets = {}
     torch.cuda.synchronize()
     t_b = time.perf_counter()
-    cfg0 = pipeline.FilterConfig(form=forms[0])
-    B = pipeline.Bank(bank, FLEN, DF, sw, cfg0, device=dev)
+    B = pipeline.Bank(bank, FLEN, DF, sw, pipeline.FilterConfig(form=forms[0]), device=dev)
     torch.cuda.synchronize()
     bank_setup = time.perf_counter() - t_b
     analysed = nch * (A1 - A0) / SR
-    for form in forms:
+    for fi, form in enumerate(forms):
         cfg = pipeline.FilterConfig(form=form)
         mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg, device=dev)
 
@@ -307,7 +331,10 @@ def main():
             Dd, IPd = cond(x)
             mf.step(Dd, IPd, isw)
 
-        nsteps, nwarm = (a.slow_steps, a.slow_steps) if form == 'f32' else (a.steps, a.warmup)
+        # the headline form runs --steps timed steps after --warmup; the comparison forms --form-steps after one
+        head = fi == 0
+        nsteps = a.steps if head else max(1, min(a.form_steps, a.steps))
+        nwarm = a.warmup if head else 1
         for _ in range(nwarm):
             step()
         torch.cuda.synchronize()
@@ -328,26 +355,26 @@ def main():
             torch.cuda.synchronize()
         barrier()
         ms = ev0.elapsed_time(ev1) / nsteps
-        launches = (cond.launches - l0c + mf.kernel_launches - l0m) // nsteps
+        launches = cond.launches - l0c + mf.kernel_launches - l0m
         ms = gdist.max_over_ranks(ms, dev)
-        # end to end through the public API: strain from pinned host memory, results back to the host
-        res_bytes = 0
-        torch.cuda.synchronize()
-        barrier()
-        e0 = time.perf_counter()
-        ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ee0.record()
-        for _ in range(nsteps):
-            x.copy_(x_host, non_blocking=True)
-            step()
-            r = mf.results()
-            res_bytes = r['n_candidates'] * (32 + 32) + 16
-        ee1.record()
-        torch.cuda.synchronize()
-        barrier()
-        ms_e2e = ee0.elapsed_time(ee1) / nsteps
-        ms_e2e = gdist.max_over_ranks(ms_e2e, dev)
-        # dominant kernel: the fused reconstruction GEMM, each launch bracketed by events in one extra step
+        ms_e2e, res_bytes = None, 0
+        if head:
+            # end to end through the public API: strain from pinned host memory, results back to the host
+            torch.cuda.synchronize()
+            barrier()
+            ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ee0.record()
+            for _ in range(nsteps):
+                x.copy_(x_host, non_blocking=True)
+                step()
+                r = mf.results()
+                res_bytes = r["n_candidates"] * (32 + 32) + 24   # counters, status word, candidates and peaks
+            ee1.record()
+            torch.cuda.synchronize()
+            barrier()
+            ms_e2e = gdist.max_over_ranks(ee0.elapsed_time(ee1) / nsteps, dev)
+        # one extra step with CUDA events around every (tile, segment) call: where the step goes, and the two
+        # dominant kernels (basis series, fused GEMM) per call
         mf.profile = {}
         ec = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         ec[0].record()
@@ -360,7 +387,6 @@ def main():
         L = mf.profile['launches']
         g_ms = [e[1].elapsed_time(e[2]) for e, n, r, kp in L]
         b_ms = [e[0].elapsed_time(e[3]) for e, n, r, kp in L]
-        # where the profiled step goes (CUDA events; the events themselves add a little)
         split = dict(conditioning=ec[0].elapsed_time(ec[1]), basis_series=float(np.sum(b_ms)),
                      stacked_a=float(np.sum([e[3].elapsed_time(e[1]) for e, n, r, kp in L])),
                      gemm=float(np.sum(g_ms)))
@@ -371,7 +397,8 @@ def main():
         split['total'] = ec[0].elapsed_time(ep)
         split = {k: round(v, 3) for k, v in split.items()}
         # algorithmic HBM bytes of one basis-series call (both passes): Vp read (tlen/2 + 1 complex per row), W
-        # written and read back (tlen complex per row), Z written (re + im over Tn, one or two 16-bit planes or fp32)
+        # written and read back (tlen complex per row), Z written (re + im over Tn, one or two 16-bit planes, fp32 or
+        # fp8)
         zb = {'bf16x3': 8, 'f16': 4, 'bf16': 4, 'f32': 8, 'fp8': 2}[form]
         b_bytes = [r * (8 * (mf.tlen // 2 + 1) + 16 * mf.tlen + zb * mf.Tn) for e, n, r, kp in L]
         useful = [8.0 * n * r * mf.Tn for e, n, r, kp in L]
@@ -379,8 +406,7 @@ def main():
         issued = [nprod * 4.0 * n * kp * mf.Tn for e, n, r, kp in L]
         mf.profile = None
         val = world * (analysed / WEEK2) / (ms / 1e3 / 3600.0)
-        val_e2e = world * (analysed / WEEK2) / (ms_e2e / 1e3 / 3600.0)
-        results[form] = dict(value=val, ms=ms, e2e=val_e2e, ms_e2e=ms_e2e, launches=launches, clocks=clk.summary(),
+        results[form] = dict(value=val, ms=ms, steps=nsteps, warmup=nwarm, launches=launches, clocks=clk.summary(),
                              n_candidates=res0['n_candidates'], n_kept=int(res0['keep'].sum()),
                              h2d=x.numel() * 4, d2h=res_bytes, gemm_ms=float(np.mean(g_ms)),
                              gemm_total_ms=float(np.sum(g_ms)), basis_total_ms=float(np.sum(b_ms)),
@@ -389,31 +415,15 @@ def main():
                                                     (2 if form == 'bf16x3' else 1) for e, n, r, kp in L])),
                              useful=float(np.mean(useful)), issued=float(np.mean(issued)), n_gemm=len(L),
                              split_ms=split)
+        if ms_e2e is not None:
+            results[form].update(e2e=world * (analysed / WEEK2) / (ms_e2e / 1e3 / 3600.0), ms_e2e=ms_e2e)
         del mf
         torch.cuda.empty_cache()
-    # precision of every form against float64 on one (tile, chunk) (after the timed regions; the split bf16 form
-    # needs r <= 128, so the tile is the one with the largest such rank)
     precision_rep = None
     if not a.no_precision and rank == 0:
-        from gwb200 import precision
-        t_p = max((i for i, s_ in enumerate(B.svd) if s_['r'] <= 128), key=lambda i: B.svd[i]['r'])
-        seg_p = 0
-        Dd, IPd = cond(x)
-        precision_rep = dict(tile=t_p, r=B.svd[t_p]['r'], segment=seg_p,
-                             reference='float64 transform and product (gwb200.precision)')
-        ref = None
-        for form in ('f32', 'bf16x3', 'f16', 'bf16', 'fp8'):
-            cfg = pipeline.FilterConfig(form=form)
-            mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg, device=dev)
-            sig = mf.norms(IPd)
-            if ref is None:
-                r0, n = B.row0[t_p], len(B.tiles[t_p])
-                ref = precision.fp64_window_snr(B.svd[t_p], Dd[seg_p], isw, sig[r0:r0 + n, seg_p], DF, TLEN, A0,
-                                                mf.Tn, mf.cw)
-            v, i = precision.form_window_snr(mf, t_p, Dd, isw, sig, seg_p)
-            precision_rep[form] = precision.compare(v, i, ref[0], ref[1], cfg.snr_threshold)
-            del mf
-            torch.cuda.empty_cache()
+        import microbench
+        precision_rep = microbench.precision_c2(B, cond, x, isw, forms, dict(df=DF, tlen=TLEN, a0=A0, an=A1 - A0,
+                                                                               cw=CW, thr=THR))
     main_form = forms[0]
     R = results[main_form]
     peaks, kind = peaks_file()
@@ -427,51 +437,115 @@ def main():
                 avg_call_ms=R['basis_ms'], calls=R['n_gemm'], share_of_step=R['basis_total_ms'] / R['ms'],
                 peak_kind='%s hbm copy' % kind,
                 traffic_source='profiles/basis_passes_c2_r128.md (dram bytes / algorithmic bytes, scaled)')
+    # the fused GEMM, timed inside a seconds-long step: against the sustained bf16 peak (the burst one beside it)
     ach = R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
-    pk = peaks.get('bf16_tflops', 1590.0) if main_form != 'f32' else None
+    pk = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops', 1590.0)) if main_form != 'f32' else None
+    pkb = peaks.get('bf16_tflops') if main_form != 'f32' else None
     g_tr = ratios.get('gemm') and ratios['gemm'] * R['z_bytes']
     gname = {'f16': 'umma_cplx2_kernel (f16, CTA pairs)', 'bf16': 'umma_cplx2_kernel (bf16, CTA pairs)',
              'f32': 'simt_absmax_kernel'}.get(main_form, 'umma_cplx_kernel (%s)' % main_form)
     roof_gemm = dict(kernel=gname,
                      bound='tensor', achieved=ach, peak=pk, unit='TFLOP/s', frac=(ach / pk) if pk else None,
+                     frac_of_burst=(ach / pkb) if pkb else None,
                      traffic=g_tr, flops_per_launch_useful=R['useful'], flops_per_launch_issued=R['issued'],
                      issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
                      launches=R['n_gemm'], share_of_step=R['gemm_total_ms'] / R['ms'],
-                     peak_kind='%s burst bf16' % kind,
+                     peak_kind='%s sustained bf16 (cuBLAS loop under the power cap)' % kind,
                      traffic_source='profiles/umma_cplx2_kernel_c2_r128.md (dram bytes / Z bytes, scaled)')
-    line = dict(metric=METRIC, value=R['value'], unit='2-det weeks / GPU-hour', n_gpus=world, steps=a.steps,
+    fp32 = results.get('f32')
+    line = dict(metric=METRIC, value=R['value'], unit=UNIT, n_gpus=world, steps=a.steps,
                 warmup=a.warmup, ms_per_step=R['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
-                dtype={'bf16x3': 'bf16 hi+lo (fp32 accumulate)', 'f16': 'f16 (fp32 accumulate)',
-                       'bf16': 'bf16 (fp32 accumulate)', 'f32': 'f32',
-                       'fp8': 'fp8 e4m3 screen (fp32 accumulate) + float64 exact stage'}[main_form],
+                dtype=DTYPES[main_form],
                 data='synthetic (seeded noise, TaylorF2 bank and injections)',
                 config=dict(workload='C2: 2 det x %d chunks x 512 s at 2048 Hz, %d TaylorF2 templates in tiles of 256, '
                                      'eps 1e-3, 16 chi-squared bins' % (a.chunks, len(bank['mass1'])),
                             form=main_form, analysed_s_per_step=analysed, r_over_n=B.r_over_n,
-                            r_per_tile=[s_['r'] for s_ in B.svd],
+                            r_per_tile=[s_['r'] for s_ in B.svd], unit_note='per GPU-hour at n_gpus = 1',
                             l2='inputs larger than L2 (strain 512 MiB, bank 24.7 GB)', parallelism='dp%d' % world),
-                e2e=dict(value=R['e2e'], unit='2-det weeks / GPU-hour', h2d_bytes_per_step=R['h2d'],
-                         d2h_bytes_per_step=R['d2h']),
-                gpu_launches=R['launches'], clocks=R['clocks'], bank_setup_s=bank_setup, roofline=roof,
-                roofline_gemm=roof_gemm, precision=precision_rep, top_peak_sets=top_peak_sets(kept_sets, 5.5),
-                forms={k: dict(value=v['value'], ms_per_step=v['ms'], e2e=v['e2e'], n_candidates=v['n_candidates'],
-                               n_kept=v['n_kept'], gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
-                               basis_share=v['basis_total_ms'] / v['ms'], split_ms=v['split_ms'])
+                e2e=dict(value=R['e2e'], unit=UNIT, h2d_bytes_per_step=R['h2d'], d2h_bytes_per_step=R['d2h']),
+                gpu_launches=R['launches'], gpu_launches_per_step=R['launches'] // max(1, R['steps']),
+                clocks=R['clocks'], bank_setup_s=bank_setup, roofline=roof,
+                roofline_gemm=roof_gemm, precision=precision_rep, top_peak_sets=top_peak_sets(kept_sets, THR),
+                mixed_over_fp32={k: v['value'] / fp32['value'] for k, v in results.items() if k != 'f32'}
+                if fp32 else None,
+                forms={k: dict(value=v['value'], ms_per_step=v['ms'], steps=v['steps'], warmup=v['warmup'],
+                               e2e=v.get('e2e'), n_candidates=v['n_candidates'], n_kept=v['n_kept'],
+                               gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
+                               basis_share=v['basis_total_ms'] / v['ms'], clocks=v['clocks'], split_ms=v['split_ms'])
                        for k, v in results.items()},
                 peaks_source=kind)
+    if rank == 0 and world == 1 and not a.no_cpu:
+        S = cpu_setup(bank if len(bank['mass1']) == N_TEMPLATES else make_bank())
+        cpu_step(S, 0)
+        times, tmpl = [], []
+        for i in range(a.cpu_steps):
+            t, n = cpu_step(S, i)
+            times.append(t)
+            tmpl.append(n)
+        line['cpu_baseline'] = dict(value=cpu_rate(times, tmpl), unit=UNIT, cores=S['workers'], kind='port',
+                                    sample=cpu_sample_desc(S, a.cpu_steps) + ' (after one untimed step)',
+                                    ms_per_step=float(np.mean(times)) * 1e3)
     if rank == 0:
-        if not a.no_cpu:
-            try:
-                per_chunk, info = cpu_reference(bank)
-                cval = ((A1 - A0) / SR / WEEK2) / (per_chunk / 3600.0)
-                line['cpu_baseline'] = dict(value=cval, unit='2-det weeks / hour', cores=os.cpu_count(), kind='port',
-                                            sample='one 512 s chunk: conditioning + one tile of 256 templates, '
-                                                   'scaled to the full bank', **info)
-            except MemoryError as ex:
-                line['cpu_baseline'] = dict(value=None, error=repr(ex))
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------------------------------
+# C4 (batched segments) and C5 (differentiation)
+# ---------------------------------------------------------------------------------------------------------------------
+def run_c4(a):
+    import microbench
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    ns = argparse.Namespace(segments=300, batch=32, seed=4, no_graph=False, production=a.production,
+                            form=a.forms.split(',')[0])
+    r = microbench.c4(ns)
+    print(json.dumps(dict(metric=METRIC, value=r['value'], unit=UNIT, n_gpus=1, steps=1, warmup=1,
+                          ms_per_step=r['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
+                          dtype=DTYPES[ns.form], data='synthetic (seeded noise, TaylorF2 bank and injections, '
+                          'sine-Gaussian glitches)', config=dict(workload=r['workload']), c4=r)), flush=True)
+
+
+def run_c5(a):
+    import microbench
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    ns = argparse.Namespace(triggers=4096, reps=max(3, a.steps))
+    r = microbench.adjoint(ns)
+    print(json.dumps(dict(metric='SNR gradients per second (7 parameters, 16 s triggers)',
+                          value=r['triggers_per_s_fp32'], unit='triggers / s', n_gpus=1, steps=ns.reps, warmup=2,
+                          ms_per_step=r['ms_grad_fp32'], higher_is_better=True, scaling='weak', vs_baseline=None,
+                          dtype='f32 sums, f64 phase', data='synthetic', config=dict(workload='C5: 4,096 triggers '
+                          'x 16 s at 2048 Hz'), c5=r)), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='gwb', choices=['gwb', 'reference'])
+    ap.add_argument('--workload', default='c2', choices=['c2', 'c4', 'c5'])
+    ap.add_argument('--chunks', type=int, default=64, help='chunks per detector')
+    ap.add_argument('--templates', type=int, default=N_TEMPLATES)
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    ap.add_argument('--cpu-steps', type=int, default=3, help='timed steps of the CPU baseline sample')
+    ap.add_argument('--no-precision', action='store_true', help='skip the float64 precision comparison')
+    ap.add_argument('--forms', default='f16,bf16x3,bf16,fp8,f32', help='forms timed (the first gives value)')
+    ap.add_argument('--form-steps', type=int, default=3, help='timed steps of each form after the first')
+    ap.add_argument('--production', action='store_true', help='c4: production selection and consolidation')
+    a = ap.parse_args()
+    if a.impl == 'reference':
+        run_reference(a)
+    elif a.workload == 'c2':
+        run_c2(a)
+    elif a.workload == 'c4':
+        run_c4(a)
+    else:
+        run_c5(a)
 
 
 if __name__ == '__main__':

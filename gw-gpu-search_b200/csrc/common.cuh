@@ -117,7 +117,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
-// TMA (no multicast anywhere in this library)
+// TMA. No TMA or bulk load in this library uses cluster multicast; the only multicast is umma_commit_pair's
+// tcgen05.commit, an mbarrier arrive on the two CTAs of one CTA pair on the same GPU.
 // ---------------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
     asm volatile(

@@ -440,6 +440,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_ctarank();
     const bool leader = rank == 0;
+    // a timeout in either CTA stops both: the flag is set here and in the peer (through its shared::cluster address)
+    const uint32_t peer_abort = mapa_shared(smem_u32((const void*)abort_flag), rank ^ 1u);
+    auto abort_pair = [&]() {
+        *abort_flag = 1;
+        asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_abort), "r"(1) : "memory");
+    };
     // grid: x = M block (the pair along x: ranks 0, 1 = M blocks 2p, 2p + 1), y = time range
     const int m0 = blockIdx.x * 128;
     const int tr = blockIdx.y;
@@ -482,6 +488,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             if (leader) mbar_arrive_expect_tx(barA, 2u * a_bytes);
             for (int a = 0; a < (int)L.a_tiles; ++a)
                 tma_load_2d_pair(sA + a * kATile, &args.tA[0], barA_l, a * C::ROWEL, m0);
+            int issued = 0;
             for (int f = 0; f < nfill; ++f) {
                 const int s = f % S;
                 const uint32_t n = (uint32_t)(f / S);
@@ -489,7 +496,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 if (*abort_flag) break;
                 if (!mbar_wait_bounded(&empty[s], (n & 1) ^ 1)) {
                     record_error(args.err, GWB_ERR_TIMEOUT, 211, tr, f);
-                    *abort_flag = 1;
+                    abort_pair();
                     break;
                 }
                 if (leader) mbar_arrive_expect_tx(&full[s], 2u * half_stage);
@@ -498,6 +505,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 uint8_t* st = sZ + s * half_stage;
                 for (int ri = 0; ri < 2; ++ri)
                     tma_load_2d_pair(st + ri * KC * 128, &args.tZ[0], full_l, x, ri * Kh + kc * KC);
+                issued = f + 1;
+            }
+            // the loads of both CTAs complete on the leader's full barriers: before the final cluster barrier (after
+            // which either CTA may exit) the leader waits, bounded, for the last phase of every stage it armed, so no
+            // copy still targets a CTA's shared memory on the abort path either
+            if (leader) {
+                mbar_wait_bounded(barA, 0);
+                for (int s = 0; s < S && s < issued; ++s) {
+                    const int nf = (issued - s + S - 1) / S;
+                    mbar_wait_bounded(&full[s], (uint32_t)((nf - 1) & 1));
+                }
             }
         }
     } else if (ntl > 0 && warp == 1) {
@@ -508,7 +526,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             bool ok = mbar_wait_bounded(barA, 0);
             if (!ok) {
                 record_error(args.err, GWB_ERR_TIMEOUT, 212, tr, 0);
-                *abort_flag = 1;
+                abort_pair();
             }
             tc_fence_after();
             for (int i = 0; i < ntl && ok; ++i) {
@@ -516,7 +534,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 const uint32_t u = (uint32_t)(i >> 1);
                 if (!mbar_wait_bounded(&tempty[b], (u & 1) ^ 1)) {
                     record_error(args.err, GWB_ERR_TIMEOUT, 214, tr, i);
-                    *abort_flag = 1;
+                    abort_pair();
                     ok = false;
                     break;
                 }
@@ -526,7 +544,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     const int f = i * nkc + kc;
                     if (*abort_flag || !mbar_wait_bounded(&full[f % S], (uint32_t)((f / S) & 1))) {
                         record_error(args.err, GWB_ERR_TIMEOUT, 213, tr, f);
-                        *abort_flag = 1;
+                        abort_pair();
                         ok = false;
                         break;
                     }
@@ -557,7 +575,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         __syncwarp();
         if (lane == 0 && !mbar_wait_bounded(done, 0)) {   // every MMA of the pair has completed
             record_error(args.err, GWB_ERR_TIMEOUT, 216, tr, (int)rank);
-            *abort_flag = 1;
+            abort_pair();
         }
         __syncwarp();
     } else if (ntl > 0) {
@@ -578,7 +596,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             int bi = 0;
             if (*abort_flag || !mbar_wait_bounded(&tfull[b], u & 1)) {
                 record_error(args.err, GWB_ERR_TIMEOUT, 215, tr, i);
-                *abort_flag = 1;
+                abort_pair();
             } else {
                 tc_fence_after();
 #pragma unroll

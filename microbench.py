@@ -1,20 +1,23 @@
 """Micro-benchmarks of single kernels on synthetic operands (used for profiling; prints one JSON line per case).
 
-    python -m gwb200.microbench gemm  [--r 128] [--n 256] [--tn 917504] [--form f16] [--reps 20]
-    python -m gwb200.microbench basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5] [--wrows 0,4,8]
-    python -m gwb200.microbench exact [--groups 512] [--peaks 1] [--tlen 1048576] [--reps 5]
-    python -m gwb200.microbench adjoint [--triggers 4096] [--reps 5]
-    python -m gwb200.microbench c4 [--segments 300] [--batch 32] [--form f16] [--no-graph] [--production]
+    python microbench.py gemm  [--r 128] [--n 256] [--tn 917504] [--form f16] [--reps 20]
+    python microbench.py basis [--r 128] [--tlen 1048576] [--form f16] [--reps 5] [--wrows 0,4,8]
+    python microbench.py exact [--groups 512] [--peaks 1] [--tlen 1048576] [--reps 5]
+    python microbench.py adjoint [--triggers 4096] [--reps 5]
+    python microbench.py c4 [--segments 300] [--batch 32] [--form f16] [--no-graph] [--production]
 
-Run from gw-gpu-search_b200/ (or with it on sys.path). Operand sizes default to one (tile, chunk) of the C2
-workload; inputs are larger than L2 where the real ones are."""
+Run from the repository root. Operand sizes default to one (tile, chunk) of the C2 workload; inputs are larger than
+L2 where the real ones are. The measurement harness lives here, outside the library package gwb200."""
 import argparse
 import json
+import os
+import sys
 
 import numpy as np
 import torch
 
-from . import _exact, _lib, fp_filter
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), 'gw-gpu-search_b200'))
+from gwb200 import _exact, _lib, fp_filter  # noqa: E402
 
 
 def _time(fn, reps):
@@ -123,7 +126,7 @@ def exact(a):
 def adjoint(a):
     """C5: n triggers of 16 s (flen 16,385) with random C2-like parameters against synthetic whitened data: gradient of
     SNR / newSNR (fp32 and fp64 sums), the 7 x 7 phase metric of 10,000 bank points, and 20 refinement steps."""
-    from . import adjoint as adj
+    from gwb200 import adjoint as adj
     n, tlen = a.triggers, 1 << 15
     flen, df = tlen // 2 + 1, 2048.0 / tlen
     kmin = int(20.0 / df)
@@ -160,7 +163,7 @@ def c4(a):
     Times filter_segments (autogating, chunking, graph-replayed batches, results) end to end on the device."""
     import time
     import numpy as np
-    from . import fp_filter, pipeline, segments as sg, templates
+    from gwb200 import pipeline, segments as sg, templates
     sr, L = 2048.0, 512.0
     tlen = int(L * sr)
     flen, df = tlen // 2 + 1, 1.0 / L
@@ -222,7 +225,7 @@ def c4(a):
         cfg = pipeline.FilterConfig(form=a.form, snr_threshold=4.0, exact_snr=5.5, rebuilt_cap=1 << 24)
         co = sg.Consolidation()
     # SVD metric of the run from a first batch of chunks, then the bank (as bench.py builds it)
-    from . import gpu_prep
+    from gwb200 import gpu_prep
     first = [s for s in segs if s['x'].shape[0] >= tlen][:a.batch]
     Xb = torch.stack([s['x'][:tlen] for s in first] + [first[0]['x'][:tlen]] * (a.batch - len(first)))
     cond = gpu_prep.BatchConditioner(a.batch, tlen, sr, 20.0, 16.0, 8.0, 63, 16.0)
@@ -276,6 +279,217 @@ def c4(a):
                 kept=int(kept.sum()), candidates=len(res['cands']), glitches=len(glitches), glitches_gated=gated,
                 injections_snr8_in_analysed=n_inj_an, injections_found=found,
                 gates=sum(len(g) for g in res['gates']), bank_setup_s=bank_s, seed=a.seed, **extra)
+
+
+# ---- precision of the arithmetic forms against float64 -------------------------------------------------------------
+# Precision of the filter's arithmetic forms against float64 on one (tile, segment): the window maxima of the SNR
+# that the fused GEMM of a form produces, against the same maxima of a float64 SNR series.
+#
+# The float64 series follows the reference's math without rounding: the basis series zb = ifft(conj(Vh) D isw) over
+# the analysed span (fp_filter.py:597-613, norm='forward', zero-padded half spectrum), z = A zb (the product the
+# stacked GEMM forms, fp_filter.py:615-621, fp_gemm.py:14-33) and snr = |z| 4 df / sqrt(sigma^2) (fp_filter.py:710-714).
+# Windows are the filter's cluster windows over the analysed span; the index is the first maximum, as the GEMM's.
+
+
+def fp64_window_snr(sv, D_seg, isw, sig_col, df, tlen, a0, Tn, cw, batch=32):
+    """float64 window maxima (n, nw) of the SNR of one tile against one segment, and their samples (relative to a0).
+    sv: the tile's SVD entry (A (n, r), Vh (r, flen)); D_seg (flen,) complex64; isw (flen,); sig_col (n,) float64."""
+    dev = D_seg.device
+    Vh = sv['Vh'].to(torch.complex128)
+    A = sv['A'].to(torch.complex128)
+    r, flen = Vh.shape
+    n = A.shape[0]
+    dw = D_seg.to(torch.complex128) * isw.to(torch.float64)
+    zb = torch.empty((r, Tn), dtype=torch.complex128, device=dev)
+    for j0 in range(0, r, batch):
+        j1 = min(r, j0 + batch)
+        q = torch.zeros((j1 - j0, tlen), dtype=torch.complex128, device=dev)
+        q[:, :flen] = torch.conj(Vh[j0:j1]) * dw
+        zb[j0:j1] = torch.fft.ifft(q, norm='forward')[:, a0:a0 + Tn]
+        del q
+    z = A @ zb
+    del zb
+    norm = 4.0 * df / torch.sqrt(sig_col.to(torch.float64))
+    snr = z.abs() * norm[:, None]
+    del z
+    nw = Tn // cw
+    v, i = snr[:, :nw * cw].reshape(n, nw, cw).max(2)
+    i = i + torch.arange(nw, device=dev)[None, :] * cw
+    return v.cpu().numpy(), i.cpu().numpy()
+
+
+def form_window_snr(mf, t, D, isw, sig, seg):
+    """Window maxima of the SNR (n, nw) and their samples from the fused GEMM of mf's form, for tile t against
+    segment seg (rows of D). Resets mf's candidate counters (the diagnostic call's candidates are not kept)."""
+    if mf.fused:
+        mf.Dp = fp_filter.fourstep_order(D, mf.tlen, isw)
+    mf.counters.zero_()
+    mf.tile_segment(t, D, isw, sig, seg)
+    torch.cuda.synchronize()
+    mf.counters.zero_()
+    n = len(mf.bank.tiles[t])
+    v = mf.V[:n].double().clamp_min(0).sqrt().cpu().numpy()
+    return v, mf.I[:n].cpu().numpy().astype(np.int64)
+
+
+def compare(v, i, v64, i64, thr):
+    """Differences of one form's window maxima from float64's: |delta SNR| (max, median), relative (max, median),
+    argmax agreement (exact, and within 2 samples: the series is smooth, so a 16-bit form may pick a neighbour of
+    an almost equal maximum), and the windows above thr in one but not the other (all, and those more than 1e-3 thr
+    away from the threshold in float64)."""
+    d = np.abs(v - v64)
+    rel = d / np.maximum(v64, 1e-30)
+    above, above64 = v > thr, v64 > thr
+    flip = above ^ above64
+    return dict(max_abs_dsnr=float(d.max()), median_abs_dsnr=float(np.median(d)), max_rel=float(rel.max()),
+                median_rel=float(np.median(rel)), argmax_agree=float(np.mean(i == i64)),
+                argmax_within2=float(np.mean(np.abs(i - i64) <= 2)), windows=int(v.size),
+                above_fp64=int(above64.sum()), set_diff=int(flip.sum()),
+                set_diff_away=int((flip & (np.abs(v64 - thr) > 1e-3 * thr)).sum()))
+
+
+def fp64_exact_at(H, rows, samples, D_seg, IP_seg, kmin, kmax, nbins, sig, df, tlen, batch=16):
+    """The exact stage in float64 at (row, sample) pairs: equal-power edges as multi_filter.edges_per_template
+    (pipeline/multi_filter.py:264-282: first k whose cumulative |h|^2 IP exceeds j / nb of the total below kmax,
+    clipped to [kmin, kmax]), bin sums Z_j = sum_{k in bin j} conj(h_k) D_k e^{2 pi i (k t mod N) / N}
+    (pipeline/chisq_kernel.py:17-82), then snr = |z| 4 df / sqrt(sig) and chisq = (nb pw - |z|^2) norm^2
+    (pipeline/fp_filter.py:837-853). H (rows of the bank) complex64, D_seg / IP_seg one segment, kmax / nbins per bank
+    row (int), sig per bank row (float64 of this segment). Returns (snr, chisq) float64 numpy arrays."""
+    dev = H.device
+    flen = H.shape[1]
+    rows = torch.as_tensor(np.asarray(rows, np.int64), device=dev)
+    samples = torch.as_tensor(np.asarray(samples, np.int64), device=dev)
+    kmax = torch.as_tensor(np.asarray(kmax, np.int64), device=dev)
+    nbins = torch.as_tensor(np.asarray(nbins, np.int64), device=dev)
+    sig = torch.as_tensor(sig, device=dev).to(torch.float64)
+    k = torch.arange(flen, device=dev, dtype=torch.int64)
+    ip = IP_seg.to(torch.float64)
+    Dd = D_seg.to(torch.complex128)
+    B = int(nbins.max()) if len(rows) else 1
+    snr_o, chi_o = [], []
+    for b0 in range(0, len(rows), batch):
+        r = rows[b0:b0 + batch]
+        t = samples[b0:b0 + batch]
+        h = H[r].to(torch.complex128)
+        nb, k1 = nbins[r], kmax[r]
+        cs = torch.cumsum((h.real ** 2 + h.imag ** 2) * ip, 1)
+        tot = cs.gather(1, (k1 - 1)[:, None])
+        j = torch.arange(B, device=dev, dtype=torch.float64)[None, :]
+        e = torch.searchsorted((cs / tot).contiguous(), (j / nb[:, None]).contiguous(), right=True)
+        e = torch.minimum(torch.maximum(e, torch.full_like(e, kmin)), k1[:, None])
+        e = torch.where(j < nb[:, None], e, k1[:, None])
+        edges = torch.cat([e, k1[:, None]], 1)                              # (b, B + 1)
+        q = torch.conj(h) * Dd
+        ph = ((k[None, :] * t[:, None]) % tlen).to(torch.float64) * (2.0 * np.pi / tlen)
+        x = q * torch.polar(torch.ones_like(ph), ph)
+        inb = (k[None, :] >= edges[:, :1]) & (k[None, :] < edges[:, -1:])
+        bidx = torch.searchsorted(edges.contiguous(), k[None, :].expand(len(r), flen).contiguous(), right=True) - 1
+        bidx = bidx.clamp(0, B - 1)
+        x = torch.where(inb, x, torch.zeros_like(x))
+        Z = torch.zeros((len(r), B), dtype=torch.complex128, device=dev)
+        Z.real.scatter_add_(1, bidx, x.real.contiguous())
+        Z.imag.scatter_add_(1, bidx, x.imag.contiguous())
+        z = Z.sum(1)
+        pw = (Z.real ** 2 + Z.imag ** 2).sum(1)
+        norm = 4.0 * df / torch.sqrt(sig[r])
+        snr_o.append((z.abs() * norm).cpu().numpy())
+        chi_o.append(((nb.to(torch.float64) * pw - z.abs() ** 2) * norm ** 2).cpu().numpy())
+        del h, cs, q, ph, x, bidx, inb
+    if not snr_o:
+        return np.zeros(0), np.zeros(0)
+    return np.concatenate(snr_o), np.concatenate(chi_o)
+
+
+def _stats(x):
+    x = np.asarray(x, np.float64)
+    if x.size == 0:
+        return dict(n=0)
+    return dict(n=int(x.size), max=float(x.max()), median=float(np.median(x)), p99=float(np.percentile(x, 99)))
+
+
+def precision_c2(B, cond, x, isw, forms, g, seg=0, n_chisq=256, seed=0):
+    """Precision of each form against float64 over every tile of one segment (seg) of a C2 step:
+    windows: the window maxima of the rebuilt SNR from the form's fused GEMM against the float64 series' (all tiles);
+    kept: the peaks kept after the form's exact stage (one step of every tile against seg) against the float64
+      series' window maxima above the threshold: set agreement (away = beyond 0.2% of the threshold in float64),
+      relative SNR error at the common windows, and relative chi-squared error against the float64 exact stage at
+      the float64 argmax for up to n_chisq sampled common windows (the loudest 32 always among them), and at the
+      form's own sample (the exact stage's own error).
+    g: dict(df, tlen, a0, an (analysed span), cw, thr)."""
+    from gwb200 import pipeline
+    Dd, IPd = cond(x)
+    rep = dict(segment=seg, tiles=len(B.tiles), reference='float64 transform, product and exact stage (torch '
+               'complex128 on the device; checked against the numpy oracle in tests/test_precision_gpu.py)')
+    mf0 = pipeline.MatchedFilter(B, g['tlen'], g['a0'], g['an'], pipeline.FilterConfig(form=forms[0]))
+    sig = mf0.norms(IPd)
+    Tn, cw = mf0.Tn, mf0.cw
+    del mf0
+    v64, i64 = [], []
+    for t in range(len(B.tiles)):
+        r0, n = B.row0[t], len(B.tiles[t])
+        v, i = fp64_window_snr(B.svd[t], Dd[seg], isw, sig[r0:r0 + n, seg], g['df'], g['tlen'], g['a0'], Tn, cw)
+        v64.append(v)
+        i64.append(i)
+    V64, I64 = np.concatenate(v64), np.concatenate(i64)                     # (M, nw), bank rows in tile order
+    thr = g['thr']
+    set64 = {tuple(p) for p in np.argwhere(V64 > thr).tolist()}
+    sig_seg = sig[:, seg].double()
+    kmax = B.kmax_h
+    nbins = np.full(B.M, B.cfg.nbins)
+    rng = np.random.default_rng(seed)
+    for form in forms:
+        cfg = pipeline.FilterConfig(form=form)
+        mf = pipeline.MatchedFilter(B, g['tlen'], g['a0'], g['an'], cfg)
+        # window maxima of every tile
+        vf, if_ = [], []
+        for t in range(len(B.tiles)):
+            v, i = form_window_snr(mf, t, Dd, isw, sig, seg)
+            vf.append(v)
+            if_.append(i)
+        Vf, If = np.concatenate(vf), np.concatenate(if_)
+        win = compare(Vf, If, V64, I64, thr)
+        # the peaks the form keeps after its exact stage, one step over every tile against seg
+        mf.step(Dd, IPd, isw, seg_ids=[seg])
+        torch.cuda.synchronize()
+        res = mf.results()
+        kc, kp = res['cands'][res['keep']], res['peaks'][res['keep']]
+        kept = {(int(r_), int(w_)): (float(s_), float(c_), int(t_))
+                for r_, w_, s_, c_, t_ in zip(kc['row'], kc['window'], kp['snr'], kp['chisq'], kc['sample'])}
+        ks = set(kept)
+        only64, onlyf = set64 - ks, ks - set64
+        away = 2e-3 * thr
+        common = sorted(ks & set64)
+        rel_snr = [abs(kept[p][0] - V64[p]) / V64[p] for p in common]
+        # chi-squared against float64 at a sample of the common windows
+        chi = dict(n=0)
+        if common:
+            loud = sorted(common, key=lambda p: -V64[p])[:32]
+            rest = [p for p in common if p not in set(loud)]
+            pick = loud + [rest[j] for j in rng.choice(len(rest), min(len(rest), max(0, n_chisq - len(loud))),
+                                                       replace=False)]
+            rows = np.array([p[0] for p in pick])
+            s64 = np.array([g['a0'] + I64[p] for p in pick])
+            sf = np.array([kept[p][2] for p in pick])
+            snr_a, chi_a = fp64_exact_at(B.H, rows, s64, Dd[seg], IPd[seg], B.kmin, kmax[rows], nbins[rows],
+                                         sig_seg[rows], g['df'], g['tlen'])
+            snr_b, chi_b = fp64_exact_at(B.H, rows, sf, Dd[seg], IPd[seg], B.kmin, kmax[rows], nbins[rows],
+                                         sig_seg[rows], g['df'], g['tlen'])
+            cf = np.array([kept[p][1] for p in pick])
+            snf = np.array([kept[p][0] for p in pick])
+            chi = dict(n=len(pick), rel_vs_fp64_argmax=_stats(np.abs(cf - chi_a) / np.maximum(np.abs(chi_a), 1e-30)),
+                       rel_vs_fp64_same_sample=_stats(np.abs(cf - chi_b) / np.maximum(np.abs(chi_b), 1e-30)),
+                       snr_rel_vs_fp64_same_sample=_stats(np.abs(snf - snr_b) / snr_b),
+                       fp64_series_vs_fp64_exact_snr=_stats(np.abs(snr_a - np.array([V64[p] for p in pick])) /
+                                                            snr_a),
+                       sample_agree=float(np.mean(s64 == sf)))
+        rep[form] = dict(windows=win, kept=dict(
+            fp64=len(set64), form=len(ks), both=len(common), only_fp64=len(only64), only_form=len(onlyf),
+            only_fp64_away=sum(V64[p] > thr + away for p in only64),
+            only_form_away=sum(V64[p] < thr - away for p in onlyf),
+            snr_rel_common=_stats(rel_snr)), chisq=chi)
+        del mf
+        torch.cuda.empty_cache()
+    return rep
 
 
 def main():

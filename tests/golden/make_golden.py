@@ -1,8 +1,9 @@
 """Writes the golden fixtures in this directory by running the reference's own code on seeded inputs.
 
-Run from the repository root in a container where the reference is mounted (it is read, never modified):
+Run from the repository root on a machine where the reference checkout is present (it is read, never modified);
+its location is given with --ref or the GWB_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--only NAME ...]
+    python tests/golden/make_golden.py --ref PATH_TO_REFERENCE [--only NAME ...]
 
 Each fixture holds the inputs and the reference's outputs for one call. The reference functions used:
   fp_gemm_*.npz      pipeline/fp_gemm.py fused_peaks (the Triton kernel under TRITON_INTERPRET=1, on the CPU)
@@ -331,9 +332,12 @@ GENERATORS = {'fp_gemm': gen_fp_gemm, 'prep': gen_prep, 'filt': gen_filt, 'edges
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--ref', default=os.environ.get('GWB_REFERENCE'),
+                    help='root of the reference checkout (the directory holding pipeline/); default $GWB_REFERENCE')
     ap.add_argument('--only', nargs='*')
     a = ap.parse_args()
+    if not a.ref:
+        ap.error('the reference checkout is required: --ref PATH or GWB_REFERENCE=PATH')
     _ref_path(a.ref)
     for name, fn in GENERATORS.items():
         if a.only and name not in a.only:
