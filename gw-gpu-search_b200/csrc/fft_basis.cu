@@ -592,10 +592,341 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// Persistent form of the two passes for N = 2^20 (N1 = N2 = 1024): W stays in L2.
+// Rows go in chunks of PC rows through a ring of PSLOT slots of W (PC rows of N each, 48 MB). Work items, taken in
+// order from a global ticket by a grid of resident CTAs:
+//   P1(c, g): pass 1 of chunk c for the 8 columns k2 = 8 g .. 8 g + 7 (one basis_pass1_w CTA's work);
+//   P2(c, b): pass 2 of chunk c for the 8 columns t1 = 8 b .. 8 b + 7 (one basis_pass2_p CTA's work).
+// Ticket order: P1(0, *), then for c = 0, 1, ...: P1(c + 1, *), P2(c, *). P2(c, *) starts when the 128 items P1(c, *)
+// (and P1(0, *), for the scale) are done; P1(c, *) starts when the 128 items P2(c - PSLOT, *) are done (its slot is
+// free). Every item waits only on items earlier in the ticket order, all held by running CTAs, so the earliest
+// unfinished item always progresses. Every wait is bounded (kWaitLimitNs): a timeout records GWB_ERR_TIMEOUT, raises
+// the abort word, and every CTA returns at its next ticket with no copy in flight.
+// After pass 2 has copied a W tile into shared memory its L2 lines are dropped without write-back (discard.global.L2),
+// so W never reaches HBM: per row only the basis filters are read and Z is written.
+// Scale: the Parseval rms of the first chunk's rows (the basis rows have unit norm under the SVD metric, so their
+// series have comparable rms; the scale cancels between Z and A); each P2 item sums the first chunk's per-column
+// partials in a fixed order. fp8: each P2 item sums its rows' per-column |q|^2 in a fixed order for the row scales.
+// ---------------------------------------------------------------------------------------------------------------------
+constexpr int PC = 2, PSLOT = 3, PG = 128;    // rows per chunk, W slots, items per chunk and pass (1024 / 8)
+
+struct PersistArgs {
+    const float2* Vp;
+    long long ldvp;
+    int rows;
+    const float2* Dp;
+    const float2* tw;
+    float2* W;                // PSLOT * PC rows of N
+    int a0, Tn;
+    void* Z;
+    void* Zlo;
+    long long ldz;
+    int im_off, row0;
+    double* partials;         // N2 doubles: the first chunk's sum of |q|^2 per column
+    float* rowpart;           // fp8: rows x N2 sums of |q|^2 per (row, column)
+    float* rowscale;          // fp8: the row scales (written by the items with b = 0)
+    float* scale_out;         // the scale (written by item P2(0, 0))
+    int* sync;                // ticket, abort, p1done[nch], p2done[nch] (zero at launch)
+    DeviceError* err;
+};
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// thread 0: wait until *p >= target, bounded; false on timeout or when another CTA aborted
+__device__ bool wait_count(const int* p, int target, const int* abort_word) {
+    if (ld_acquire(p) >= target) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (true) {
+        for (int i = 0; i < 16; ++i) {
+            __nanosleep(64);
+            if (ld_acquire(p) >= target) return true;
+        }
+        if (*(volatile const int*)abort_word) return false;
+        if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    }
+}
+
+// item t of the ticket order: type 1 = P1, 2 = P2; false past the end
+__device__ __forceinline__ bool persist_item(int t, int nch, int& type, int& c, int& g) {
+    if (t < PG) {
+        type = 1;
+        c = 0;
+        g = t;
+        return nch > 0;
+    }
+    t -= PG;
+    const int j = t / (2 * PG), o = t % (2 * PG);
+    if (j >= nch) return false;
+    if (j + 1 < nch) {
+        type = o < PG ? 1 : 2;
+        c = o < PG ? j + 1 : j;
+        g = o < PG ? o : o - PG;
+        return true;
+    }
+    if (o >= PG) return false;
+    type = 2;
+    c = j;
+    g = o;
+    return true;
+}
+
+// pass 1 of chunk c, columns k2 = 8 g + warp (the body of basis_pass1_w over the chunk's rows)
+__device__ __forceinline__ void persist_p1(float2* sm, const PersistArgs& a, int c, int g) {
+    constexpr int N = 1 << 20, N1 = 1024, N2 = 1024, R = 32, H = N1 / 2, NW = 8, YS = R * (R + 1);
+    constexpr int WS = YS + R + H;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float2* tw2 = sm;
+    float2* Yw = sm + N1 + warp * WS;
+    float2* THw = Yw + YS;
+    float2* Vs = THw + R;
+    const int k2 = g * NW + warp;
+    const int j0 = c * PC, j1 = min(j0 + PC, a.rows);
+    constexpr int mask = N - 1;
+    float2* Wslot = a.W + (long long)(c % PSLOT) * PC * N;
+    auto fetch = [&](int j) {
+        const char* gp = reinterpret_cast<const char*>(a.Vp + (long long)j * a.ldvp + k2 * H);
+        char* d = reinterpret_cast<char*>(Vs);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) cp_async16(d + i * 512 + lane * 16, gp + i * 512 + lane * 16);
+        cp_async_commit();
+    };
+    fetch(j0);
+    float2 dk[R / 2];
+#pragma unroll
+    for (int q = 0; q < R / 2; ++q) dk[q] = __ldg(a.Dp + k2 * H + R * q + lane);
+    const float2 dN = a.Dp[N / 2];
+    THw[lane] = a.tw[(k2 * (R * lane)) & mask];
+    const float2 tl = a.tw[(k2 * lane) & mask];
+    __syncwarp();
+    double acc = 0.0;
+    for (int j = j0; j < j1; ++j) {
+        cp_async_wait_all();
+        __syncwarp();
+        float2 x[R];
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) x[q] = Vs[R * q + lane];
+        __syncwarp();
+        if (j + 1 < j1) fetch(j + 1);
+        float part = 0.f;
+#pragma unroll
+        for (int q = 0; q < R / 2; ++q) {
+            const float2 av = x[q];
+            x[q] = make_float2(fmaf(av.x, dk[q].x, av.y * dk[q].y), fmaf(av.x, dk[q].y, -(av.y * dk[q].x)));
+            part = fmaf(x[q].x, x[q].x, fmaf(x[q].y, x[q].y, part));
+        }
+        x[R / 2] = make_float2(0.f, 0.f);
+        if (k2 == 0 && lane == 0) {                         // the bin N / 2
+            const float2 av = a.Vp[(long long)j * a.ldvp + N / 2];
+            x[R / 2] = make_float2(fmaf(av.x, dN.x, av.y * dN.y), fmaf(av.x, dN.y, -(av.y * dN.x)));
+            part = fmaf(x[R / 2].x, x[R / 2].x, fmaf(x[R / 2].y, x[R / 2].y, part));
+        }
+#pragma unroll
+        for (int q = R / 2 + 1; q < R; ++q) x[q] = make_float2(0.f, 0.f);
+        acc += (double)part;
+        if (a.rowpart) {
+            float ps = part;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, off);
+            if (lane == 0) a.rowpart[(long long)j * N2 + k2] = ps;
+        }
+        dft_reg<R>(x);
+        static_for<R>([&](auto U) {
+            constexpr int u = decltype(U)::value;
+            Yw[lane * (R + 1) + u] = cmul(x[brev(u, ilog2(R))], tw2[u * R + lane]);
+        });
+        __syncwarp();
+#pragma unroll
+        for (int bb = 0; bb < R; ++bb) x[bb] = Yw[bb * (R + 1) + lane];
+        __syncwarp();
+        dft_reg<R>(x);
+        float2* wc = Wslot + (long long)(j - j0) * N + (lane >> 3) * (N2 * 8) + k2 * 8 + (lane & 7);
+        static_for<R>([&](auto V) {
+            constexpr int vv = decltype(V)::value;
+            wc[4 * vv * (N2 * 8)] = cmul(x[brev(vv, ilog2(R))], cmul(tl, THw[vv]));
+        });
+    }
+    if (c == 0) {                                           // the scale's partials: the first chunk, per column
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) a.partials[k2] = acc;
+    }
+    __threadfence();                                        // W (and the partials) before the item's done count
+}
+
+// sum of n doubles (or floats as doubles) by one warp in a fixed order: lane l adds l, l + 32, ... then a fixed tree
+template <typename T>
+__device__ __forceinline__ double warp_fixed_sum(const T* v, int n) {
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32) s += (double)v[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    return s;
+}
+
+// pass 2 of chunk c, t1 = 8 b .. 8 b + 7 (the body of basis_pass2_p over the chunk's rows)
+template <int FORM>
+__device__ __forceinline__ void persist_p2(float2* sm, const PersistArgs& a, int c, int b, float* s_inv) {
+    constexpr int N = 1 << 20, N1 = 1024, N2 = 1024;
+    using S = Split<N2, 2>;
+    constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC, P2 = S::P2;
+    constexpr int ES = FORM == 1 ? 4 : (FORM == 4 ? 1 : 2);
+    constexpr int CP = TB * N2 * 8 / 16 / NT;
+    static_assert(NT == 256 && SC >= N2, "persistent pass 2 layout");
+    const float2* tw2 = sm;                                 // e^{2 pi i b u / N2}: the same table as pass 1's
+    float2* Bt = sm + N1;
+    const int tid = threadIdx.x, t10 = b * TB;
+    const int j0 = c * PC, j1 = min(j0 + PC, a.rows);
+    const float2* Wslot = a.W + (long long)(c % PSLOT) * PC * N;
+    auto tile = [&](int j) { return Wslot + (long long)(j - j0) * N + (long long)b * (N2 * TB); };
+    auto fetch = [&](int j) {
+        const char* gp = reinterpret_cast<const char*>(tile(j));
+        char* d = reinterpret_cast<char*>(Bt);
+#pragma unroll
+        for (int i = 0; i < CP; ++i) cp_async16(d + (i * NT + tid) * 16, gp + (i * NT + tid) * 16);
+        cp_async_commit();
+    };
+    fetch(j0);
+    // scales: the first chunk's Parseval rms (all forms; written once for the caller), and the fp8 row scales
+    const int warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        const double s = warp_fixed_sum(a.partials, N2);
+        const int nf = min(PC, a.rows);
+        const float sc = (float)sqrt(s / (double)nf / 2.0);
+        if (lane == 0) {
+            s_inv[0] = 1.0f / sc;
+            if (c == 0 && b == 0) *a.scale_out = sc;
+        }
+    }
+    if (FORM == 4 && warp >= 1 && warp <= PC && j0 + warp - 1 < j1) {
+        const int j = j0 + warp - 1;
+        const double t = warp_fixed_sum(a.rowpart + (long long)j * N2, N2);
+        const float rs = t > 0.0 ? (float)(sqrt(t / 2.0) / 16.0) : 1.f;
+        if (lane == 0) {
+            s_inv[warp] = 1.0f / rs;
+            if (b == 0) a.rowscale[j] = rs;
+        }
+    }
+    __syncthreads();
+    const int cc = tid % TB, bb = tid / TB;
+    char* zb = static_cast<char*>(a.Z);
+    char* zl = static_cast<char*>(a.Zlo);
+    for (int j = j0; j < j1; ++j) {
+        const float inv = FORM == 4 ? s_inv[1 + j - j0] : s_inv[0];
+        cp_async_wait_all();
+        __syncthreads();
+        {   // the W tile is in shared memory: drop its L2 lines without write-back (512 lines of 128 bytes)
+            const char* gp = reinterpret_cast<const char*>(tile(j));
+            asm volatile("discard.global.L2 [%0], 128;" ::"l"(gp + tid * 128) : "memory");
+            asm volatile("discard.global.L2 [%0], 128;" ::"l"(gp + (tid + NT) * 128) : "memory");
+        }
+        float2 x[R1];
+#pragma unroll
+        for (int q = 0; q < R1; ++q) x[q] = Bt[(R2 * q + bb) * TB + cc];
+        __syncthreads();
+        dft_reg<R1>(x);
+        static_for<R1>([&](auto U) {
+            constexpr int u = decltype(U)::value;
+            Bt[cc * SC + bb * SB + u] = cmul(x[brev(u, ilog2(R1))], tw2[u * R2 + bb]);
+        });
+        __syncthreads();
+        float2 y[P2][R2];
+#pragma unroll
+        for (int p = 0; p < P2; ++p) {
+            const int d = tid + NT * p;
+            const int c2 = d % TB, u = d / TB;
+#pragma unroll
+            for (int q = 0; q < R2; ++q) y[p][q] = Bt[c2 * SC + q * SB + u];
+        }
+        __syncthreads();
+        if (j + 1 < j1) fetch(j + 1);
+        const long long re_off = (long long)(a.row0 + j) * a.ldz * ES;
+        const long long im_off_b = (long long)(a.im_off + a.row0 + j) * a.ldz * ES;
+        void* Zr = zb + re_off;
+        void* Zi = zb + im_off_b;
+        void* Zlr = FORM == 2 ? (void*)(zl + re_off) : nullptr;
+        void* Zli = FORM == 2 ? (void*)(zl + im_off_b) : nullptr;
+#pragma unroll
+        for (int p = 0; p < P2; ++p) {
+            const int d = tid + NT * p;
+            const int c2 = d % TB, u = d / TB;
+            dft_reg<R2>(y[p]);
+            const int t0 = t10 + c2 + N1 * u - a.a0;
+            static_for<R2>([&](auto V) {
+                constexpr int vv = decltype(V)::value;
+                const int t = t0 + N1 * (R1 * vv);
+                if (t >= 0 && t < a.Tn) {
+                    const float2 z = y[p][brev(vv, ilog2(R2))];
+                    store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * inv, z.y * inv);
+                }
+            });
+        }
+    }
+}
+
+template <int FORM>
+__global__ void __launch_bounds__(256, 2) basis_persist(const __grid_constant__ PersistArgs a) {
+    constexpr int N1 = 1024, N = 1 << 20;
+    extern __shared__ float2 sm[];
+    __shared__ int s_t, s_ok;
+    __shared__ float s_inv[1 + PC];
+    for (int e = threadIdx.x; e < N1; e += blockDim.x) sm[e] = a.tw[(e % 32) * (e / 32) * (N / N1)];
+    __syncthreads();
+    const int nch = (a.rows + PC - 1) / PC;
+    int* ticket = a.sync;
+    int* abort_word = a.sync + 1;
+    int* p1done = a.sync + 2;
+    int* p2done = p1done + nch;
+    while (true) {
+        if (threadIdx.x == 0) s_t = *(volatile int*)abort_word ? 0x7fffffff : atomicAdd(ticket, 1);
+        __syncthreads();
+        int type = 0, c = 0, g = 0;
+        if (!persist_item(s_t, nch, type, c, g)) break;     // uniform over the CTA
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            if (type == 1 && c >= PSLOT) ok = wait_count(&p2done[c - PSLOT], PG, abort_word);
+            if (type == 2) ok = wait_count(&p1done[0], PG, abort_word) && wait_count(&p1done[c], PG, abort_word);
+            if (!ok) {
+                record_error(a.err, GWB_ERR_TIMEOUT, 301, type, c);
+                atomicExch(abort_word, 1);
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        if (type == 1) persist_p1(sm, a, c, g);
+        else persist_p2<FORM>(sm, a, c, g, s_inv);
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(type == 1 ? &p1done[c] : &p2done[c], 1);
+    }
+}
+
 int log2i(long long n) {
     int l = 0;
     while ((1ll << l) < n) ++l;
     return l;
+}
+
+size_t persist_smem() { return (size_t)(1024 + 8 * (32 * 33 + 32 + 512)) * sizeof(float2); }
+
+template <int FORM>
+int launch_persist(const PersistArgs& a, cudaStream_t s) {
+    auto k = basis_persist<FORM>;
+    const size_t smem = persist_smem();
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    GWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+    GWB_CHECK_ARG(per_sm >= 1, GWB_ERR_CUDA, "basis_persist: no CTA fits on an SM");
+    const int nch = (a.rows + PC - 1) / PC;
+    const int grid = std::min(per_sm * num_sms(), 2 * PG * nch);
+    k<<<grid, 256, smem, s>>>(a);
+    GWB_LAUNCH_CHECK("basis_persist");
+    return GWB_OK;
 }
 
 int launch_pass1_w(const float2* Vp, long long ldvp, int rows, const float2* Dp, int N, int N2, const float2* tw,
@@ -698,6 +1029,58 @@ int gwb_fourstep_order(const float* X, long long ldx, int rows, const float* isw
         reinterpret_cast<const float2*>(X), ldx, isw, flen, N2, N1 / 2, reinterpret_cast<float2*>(P), ldp);
     GWB_LAUNCH_CHECK("fourstep_order_kernel");
     return GWB_OK;
+}
+
+int gwb_basis_ring_rows(void) { return gwb::PSLOT * gwb::PC; }
+
+int gwb_basis_ring_sync_ints(int rows) { return 2 + 2 * ((rows + gwb::PC - 1) / gwb::PC); }
+
+int gwb_basis_fused_ring(const float* Vp, long long ldvp, int rows, const float* Dp, long long N, const float* tw,
+                         float* W, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz, int im_off,
+                         int row0, double* partials, long long npartials, float* scale, float* rowscale,
+                         float* rowpart, long long rowpart_elems, int32_t* sync, long long sync_ints, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(Vp && Dp && tw && W && Z && scale && partials && sync && (form != 2 || Zlo), GWB_ERR_ARG,
+                  "basis_fused_ring: null pointer");
+    GWB_CHECK_ARG(form >= 0 && form <= 4, GWB_ERR_ARG, "basis_fused_ring: form %d", form);
+    GWB_CHECK_ARG(N == (1 << 20), GWB_ERR_NOT_POW2, "basis_fused_ring: N=%lld (the ring form is for N = 2^20)", N);
+    GWB_CHECK_ARG(rows > 0 && rows < 65536 && ldvp >= N / 2 + 1 && ldvp % 2 == 0 && (uintptr_t)Vp % 16 == 0 &&
+                      a0 >= 0 && Tn > 0 && a0 + Tn <= N && ldz >= Tn && row0 >= 0 && row0 + rows <= im_off,
+                  GWB_ERR_SHAPE, "basis_fused_ring: rows=%d ldvp=%lld a0=%lld Tn=%lld", rows, ldvp, a0, Tn);
+    GWB_CHECK_ARG(npartials >= 1024 && sync_ints >= gwb_basis_ring_sync_ints(rows) && aligned(W, 128),
+                  GWB_ERR_SHAPE, "basis_fused_ring: partials %lld (1024 needed), sync %lld ints (%d needed), W "
+                  "128-byte aligned", npartials, sync_ints, gwb_basis_ring_sync_ints(rows));
+    GWB_CHECK_ARG(form != 4 || (rowscale && rowpart && rowpart_elems >= (long long)rows * 1024), GWB_ERR_SHAPE,
+                  "basis_fused_ring: the fp8 form needs rowscale (rows floats) and rowpart (rows x 1024 floats)");
+    cudaStream_t s = (cudaStream_t)stream;
+    GWB_CUDA(cudaMemsetAsync(sync, 0, sizeof(int32_t) * gwb_basis_ring_sync_ints(rows), s));
+    PersistArgs a;
+    a.Vp = reinterpret_cast<const float2*>(Vp);
+    a.ldvp = ldvp;
+    a.rows = rows;
+    a.Dp = reinterpret_cast<const float2*>(Dp);
+    a.tw = reinterpret_cast<const float2*>(tw);
+    a.W = reinterpret_cast<float2*>(W);
+    a.a0 = (int)a0;
+    a.Tn = (int)Tn;
+    a.Z = Z;
+    a.Zlo = Zlo;
+    a.ldz = ldz;
+    a.im_off = im_off;
+    a.row0 = row0;
+    a.partials = partials;
+    a.rowpart = form == 4 ? rowpart : nullptr;
+    a.rowscale = form == 4 ? rowscale : nullptr;
+    a.scale_out = scale;
+    a.sync = sync;
+    a.err = device_error_ptr();
+    switch (form) {
+        case 0: return launch_persist<0>(a, s);
+        case 1: return launch_persist<1>(a, s);
+        case 2: return launch_persist<2>(a, s);
+        case 3: return launch_persist<3>(a, s);
+        default: return launch_persist<4>(a, s);
+    }
 }
 
 int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const float* Dp, long long N, const float* tw, float* W,

@@ -15,6 +15,7 @@
 // that the epilogue applies, V = rowscale^2 max |z|^2).
 #include <stdlib.h>
 #include <string.h>
+#include <mutex>
 #include "common.cuh"
 
 namespace gwb {
@@ -35,6 +36,9 @@ struct __align__(64) CplxArgs {
     long long ldv;
     long long Tn;
     int M, Kh, ntiles, group, nout, stages, MB, KC;
+    // split bf16 with Kh > 128: A hi resident, A lo streamed with the Z ring (16 K rows per stage, 32-byte swizzle)
+    int lo_stream;
+    int order;   // CTA-pair kernel: order of the complex products' MMAs (0-3, see the kernel)
     // tile-granular CTA ranges (balanced to one tile): windows cut by a range boundary are written as partial
     // (max, first index) records, pv/pi[(row * gridDim.x + cta) * 2 + slot] (slot 0: the window began before the
     // CTA's range, 1: it goes on after it), and merged by window_merge_kernel; null: window-aligned ranges
@@ -72,13 +76,30 @@ __host__ __device__ inline Layout layout_of(int nh, int MB, int Kh, int KC, int 
     return L;
 }
 
+// The split bf16 form with A lo streamed: A hi resident (128 rows x 2 Kh), stages of Z (re, im) x (hi, lo) x KC rows
+// x 128 samples followed by A lo (re, im) x 128 rows x KC columns (KC = 16: one 32-byte swizzle atom per row).
+__host__ __device__ inline Layout layout_split_stream(int Kh, int KC, int stages) {
+    Layout L;
+    L.a_tiles = (uint32_t)((2 * Kh + 63) / 64);
+    L.a_bytes = L.a_tiles * kATile;
+    L.z_off = L.a_bytes;
+    L.stage_bytes = 2u * 2u * 2u * (uint32_t)KC * 128u + 2u * 128u * (uint32_t)KC * 2u;
+    L.x_off = L.z_off + (uint32_t)stages * L.stage_bytes;
+    L.bar_off = L.x_off + 2048u;
+    L.total = L.bar_off + (uint32_t)(2 * stages + 6) * 8u + 16u;
+    return L;
+}
+
 template <int FORM>
 __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_constant__ CplxArgs args) {
     using C = Cfg<FORM>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int Kh = args.Kh, KC = args.KC, S = args.stages, MB = args.MB;
-    const Layout L = layout_of(C::NH, MB, Kh, KC, S, C::ROWEL);
+    const bool los = FORM == 2 && args.lo_stream != 0;    // A lo streamed (MB = 1, KC = 16)
+    const int nres = los ? 1 : C::NH;                     // resident copies of A
+    const Layout L = los ? layout_split_stream(Kh, KC, S) : layout_of(C::NH, MB, Kh, KC, S, C::ROWEL);
+    const uint32_t zst_bytes = 2u * C::NH * C::HALVES * (uint32_t)KC * 128u;   // the Z part of a stage
     const int nkc = (Kh + KC - 1) / KC;
     uint8_t* sA = smem;
     uint8_t* sZ = smem + L.z_off;
@@ -140,11 +161,11 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                 prefetch_tmap(&args.tA[h]);
                 prefetch_tmap(&args.tZ[h]);
             }
-            mbar_arrive_expect_tx(barA, (uint32_t)(MBe * C::NH * L.a_tiles * kATile));
+            mbar_arrive_expect_tx(barA, (uint32_t)(MBe * nres * L.a_tiles * kATile));
             for (int mb = 0; mb < MBe; ++mb)
-                for (int h = 0; h < C::NH; ++h)
+                for (int h = 0; h < nres; ++h)
                     for (int a = 0; a < (int)L.a_tiles; ++a)
-                        tma_load_2d(sA + ((mb * C::NH + h) * L.a_tiles + a) * kATile, &args.tA[h], barA,
+                        tma_load_2d(sA + ((mb * nres + h) * L.a_tiles + a) * kATile, &args.tA[h], barA,
                                     a * C::ROWEL, m0 + mb * 128);
             for (int f = 0; f < nfill; ++f) {
                 const int s = f % S;
@@ -164,6 +185,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                         for (int half = 0; half < C::HALVES; ++half)
                             tma_load_2d(st + ((ri * C::NH + h) * C::HALVES + half) * KC * 128, &args.tZ[h],
                                         &full[s], x + C::ROWEL * half, ri * Kh + kc * KC);
+                if (los)            // A lo, re then im columns of this K chunk (x a multiple of 16 elements)
+                    for (int ri = 0; ri < 2; ++ri)
+                        tma_load_2d(st + zst_bytes + ri * 128 * KC * 2, &args.tA[1], &full[s], ri * Kh + kc * KC, m0);
             }
             mbar_wait_bounded(barA, 0);
             for (int s = 0; s < S && s < nfill; ++s) {
@@ -190,13 +214,22 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                     const int k = kc * KC + sk * C::KSTEP;
                     for (int pr = 0; pr < C::NPROD; ++pr) {
                         const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
-                        const uint32_t abase = a_base + (mb * C::NH + ha) * L.a_tiles * kATile;
+                        const uint32_t abase = a_base + (mb * nres + ha) * L.a_tiles * kATile;
                         const uint32_t are = abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
                         const uint32_t aim = abase + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
                         // K step = KSTEP rows of 128 bytes (2048 bytes for 16-bit, 4096 for 8-bit)
                         const uint32_t zre = st + ((0 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
                         const uint32_t zim = st + ((1 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
-                        const uint64_t dAre = smem_desc(are, 16, 1024, 2), dAim = smem_desc(aim, 16, 1024, 2);
+                        uint64_t dAre, dAim;
+                        if (los && ha == 1) {
+                            // A lo of this stage: 128 rows x 16 columns, 32-byte rows, 32-byte swizzle (8-row atoms
+                            // of 256 bytes)
+                            dAre = smem_desc(st + zst_bytes, 16, 256, 6);
+                            dAim = smem_desc(st + zst_bytes + 128 * KC * 2, 16, 256, 6);
+                        } else {
+                            dAre = smem_desc(are, 16, 1024, 2);
+                            dAim = smem_desc(aim, 16, 1024, 2);
+                        }
                         const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
                         const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
                         const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
@@ -522,6 +555,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         if (lane == 0 && leader) {
             const uint32_t idesc = instr_desc(256, 128, C::FMT, C::FMT, 0, 1);
             const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
+            const int order = args.order;
             const uint32_t a_base = smem_u32(sA), z_base = smem_u32(sZ);
             bool ok = mbar_wait_bounded(barA, 0);
             if (!ok) {
@@ -551,20 +585,44 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     tc_fence_after();
                     const uint32_t st = z_base + (f % S) * half_stage;
                     const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
-                    for (int sk = 0; sk < nsteps; ++sk) {
-                        const int k = kc * KC + sk * C::KSTEP;
-                        const uint32_t are = a_base + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
-                        const uint32_t aim = a_base + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
-                        const uint32_t zre = st + sk * C::KSTEP * 128;
-                        const uint32_t zim = st + KC * 128 + sk * C::KSTEP * 128;
-                        const uint64_t dAre = smem_desc(are, 16, 1024, 2), dAim = smem_desc(aim, 16, 1024, 2);
-                        const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
-                        const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
-                        const uint32_t acc = (kc > 0 || sk > 0) ? 1u : 0u;
-                        umma_f16_pair(dre, dAre, dZre, idesc, acc);
-                        umma_f16_pair(dre, dAim, dZim, idesc_neg, 1u);
-                        umma_f16_pair(dim, dAim, dZre, idesc, acc);
-                        umma_f16_pair(dim, dAre, dZim, idesc, 1u);
+                    // descriptors of K step sk: A re / im halves (K-major), Z re / im halves (sample-major)
+                    auto dA = [&](int sk, int im) {
+                        const int k = (im ? Kh : 0) + kc * KC + sk * C::KSTEP;
+                        return smem_desc(a_base + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES, 16, 1024, 2);
+                    };
+                    auto dZ = [&](int sk, int im) {
+                        return smem_desc(st + (im ? KC * 128 : 0) + sk * C::KSTEP * 128, (uint32_t)KC * 128u, 1024, 2);
+                    };
+                    // the first MMA into each accumulator of a tile overwrites it
+                    auto acc0 = [&](int sk) { return (kc > 0 || sk > 0) ? 1u : 0u; };
+                    if (order == 1) {            // per K step, grouped by A half
+                        for (int sk = 0; sk < nsteps; ++sk) {
+                            umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                            umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
+                            umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                            umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
+                        }
+                    } else if (order == 2) {     // the chunk's real-part MMAs, then its imaginary-part MMAs
+                        for (int sk = 0; sk < nsteps; ++sk) {
+                            umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                            umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                        }
+                        for (int sk = 0; sk < nsteps; ++sk) {
+                            umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
+                            umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
+                        }
+                    } else if (order == 3) {     // one product at a time over the chunk's K steps
+                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
+                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
+                    } else {                     // per K step: re += ReA ReZ, re -= ImA ImZ, im += ImA ReZ, += ReA ImZ
+                        for (int sk = 0; sk < nsteps; ++sk) {
+                            umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                            umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                            umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, acc0(sk));
+                            umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, 1u);
+                        }
                     }
                     umma_commit_pair(&empty[f % S]);
                 }
@@ -711,22 +769,31 @@ __global__ void window_merge_kernel(int M, int ntiles, int group, int nout, int 
     I[(long long)row * ldv + o] = bi;
 }
 
-// CTA pairs are the default for fp16 / bf16; GWB_GEMM_PAIR=0 selects the one-CTA kernel (for comparison)
-inline bool pair_mode() {
-    static const bool on = [] {
-        const char* e = getenv("GWB_GEMM_PAIR");
-        return !(e && e[0] == '0');
-    }();
-    return on;
+// Launch configuration per (form, Kh): the table the autotuner fills (gwb_gemm_set_config). Defaults: CTA pairs for
+// fp16 / bf16, the deepest Z ring that fits, the MMA order 0.
+struct GemmTune {
+    int form, kh, pair, stages, order;
+};
+std::mutex g_tune_mu;
+GemmTune g_tune[128];
+int g_ntune = 0;
+
+GemmTune gemm_tune(int form, int kh) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int i = 0; i < g_ntune; ++i)
+        if (g_tune[i].form == form && g_tune[i].kh == kh) return g_tune[i];
+    return GemmTune{form, kh, 1, 0, 0};
 }
 
 template <int FORM>
 int launch_pair(CplxArgs args, int M, long long ntiles, long long nout, int group, float* V, int32_t* I,
-                long long ldv, void* work, long long work_bytes, cudaStream_t stream) {
+                long long ldv, void* work, long long work_bytes, const GemmTune& tune, cudaStream_t stream) {
     const uint32_t max_smem = 227 * 1024;
     const int KC = 64;
     int stages = 8;
     while (stages > 0 && layout_pair(args.Kh, KC, stages).total + 1024 > max_smem) --stages;
+    if (tune.stages >= 2) stages = std::min(stages, tune.stages);
+    args.order = tune.order;
     GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d does not fit the CTA-pair form", args.Kh);
     const int npair = (M + 255) / 256;
     const long long per = (long long)std::max(1, num_sms() / (2 * npair));
@@ -793,7 +860,7 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     const long long nout = cdiv(ntiles, group);
     GWB_CHECK_ARG(ldv >= nout, GWB_ERR_SHAPE, "fused_peaks_cplx: ldv=%lld < outputs per row %lld", ldv, nout);
     const uint32_t max_smem = 227 * 1024;
-    const int KC = FORM == 2 ? 32 : (C::F8 ? 128 : 64);    // K rows per Z stage (32 KB per stage in every form)
+    int KC = FORM == 2 ? 32 : (C::F8 ? 128 : 64);          // K rows per Z stage (32 KB per stage in every form)
     auto fits = [&](int mb, int st) { return layout_of(C::NH, mb, Kh, KC, st, C::ROWEL).total + 1024 <= max_smem; };
     auto most_stages = [&](int mb) {
         int st = 6;
@@ -804,17 +871,29 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     // 128, Tn = 917,504; the second M group's Z reads hit L2), with the TMEM double buffer spanning tiles. The kernel
     // also runs two M blocks per CTA (each Z tile read once for both) when MB = 2.
     const int MB = 1;
-    const int stages = most_stages(MB);
-    GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE,
-                  "fused_peaks_cplx: Kh=%d does not fit in shared memory for this form (at most %d)", Kh,
-                  FORM == 2 ? 128 : 192);
+    const GemmTune tune = gemm_tune(FORM, Kh);
+    int stages = most_stages(MB);
+    if (tune.stages >= 2 && stages >= 2) stages = std::min(stages, tune.stages);
+    // split bf16 beyond Kh = 128: A hi + lo no longer fit beside the Z ring, so A lo is streamed with it
+    const bool los = FORM == 2 && stages < 2;
+    if (los) {
+        KC = 16;
+        stages = 8;
+        while (stages > 0 && layout_split_stream(Kh, KC, stages).total + 1024 > max_smem) --stages;
+        if (tune.stages >= 2) stages = std::min(stages, tune.stages);
+    }
+    GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d does not fit in shared memory for this form",
+                  Kh);
     CplxArgs args;
     memset(&args, 0, sizeof(args));
     const CUtensorMapDataType dt = C::F8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
                                    : FORM == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     for (int h = 0; h < C::NH; ++h) {
+        // A lo streamed: boxes of 16 columns (32 bytes) x 128 rows, 32-byte swizzle
+        const bool lo_box = los && h == 1;
         int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)(lda * C::ES),
-                               C::ROWEL, 128, CU_TENSOR_MAP_SWIZZLE_128B);
+                               lo_box ? 16u : (uint32_t)C::ROWEL, 128,
+                               lo_box ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_128B);
         if (r) return r;
         r = encode_tmap_2d(&args.tZ[h], dt, Zp[h], (uint64_t)Tn, (uint64_t)(2 * Kh), (uint64_t)(ldz * C::ES), C::ROWEL,
                            (uint32_t)KC, CU_TENSOR_MAP_SWIZZLE_128B);
@@ -833,13 +912,15 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     args.stages = stages;
     args.MB = MB;
     args.KC = KC;
+    args.lo_stream = los ? 1 : 0;
     args.err = device_error_ptr();
-    const uint32_t smem = layout_of(C::NH, MB, Kh, KC, stages, C::ROWEL).total + 1024;
+    const uint32_t smem = (los ? layout_split_stream(Kh, KC, stages) : layout_of(C::NH, MB, Kh, KC, stages,
+                                                                                  C::ROWEL)).total + 1024;
     auto kern = umma_cplx_kernel<FORM>;
     GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if constexpr (FORM == 0 || FORM == 1) {
-        if (work != nullptr && pair_mode()) return launch_pair<FORM>(args, M, ntiles, nout, group, V, I, ldv, work,
-                                                                     work_bytes, stream);
+        if (work != nullptr && tune.pair) return launch_pair<FORM>(args, M, ntiles, nout, group, V, I, ldv, work,
+                                                                   work_bytes, tune, stream);
     }
     const int mgroups = (M + 128 * MB - 1) / (128 * MB);
     const long long per = (long long)std::max(1, num_sms() / mgroups);
@@ -876,6 +957,28 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
 }  // namespace gwb
 
 extern "C" long long gwb_fused_peaks_cplx_work_bytes(int M) { return 16ll * M * gwb::num_sms(); }
+
+extern "C" int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order) {
+    using namespace gwb;
+    GWB_CHECK_ARG(form >= 0 && form <= 3 && kh > 0 && (pair == 0 || pair == 1) && stages >= 0 && stages <= 8 &&
+                      order >= 0 && order <= 3, GWB_ERR_ARG,
+                  "gemm_set_config: form=%d kh=%d pair=%d stages=%d order=%d", form, kh, pair, stages, order);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int i = 0; i < g_ntune; ++i)
+        if (g_tune[i].form == form && g_tune[i].kh == kh) {
+            g_tune[i] = GemmTune{form, kh, pair, stages, order};
+            return GWB_OK;
+        }
+    GWB_CHECK_ARG(g_ntune < 128, GWB_ERR_CAPACITY, "gemm_set_config: the table holds 128 shapes");
+    g_tune[g_ntune++] = GemmTune{form, kh, pair, stages, order};
+    return GWB_OK;
+}
+
+extern "C" int gwb_gemm_clear_configs(void) {
+    std::lock_guard<std::mutex> lk(gwb::g_tune_mu);
+    gwb::g_ntune = 0;
+    return GWB_OK;
+}
 
 extern "C" int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
                                     const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,

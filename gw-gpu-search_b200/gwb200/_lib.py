@@ -43,12 +43,18 @@ SIGNATURES = {
     'gwb_fused_peaks_f32': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_cplx': [_I, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P, _P, _LL, _P],
     'gwb_fused_peaks_cplx_work_bytes': [_I],
+    'gwb_gemm_set_config': [_I, _I, _I, _I, _I],
+    'gwb_gemm_clear_configs': [],
     'gwb_basis_premul': [_P, _LL, _I, _P, _LL, _I, _P, _LL, _P, _LL, _P],
     'gwb_basis_scale': [_P, _LL, _I, _LL, _LL, _P, _I, _P, _P, _P],
     'gwb_fft_twiddles': [_LL, _P, _P],
     'gwb_fourstep_order': [_P, _LL, _I, _P, _LL, _LL, _P, _LL, _P],
     'gwb_basis_fused': [_P, _LL, _I, _P, _LL, _P, _P, _I, _LL, _LL, _I, _P, _P, _LL, _I, _I, _I, _P, _LL, _P, _P, _P,
                         _P, _LL, _P],
+    'gwb_basis_fused_ring': [_P, _LL, _I, _P, _LL, _P, _P, _LL, _LL, _I, _P, _P, _LL, _I, _I, _P, _LL, _P, _P, _P, _LL,
+                             _P, _LL, _P],
+    'gwb_basis_ring_rows': [],
+    'gwb_basis_ring_sync_ints': [_I],
     'gwb_basis_pack': [_P, _LL, _I, _I, _I, _LL, _LL, _P, _I, _P, _P, _LL, _P],
     'gwb_stacked_a': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _I, _I, _P, _P, _P, _P, _LL, _P],
     'gwb_stacked_a8': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _P, _LL, _P, _P],
@@ -63,6 +69,8 @@ SIGNATURES = {
     'gwb_exact_chunks': [_I, _I],
     'gwb_bin_sums_ordered': [_P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _LL, _P, _LL, _I, _I, _LL, _P, _LL, _P, _P, _P],
     'gwb_bin_sums_work_bytes': [_I, _I],
+    'gwb_select_top': [_P, _P, _P, _P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _I, _P, _LL, _P],
+    'gwb_select_top_work_bytes': [_I, _I],
     'gwb_sigma2': [_P, _LL, _I, _P, _LL, _I, _I, _I, _D, _P, _LL, _P, _LL, _P],
     'gwb_sigma2_noalloc': [_P, _LL, _I, _P, _LL, _I, _I, _I, _D, _P, _LL, _P],
     'gwb_gram': [_P, _LL, _I, _P, _I, _I, _P, _LL, _P, _P],
@@ -117,6 +125,7 @@ def load():
         lib.gwb_consolidate_work_bytes.restype = ctypes.c_longlong
         lib.gwb_bin_sums_work_bytes.restype = ctypes.c_longlong
         lib.gwb_fused_peaks_cplx_work_bytes.restype = ctypes.c_longlong
+        lib.gwb_select_top_work_bytes.restype = ctypes.c_longlong
         _lib = lib
     return _lib
 

@@ -120,15 +120,25 @@ def fourstep_order(X, N, isw=None, out=None):
     return out if X.dim() == 2 else out[0]
 
 
-class FusedBasisWorkspace:
-    """Workspace of the fused two-pass basis series: the intermediate W (wrows x tlen complex; the rows go through it
-    in batches of wrows), the twiddle table, the scale partials and ticket."""
+RING_N = 1 << 20   # the transform length of the persistent ring form (gwb_basis_fused_ring)
 
-    def __init__(self, tlen, flen, rows, device='cuda', wrows=None):
+
+class FusedBasisWorkspace:
+    """Workspace of the fused basis series: the intermediate W, the twiddle table, the scale partials and ticket.
+    ring (tlen = 2^20 only; the default there): one persistent launch with W in a ring of gwb_basis_ring_rows() rows
+    kept in L2; else two passes with W of wrows x tlen complex (the rows go through it in batches of wrows)."""
+
+    def __init__(self, tlen, flen, rows, device='cuda', wrows=None, ring=None):
         assert FUSED_MIN <= tlen <= FUSED_MAX and flen <= tlen // 2 + 1
         self.tlen, self.flen, self.rows = tlen, flen, rows
+        self.ring = (tlen == RING_N) if ring is None else bool(ring)
+        assert not self.ring or tlen == RING_N, 'the ring form is for tlen = 2^20'
         self.wrows = rows if wrows is None else max(1, min(int(wrows), rows))
-        self.W = torch.empty((self.wrows, tlen), dtype=torch.complex64, device=device)
+        lib = _lib.load()
+        wr = lib.gwb_basis_ring_rows() if self.ring else self.wrows
+        self.W = torch.empty((wr, tlen), dtype=torch.complex64, device=device)
+        self.sync = (torch.zeros(lib.gwb_basis_ring_sync_ints(rows), dtype=torch.int32, device=device)
+                     if self.ring else None)
         self.tw = twiddles(tlen, device)
         self.partials = torch.empty(RB * max(1, tlen // 64), dtype=torch.float64, device=device)
         self.ticket = torch.zeros(1, dtype=torch.int32, device=device)
@@ -136,7 +146,7 @@ class FusedBasisWorkspace:
         # fp8 form: one scale per basis row, and the per-row |q|^2 partial sums behind it (at most N2 per row)
         self.rowscale = torch.empty(rows, dtype=torch.float32, device=device)
         n2 = tlen >> ((tlen.bit_length() - 1 + 1) // 2)
-        self.rowpart = torch.empty(self.wrows * n2, dtype=torch.float32, device=device)
+        self.rowpart = torch.empty((rows if self.ring else self.wrows) * n2, dtype=torch.float32, device=device)
 
 
 def basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo=None, form='f16', im_off=None):
@@ -147,6 +157,13 @@ def basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo=None, form='f16', im_off=None)
     r = Vp.shape[0]
     assert r <= ws.rows and Vp.shape[1] >= ws.tlen // 2 + 1 and Dp.numel() >= ws.tlen // 2 + 1
     im_off = r if im_off is None else im_off
+    if ws.ring:
+        # one persistent launch, W in an L2-resident ring; the scale from the first two rows
+        _lib.call('gwb_basis_fused_ring', _lib.ptr(Vp), Vp.stride(0), r, _lib.ptr(Dp), ws.tlen, _lib.ptr(ws.tw),
+                  _lib.ptr(ws.W), int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0), int(im_off),
+                  0, _lib.ptr(ws.partials), ws.partials.numel(), _lib.ptr(ws.scale), _lib.ptr(ws.rowscale),
+                  _lib.ptr(ws.rowpart), ws.rowpart.numel(), _lib.ptr(ws.sync), ws.sync.numel(), _lib.stream_ptr())
+        return ws.scale
     _lib.call('gwb_basis_fused', _lib.ptr(Vp), Vp.stride(0), r, _lib.ptr(Dp), ws.tlen, _lib.ptr(ws.tw),
               _lib.ptr(ws.W), ws.wrows, int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0),
               int(im_off), 0, min(RB, r), _lib.ptr(ws.partials), ws.partials.numel(), _lib.ptr(ws.ticket),

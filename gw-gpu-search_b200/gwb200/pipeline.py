@@ -44,6 +44,11 @@ class FilterConfig:
     # exact_snr (1 - margin) skip the exact stage and keep their rebuilt SNR and phase when above snr_threshold;
     # 0 sends every candidate to the exact stage (PyCBC-equivalent values)
     exact_snr: float = 0.0
+    # rank rules instead (gwb_select_top): per segment only the exact_top loudest candidates by rebuilt SNR, or the
+    # loudest fraction exact_top_frac of them, go to the exact stage; the others above snr_threshold keep their
+    # rebuilt SNR and phase (rebuilt peaks). 0: off
+    exact_top: int = 0
+    exact_top_frac: float = 0.0
     rebuilt_cap: int = 0          # capacity of the rebuilt-peak list (0: cand_cap)
     exact_order: bool = True      # exact stage in template-row order, chunk by chunk (gwb_bin_sums_ordered)
 
@@ -153,9 +158,19 @@ class MatchedFilter:
         assert not (self.fp8 and cfg.exact_snr > 0), 'the fp8 screen keeps no rebuilt values: use exact_snr = 0'
         self.ecut = float(np.float32(cfg.exact_snr * (1 - cfg.margin))) if cfg.exact_snr > 0 else 0.0
         self.rthr = float(np.float32(cfg.snr_threshold))
+        self.top = cfg.exact_top > 0 or cfg.exact_top_frac > 0
+        assert not (self.top and cfg.exact_snr > 0), 'one exact-stage rule at a time: exact_snr or exact_top(_frac)'
         self.rebuilt_cap = cfg.rebuilt_cap or cap
         self.rebuilt = (torch.empty(self.rebuilt_cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
-                        if cfg.exact_snr > 0 else None)
+                        if cfg.exact_snr > 0 or self.top else None)
+        # the selection's own lists: with a rank rule the windows are selected into these, then gwb_select_top
+        # moves the ranked subset into cands / groups / units / counters for the exact stage
+        if self.top:
+            self.sel = dict(cands=torch.empty_like(self.cands), groups=torch.empty_like(self.groups),
+                            units=torch.empty_like(self.units), counters=torch.zeros_like(self.counters))
+            self.top_work = None
+        else:
+            self.sel = dict(cands=self.cands, groups=self.groups, units=self.units, counters=self.counters)
         self.kernel_launches = 0
         self.fft_launches = 0
         # set to {} to record CUDA events per (tile, segment): e0 basis series e3 stacked A e1 GEMM e2 (then the
@@ -213,10 +228,13 @@ class MatchedFilter:
         _lib.call('gwb_select_windows', _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), n, self.nw, self.thr2,
                   self.ecut, self.rthr, self.a0, b.row0[t], seg, _lib.ptr(self.Are), _lib.ptr(self.Aim),
                   _lib.ptr(self.Are_lo), _lib.ptr(self.Aim_lo), self.Are.stride(0), _lib.ptr(self.Z),
-                  _lib.ptr(self.Zlo), self.Z.stride(0), K, Kh, f, _lib.ptr(self.sa), _lib.ptr(self.cands), cap,
-                  _lib.ptr(self.groups), cap, _lib.ptr(self.units), cap, _lib.ptr(self.rebuilt),
-                  self.rebuilt_cap if self.rebuilt is not None else 0, _lib.ptr(self.counters), _lib.stream_ptr())
-        if self.fused:
+                  _lib.ptr(self.Zlo), self.Z.stride(0), K, Kh, f, _lib.ptr(self.sa), _lib.ptr(self.sel['cands']), cap,
+                  _lib.ptr(self.sel['groups']), cap, _lib.ptr(self.sel['units']), cap, _lib.ptr(self.rebuilt),
+                  self.rebuilt_cap if self.rebuilt is not None else 0, _lib.ptr(self.sel['counters']),
+                  _lib.stream_ptr())
+        if self.fused and self.fws.ring:
+            self.kernel_launches += 4           # the persistent basis series, stacked A, GEMM, selection
+        elif self.fused:
             nb = -(-r // self.fws.wrows)
             self.kernel_launches += 2 * nb + 3  # two basis passes per row batch, stacked A, GEMM, selection
         else:
@@ -242,6 +260,17 @@ class MatchedFilter:
         cap = self.cfg.cand_cap
         s = _lib.stream_ptr()
         cnt = self.counters
+        if self.top:
+            nseg = D.shape[0]
+            if self.top_work is None or self.top_work.numel() < _lib.load().gwb_select_top_work_bytes(nseg, cap):
+                self.top_work = torch.empty(_lib.load().gwb_select_top_work_bytes(nseg, cap), dtype=torch.uint8,
+                                            device=D.device)
+            sc = self.sel
+            _lib.call('gwb_select_top', _lib.ptr(sc['cands']), _lib.ptr(sc['groups']), _lib.ptr(sc['units']),
+                      _lib.ptr(sc['counters']), cap, nseg, int(self.cfg.exact_top), float(self.cfg.exact_top_frac),
+                      self.rthr, _lib.ptr(self.cands), _lib.ptr(self.groups), _lib.ptr(self.units), _lib.ptr(cnt),
+                      _lib.ptr(self.rebuilt), self.rebuilt_cap, _lib.ptr(self.top_work), self.top_work.numel(), s)
+            self.kernel_launches += 5
         _lib.call('gwb_edges', _lib.ptr(self.units), _lib.ptr(cnt[2:]), cap, _lib.ptr(b.H), b.H.stride(0),
                   _lib.ptr(IP), IP.stride(0), _lib.ptr(b.nbins), _lib.ptr(b.kmax), b.kmin, self.B, 0, _lib.ptr(self.E), s)
         if self.slots is None:
@@ -266,6 +295,8 @@ class MatchedFilter:
         """Queue one step on the current stream: every tile against every segment in seg_ids (rows of D / IP).
         Nothing is copied back; call results() after the stream is synchronised."""
         self.counters.zero_()
+        if self.top:
+            self.sel['counters'].zero_()
         prof = self.profile
         ev = (lambda: torch.cuda.Event(enable_timing=True)) if prof is not None else None
         if prof is not None:
@@ -305,7 +336,7 @@ class MatchedFilter:
         and phase are the rebuilt ones: `rebuilt`, GwbCand records, or with rebuilt_on_device `rebuilt_dev`, a view
         of the device list as an (n, 8) int32 tensor of the GwbCand fields)."""
         c = self.counters.cpu().numpy()
-        if c[3]:
+        if c[3] or (self.top and int(self.sel['counters'][3].item())):
             raise _lib.GwbError('select', _lib.GWB_ERR_CAPACITY, 'candidate capacity %d exceeded' % self.cfg.cand_cap)
         if self.cfg.exact_order and int(self.sort_status.item()):
             raise _lib.GwbError('bin_sums_ordered', _lib.GWB_ERR_SHAPE, 'a unit row outside the bank')

@@ -115,14 +115,24 @@ GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long ld
  * reference's stacked Are/Aim (pipeline/fp_filter.py:615-621) and stays in shared memory. form 0: fp16 A_hi, Z_hi;
  * 1: bf16; 2: split bf16 with A_lo, Z_lo (hi.hi + hi.lo + lo.hi); 3: fp8 e4m3 (the screening form, no reference
  * counterpart; Kh a multiple of 32), V = rowscale[i]^2 max |z|^2 with rowscale the per-row scale of A
- * (gwb_stacked_a8); rowscale is ignored by the other forms (may be NULL). Kh <= 192 (forms 0, 1, 3) or 128 (form 2).
- * lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
+ * (gwb_stacked_a8); rowscale is ignored by the other forms (may be NULL). Kh <= 192 (forms 0, 1, 3); form 2 keeps
+ * A hi and lo in shared memory up to Kh = 128 and beyond that keeps A hi there and streams A lo with the Z chunks
+ * (Kh <= 320). lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
  * be NULL): with it the CTAs take tile-granular ranges of the time axis (balanced to one 128-sample tile) and windows
  * cut by a range boundary are merged by a second kernel, bit for bit the same V and I; without it every CTA takes
  * whole windows (up to one window of imbalance between CTAs). With work, forms 0 and 1 run on CTA pairs (clusters
- * of two CTAs, tcgen05.mma.cta_group::2 with M = 256 over two SMs, each SM loading half of every Z tile; the
- * environment variable GWB_GEMM_PAIR=0 selects the one-CTA kernel). */
+ * of two CTAs, tcgen05.mma.cta_group::2 with M = 256 over two SMs, each SM loading half of every Z tile) unless the
+ * launch table says otherwise (gwb_gemm_set_config). */
 GWB_API long long gwb_fused_peaks_cplx_work_bytes(int M);
+/* Launch table of gwb_fused_peaks_cplx, per (form, Kh), filled by the autotuner (no reference counterpart; the
+ * reference's own tuner is fp_gemm.pick_cfg, pipeline/fp_gemm.py:47-64): pair 1 = CTA pairs (forms 0, 1 with a
+ * work buffer), 0 = one CTA per M block; stages = depth of the Z ring (0 = the most that fit, else at most that);
+ * order = the CTA-pair kernel's MMA order (0: per K step re+=ReA.ReZ, re-=ImA.ImZ, im+=ImA.ReZ, im+=ReA.ImZ; 1: per K
+ * step grouped by A half; 2: per Z chunk all real-part MMAs, then all imaginary-part ones; 3: per Z chunk one product
+ * at a time). Process-wide, guarded by a mutex; a shape without an entry uses pair 1, stages 0, order 0. Every entry
+ * gives the same V and I. */
+GWB_API int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order);
+GWB_API int gwb_gemm_clear_configs(void);
 GWB_API int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
                                  const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,
                                  int32_t* I, long long ldv, const float* rowscale, void* work, long long work_bytes,
@@ -274,6 +284,22 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
                             float* W, int wrows, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz,
                             int im_off, int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket,
                             float* scale, float* rowscale, float* rowpart, long long rowpart_elems, void* stream);
+/* The same basis series for N = 2^20 in one persistent launch that keeps W in L2 (same reference call,
+ * fp_filter.py:597-613): rows go in chunks of 2 through a ring of gwb_basis_ring_rows() rows of W (W: that many rows
+ * of N complex, 128-byte aligned), pass 1 of one chunk running beside pass 2 of the previous one; each W tile's L2
+ * lines are dropped after pass 2 has read it, so per row HBM carries the basis filters in and Z out. Work items are
+ * taken in order from a ticket; an item waits (bounded, one second, then GWB_ERR_TIMEOUT in the device error word)
+ * only for items earlier in that order. The scale is the Parseval rms of the first chunk's rows (min(2, rows) rows)
+ * instead of min(nfirst, wrows) rows. partials: >= 1024 doubles; sync: gwb_basis_ring_sync_ints(rows) int32, cleared
+ * by the call on the stream; fp8: rowpart >= rows x 1024 floats, rowscale rows floats. Other arguments as
+ * gwb_basis_fused. */
+GWB_API int gwb_basis_ring_rows(void);
+GWB_API int gwb_basis_ring_sync_ints(int rows);
+GWB_API int gwb_basis_fused_ring(const float* Vp, long long ldvp, int rows, const float* Dp, long long N,
+                                 const float* tw, float* W, long long a0, long long Tn, int form, void* Z, void* Zlo,
+                                 long long ldz, int im_off, int row0, double* partials, long long npartials,
+                                 float* scale, float* rowscale, float* rowpart, long long rowpart_elems,
+                                 int32_t* sync, long long sync_ints, void* stream);
 
 /* ---- differentiation (the adjoint form; no reference counterpart: the reference has no gradients) ------------- */
 /* Per trigger i, parameters params[i * 7 + (0..6)] = (Mc [M_sun], q = m2/m1 <= 1, chi1z, chi2z, e0 at f_ecc, t_c [s],
@@ -316,6 +342,20 @@ GWB_API int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv
                                const void* Zlo, long long ldz, int Kp, int kh, int form, const float* rowscale,
                                GwbCand* cands, int cand_cap, GwbGroup* groups, int group_cap, GwbUnit* units,
                                int unit_cap, GwbCand* rebuilt, int rebuilt_cap, int32_t* counters, void* stream);
+/* Exact-stage selection by rank (the rank form of the reference's exact/rebuilt split, fp_filter.py:769-781): from
+ * the lists gwb_select_windows wrote for a whole step with ecut <= 0 (cands, units, counters; every candidate
+ * carries its rebuilt z), per segment only the candidates whose rebuilt SNR is at least the k-th largest of their
+ * segment (ties kept) become exact-stage candidates in cands_out / groups_out / units_out / counters_out (same
+ * record layout, candidate order kept within each unit); the others with rebuilt SNR > rthr are appended to
+ * `rebuilt` (unit -1, counting on from counters[4]) and keep their rebuilt SNR and z. k = top_n (> 0), else
+ * ceil(top_frac * count of the segment's candidates) with top_frac in (0, 1]. Segments are 0..nseg-1; the output
+ * lists have cand_cap entries each. work: gwb_select_top_work_bytes(nseg, cand_cap) bytes, 256-byte aligned. No host
+ * synchronisation: every count is read on the device. */
+GWB_API long long gwb_select_top_work_bytes(int nseg, int cand_cap);
+GWB_API int gwb_select_top(const GwbCand* cands, const GwbGroup* groups, const GwbUnit* units, const int32_t* counters,
+                           int cand_cap, int nseg, int top_n, float top_frac, float rthr, GwbCand* cands_out,
+                           GwbGroup* groups_out, GwbUnit* units_out, int32_t* counters_out, GwbCand* rebuilt,
+                           int rebuilt_cap, void* work, long long work_bytes, void* stream);
 /* Chi-squared bin edges per unit (multi_filter.edges_per_template, pipeline/multi_filter.py:264-282; the fused
  * kernel of chisq_edges.py:92-143): E[u, 0..B] int32, B >= max nbins. Unit count = min(*ucount, umax) when ucount is
  * not NULL, else umax. nbins and kmax are indexed by the unit's row. offset_mode 1 reproduces the reference's

@@ -57,12 +57,25 @@ def gemm(a):
         _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(A), _lib.ptr(lo[0]), A.stride(0), _lib.ptr(Z), _lib.ptr(lo[1]),
                   Z.stride(0), n, Kh, Tn, 16, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rs), _lib.ptr(wk),
                   0 if wk is None else wk.numel(), _lib.stream_ptr())
-    ms = _time(f, a.reps)
     useful = 8.0 * n * r * Tn
     issued = (3 if code == 2 else 1) * 4.0 * n * 2 * Kh * Tn
     zbytes = 2 * Kh * Tn * (1 if code == 3 else 2) * (2 if code == 2 else 1)
-    return dict(kernel='umma_cplx_kernel', form=a.form, n=n, r=r, Kh=Kh, Tn=Tn, ms=ms, useful_tflops=useful / ms / 1e9,
-                issued_tflops=issued / ms / 1e9, z_gbs=zbytes / ms / 1e6)
+    out = dict(kernel='umma_cplx_kernel', form=a.form, n=n, r=r, Kh=Kh, Tn=Tn)
+    # launch configurations (gwb_gemm_set_config): pair x stages x order; results must not depend on them
+    ref = None
+    for pair in [int(x) for x in a.pair.split(',')]:
+        for st in [int(x) for x in a.stages.split(',')]:
+            for order in [int(x) for x in a.orders.split(',')]:
+                _lib.call('gwb_gemm_set_config', code, Kh, pair, st, order)
+                ms = _time(f, a.reps)
+                if ref is None:
+                    ref = (V.clone(), I.clone())
+                same = bool(torch.equal(ref[0], V) and torch.equal(ref[1], I))
+                out['p%d_s%d_o%d' % (pair, st, order)] = dict(ms=ms, useful_tflops=useful / ms / 1e9,
+                                                              issued_tflops=issued / ms / 1e9,
+                                                              z_gbs=zbytes / ms / 1e6, same_output=same)
+    _lib.call('gwb_gemm_clear_configs')
+    return out
 
 
 def basis(a):
@@ -85,11 +98,21 @@ def basis(a):
         out.update(ms_cufft_path=ms, us_per_row_cufft=ms * 1e3 / r)
     zb = 2 * Tn * {'f16': 2, 'bf16': 2, 'fp8': 1}.get(a.form, 4)
     for wr in [int(x) for x in a.wrows.split(',')]:
-        fws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wr or None)
+        fws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wr or None, ring=False)
         msf = _time(lambda: fp_filter.basis_series_fused(fws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
         # HBM bytes of the fused form when W stays in L2: Vh read and Z written (D isw stays in L2)
         out[f'us_per_row_fused_w{fws.wrows}'] = msf * 1e3 / r
         out[f'hbm_gbs_w{fws.wrows}'] = r * (8 * flen + zb) / msf / 1e6
+    if tlen == fp_filter.RING_N:
+        ref, ref_scale = Z.double() * fws.scale.double(), fws.scale.double()
+        rws = fp_filter.FusedBasisWorkspace(tlen, flen, r, ring=True)
+        msr = _time(lambda: fp_filter.basis_series_fused(rws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
+        out['us_per_row_ring'] = msr * 1e3 / r
+        out['hbm_gbs_ring'] = r * (8 * flen + zb) / msr / 1e6
+        # the ring form's scale comes from 2 rows instead of 64: compare the series times their scales
+        got = Z.double() * rws.scale.double()
+        out['ring_vs_two_pass_max_rel'] = float(((got - ref).abs().max() / ref.abs().max()).item())
+        out['ring_scale_over_two_pass'] = float((rws.scale.double() / ref_scale).item())
     return out
 
 
@@ -511,6 +534,9 @@ def main():
     ap.add_argument('--peaks', type=int, default=1)
     ap.add_argument('--reps', type=int, default=10)
     ap.add_argument('--wrows', default='0', help='basis: comma list of W row batches (0: all rows at once)')
+    ap.add_argument('--pair', default='1', help='gemm: comma list, 1 CTA pairs, 0 one CTA per M block')
+    ap.add_argument('--stages', default='0', help='gemm: comma list of Z ring depths (0: the most that fit)')
+    ap.add_argument('--orders', default='0', help='gemm: comma list of MMA orders of the CTA-pair kernel (0-3)')
     a = ap.parse_args()
     print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact, 'adjoint': adjoint, 'c4': c4}[a.what](a)))
 

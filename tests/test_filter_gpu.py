@@ -111,11 +111,12 @@ def test_fourstep_order(tlen, flen):
     assert np.array_equal(P, ref)
 
 
-@pytest.mark.parametrize('tlen,wrows', [(1 << 12, None), (1 << 13, 32), (1 << 15, None), (1 << 16, 32), (1 << 20, 8),
-                                        (1 << 20, None)])
-def test_fused_basis_series_matches_float64_transform(tlen, wrows):
-    """The fused two-pass basis series (fp32 output) times its scale equals ifft(conj(Vh) D isw) over the span, with the
-    rows in batches of wrows through W."""
+@pytest.mark.parametrize('tlen,wrows,ring', [(1 << 12, None, False), (1 << 13, 32, False), (1 << 15, None, False),
+                                             (1 << 16, 32, False), (1 << 20, 8, False), (1 << 20, None, False),
+                                             (1 << 20, None, True)])
+def test_fused_basis_series_matches_float64_transform(tlen, wrows, ring):
+    """The fused basis series (fp32 output) times its scale equals ifft(conj(Vh) D isw) over the span: two passes with
+    the rows in batches of wrows through W, or (2^20) the persistent ring form with W in L2."""
     from gwb200 import fp_filter
     rng = np.random.default_rng(tlen % 1000)
     flen = tlen // 2 + 1
@@ -125,7 +126,7 @@ def test_fused_basis_series_matches_float64_transform(tlen, wrows):
     isw = rng.uniform(0.5, 2, flen).astype(np.float32)
     Dw = D * isw
     a0, Tn = tlen // 16, tlen - tlen // 8
-    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wrows)
+    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wrows, ring=ring)
     Z = torch.zeros((2 * r, Tn), dtype=torch.float32, device='cuda')
     Vp = fp_filter.fourstep_order(torch.from_numpy(Vh).cuda(), tlen)
     Dp = fp_filter.fourstep_order(torch.from_numpy(D).cuda(), tlen, torch.from_numpy(isw).cuda())
@@ -135,14 +136,15 @@ def test_fused_basis_series_matches_float64_transform(tlen, wrows):
     got = (Z[:r].double() + 1j * Z[r:].double()).cpu().numpy() * scale
     err = np.abs(got - zb).max() / np.abs(zb).max()
     assert err < 2e-5, err
-    # Parseval scale over the first min(64, wrows) rows
-    nf = min(64, ws.wrows)
+    # Parseval scale over the first min(64, wrows) rows (the ring form: the first chunk of two rows)
+    nf = 2 if ring else min(64, ws.wrows)
     q = np.conj(Vh[:nf].astype(np.complex128)) * Dw
     assert abs(scale - np.sqrt((np.abs(q) ** 2).sum() / nf / 2)) < 1e-5 * scale
 
 
-@pytest.mark.parametrize('tlen,wrows', [(1 << 13, None), (1 << 16, 32), (1 << 20, 8)])
-def test_fused_basis_series_fp8_rows(tlen, wrows):
+@pytest.mark.parametrize('tlen,wrows,ring', [(1 << 13, None, False), (1 << 16, 32, False), (1 << 20, 8, False),
+                                             (1 << 20, None, True)])
+def test_fused_basis_series_fp8_rows(tlen, wrows, ring):
     """fp8 form: rowscale[j] = sqrt(sum_k |q_jk|^2 / 2) / 16 (Parseval), and Z row j holds z_j / rowscale[j] rounded to
     e4m3 (3 mantissa bits: within 2^-4 relative, or half the smallest subnormal step for the smallest values), plus
     the float32 transform's own error (which can move a value across a rounding midpoint)."""
@@ -156,7 +158,7 @@ def test_fused_basis_series_fp8_rows(tlen, wrows):
     isw = rng.uniform(0.5, 2, flen).astype(np.float32)
     Dw = D * isw
     a0, Tn = tlen // 16, tlen - tlen // 8
-    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wrows)
+    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wrows, ring=ring)
     Kh = fp_filter.kh_of(r, 'fp8')
     Z = torch.zeros((2 * Kh, -(-Tn // 16) * 16), dtype=torch.uint8, device='cuda')
     Vp = fp_filter.fourstep_order(torch.from_numpy(Vh).cuda(), tlen)
@@ -174,3 +176,31 @@ def test_fused_basis_series_fp8_rows(tlen, wrows):
         bound = np.maximum(2.0 ** -4 * np.abs(part_ref), 2.0 ** -10) + 1e-5 * np.abs(ref).max()
         assert (err <= bound).all(), (err - bound).max()
     assert np.abs(ref).max() < 448                                   # no saturation at this scale
+
+
+@pytest.mark.parametrize('form', ['f16', 'bf16', 'bf16x3'])
+def test_ring_basis_series_16bit_forms(form):
+    """The persistent ring form (N = 2^20) packing 16-bit Z: fp16 and bf16 within their rounding of the float64
+    transform, split bf16 (hi + lo) within 2^-16 relative to the series' maximum, against the same scale."""
+    from gwb200 import fp_filter
+    tlen = 1 << 20
+    rng = np.random.default_rng(5)
+    flen = tlen // 2 + 1
+    r = 9
+    Vh = (rng.standard_normal((r, flen)) + 1j * rng.standard_normal((r, flen))).astype(np.complex64)
+    D = (rng.standard_normal(flen) + 1j * rng.standard_normal(flen)).astype(np.complex64)
+    isw = rng.uniform(0.5, 2, flen).astype(np.float32)
+    a0, Tn = tlen // 16, tlen - tlen // 8
+    ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, ring=True)
+    Kh = fp_filter.kh_of(r, form)
+    dt = fp_filter._z_dtype(form)
+    Z = torch.zeros((2 * Kh, Tn), dtype=dt, device='cuda')
+    Zlo = torch.zeros_like(Z) if form == 'bf16x3' else None
+    Vp = fp_filter.fourstep_order(torch.from_numpy(Vh).cuda(), tlen)
+    Dp = fp_filter.fourstep_order(torch.from_numpy(D).cuda(), tlen, torch.from_numpy(isw).cuda())
+    scale = float(fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo, form, im_off=Kh).item())
+    zf = Z.double() + (Zlo.double() if Zlo is not None else 0)
+    got = (zf[:r] + 1j * zf[Kh:Kh + r]).cpu().numpy() * scale
+    zb = of.basis_series_complex(Vh, D * isw, a0, Tn, tlen)
+    err = np.abs(got - zb) / np.abs(zb).max()
+    assert err.max() < {'f16': 1e-3, 'bf16': 8e-3, 'bf16x3': 3e-5}[form], err.max()

@@ -190,8 +190,10 @@ def test_cplx_f16_against_oracle(M, r, Tn, group, split):
     _check(V.cpu().numpy(), I.cpu().numpy(), Vr, Ir, tie)
 
 
-@pytest.mark.parametrize('form,r', [(1, 120), (2, 120), (2, 40)])
+@pytest.mark.parametrize('form,r', [(1, 120), (2, 120), (2, 40), (2, 150), (2, 192), (2, 250)])
 def test_cplx_bf16_forms_against_oracle(form, r):
+    """bf16 and split bf16 (Kh <= 128: A hi and lo resident; beyond: A hi resident, A lo streamed with Z) against
+    the float64 stacked product, with whole windows per CTA and with tile-granular ranges (merged windows)."""
     from gwb200 import _lib
     rng = np.random.default_rng(form * 100 + r)
     M, Tn, group = 256, 2048 * 8, 16
@@ -208,26 +210,30 @@ def test_cplx_bf16_forms_against_oracle(form, r):
     nout = -(-(Tn // 128) // group)
     V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
     I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
-    _lib.call('gwb_fused_peaks_cplx', form, _lib.ptr(Ah), _lib.ptr(Al if form == 2 else None), Ah.stride(0),
-              _lib.ptr(Zh), _lib.ptr(Zl if form == 2 else None), Zh.stride(0), M, Kh, Tn, group, _lib.ptr(V),
-              _lib.ptr(I), V.stride(0), None, None, 0, _lib.stream_ptr())
     Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
     Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
     Vr, Ir = og.group_reduce(*og.gemm_absmax(Are, Aim, Z, M, Tn), group)
-    rel = np.abs(V.cpu().numpy() - Vr) / Vr
-    # split bf16 carries ~16 bits per operand; one bf16 product ~8 bits, averaged over K terms
-    assert rel.max() < (5e-5 if form == 2 else 2e-2), rel.max()
-    assert (I.cpu().numpy() == Ir).mean() > (0.99 if form == 2 else 0.8)
+    work = torch.empty(_lib.load().gwb_fused_peaks_cplx_work_bytes(M), dtype=torch.uint8, device='cuda')
+    for wk in (None, work):
+        V.fill_(-7.0)
+        _lib.call('gwb_fused_peaks_cplx', form, _lib.ptr(Ah), _lib.ptr(Al if form == 2 else None), Ah.stride(0),
+                  _lib.ptr(Zh), _lib.ptr(Zl if form == 2 else None), Zh.stride(0), M, Kh, Tn, group, _lib.ptr(V),
+                  _lib.ptr(I), V.stride(0), None, _lib.ptr(wk), 0 if wk is None else wk.numel(), _lib.stream_ptr())
+        rel = np.abs(V.cpu().numpy() - Vr) / Vr
+        # split bf16 carries ~16 bits per operand; one bf16 product ~8 bits, averaged over K terms
+        assert rel.max() < (5e-5 if form == 2 else 2e-2), rel.max()
+        assert (I.cpu().numpy() == Ir).mean() > (0.99 if form == 2 else 0.8)
 
 
 def test_cplx_rejects_oversized_kh():
     from gwb200 import _lib
     with pytest.raises(_lib.GwbError, match='shared memory'):
-        x = torch.zeros((256, 512), dtype=torch.bfloat16, device='cuda')
-        z = torch.zeros((512, 4096), dtype=torch.bfloat16, device='cuda')
+        # Kh = 336: A hi alone (11 swizzle tiles of 16 KB) and two stages exceed the 227 KB of a CTA
+        x = torch.zeros((256, 672), dtype=torch.bfloat16, device='cuda')
+        z = torch.zeros((672, 4096), dtype=torch.bfloat16, device='cuda')
         V = torch.empty((256, 2), dtype=torch.float32, device='cuda')
         I = torch.empty((256, 2), dtype=torch.int32, device='cuda')
-        _lib.call('gwb_fused_peaks_cplx', 2, _lib.ptr(x), _lib.ptr(x), 512, _lib.ptr(z), _lib.ptr(z), 4096, 256, 256,
+        _lib.call('gwb_fused_peaks_cplx', 2, _lib.ptr(x), _lib.ptr(x), 672, _lib.ptr(z), _lib.ptr(z), 4096, 256, 336,
                   4096, 16, _lib.ptr(V), _lib.ptr(I), 2, None, None, 0, _lib.stream_ptr())
 
 
