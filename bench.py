@@ -284,6 +284,15 @@ def traffic_ratios():
     return out
 
 
+def form_config(form, autotune=False):
+    """The filter configuration of a form: the fp8 screen with its exact-stage local search (+-2 samples around the
+    screened argmax) and a candidate list for its wider margin."""
+    from gwb200 import pipeline
+    if form == 'fp8':
+        return pipeline.FilterConfig(form=form, screen_search=2, autotune=autotune)
+    return pipeline.FilterConfig(form=form, autotune=autotune)
+
+
 def run_c2(a):
     import torch
     import torch.distributed as dist
@@ -317,6 +326,7 @@ def run_c2(a):
     forms = a.forms.split(',')
     results = {}
     kept_sets = {}
+    tunings = {}
     torch.cuda.synchronize()
     t_b = time.perf_counter()
     B = pipeline.Bank(bank, FLEN, DF, sw, pipeline.FilterConfig(form=forms[0]), device=dev)
@@ -324,8 +334,9 @@ def run_c2(a):
     bank_setup = time.perf_counter() - t_b
     analysed = nch * (A1 - A0) / SR
     for fi, form in enumerate(forms):
-        cfg = pipeline.FilterConfig(form=form)
+        cfg = form_config(form, autotune=not a.no_autotune)
         mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg, device=dev)
+        tunings[form] = mf.tuning
 
         def step():
             Dd, IPd = cond(x)
@@ -417,12 +428,26 @@ def run_c2(a):
                              split_ms=split)
         if ms_e2e is not None:
             results[form].update(e2e=world * (analysed / WEEK2) / (ms_e2e / 1e3 / 3600.0), ms_e2e=ms_e2e)
+        if head:
+            # the exact stage with its bands staged in shared memory by bulk copies (TMA) instead of direct loads
+            from gwb200 import _lib as glib
+            glib.call('gwb_exact_set_staging', 1)
+            mf.profile = {}
+            Dd, IPd = cond(x)
+            mf.step(Dd, IPd, isw)
+            torch.cuda.synchronize()
+            results[form]['exact_ms_bulk'] = [a_.elapsed_time(b_) for nm, (a_, b_) in mf.profile['parts']
+                                              if nm == 'exact'][0]
+            results[form]['exact_ms_direct'] = split.get('exact')
+            mf.profile = None
+            glib.call('gwb_exact_set_staging', 0)
         del mf
         torch.cuda.empty_cache()
     precision_rep = None
     if not a.no_precision and rank == 0:
         import microbench
-        precision_rep = microbench.precision_c2(B, cond, x, isw, forms, dict(df=DF, tlen=TLEN, a0=A0, an=A1 - A0,
+        precision_rep = microbench.precision_c2(B, cond, x, isw, forms, form_config,
+                                                dict(df=DF, tlen=TLEN, a0=A0, an=A1 - A0,
                                                                                cw=CW, thr=THR))
     main_form = forms[0]
     R = results[main_form]
@@ -471,9 +496,13 @@ def run_c2(a):
                 forms={k: dict(value=v['value'], ms_per_step=v['ms'], steps=v['steps'], warmup=v['warmup'],
                                e2e=v.get('e2e'), n_candidates=v['n_candidates'], n_kept=v['n_kept'],
                                gemm_ms_per_launch=v['gemm_ms'], gemm_share=v['gemm_total_ms'] / v['ms'],
-                               basis_share=v['basis_total_ms'] / v['ms'], clocks=v['clocks'], split_ms=v['split_ms'])
+                               basis_share=v['basis_total_ms'] / v['ms'], clocks=v['clocks'], split_ms=v['split_ms'],
+                               exact_ms_direct=v.get('exact_ms_direct'), exact_ms_bulk=v.get('exact_ms_bulk'))
                        for k, v in results.items()},
-                peaks_source=kind)
+                peaks_source=kind,
+                autotune={f: (None if t is None else dict(gemm={str(k): v['best'] for k, v in t['gemm'].items()},
+                                                            basis=t['basis'] and t['basis']['best']))
+                          for f, t in tunings.items()})
     if rank == 0 and world == 1 and not a.no_cpu:
         S = cpu_setup(bank if len(bank['mass1']) == N_TEMPLATES else make_bank())
         cpu_step(S, 0)
@@ -537,6 +566,7 @@ def main():
     ap.add_argument('--forms', default='f16,bf16x3,bf16,fp8,f32', help='forms timed (the first gives value)')
     ap.add_argument('--form-steps', type=int, default=3, help='timed steps of each form after the first')
     ap.add_argument('--production', action='store_true', help='c4: production selection and consolidation')
+    ap.add_argument('--no-autotune', action='store_true', help='c2: default launch shapes instead of tuned ones')
     a = ap.parse_args()
     if a.impl == 'reference':
         run_reference(a)

@@ -16,6 +16,7 @@
 // finalize: per peak, Z_j = sum over chunks of its slots (fp32, chunk order); z = sum_j Z_j and pw = sum_j |Z_j|^2
 //   in float64; then snr = |z| norm, chisq = (nb pw - |z|^2) norm^2, dof = 2 nb - 2, newsnr, fpeak
 //   (fp_filter.py:837-853, exact_stage.py:236-238, coinc_rank.py:39-46) with norm = 4 df / sqrt(sigma^2).
+#include <atomic>
 #include "common.cuh"
 
 namespace gwb {
@@ -26,6 +27,8 @@ constexpr int kSumThreads = 256;
 constexpr int kChunk = 32768;
 constexpr int kReseed = 16;
 constexpr int kMaxPeaks = 8;
+// the ordered binned sums stage their bands with bulk copies (gwb_exact_set_staging); process-wide
+std::atomic<bool> g_exact_bulk{false};
 
 __device__ __forceinline__ int count_of(const int32_t* dev, int host_max) {
     return dev ? min(*dev, host_max) : host_max;
@@ -200,6 +203,176 @@ __global__ void __launch_bounds__(kSumThreads) binsum_kernel(const GwbGroup* __r
                         w[p] = make_float2(fmaf(ww.x, rot[p].x, -(ww.y * rot[p].y)), fmaf(ww.x, rot[p].y, ww.y * rot[p].x));
                     }
                 }
+            }
+#pragma unroll
+            for (int p = 0; p < kMaxPeaks; ++p) {
+                float x = acc[p].x, y = acc[p].y;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    x += __shfl_down_sync(0xffffffffu, x, off);
+                    y += __shfl_down_sync(0xffffffffu, y, off);
+                }
+                if (lane == 0) red[warp][p] = make_float2(x, y);
+            }
+            __syncthreads();
+            if (t < np) {
+                float x = 0.f, y = 0.f;
+                for (int q = 0; q < kSumThreads / 32; ++q) {
+                    x += red[q][t].x;
+                    y += red[q][t].y;
+                }
+                slots[((long long)(gr.first + t) * nchunk + c) * B + j] = make_float2(x, y);
+            }
+            __syncthreads();
+            a = b;
+            ++j;
+        }
+    }
+}
+
+// The same binned sums with the template and data bands staged in shared memory by the bulk-copy (TMA) engine:
+// every bin sub-range of an item is cut into tiles of kTile bins, and one thread issues cp.async.bulk copies of the
+// tile's h and D runs (16-byte aligned: a run starts at the aligned address below its first bin and is rounded up to 16
+// bytes, so it covers one bin more on either side at most, both inside the row) into one of two stages while the
+// block computes the previous tile from the other. Each thread visits the same bins in the same order with the same
+// recurrence and reseeds as binsum_kernel, so the slots are bit for bit the same. Every wait is bounded.
+constexpr int kTile = 2048;
+constexpr int kStage = kTile + 4;              // float2 per stage and operand (alignment slack)
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+__global__ void __launch_bounds__(kSumThreads) binsum_bulk_kernel(
+    const GwbGroup* __restrict__ groups, const int32_t* gcount, int gmax, const GwbUnit* __restrict__ units,
+    const GwbCand* __restrict__ cands, const int32_t* __restrict__ E, int B, const int32_t* __restrict__ nbins,
+    const float2* __restrict__ H, long long ldh, const float2* __restrict__ D, long long ldd, int kmin, int nchunk,
+    unsigned nmask, float inv_half_n, const int32_t* __restrict__ order, float2* __restrict__ slots,
+    DeviceError* err) {
+    __shared__ float2 red[kSumThreads / 32][kMaxPeaks];
+    extern __shared__ __align__(16) float2 stg[];            // sh[2][kStage], then sd[2][kStage]
+    float2 (*sh)[kStage] = reinterpret_cast<float2 (*)[kStage]>(stg);
+    float2 (*sd)[kStage] = reinterpret_cast<float2 (*)[kStage]>(stg + 2 * kStage);
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ int s_off[2][2];                    // per stage: index of the tile's first bin in sh, sd
+    __shared__ int s_abort;
+    const int ng = count_of(gcount, gmax);
+    const long long nitems = (long long)ng * nchunk;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        s_abort = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t issued = 0;                           // tiles issued by this CTA (stage = issued & 1)
+    // thread 0: copy the h and D runs of bins [k0, k1) into the next stage
+    auto issue = [&](const float2* h, const float2* d, int k0, int k1) {
+        const int st = issued & 1;
+        const uintptr_t ha = reinterpret_cast<uintptr_t>(h + k0) & ~(uintptr_t)15;
+        const uintptr_t he = (reinterpret_cast<uintptr_t>(h + k1) + 15) & ~(uintptr_t)15;
+        const uintptr_t da = reinterpret_cast<uintptr_t>(d + k0) & ~(uintptr_t)15;
+        const uintptr_t de = (reinterpret_cast<uintptr_t>(d + k1) + 15) & ~(uintptr_t)15;
+        s_off[st][0] = (int)((reinterpret_cast<uintptr_t>(h + k0) - ha) / sizeof(float2));
+        s_off[st][1] = (int)((reinterpret_cast<uintptr_t>(d + k0) - da) / sizeof(float2));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_expect_tx(&full[st], (uint32_t)((he - ha) + (de - da)));
+        bulk_g2s(sh[st], reinterpret_cast<const void*>(ha), (uint32_t)(he - ha), &full[st]);
+        bulk_g2s(sd[st], reinterpret_cast<const void*>(da), (uint32_t)(de - da), &full[st]);
+        ++issued;
+    };
+    uint32_t consumed = 0;
+    for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
+        int g, c;
+        if (order) {
+            c = (int)(it / ng);
+            g = order[(int)(it % ng)];
+        } else {
+            g = (int)(it / nchunk);
+            c = (int)(it % nchunk);
+        }
+        const GwbGroup gr = groups[g];
+        const GwbUnit un = units[gr.unit];
+        const int np = gr.count;
+        const int nb = max(nbins[un.row], 1);
+        const int32_t* e = E + (long long)gr.unit * (B + 1);
+        const int c0 = kmin + c * kChunk, c1 = c0 + kChunk;
+        const int lo = max(c0, e[0]), hi = min(c1, e[nb]);
+        if (lo >= hi) continue;   // uniform
+        unsigned tp[kMaxPeaks];
+        float2 rot[kMaxPeaks];
+#pragma unroll
+        for (int p = 0; p < kMaxPeaks; ++p) {
+            tp[p] = p < np ? (unsigned)cands[gr.first + p].sample : 0u;
+            float sn, cs;
+            sincospif((float)(((unsigned)kSumThreads * tp[p]) & nmask) * inv_half_n, &sn, &cs);
+            rot[p] = make_float2(cs, sn);
+        }
+        const float2* h = H + (long long)un.row * ldh;
+        const float2* d = D + (long long)un.seg * ldd;
+        int j = bin_of(e, nb, lo);
+        int a = lo;
+        // the item's tiles: bin sub-range [a, b) cut at a + kTile m; the first is issued here, each next one while
+        // the current is computed
+        int tb = min(min(hi, e[j + 1]), a + kTile);
+        if (t == 0) issue(h, d, a, tb);
+        while (a < hi) {
+            const int b = min(hi, e[j + 1]);
+            float2 acc[kMaxPeaks];
+            float2 w[kMaxPeaks];
+#pragma unroll
+            for (int p = 0; p < kMaxPeaks; ++p) acc[p] = make_float2(0.f, 0.f);
+            int step = 0;
+            for (int ta = a; ta < b; ta += kTile) {
+                const int te = min(b, ta + kTile);
+                // the next tile: the rest of this sub-range, else the first bins of the next non-empty sub-range
+                if (t == 0) {
+                    if (te < b) {
+                        issue(h, d, te, min(b, te + kTile));
+                    } else if (b < hi) {
+                        int jj = j + 1;
+                        while (jj < nb && min(hi, e[jj + 1]) <= b) ++jj;   // empty bins hold no tile
+                        issue(h, d, b, min(min(hi, e[jj + 1]), b + kTile));
+                    }
+                }
+                const int st = consumed & 1;
+                if (t == 0 && !mbar_wait_bounded(&full[st], (consumed >> 1) & 1)) {
+                    record_error(err, GWB_ERR_TIMEOUT, 401, (int)blockIdx.x, (int)consumed);
+                    s_abort = 1;
+                    // the other stage's copy, if one was issued, must land before the block leaves
+                    for (uint32_t u = consumed + 1; u < issued; ++u) mbar_wait_bounded(&full[u & 1], (u >> 1) & 1);
+                }
+                __syncthreads();
+                if (s_abort) return;                       // uniform; the error word tells the host
+                const float2* hs = sh[st] + s_off[st][0] - ta;
+                const float2* ds = sd[st] + s_off[st][1] - ta;
+                for (int k = ta + t; k < te; k += kSumThreads, ++step) {
+                    if ((step & (kReseed - 1)) == 0) {
+#pragma unroll
+                        for (int p = 0; p < kMaxPeaks; ++p) {
+                            float sn, cs;
+                            sincospif((float)(((unsigned)k * tp[p]) & nmask) * inv_half_n, &sn, &cs);
+                            w[p] = make_float2(cs, sn);
+                        }
+                    }
+                    const float2 hk = hs[k], dk = ds[k];
+                    const float qx = fmaf(hk.x, dk.x, hk.y * dk.y);      // conj(h) D
+                    const float qy = fmaf(hk.x, dk.y, -(hk.y * dk.x));
+#pragma unroll
+                    for (int p = 0; p < kMaxPeaks; ++p) {
+                        if (p < np) {
+                            acc[p].x = fmaf(qx, w[p].x, fmaf(-qy, w[p].y, acc[p].x));
+                            acc[p].y = fmaf(qx, w[p].y, fmaf(qy, w[p].x, acc[p].y));
+                            const float2 ww = w[p];
+                            w[p] = make_float2(fmaf(ww.x, rot[p].x, -(ww.y * rot[p].y)),
+                                               fmaf(ww.x, rot[p].y, ww.y * rot[p].x));
+                        }
+                    }
+                }
+                ++consumed;
+                __syncthreads();                           // the stage is free for the copy after next
             }
 #pragma unroll
             for (int p = 0; p < kMaxPeaks; ++p) {
@@ -402,11 +575,26 @@ int gwb_bin_sums_ordered(const GwbGroup* groups, const int32_t* gcount, int gmax
     const int nchunk = (int)cdiv(flen - kmin, kChunk);
     const long long items = (long long)gmax * nchunk;
     const int grid = (int)std::min<long long>(items, 16ll * num_sms());
+    if (g_exact_bulk.load()) {
+        const size_t smem = 4 * kStage * sizeof(float2);
+        GWB_CUDA(cudaFuncSetAttribute(binsum_bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        binsum_bulk_kernel<<<grid, kSumThreads, smem, s>>>(
+            groups, gcount, gmax, units, cands, E, B, nbins, reinterpret_cast<const float2*>(H), ldh,
+            reinterpret_cast<const float2*>(D), ldd, kmin, nchunk, (unsigned)(tlen - 1), (float)(2.0 / (double)tlen),
+            order, reinterpret_cast<float2*>(slots), device_error_ptr());
+        GWB_LAUNCH_CHECK("binsum_bulk_kernel");
+        return GWB_OK;
+    }
     binsum_kernel<<<grid, kSumThreads, 0, s>>>(
         groups, gcount, gmax, units, cands, E, B, nbins, reinterpret_cast<const float2*>(H), ldh,
         reinterpret_cast<const float2*>(D), ldd, kmin, nchunk, (unsigned)(tlen - 1), (float)(2.0 / (double)tlen),
         order, reinterpret_cast<float2*>(slots));
     GWB_LAUNCH_CHECK("binsum_kernel");
+    return GWB_OK;
+}
+
+int gwb_exact_set_staging(int bulk) {
+    gwb::g_exact_bulk.store(bulk != 0);
     return GWB_OK;
 }
 

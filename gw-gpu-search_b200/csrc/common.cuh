@@ -39,6 +39,8 @@ inline bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
 inline long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
 
 int num_sms();
+// the GEMM launch table: true and the entry's values when (form, kh) has one
+bool tune_lookup(int form, int kh, int* pair, int* stages, int* order);
 int encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, uint64_t inner, uint64_t outer,
                    uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swz);
 

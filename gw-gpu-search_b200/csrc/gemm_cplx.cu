@@ -15,7 +15,6 @@
 // that the epilogue applies, V = rowscale^2 max |z|^2).
 #include <stdlib.h>
 #include <string.h>
-#include <mutex>
 #include "common.cuh"
 
 namespace gwb {
@@ -769,20 +768,16 @@ __global__ void window_merge_kernel(int M, int ntiles, int group, int nout, int 
     I[(long long)row * ldv + o] = bi;
 }
 
-// Launch configuration per (form, Kh): the table the autotuner fills (gwb_gemm_set_config). Defaults: CTA pairs for
+// Launch configuration per (form, Kh) from the autotuner's table (gwb_gemm_set_config). Defaults: CTA pairs for
 // fp16 / bf16, the deepest Z ring that fits, the MMA order 0.
 struct GemmTune {
     int form, kh, pair, stages, order;
 };
-std::mutex g_tune_mu;
-GemmTune g_tune[128];
-int g_ntune = 0;
 
 GemmTune gemm_tune(int form, int kh) {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    for (int i = 0; i < g_ntune; ++i)
-        if (g_tune[i].form == form && g_tune[i].kh == kh) return g_tune[i];
-    return GemmTune{form, kh, 1, 0, 0};
+    GemmTune t{form, kh, 1, 0, 0};
+    tune_lookup(form, kh, &t.pair, &t.stages, &t.order);
+    return t;
 }
 
 template <int FORM>
@@ -957,28 +952,6 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
 }  // namespace gwb
 
 extern "C" long long gwb_fused_peaks_cplx_work_bytes(int M) { return 16ll * M * gwb::num_sms(); }
-
-extern "C" int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order) {
-    using namespace gwb;
-    GWB_CHECK_ARG(form >= 0 && form <= 3 && kh > 0 && (pair == 0 || pair == 1) && stages >= 0 && stages <= 8 &&
-                      order >= 0 && order <= 3, GWB_ERR_ARG,
-                  "gemm_set_config: form=%d kh=%d pair=%d stages=%d order=%d", form, kh, pair, stages, order);
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    for (int i = 0; i < g_ntune; ++i)
-        if (g_tune[i].form == form && g_tune[i].kh == kh) {
-            g_tune[i] = GemmTune{form, kh, pair, stages, order};
-            return GWB_OK;
-        }
-    GWB_CHECK_ARG(g_ntune < 128, GWB_ERR_CAPACITY, "gemm_set_config: the table holds 128 shapes");
-    g_tune[g_ntune++] = GemmTune{form, kh, pair, stages, order};
-    return GWB_OK;
-}
-
-extern "C" int gwb_gemm_clear_configs(void) {
-    std::lock_guard<std::mutex> lk(gwb::g_tune_mu);
-    gwb::g_ntune = 0;
-    return GWB_OK;
-}
 
 extern "C" int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
                                     const void* Z_lo, long long ldz, int M, int Kh, long long Tn, int group, float* V,

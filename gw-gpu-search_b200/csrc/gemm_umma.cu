@@ -349,6 +349,10 @@ int launch_umma(const uint16_t* const* A, const uint16_t* const* Zp, long long l
     const int max_smem = 227 * 1024;
     int stages = 8;
     while (stages > 1 && smem_layout(C::NA, C::NZ, nkc, K, stages).total + 1024 > (uint32_t)max_smem) --stages;
+    {   // the launch table may ask for a shallower Z ring (forms 4: stacked fp16, 5: stacked split bf16; kh = K)
+        int pair = 0, st = 0, order = 0;
+        if (tune_lookup(FORM == kF16 ? 4 : 5, K, &pair, &st, &order) && st >= 2) stages = std::min(stages, st);
+    }
     const uint32_t smem = smem_layout(C::NA, C::NZ, nkc, K, stages).total + 1024;
     GWB_CHECK_ARG(smem <= (uint32_t)max_smem, GWB_ERR_SHAPE, "fused_peaks: K=%d needs %u bytes of shared memory", K,
                   smem);

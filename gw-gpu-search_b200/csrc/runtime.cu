@@ -52,6 +52,28 @@ DeviceError* device_error_ptr() {
     return g_err[d];
 }
 
+// The GEMM launch table (gwb_gemm_set_config), process-wide under a mutex.
+namespace {
+struct TuneEntry {
+    int form, kh, pair, stages, order;
+};
+std::mutex g_tune_mu;
+TuneEntry g_tune[128];
+int g_ntune = 0;
+}  // namespace
+
+bool tune_lookup(int form, int kh, int* pair, int* stages, int* order) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int i = 0; i < g_ntune; ++i)
+        if (g_tune[i].form == form && g_tune[i].kh == kh) {
+            *pair = g_tune[i].pair;
+            *stages = g_tune[i].stages;
+            *order = g_tune[i].order;
+            return true;
+        }
+    return false;
+}
+
 int num_sms() {
     int d = current_device();
     if (d >= 0 && d < kMaxDev && g_sms[d] > 0) return g_sms[d];
@@ -140,3 +162,25 @@ int gwb_device_error(int* code, int* where, int* info0, int* info1, int clear) {
 int gwb_num_sms(void) { return gwb::num_sms(); }
 
 }  // extern "C"
+
+extern "C" int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order) {
+    using namespace gwb;
+    GWB_CHECK_ARG(form >= 0 && form <= 5 && kh > 0 && (pair == 0 || pair == 1) && stages >= 0 && stages <= 8 &&
+                      order >= 0 && order <= 3, GWB_ERR_ARG,
+                  "gemm_set_config: form=%d kh=%d pair=%d stages=%d order=%d", form, kh, pair, stages, order);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int i = 0; i < g_ntune; ++i)
+        if (g_tune[i].form == form && g_tune[i].kh == kh) {
+            g_tune[i] = TuneEntry{form, kh, pair, stages, order};
+            return GWB_OK;
+        }
+    GWB_CHECK_ARG(g_ntune < 128, GWB_ERR_CAPACITY, "gemm_set_config: the table holds 128 shapes");
+    g_tune[g_ntune++] = TuneEntry{form, kh, pair, stages, order};
+    return GWB_OK;
+}
+
+extern "C" int gwb_gemm_clear_configs(void) {
+    std::lock_guard<std::mutex> lk(gwb::g_tune_mu);
+    gwb::g_ntune = 0;
+    return GWB_OK;
+}

@@ -265,3 +265,94 @@ int gwb_select_top(const GwbCand* cands, const GwbGroup* groups, const GwbUnit* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Local search of a screening form (fp8): every candidate becomes 2L + 1 exact-stage candidates at the samples s - L
+// .. s + L (clamped into the candidate's own cluster window), in the same unit; after the exact stage
+// gwb_search_best keeps the loudest of each run (first on ties) and marks the others with snr = -1. The screen's
+// argmax then only has to fall within L samples of the window's true peak.
+// ---------------------------------------------------------------------------------------------------------------------
+namespace gwb {
+namespace {
+
+__global__ void search_expand_kernel(const GwbCand* __restrict__ cin, const GwbUnit* __restrict__ uin,
+                                     const int32_t* __restrict__ cnt_in, int L, long long a0, int cw,
+                                     GwbCand* __restrict__ cout, int cand_cap, GwbGroup* __restrict__ gout,
+                                     int group_cap, GwbUnit* __restrict__ uout, int unit_cap,
+                                     int32_t* __restrict__ counters) {
+    __shared__ int s_base, s_gbase, s_unit, s_ok;
+    const int nu = cnt_in[2];
+    const int W = 2 * L + 1;
+    for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+        const GwbUnit U = uin[u];
+        const int total = U.count * W, ng = (total + 7) / 8;
+        if (threadIdx.x == 0) {
+            s_base = atomicAdd(&counters[0], total);
+            s_gbase = atomicAdd(&counters[1], ng);
+            s_unit = atomicAdd(&counters[2], 1);
+            s_ok = !(s_base + total > cand_cap || s_gbase + ng > group_cap || s_unit >= unit_cap);
+            if (!s_ok) atomicOr(&counters[3], 1);
+            else uout[s_unit] = GwbUnit{U.row, U.seg, s_base, total};
+        }
+        __syncthreads();
+        if (s_ok) {
+            for (int g = threadIdx.x; g < ng; g += kT)
+                gout[s_gbase + g] = GwbGroup{s_unit, s_base + 8 * g, min(8, total - 8 * g), 0};
+            for (int o = threadIdx.x; o < total; o += kT) {
+                GwbCand cd = cin[U.first + o / W];
+                const long long w0 = a0 + (long long)cd.window * cw;
+                const long long s = min(max((long long)cd.sample + (o % W) - L, w0), w0 + cw - 1);
+                cd.sample = (int)s;
+                cd.unit = s_unit;
+                cout[s_base + o] = cd;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void search_best_kernel(const int32_t* __restrict__ ccount, int cmax, int W, GwbPeak* __restrict__ peaks) {
+    const int n = min(*ccount, cmax) / W;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        GwbPeak* p = peaks + (long long)i * W;
+        int best = 0;
+        for (int d = 1; d < W; ++d)
+            if (p[d].snr > p[best].snr) best = d;
+        for (int d = 0; d < W; ++d)
+            if (d != best) p[d].snr = -1.f;
+    }
+}
+
+}  // namespace
+}  // namespace gwb
+
+extern "C" {
+
+int gwb_search_expand(const GwbCand* cands, const GwbUnit* units, const int32_t* counters, int radius, long long a0,
+                      int cw, GwbCand* cands_out, int cand_cap, GwbGroup* groups_out, GwbUnit* units_out,
+                      int32_t* counters_out, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(cands && units && counters && cands_out && groups_out && units_out && counters_out, GWB_ERR_ARG,
+                  "search_expand: null pointer");
+    GWB_CHECK_ARG(radius >= 1 && radius <= 8 && cw > 2 * radius && a0 >= 0 && cand_cap > 0, GWB_ERR_SHAPE,
+                  "search_expand: radius=%d (1..8) cw=%d a0=%lld", radius, cw, a0);
+    cudaStream_t s = (cudaStream_t)stream;
+    GWB_CUDA(cudaMemsetAsync(counters_out, 0, 4 * sizeof(int32_t), s));
+    // the selection's rebuilt-peak count passes through
+    GWB_CUDA(cudaMemcpyAsync(counters_out + 4, counters + 4, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    search_expand_kernel<<<num_sms() * 4, kT, 0, s>>>(cands, units, counters, radius, a0, cw, cands_out, cand_cap,
+                                                      groups_out, cand_cap, units_out, cand_cap, counters_out);
+    GWB_LAUNCH_CHECK("search_expand_kernel");
+    return GWB_OK;
+}
+
+int gwb_search_best(const int32_t* ccount, int cmax, int radius, GwbPeak* peaks, void* stream) {
+    using namespace gwb;
+    GWB_CHECK_ARG(ccount && peaks && radius >= 1 && radius <= 8 && cmax > 0, GWB_ERR_ARG,
+                  "search_best: radius=%d cmax=%d", radius, cmax);
+    search_best_kernel<<<num_sms() * 4, kT, 0, (cudaStream_t)stream>>>(ccount, cmax, 2 * radius + 1, peaks);
+    GWB_LAUNCH_CHECK("search_best_kernel");
+    return GWB_OK;
+}
+
+}  // extern "C"

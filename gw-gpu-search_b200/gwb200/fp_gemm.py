@@ -17,9 +17,10 @@ from . import _lib
 
 BN = 128
 
-# Our kernel has no Triton-style tile parameters; a cfg is ('umma', group) or the reference's (BM, BK, warps,
-# stages) tuple, which is accepted for call compatibility (only its BK divisibility rule is checked).
-DEFAULT_CFG = ('umma', 1)
+# A cfg is ('umma', stages) (the depth of the kernel's Z ring, 0 = the most that fit; pick_cfg times them; None =
+# whatever the launch table holds) or the reference's (BM, BK, warps, stages) Triton tuple, accepted for call
+# compatibility (only its BK divisibility rule is checked).
+DEFAULT_CFG = ('umma', None)
 
 
 def _check(Are, Aim, Z, M, Tn):
@@ -45,6 +46,9 @@ def fused_peaks(Are, Aim, Z, M, Tn, cfg=DEFAULT_CFG, group=1):
         assert K % cfg[1] == 0, 'K must be a multiple of BK'
     V, I = _outputs(M, Tn, group, Z.device)
     s = _lib.stream_ptr(Z.device)
+    if isinstance(cfg, tuple) and len(cfg) == 2 and cfg[0] == 'umma' and cfg[1] is not None and \
+            Z.dtype == torch.float16:
+        _lib.call('gwb_gemm_set_config', 4, int(K), 0, int(cfg[1]), 0)   # ('umma', stages): the Z ring depth
     if Z.dtype == torch.float16:
         assert Are.dtype == torch.float16 and Aim.dtype == torch.float16
         _lib.call('gwb_fused_peaks_f16', _lib.ptr(Are), _lib.ptr(Aim), Are.stride(0), _lib.ptr(Z), Z.stride(0), int(M),
@@ -74,13 +78,15 @@ def fused_peaks_split(Are_hi, Are_lo, Aim_hi, Aim_lo, Z_hi, Z_lo, M, Tn, group=1
 
 
 def pick_cfg(dev='cuda', M=1024, K=128, Tn=1 << 20):
-    """Time the available forms once on a representative shape; returns (fastest cfg, {cfg: seconds}).
-    Same contract as the reference's autotuner (fp_gemm.py:47-64): raises if nothing runs."""
+    """Times the stacked fp16 kernel's launch configurations (the depth of its Z ring: the most that fit, 4, 3, 2) on
+    the shape and keeps the fastest in the library's launch table (gwb_gemm_set_config, form 4, kh = K); returns
+    (fastest cfg, {cfg: seconds or error text}). Same contract as the reference's autotuner (fp_gemm.py:47-64):
+    raises if nothing runs. cfg = ('umma', stages)."""
     Ar = torch.randn((M, K), device=dev).half()
     Ai = torch.randn((M, K), device=dev).half()
     Zs = torch.randn((K, Tn), device=dev).half()
     res, best = {}, None
-    for c in [('umma', 1)]:
+    for c in [('umma', 0), ('umma', 4), ('umma', 3), ('umma', 2)]:
         try:
             fused_peaks(Ar, Ai, Zs, M, Tn, c)
             torch.cuda.synchronize()
@@ -96,4 +102,5 @@ def pick_cfg(dev='cuda', M=1024, K=128, Tn=1 << 20):
             best = c
     if best is None:
         raise RuntimeError('no GEMM config ran: %r' % res)
+    _lib.call('gwb_gemm_set_config', 4, int(K), 0, int(best[1]), 0)
     return best, res

@@ -21,7 +21,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from . import _exact, _lib, fp_filter, templates
+from . import _exact, _lib, autotune, fp_filter, templates
 
 BN = 128
 
@@ -49,8 +49,14 @@ class FilterConfig:
     # rebuilt SNR and phase (rebuilt peaks). 0: off
     exact_top: int = 0
     exact_top_frac: float = 0.0
+    # local search of a screening form (gwb_search_expand / gwb_search_best): the exact stage at the 2 r + 1 samples
+    # around each candidate's rebuilt argmax inside its window, keeping the loudest; 0: off
+    screen_search: int = 0
     rebuilt_cap: int = 0          # capacity of the rebuilt-peak list (0: cand_cap)
     exact_order: bool = True      # exact stage in template-row order, chunk by chunk (gwb_bin_sums_ordered)
+    # time the GEMM launch configurations of every tile width and the basis-series forms on this run's shapes before
+    # the first step, and use the fastest (gwb200.autotune)
+    autotune: bool = False
 
 
 class Bank:
@@ -108,8 +114,13 @@ class MatchedFilter:
         # the fused two-pass basis series (premul and pack folded into the transform passes) where the length allows,
         # else premul + cuFFT + pack
         self.fused = fp_filter.FUSED_MIN <= tlen <= fp_filter.FUSED_MAX
+        self.tuning = None
+        if cfg.autotune:
+            self.tuning = autotune.tune_filter(bank, tlen, self.Tn, self.form, self.group, device=device)
         if self.fused:
-            self.fws = fp_filter.FusedBasisWorkspace(tlen, bank.flen, rmax, device)
+            bt = self.tuning['basis']['best'] if self.tuning and self.tuning['basis'] else {}
+            self.fws = fp_filter.FusedBasisWorkspace(tlen, bank.flen, rmax, device, wrows=bt.get('wrows'),
+                                                     ring=bt.get('ring'))
             # basis filters in the four-step order of the transform, once per tile; D isw per step (self.Dp)
             self.vp = [fp_filter.fourstep_order(s['Vh'], tlen) for s in bank.svd]
             self.Dp = None
@@ -138,21 +149,25 @@ class MatchedFilter:
                                      device=device) if self.compact else None
         self.I = torch.empty((nmax, self.nw), dtype=torch.int32, device=device)
         cap = cfg.cand_cap
-        self.cands = torch.empty(cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
-        self.groups = torch.empty(cap * _exact.GROUP.itemsize, dtype=torch.uint8, device=device)
-        self.units = torch.empty(cap * _exact.UNIT.itemsize, dtype=torch.uint8, device=device)
+        # the exact stage's lists: with a local search each selected window becomes 2 r + 1 candidates
+        self.search = int(cfg.screen_search)
+        self.search_w = 2 * self.search + 1 if self.search else 1
+        capx = cap * self.search_w
+        self.cands = torch.empty(capx * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
+        self.groups = torch.empty(capx * _exact.GROUP.itemsize, dtype=torch.uint8, device=device)
+        self.units = torch.empty(capx * _exact.UNIT.itemsize, dtype=torch.uint8, device=device)
         self.counters = torch.zeros(5, dtype=torch.int32, device=device)
         self.B = cfg.nbins
-        self.E = torch.empty((cap, self.B + 1), dtype=torch.int32, device=device)
+        self.E = torch.empty((capx, self.B + 1), dtype=torch.int32, device=device)
         self.nchunk = _lib.load().gwb_exact_chunks(bank.flen, bank.kmin)
-        self.slot_cap = cap
-        assert cap <= 1 << 22
+        self.slot_cap = capx
+        assert capx <= 1 << 24
         self.slots = None
         if cfg.exact_order:
-            wb = _lib.load().gwb_bin_sums_work_bytes(cap, bank.M)
+            wb = _lib.load().gwb_bin_sums_work_bytes(capx, bank.M)
             self.sort_work = torch.empty(wb, dtype=torch.uint8, device=device)
             self.sort_status = torch.zeros(1, dtype=torch.int32, device=device)
-        self.peaks = torch.empty(cap * _exact.PEAK.itemsize, dtype=torch.uint8, device=device)
+        self.peaks = torch.empty(capx * _exact.PEAK.itemsize, dtype=torch.uint8, device=device)
         margin = max(cfg.margin, cfg.screen_margin) if self.fp8 else cfg.margin
         self.thr2 = float((cfg.snr_threshold * (1 - margin)) ** 2)
         assert not (self.fp8 and cfg.exact_snr > 0), 'the fp8 screen keeps no rebuilt values: use exact_snr = 0'
@@ -160,14 +175,17 @@ class MatchedFilter:
         self.rthr = float(np.float32(cfg.snr_threshold))
         self.top = cfg.exact_top > 0 or cfg.exact_top_frac > 0
         assert not (self.top and cfg.exact_snr > 0), 'one exact-stage rule at a time: exact_snr or exact_top(_frac)'
+        assert not (self.search and (self.top or cfg.exact_snr > 0)), 'the local search takes every candidate'
         self.rebuilt_cap = cfg.rebuilt_cap or cap
         self.rebuilt = (torch.empty(self.rebuilt_cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device)
                         if cfg.exact_snr > 0 or self.top else None)
         # the selection's own lists: with a rank rule the windows are selected into these, then gwb_select_top
         # moves the ranked subset into cands / groups / units / counters for the exact stage
-        if self.top:
-            self.sel = dict(cands=torch.empty_like(self.cands), groups=torch.empty_like(self.groups),
-                            units=torch.empty_like(self.units), counters=torch.zeros_like(self.counters))
+        if self.top or self.search:
+            self.sel = dict(cands=torch.empty(cap * _exact.CAND.itemsize, dtype=torch.uint8, device=device),
+                            groups=torch.empty(cap * _exact.GROUP.itemsize, dtype=torch.uint8, device=device),
+                            units=torch.empty(cap * _exact.UNIT.itemsize, dtype=torch.uint8, device=device),
+                            counters=torch.zeros_like(self.counters))
             self.top_work = None
         else:
             self.sel = dict(cands=self.cands, groups=self.groups, units=self.units, counters=self.counters)
@@ -271,6 +289,13 @@ class MatchedFilter:
                       self.rthr, _lib.ptr(self.cands), _lib.ptr(self.groups), _lib.ptr(self.units), _lib.ptr(cnt),
                       _lib.ptr(self.rebuilt), self.rebuilt_cap, _lib.ptr(self.top_work), self.top_work.numel(), s)
             self.kernel_launches += 5
+        if self.search:
+            sc = self.sel
+            _lib.call('gwb_search_expand', _lib.ptr(sc['cands']), _lib.ptr(sc['units']), _lib.ptr(sc['counters']),
+                      self.search, self.a0, self.cw, _lib.ptr(self.cands), self.slot_cap, _lib.ptr(self.groups),
+                      _lib.ptr(self.units), _lib.ptr(cnt), s)
+            self.kernel_launches += 1
+        cap = self.slot_cap                    # the exact stage's lists
         _lib.call('gwb_edges', _lib.ptr(self.units), _lib.ptr(cnt[2:]), cap, _lib.ptr(b.H), b.H.stride(0),
                   _lib.ptr(IP), IP.stride(0), _lib.ptr(b.nbins), _lib.ptr(b.kmax), b.kmin, self.B, 0, _lib.ptr(self.E), s)
         if self.slots is None:
@@ -290,12 +315,15 @@ class MatchedFilter:
                   _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), b.kmin, b.flen, _lib.ptr(self.slots), _lib.ptr(sig),
                   sig.stride(0), float(b.df), _lib.ptr(self.peaks), s)
         self.kernel_launches += 3
+        if self.search:
+            _lib.call('gwb_search_best', _lib.ptr(cnt[0:]), cap, self.search, _lib.ptr(self.peaks), s)
+            self.kernel_launches += 1
 
     def step(self, D, IP, isw, seg_ids=None):
         """Queue one step on the current stream: every tile against every segment in seg_ids (rows of D / IP).
         Nothing is copied back; call results() after the stream is synchronised."""
         self.counters.zero_()
-        if self.top:
+        if self.top or self.search:
             self.sel['counters'].zero_()
         prof = self.profile
         ev = (lambda: torch.cuda.Event(enable_timing=True)) if prof is not None else None
@@ -336,7 +364,7 @@ class MatchedFilter:
         and phase are the rebuilt ones: `rebuilt`, GwbCand records, or with rebuilt_on_device `rebuilt_dev`, a view
         of the device list as an (n, 8) int32 tensor of the GwbCand fields)."""
         c = self.counters.cpu().numpy()
-        if c[3] or (self.top and int(self.sel['counters'][3].item())):
+        if c[3] or ((self.top or self.search) and int(self.sel['counters'][3].item())):
             raise _lib.GwbError('select', _lib.GWB_ERR_CAPACITY, 'candidate capacity %d exceeded' % self.cfg.cand_cap)
         if self.cfg.exact_order and int(self.sort_status.item()):
             raise _lib.GwbError('bin_sums_ordered', _lib.GWB_ERR_SHAPE, 'a unit row outside the bank')

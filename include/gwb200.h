@@ -129,8 +129,9 @@ GWB_API long long gwb_fused_peaks_cplx_work_bytes(int M);
  * work buffer), 0 = one CTA per M block; stages = depth of the Z ring (0 = the most that fit, else at most that);
  * order = the CTA-pair kernel's MMA order (0: per K step re+=ReA.ReZ, re-=ImA.ImZ, im+=ImA.ReZ, im+=ReA.ImZ; 1: per K
  * step grouped by A half; 2: per Z chunk all real-part MMAs, then all imaginary-part ones; 3: per Z chunk one product
- * at a time). Process-wide, guarded by a mutex; a shape without an entry uses pair 1, stages 0, order 0. Every entry
- * gives the same V and I. */
+ * at a time). Forms 4 and 5 are the stacked drop-in kernels (gwb_fused_peaks_f16, gwb_fused_peaks_bf16x3; kh = K;
+ * only stages applies). Process-wide, guarded by a mutex; a shape without an entry uses pair 1, stages 0, order 0.
+ * Every entry gives the same V and I. */
 GWB_API int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order);
 GWB_API int gwb_gemm_clear_configs(void);
 GWB_API int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
@@ -356,6 +357,16 @@ GWB_API int gwb_select_top(const GwbCand* cands, const GwbGroup* groups, const G
                            int cand_cap, int nseg, int top_n, float top_frac, float rthr, GwbCand* cands_out,
                            GwbGroup* groups_out, GwbUnit* units_out, int32_t* counters_out, GwbCand* rebuilt,
                            int rebuilt_cap, void* work, long long work_bytes, void* stream);
+/* Local search of a screening form (no reference counterpart; the fp8 screen's argmax is only near the window's
+ * peak): every candidate of the selection's lists (cands, units, counters as gwb_select_windows writes them) becomes
+ * 2 radius + 1 consecutive exact-stage candidates in cands_out / groups_out / units_out / counters_out at the samples
+ * s - radius .. s + radius, clamped into its cluster window [a0 + window cw, a0 + (window + 1) cw); counters[4]
+ * (rebuilt peaks) passes through. After gwb_exact_finalize on those lists, gwb_search_best keeps in each run of
+ * 2 radius + 1 peaks the one with the largest snr (first on ties) and sets the others' snr to -1. radius 1..8. */
+GWB_API int gwb_search_expand(const GwbCand* cands, const GwbUnit* units, const int32_t* counters, int radius,
+                              long long a0, int cw, GwbCand* cands_out, int cand_cap, GwbGroup* groups_out,
+                              GwbUnit* units_out, int32_t* counters_out, void* stream);
+GWB_API int gwb_search_best(const int32_t* ccount, int cmax, int radius, GwbPeak* peaks, void* stream);
 /* Chi-squared bin edges per unit (multi_filter.edges_per_template, pipeline/multi_filter.py:264-282; the fused
  * kernel of chisq_edges.py:92-143): E[u, 0..B] int32, B >= max nbins. Unit count = min(*ucount, umax) when ucount is
  * not NULL, else umax. nbins and kmax are indexed by the unit's row. offset_mode 1 reproduces the reference's
@@ -385,6 +396,10 @@ GWB_API int gwb_bin_sums_ordered(const GwbGroup* groups, const int32_t* gcount, 
 GWB_API int gwb_exact_chunks(int flen, int kmin);
 /* Per candidate: z, pw from the slots (float64 sums), and with sig given (float64, sig[row * ldsig + seg]) snr,
  * chisq, dof, newsnr (fp_filter.py:837-853, coinc_rank.py:39-46); fpeak (exact_stage.py:236-238). */
+/* Process-wide choice of gwb_bin_sums_ordered's loads (the TMA-staged chi-squared tiles; no reference counterpart):
+ * bulk 1 stages every tile of 2048 bins of the template and data bands in shared memory with cp.async.bulk copies
+ * (double-buffered, bounded waits) instead of loading them straight from L2; the slots are bit for bit the same. */
+GWB_API int gwb_exact_set_staging(int bulk);
 GWB_API int gwb_exact_finalize(const GwbCand* cands, const int32_t* ccount, int cmax, const GwbUnit* units,
                                const int32_t* E, int B, const int32_t* nbins, int kmin, int flen, const float* slots,
                                const double* sig, long long ldsig, double df, GwbPeak* out, void* stream);

@@ -430,7 +430,7 @@ def _stats(x):
     return dict(n=int(x.size), max=float(x.max()), median=float(np.median(x)), p99=float(np.percentile(x, 99)))
 
 
-def precision_c2(B, cond, x, isw, forms, g, seg=0, n_chisq=256, seed=0):
+def precision_c2(B, cond, x, isw, forms, form_config, g, seg=0, n_chisq=256, seed=0):
     """Precision of each form against float64 over every tile of one segment (seg) of a C2 step:
     windows: the window maxima of the rebuilt SNR from the form's fused GEMM against the float64 series' (all tiles);
     kept: the peaks kept after the form's exact stage (one step of every tile against seg) against the float64
@@ -438,7 +438,7 @@ def precision_c2(B, cond, x, isw, forms, g, seg=0, n_chisq=256, seed=0):
       relative SNR error at the common windows, and relative chi-squared error against the float64 exact stage at
       the float64 argmax for up to n_chisq sampled common windows (the loudest 32 always among them), and at the
       form's own sample (the exact stage's own error).
-    g: dict(df, tlen, a0, an (analysed span), cw, thr)."""
+    form_config(form): the FilterConfig of a form. g: dict(df, tlen, a0, an (analysed span), cw, thr)."""
     from gwb200 import pipeline
     Dd, IPd = cond(x)
     rep = dict(segment=seg, tiles=len(B.tiles), reference='float64 transform, product and exact stage (torch '
@@ -461,7 +461,7 @@ def precision_c2(B, cond, x, isw, forms, g, seg=0, n_chisq=256, seed=0):
     nbins = np.full(B.M, B.cfg.nbins)
     rng = np.random.default_rng(seed)
     for form in forms:
-        cfg = pipeline.FilterConfig(form=form)
+        cfg = form_config(form)
         mf = pipeline.MatchedFilter(B, g['tlen'], g['a0'], g['an'], cfg)
         # window maxima of every tile
         vf, if_ = [], []

@@ -196,3 +196,37 @@ def test_exact_stage_order_is_bitwise_neutral():
     for c, p in zip(b['cands'], b['peaks']):
         q = ka[(c['row'], c['seg'], c['sample'])]
         assert p.tobytes() == q.tobytes()
+
+
+def test_fp8_screen_with_local_search_keeps_the_fp32_peaks():
+    """The fp8 screen followed by the exact stage at the 5 samples around each screened argmax (screen_search = 2,
+    gwb_search_expand / gwb_search_best): the same kept windows as the plain fp32 form away from the threshold, and
+    where both forms evaluate the same sample the same exact SNR (the exact stage does not depend on the form)."""
+    from gwb200 import fp_filter, pipeline
+    bank, D, IP, kmin, inj = _case()
+    Dd, IPd = torch.from_numpy(D).cuda(), torch.from_numpy(IP).cuda()
+    sw, isw = fp_filter.derive_sw(IPd)
+    out = {}
+    for form, search in (('f32', 0), ('fp8', 2)):
+        cfg = pipeline.FilterConfig(tile=24, eps=1e-3, nbins=16, snr_threshold=5.0, margin=0.04, form=form,
+                                    cand_cap=1 << 16, screen_search=search)
+        B = pipeline.Bank(bank, FLEN, DF, sw, cfg)
+        mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg)
+        mf.step(Dd, IPd, isw)
+        torch.cuda.synchronize()
+        res = mf.results()
+        c, p = res['cands'][res['keep']], res['peaks'][res['keep']]
+        out[form] = {(int(a['row']), int(a['seg']), int(a['window'])): (float(b['snr']), int(a['sample']))
+                     for a, b in zip(c, p)}
+        if search:
+            # one kept peak per window at most; every run of 5 has exactly one best
+            assert len(out[form]) == int(res['keep'].sum())
+    thr = 5.0
+    for a, b in (('f32', 'fp8'), ('fp8', 'f32')):
+        for k, (v, smp) in out[a].items():
+            if v > 1.03 * thr:
+                assert k in out[b], (a, b, k, v)
+                if out[b][k][1] == smp:
+                    assert abs(out[b][k][0] - v) <= 1e-5 * v, (k, v, out[b][k])
+                else:
+                    assert abs(out[b][k][0] - v) <= 2e-2 * v, (k, v, out[b][k])
