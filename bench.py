@@ -528,8 +528,9 @@ def run_c4(a):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
-    ns = argparse.Namespace(segments=300, batch=32, seed=4, no_graph=False, production=a.production,
-                            form=a.forms.split(',')[0])
+    # the batched form's configuration names the split-bf16 GEMM; --forms overrides it
+    form = a.forms.split(',')[0] if a.forms_given else 'bf16x3'
+    ns = argparse.Namespace(segments=300, batch=32, seed=4, no_graph=False, production=a.production, form=form)
     r = microbench.c4(ns)
     print(json.dumps(dict(metric=METRIC, value=r['value'], unit=UNIT, n_gpus=1, steps=1, warmup=1,
                           ms_per_step=r['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
@@ -568,6 +569,7 @@ def main():
     ap.add_argument('--production', action='store_true', help='c4: production selection and consolidation')
     ap.add_argument('--no-autotune', action='store_true', help='c2: default launch shapes instead of tuned ones')
     a = ap.parse_args()
+    a.forms_given = any(x == '--forms' or x.startswith('--forms=') for x in sys.argv[1:])
     if a.impl == 'reference':
         run_reference(a)
     elif a.workload == 'c2':

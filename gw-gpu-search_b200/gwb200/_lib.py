@@ -70,6 +70,7 @@ SIGNATURES = {
     'gwb_bin_sums_ordered': [_P, _P, _I, _P, _P, _P, _I, _P, _I, _P, _LL, _P, _LL, _I, _I, _LL, _P, _LL, _P, _P, _P],
     'gwb_bin_sums_work_bytes': [_I, _I],
     'gwb_exact_set_staging': [_I],
+    'gwb_append_results': [_P, _P, _P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P],
     'gwb_select_top': [_P, _P, _P, _P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _I, _P, _LL, _P],
     'gwb_select_top_work_bytes': [_I, _I],
     'gwb_search_expand': [_P, _P, _P, _I, _LL, _I, _P, _I, _P, _P, _P, _P],

@@ -204,6 +204,24 @@ def cluster_over_window(idx, vals, window):
 
 def whitened_above(strain, sr, threshold, low_freq_cutoff, corrupt_time, psd_duration=4., psd_stride=2., cap=1 << 20):
     """The device part of detect_loud_glitches: indices (sorted) and values of whitened |x| > threshold."""
+    return above_collect(*whitened_above_queue(strain, sr, threshold, low_freq_cutoff, corrupt_time, psd_duration,
+                                               psd_stride, cap))
+
+
+def above_collect(idx, val, cnt, tapered, cap):
+    """Host side of whitened_above_queue's result (synchronises on its count): sorted indices, values, tapered."""
+    c = int(cnt.item())
+    if c > cap:
+        raise _lib.GwbError('gwb_above', _lib.GWB_ERR_CAPACITY, '%d samples above threshold, capacity %d' % (c, cap))
+    ih, vh = idx[:c].cpu().numpy(), val[:c].cpu().numpy()
+    o = np.argsort(ih, kind='stable')
+    return ih[o], vh[o], tapered
+
+
+def whitened_above_queue(strain, sr, threshold, low_freq_cutoff, corrupt_time, psd_duration=4., psd_stride=2.,
+                         cap=1 << 20):
+    """whitened_above's device work, queued without a host synchronisation: returns (idx, val, cnt, tapered, cap)
+    device tensors for above_collect (so many segments can be queued before one synchronisation)."""
     s = _dev(strain, torch.float32)
     dt = 1.0 / sr
     n = s.shape[0]
@@ -228,18 +246,18 @@ def whitened_above(strain, sr, threshold, low_freq_cutoff, corrupt_time, psd_dur
     cnt = torch.zeros(1, dtype=torch.int32, device=s.device)
     _lib.call('gwb_above', _lib.ptr(wt), pad_start, n, cl, float(np.float32(df)), float(threshold), _lib.ptr(idx),
               _lib.ptr(val), cap, _lib.ptr(cnt), _s())
-    c = int(cnt.item())
-    if c > cap:
-        raise _lib.GwbError('gwb_above', _lib.GWB_ERR_CAPACITY, '%d samples above threshold, capacity %d' % (c, cap))
-    ih, vh = idx[:c].cpu().numpy(), val[:c].cpu().numpy()
-    o = np.argsort(ih, kind='stable')
-    return ih[o], vh[o], tapered
+    return idx, val, cnt, tapered, cap
 
 
 def detect_loud_glitches(xp, strain, sr, start_gps, threshold, cluster_window, low_freq_cutoff, corrupt_time,
                          psd_duration=4., psd_stride=2.):
     """pycbc.strain.detect_loud_glitches (gpu_prep.py:175-209). Returns GPS times (integer nanoseconds)."""
     ind, v, _ = whitened_above(strain, sr, threshold, low_freq_cutoff, corrupt_time, psd_duration, psd_stride)
+    return glitch_times(ind, v, sr, start_gps, cluster_window)
+
+
+def glitch_times(ind, v, sr, start_gps, cluster_window):
+    """The host end of detect_loud_glitches (gpu_prep.py:199-209): clustering over the window, GPS times."""
     keep = cluster_over_window(ind.astype(np.int32), v, int(cluster_window * sr))
     t0 = GPS(start_gps)
     r = int(sr)

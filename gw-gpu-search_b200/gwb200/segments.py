@@ -20,7 +20,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from . import consolidate as cons_, gpu_prep, pipeline
+from . import _exact, _lib, consolidate as cons_, gpu_prep, pipeline
 
 
 @dataclass
@@ -106,6 +106,97 @@ class SegmentFilter:
             if not gt:
                 break
         return [(float(t), w, tp) for t, w, tp in gates]
+
+    def gate_all(self, segments, cap=1 << 16):
+        """gate() for every segment with one host synchronisation per gating iteration for all of them: the whitening
+        and thresholding of every segment are queued first, then the counts are read once and the clustering (host,
+        as the reference's) and the gates follow. Same gates as gate() per segment."""
+        g = self.gating
+        gates = [[] for _ in segments]
+        todo = list(range(len(segments)))
+        for _ in range(g.max_iterations):
+            if not todo:
+                break
+            queued = [gpu_prep.whitened_above_queue(segments[i]['x'], self.sr, g.threshold, g.f_low, g.pad, cap=cap)
+                      for i in todo]
+            nxt = []
+            for i, q in zip(todo, queued):
+                ind, v, _ = gpu_prep.above_collect(*q)
+                gt = gpu_prep.glitch_times(ind, v, self.sr, segments[i]['start_gps'], g.cluster)
+                gp = [(t, g.width, g.taper) for t in gt]
+                gates[i] += gp
+                gpu_prep.gate_taper(torch, segments[i]['x'], self.sr, segments[i]['start_gps'], gp)
+                if gt:
+                    nxt.append(i)
+            todo = nxt
+        return [[(float(t), w, tp) for t, w, tp in gs] for gs in gates]
+
+    def prepare(self, segments, arena_cap=1 << 23):
+        """Captures the whole run over these segments as one CUDA graph: for every batch of chunks the copies of the
+        chunks into the batch buffer, the conditioning and filter step, and the append of the batch's exact-stage
+        results to a run-wide list on the device (gwb_append_results). The graph reads the segments' strain where it
+        is, so gating them in place afterwards (run_graph) changes nothing in it. Returns the capture's seconds."""
+        import time
+        t0 = time.perf_counter()
+        chunks, skipped = self.plan(segments)
+        nb = -(-len(chunks) // self.batch)
+        dev = self.device
+        mf = self.mf
+        cap = mf.slot_cap
+        self.arena = dict(cands=torch.empty(arena_cap * 32, dtype=torch.uint8, device=dev),
+                          peaks=torch.empty(arena_cap * 32, dtype=torch.uint8, device=dev),
+                          tag=torch.empty(arena_cap, dtype=torch.int32, device=dev),
+                          count=torch.zeros(1, dtype=torch.int32, device=dev),
+                          work=torch.zeros(2, dtype=torch.int32, device=dev),
+                          meta=torch.zeros((max(nb, 1), 8), dtype=torch.int32, device=dev), cap=arena_cap)
+        A = self.arena
+        self._step()                           # warm-up: plans, workspaces and cached tables outside the capture
+        torch.cuda.synchronize()
+        self.run_graph_ = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.run_graph_):
+            for b in range(nb):
+                part = chunks[b * self.batch:(b + 1) * self.batch]
+                for r in range(self.batch):
+                    i, (s0, s1), _ = part[min(r, len(part) - 1)]   # unused rows repeat a real chunk (dropped later)
+                    self.X[r].copy_(segments[i]['x'][s0:s1])
+                self._step()
+                _lib.call('gwb_append_results', _lib.ptr(mf.cands), _lib.ptr(mf.peaks), _lib.ptr(mf.counters), cap,
+                          b, _lib.ptr(A['cands']), _lib.ptr(A['peaks']), _lib.ptr(A['tag']), _lib.ptr(A['count']),
+                          arena_cap, _lib.ptr(A['work']), _lib.ptr(A['meta']), _lib.stream_ptr())
+        torch.cuda.synchronize()
+        self.prepared = dict(chunks=chunks, skipped=skipped, nb=nb, segments=segments)
+        return time.perf_counter() - t0
+
+    def run_graph(self, gate=True):
+        """The prepared run: gating of every segment (gate_all), one replay of the run's graph, one copy of the
+        run-wide result list to the host. Returns run()'s dict (without consolidation)."""
+        P = self.prepared
+        segments, chunks = P['segments'], P['chunks']
+        gates = self.gate_all(segments) if gate else [[] for _ in segments]
+        A = self.arena
+        A['count'].zero_()
+        self.run_graph_.replay()
+        torch.cuda.synchronize()
+        meta = A['meta'].cpu().numpy()
+        if np.any(meta[:P['nb'], 3]) or np.any(meta[:P['nb'], 7]):
+            raise _lib.GwbError('run_graph', _lib.GWB_ERR_CAPACITY, 'a candidate list or the run list overflowed')
+        n = int(A['count'].item())
+        c = _exact.from_dev(A['cands'], _exact.CAND, n)
+        p = _exact.from_dev(A['peaks'], _exact.PEAK, n)
+        tag = A['tag'][:n].cpu().numpy().astype(np.int64)
+        row = tag * self.batch + c['seg'].astype(np.int64)       # the chunk of each candidate
+        ok = (c['seg'] < self.batch) & (row < len(chunks))
+        rowc = np.minimum(row, len(chunks) - 1)
+        a_lo = np.array([an[0] for _, _, an in chunks])[rowc]
+        a_hi = np.array([an[1] for _, _, an in chunks])[rowc]
+        ok &= (c['sample'] >= a_lo) & (c['sample'] < a_hi)
+        c, p, rowc = c[ok], p[ok], rowc[ok]
+        keep = p['snr'] > self.cfg.snr_threshold
+        analysed = sum(an[1] - an[0] for _, _, an in chunks) / self.sr
+        skipped_s = sum(segments[i]['x'].shape[0] for i in P['skipped']) / self.sr
+        return dict(cands=c, peaks=p, keep=keep, segment=np.array([chunks[r][0] for r in rowc], np.int64),
+                    chunk=rowc, gates=gates, analysed_s=analysed, skipped_s=skipped_s, skipped=P['skipped'],
+                    n_chunks=len(chunks), batches=P['nb'], plan=chunks, graph_launches=1)
 
     def plan(self, segments):
         """Chunks of every segment: list of (segment index, (s0, s1) samples, (a0, a1) analysed samples in the chunk),

@@ -396,6 +396,15 @@ GWB_API int gwb_bin_sums_ordered(const GwbGroup* groups, const int32_t* gcount, 
 GWB_API int gwb_exact_chunks(int flen, int kmin);
 /* Per candidate: z, pw from the slots (float64 sums), and with sig given (float64, sig[row * ldsig + seg]) snr,
  * chisq, dof, newsnr (fp_filter.py:837-853, coinc_rank.py:39-46); fpeak (exact_stage.py:236-238). */
+/* Appends one step's exact-stage results to a run-wide list on the device (no reference counterpart: the reference
+ * copies peaks to the host per (tile, segment), fp_filter.py:752-753): n = min(counters[0], cap) candidates and their
+ * peaks go to out_cands / out_peaks at the next free place of out_count (at most out_cap in all), each tagged `tag` in
+ * out_tag; meta[tag * 8 + 0..7] records the step's five counters, the first place, the number appended and 1 when the
+ * run list overflowed. work: 2 int32 of scratch. Sizes are read on the device: many steps can be queued (or captured
+ * in one graph) and copied to the host once. */
+GWB_API int gwb_append_results(const GwbCand* cands, const GwbPeak* peaks, const int32_t* counters, int cap, int tag,
+                               GwbCand* out_cands, GwbPeak* out_peaks, int32_t* out_tag, int32_t* out_count,
+                               int out_cap, int32_t* work, int32_t* meta, void* stream);
 /* Process-wide choice of gwb_bin_sums_ordered's loads (the TMA-staged chi-squared tiles; no reference counterpart):
  * bulk 1 stages every tile of 2048 bins of the template and data bands in shared memory with cp.async.bulk copies
  * (double-buffered, bounded waits) instead of loading them straight from L2; the slots are bit for bit the same. */

@@ -108,3 +108,37 @@ def test_filter_segments_consolidated_tables():
     t0 = r['tables'][0]
     near = np.abs(t0['end_time'] - (1000000000 + 150.0)) < 0.1
     assert near.any() and abs(t0['snr'][near].max() - 15.0) < 3.0
+
+
+def test_whole_run_graph_matches_the_direct_run():
+    """The whole run captured as one graph (SegmentFilter.prepare, then run_graph: batched gating, one replay, one
+    copy of the run-wide result list) gives the same gates and the same peaks as the direct batch-by-batch run."""
+    from gwb200 import fp_filter, gpu_prep, pipeline, segments
+    rng = np.random.default_rng(11)
+    bank = synth.random_bank_c1(48, 3)
+    segs = [dict(x=_segment(300, rng, bank, inj=(7, 150.0, 15.0)), start_gps=1000000000, det=0),
+            dict(x=_segment(200, rng, glitch=(100.0, 120.0, 200.0)), start_gps=1000001000, det=1),
+            dict(x=_segment(100, rng), start_gps=1000002000, det=0),
+            dict(x=_segment(420, rng), start_gps=1000003000, det=1)]
+    cond = gpu_prep.BatchConditioner(4, TLEN, SR, 20.0, 16.0, 8.0, 15, 16.0)
+    _, IP = cond(torch.stack([segs[0]['x'][:TLEN]] * 4).contiguous())
+    sw, isw = fp_filter.derive_sw(IP)
+    cfg = pipeline.FilterConfig(tile=24, form='f16', snr_threshold=5.5, cand_cap=1 << 16)
+    B = pipeline.Bank(bank, FLEN, DF, sw.clone(), cfg)
+    out = {}
+    for mode in ('direct', 'graph'):
+        sg = [dict(s, x=s['x'].clone()) for s in segs]
+        F = segments.SegmentFilter(B, cfg, seg_len=L, start_pad=SP, end_pad=EP, batch=4, psd=(16.0, 8.0, 15, 16.0),
+                                   isw=isw.clone(), graph=False)
+        if mode == 'graph':
+            F.prepare(sg)
+            out[mode] = F.run_graph()
+            assert out[mode]['graph_launches'] == 1 and out[mode]['batches'] >= 2
+        else:
+            out[mode] = F.run(sg)
+    a, b = out['direct'], out['graph']
+    assert a['gates'] == b['gates'] and a['skipped'] == b['skipped'] and a['analysed_s'] == b['analysed_s']
+    key = lambda x: sorted(zip(x['segment'].tolist(), x['chunk'].tolist(), x['cands']['row'].tolist(),
+                               x['cands']['sample'].tolist(), np.round(x['peaks']['snr'], 4).tolist()))
+    assert key(a) == key(b)
+    assert np.array_equal(np.sort(a['keep']), np.sort(b['keep']))
