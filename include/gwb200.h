@@ -394,8 +394,6 @@ GWB_API int gwb_bin_sums_ordered(const GwbGroup* groups, const int32_t* gcount, 
                                  void* stream);
 /* Number of band chunks the slots are laid out for. */
 GWB_API int gwb_exact_chunks(int flen, int kmin);
-/* Per candidate: z, pw from the slots (float64 sums), and with sig given (float64, sig[row * ldsig + seg]) snr,
- * chisq, dof, newsnr (fp_filter.py:837-853, coinc_rank.py:39-46); fpeak (exact_stage.py:236-238). */
 /* Appends one step's exact-stage results to a run-wide list on the device (no reference counterpart: the reference
  * copies peaks to the host per (tile, segment), fp_filter.py:752-753): n = min(counters[0], cap) candidates and their
  * peaks go to out_cands / out_peaks at the next free place of out_count (at most out_cap in all), each tagged `tag` in
@@ -409,9 +407,45 @@ GWB_API int gwb_append_results(const GwbCand* cands, const GwbPeak* peaks, const
  * bulk 1 stages every tile of 2048 bins of the template and data bands in shared memory with cp.async.bulk copies
  * (double-buffered, bounded waits) instead of loading them straight from L2; the slots are bit for bit the same. */
 GWB_API int gwb_exact_set_staging(int bulk);
+/* Per candidate: z, pw from the slots (float64 sums), and with sig given (float64, sig[row * ldsig + seg]) snr,
+ * chisq, dof, newsnr (fp_filter.py:837-853, coinc_rank.py:39-46); fpeak (exact_stage.py:236-238). */
 GWB_API int gwb_exact_finalize(const GwbCand* cands, const int32_t* ccount, int cmax, const GwbUnit* units,
                                const int32_t* E, int B, const int32_t* nbins, int kmin, int flen, const float* slots,
                                const double* sig, long long ldsig, double df, GwbPeak* out, void* stream);
+
+/* ---- the whole filter step ---------------------------------------------------------------------------------- */
+/* One tile of the bank as the step reads it (made once per bank: the SVD, fp_filter.py:576-593, and
+ * gwb_fourstep_order of its basis filters). */
+typedef struct {
+    const float* Vp;     /* (r, ldvp) complex: basis filters in four-step order (ldvp even, rows 16-byte aligned) */
+    long long ldvp;
+    const float* A;      /* (n, r) complex64 mixing matrix, row stride lda (complex elements) */
+    long long lda;
+    int r, n, row0;      /* rank, templates, first row of the tile in the bank arrays */
+} GwbTile;
+typedef struct {
+    int form;            /* GEMM precision: 0 fp16, 1 bf16, 2 split bf16 */
+    int cw;              /* cluster window in samples, a multiple of 128 */
+    long long a0, Tn;    /* analysed span of each segment: samples [a0, a0 + Tn) (Tn cut to whole windows) */
+    float snr_threshold; /* exact-stage threshold; windows above (thr (1 - margin))^2 are candidates */
+    float margin;
+    int nbins_max;       /* B: the largest chi-squared bin count of the bank */
+    int cand_cap;        /* capacity of the candidate, group and unit lists */
+} GwbStepConfig;
+/* One step of the compressed filter over a batch of conditioned segments (the loop of fp_filter.py:700-888, run_group
+ * :741-836, with every candidate sent to the exact stage): template norms sig (M x nseg, float64, out), D isw in
+ * four-step order, then for every tile and segment the fused basis series (the ring form for tlen = 2^20), stacked A,
+ * the fused GEMM with |z|^2 and windowed argmax, the window selection; then edges, binned sums in template-row order
+ * and the finalisation into cands / peaks (cand_cap each) with counters[0..4] as gwb_select_windows (counters[3] = 1:
+ * a list overflowed). H (M x ldh complex), kmax and nbins per bank row; D, IP (nseg rows); isw = 1 / sw of the SVD
+ * metric. work: gwb_filter_step_work_bytes(...) bytes; nothing is allocated and nothing is copied to the host. */
+GWB_API long long gwb_filter_step_work_bytes(const GwbTile* tiles, int ntiles, int M, int nseg, long long tlen,
+                                             int flen, int kmin, const GwbStepConfig* cfg);
+GWB_API int gwb_filter_step(const GwbTile* tiles, int ntiles, const float* H, long long ldh, int M,
+                            const int32_t* kmax, const int32_t* nbins, int kmin, double df, const float* D,
+                            const float* IP, long long ldd, long long ldip, int nseg, const float* isw, long long tlen,
+                            int flen, const GwbStepConfig* cfg, void* work, long long work_bytes, GwbCand* cands,
+                            GwbPeak* peaks, int32_t* counters, double* sig, void* stream);
 
 /* ---- consolidation (downstream of the exact stage) -------------------------------------------------------- */
 /* Workspace bytes of gwb_consolidate for n items and nwin keep-loudest windows. */

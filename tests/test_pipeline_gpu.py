@@ -230,3 +230,28 @@ def test_fp8_screen_with_local_search_keeps_the_fp32_peaks():
                     assert abs(out[b][k][0] - v) <= 1e-5 * v, (k, v, out[b][k])
                 else:
                     assert abs(out[b][k][0] - v) <= 2e-2 * v, (k, v, out[b][k])
+
+
+@pytest.mark.parametrize('form', ['f16', 'bf16x3'])
+def test_c_filter_step_matches_the_python_step(form):
+    """The whole step through the one C entry gwb_filter_step (gwb200.cstep) gives the same candidates and exact
+    values as MatchedFilter.step, which calls the same kernels one by one from Python."""
+    from gwb200 import cstep, fp_filter, pipeline
+    bank, D, IP, kmin, inj = _case()
+    Dd, IPd = torch.from_numpy(D).cuda(), torch.from_numpy(IP).cuda()
+    sw, isw = fp_filter.derive_sw(IPd)
+    cfg = pipeline.FilterConfig(tile=24, form=form, snr_threshold=5.0, cand_cap=1 << 16)
+    B = pipeline.Bank(bank, FLEN, DF, sw, cfg)
+    mf = pipeline.MatchedFilter(B, TLEN, A0, A1 - A0, cfg)
+    sig_py = mf.step(Dd, IPd, isw)
+    torch.cuda.synchronize()
+    r_py = mf.results()
+    cs = cstep.CStep(B, TLEN, A0, A1 - A0, 2, cfg)
+    sig_c = cs.step(Dd, IPd, isw)
+    torch.cuda.synchronize()
+    r_c = cs.results()
+    assert torch.equal(sig_py, sig_c)
+    key = lambda r: {(int(c['row']), int(c['seg']), int(c['window'])): (int(c['sample']), p.tobytes())
+                     for c, p in zip(r['cands'], r['peaks'])}
+    assert r_c['n_candidates'] == r_py['n_candidates'] > 0
+    assert key(r_c) == key(r_py)
