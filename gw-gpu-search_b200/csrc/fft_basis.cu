@@ -20,6 +20,7 @@
 // outputs. The scale only normalises Z for its 16-bit range: A is multiplied by the same scale, so the SNR is
 // unchanged (fp_filter.py:617).
 #include "common.cuh"
+#include <atomic>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
@@ -594,13 +595,13 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
 
 // ---------------------------------------------------------------------------------------------------------------------
 // Persistent form of the two passes for N = 2^20 (N1 = N2 = 1024): W stays in L2.
-// Rows go in chunks of PC rows through a ring of PSLOT slots of W (PC rows of N each, 48 MB). Work items, taken in
-// order from a global ticket by a grid of resident CTAs:
+// Rows go in chunks of pc rows through a ring of nslot slots of W (pc rows of N each). Work items, taken in order from
+// a global ticket by a grid of resident CTAs:
 //   P1(c, g): pass 1 of chunk c for the 8 columns k2 = 8 g .. 8 g + 7 (one basis_pass1_w CTA's work);
 //   P2(c, b): pass 2 of chunk c for the 8 columns t1 = 8 b .. 8 b + 7 (one basis_pass2_p CTA's work).
-// Ticket order: P1(0, *), then for c = 0, 1, ...: P1(c + 1, *), P2(c, *). P2(c, *) starts when the 128 items P1(c, *)
-// (and P1(0, *), for the scale) are done; P1(c, *) starts when the 128 items P2(c - PSLOT, *) are done (its slot is
-// free). Every item waits only on items earlier in the ticket order, all held by running CTAs, so the earliest
+// Ticket order with lookahead L: P1(0 .. L-1, *), then for c = 0, 1, ...: P1(c + L, *), P2(c, *). P2(c, *) starts when
+// the 128 items P1(c, *) (and P1(0, *), for the scale) are done; P1(c, *) starts when the 128 items P2(c - nslot, *)
+// are done (its slot is free; nslot > L, so those come earlier). Every item waits only on items earlier in the ticket order, all held by running CTAs, so the earliest
 // unfinished item always progresses. Every wait is bounded (kWaitLimitNs): a timeout records GWB_ERR_TIMEOUT, raises
 // the abort word, and every CTA returns at its next ticket with no copy in flight.
 // After pass 2 has copied a W tile into shared memory its L2 lines are dropped without write-back (discard.global.L2),
@@ -609,7 +610,8 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
 // series have comparable rms; the scale cancels between Z and A); each P2 item sums the first chunk's per-column
 // partials in a fixed order. fp8: each P2 item sums its rows' per-column |q|^2 in a fixed order for the row scales.
 // ---------------------------------------------------------------------------------------------------------------------
-constexpr int PC = 2, PSLOT = 3, PG = 128;    // rows per chunk, W slots, items per chunk and pass (1024 / 8)
+constexpr int PG = 128;                       // items per chunk and pass (1024 / 8)
+constexpr int PC_MAX = 4;                     // rows per chunk at most (the fp8 row scales take one warp per row)
 
 struct PersistArgs {
     const float2* Vp;
@@ -617,7 +619,8 @@ struct PersistArgs {
     int rows;
     const float2* Dp;
     const float2* tw;
-    float2* W;                // PSLOT * PC rows of N
+    float2* W;                // nslot * pc rows of N
+    int pc, nslot, look;      // rows per chunk, W slots, lookahead (chunks of pass 1 ahead of pass 2)
     int a0, Tn;
     void* Z;
     void* Zlo;
@@ -652,26 +655,29 @@ __device__ bool wait_count(const int* p, int target, const int* abort_word) {
 }
 
 // item t of the ticket order: type 1 = P1, 2 = P2; false past the end
-__device__ __forceinline__ bool persist_item(int t, int nch, int& type, int& c, int& g) {
-    if (t < PG) {
+__device__ __forceinline__ bool persist_item(int t, int nch, int look, int& type, int& c, int& g) {
+    const int pre = min(look, nch);                      // P1 of the first chunks
+    if (t < pre * PG) {
         type = 1;
-        c = 0;
-        g = t;
-        return nch > 0;
+        c = t / PG;
+        g = t % PG;
+        return true;
     }
-    t -= PG;
-    const int j = t / (2 * PG), o = t % (2 * PG);
-    if (j >= nch) return false;
-    if (j + 1 < nch) {
+    t -= pre * PG;
+    const int full = max(0, nch - look);                 // blocks P1(c + look, *), P2(c, *)
+    if (t < full * 2 * PG) {
+        const int j = t / (2 * PG), o = t % (2 * PG);
         type = o < PG ? 1 : 2;
-        c = o < PG ? j + 1 : j;
+        c = o < PG ? j + look : j;
         g = o < PG ? o : o - PG;
         return true;
     }
-    if (o >= PG) return false;
+    t -= full * 2 * PG;
+    const int j = full + t / PG;                         // the last chunks: P2 only
+    if (j >= nch) return false;
     type = 2;
     c = j;
-    g = o;
+    g = t % PG;
     return true;
 }
 
@@ -685,9 +691,9 @@ __device__ __forceinline__ void persist_p1(float2* sm, const PersistArgs& a, int
     float2* THw = Yw + YS;
     float2* Vs = THw + R;
     const int k2 = g * NW + warp;
-    const int j0 = c * PC, j1 = min(j0 + PC, a.rows);
+    const int j0 = c * a.pc, j1 = min(j0 + a.pc, a.rows);
     constexpr int mask = N - 1;
-    float2* Wslot = a.W + (long long)(c % PSLOT) * PC * N;
+    float2* Wslot = a.W + (long long)(c % a.nslot) * a.pc * N;
     auto fetch = [&](int j) {
         const char* gp = reinterpret_cast<const char*>(a.Vp + (long long)j * a.ldvp + k2 * H);
         char* d = reinterpret_cast<char*>(Vs);
@@ -781,8 +787,8 @@ __device__ __forceinline__ void persist_p2(float2* sm, const PersistArgs& a, int
     const float2* tw2 = sm;                                 // e^{2 pi i b u / N2}: the same table as pass 1's
     float2* Bt = sm + N1;
     const int tid = threadIdx.x, t10 = b * TB;
-    const int j0 = c * PC, j1 = min(j0 + PC, a.rows);
-    const float2* Wslot = a.W + (long long)(c % PSLOT) * PC * N;
+    const int j0 = c * a.pc, j1 = min(j0 + a.pc, a.rows);
+    const float2* Wslot = a.W + (long long)(c % a.nslot) * a.pc * N;
     auto tile = [&](int j) { return Wslot + (long long)(j - j0) * N + (long long)b * (N2 * TB); };
     auto fetch = [&](int j) {
         const char* gp = reinterpret_cast<const char*>(tile(j));
@@ -796,14 +802,14 @@ __device__ __forceinline__ void persist_p2(float2* sm, const PersistArgs& a, int
     const int warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
         const double s = warp_fixed_sum(a.partials, N2);
-        const int nf = min(PC, a.rows);
+        const int nf = min(a.pc, a.rows);
         const float sc = (float)sqrt(s / (double)nf / 2.0);
         if (lane == 0) {
             s_inv[0] = 1.0f / sc;
             if (c == 0 && b == 0) *a.scale_out = sc;
         }
     }
-    if (FORM == 4 && warp >= 1 && warp <= PC && j0 + warp - 1 < j1) {
+    if (FORM == 4 && warp >= 1 && warp <= a.pc && j0 + warp - 1 < j1) {
         const int j = j0 + warp - 1;
         const double t = warp_fixed_sum(a.rowpart + (long long)j * N2, N2);
         const float rs = t > 0.0 ? (float)(sqrt(t / 2.0) / 16.0) : 1.f;
@@ -874,10 +880,10 @@ __global__ void __launch_bounds__(256, 2) basis_persist(const __grid_constant__ 
     constexpr int N1 = 1024, N = 1 << 20;
     extern __shared__ float2 sm[];
     __shared__ int s_t, s_ok;
-    __shared__ float s_inv[1 + PC];
+    __shared__ float s_inv[1 + PC_MAX];
     for (int e = threadIdx.x; e < N1; e += blockDim.x) sm[e] = a.tw[(e % 32) * (e / 32) * (N / N1)];
     __syncthreads();
-    const int nch = (a.rows + PC - 1) / PC;
+    const int nch = (a.rows + a.pc - 1) / a.pc;
     int* ticket = a.sync;
     int* abort_word = a.sync + 1;
     int* p1done = a.sync + 2;
@@ -886,10 +892,10 @@ __global__ void __launch_bounds__(256, 2) basis_persist(const __grid_constant__ 
         if (threadIdx.x == 0) s_t = *(volatile int*)abort_word ? 0x7fffffff : atomicAdd(ticket, 1);
         __syncthreads();
         int type = 0, c = 0, g = 0;
-        if (!persist_item(s_t, nch, type, c, g)) break;     // uniform over the CTA
+        if (!persist_item(s_t, nch, a.look, type, c, g)) break;   // uniform over the CTA
         if (threadIdx.x == 0) {
             bool ok = true;
-            if (type == 1 && c >= PSLOT) ok = wait_count(&p2done[c - PSLOT], PG, abort_word);
+            if (type == 1 && c >= a.nslot) ok = wait_count(&p2done[c - a.nslot], PG, abort_word);
             if (type == 2) ok = wait_count(&p1done[0], PG, abort_word) && wait_count(&p1done[c], PG, abort_word);
             if (!ok) {
                 record_error(a.err, GWB_ERR_TIMEOUT, 301, type, c);
@@ -922,7 +928,7 @@ int launch_persist(const PersistArgs& a, cudaStream_t s) {
     int per_sm = 0;
     GWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
     GWB_CHECK_ARG(per_sm >= 1, GWB_ERR_CUDA, "basis_persist: no CTA fits on an SM");
-    const int nch = (a.rows + PC - 1) / PC;
+    const int nch = (a.rows + a.pc - 1) / a.pc;
     const int grid = std::min(per_sm * num_sms(), 2 * PG * nch);
     k<<<grid, 256, smem, s>>>(a);
     GWB_LAUNCH_CHECK("basis_persist");
@@ -1031,12 +1037,33 @@ int gwb_fourstep_order(const float* X, long long ldx, int rows, const float* isw
     return GWB_OK;
 }
 
-int gwb_basis_ring_rows(void) { return gwb::PSLOT * gwb::PC; }
+namespace gwb {
+namespace {
+// the ring's configuration (gwb_basis_ring_set_config), process-wide: rows per chunk, W slots, lookahead
+std::atomic<int> g_ring_pc{2}, g_ring_nslot{3}, g_ring_look{1};
+}  // namespace
+}  // namespace gwb
 
-int gwb_basis_ring_sync_ints(int rows) { return 2 + 2 * ((rows + gwb::PC - 1) / gwb::PC); }
+int gwb_basis_ring_set_config(int pc, int nslot, int look) {
+    using namespace gwb;
+    GWB_CHECK_ARG(pc >= 1 && pc <= PC_MAX && look >= 1 && nslot > look && nslot <= 16, GWB_ERR_ARG,
+                  "basis_ring_set_config: pc=%d (1..%d) nslot=%d (> look, <= 16) look=%d (>= 1)", pc, PC_MAX, nslot,
+                  look);
+    g_ring_pc.store(pc);
+    g_ring_nslot.store(nslot);
+    g_ring_look.store(look);
+    return GWB_OK;
+}
+
+int gwb_basis_ring_rows(void) { return gwb::g_ring_pc.load() * gwb::g_ring_nslot.load(); }
+
+int gwb_basis_ring_sync_ints(int rows) {
+    const int pc = gwb::g_ring_pc.load();
+    return 2 + 2 * ((rows + pc - 1) / pc);
+}
 
 int gwb_basis_fused_ring(const float* Vp, long long ldvp, int rows, const float* Dp, long long N, const float* tw,
-                         float* W, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz, int im_off,
+                         float* W, int wrows, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz, int im_off,
                          int row0, double* partials, long long npartials, float* scale, float* rowscale,
                          float* rowpart, long long rowpart_elems, int32_t* sync, long long sync_ints, void* stream) {
     using namespace gwb;
@@ -1052,9 +1079,15 @@ int gwb_basis_fused_ring(const float* Vp, long long ldvp, int rows, const float*
                   "128-byte aligned", npartials, sync_ints, gwb_basis_ring_sync_ints(rows));
     GWB_CHECK_ARG(form != 4 || (rowscale && rowpart && rowpart_elems >= (long long)rows * 1024), GWB_ERR_SHAPE,
                   "basis_fused_ring: the fp8 form needs rowscale (rows floats) and rowpart (rows x 1024 floats)");
+    const int pc = g_ring_pc.load(), nslot = g_ring_nslot.load(), look = g_ring_look.load();
+    GWB_CHECK_ARG(wrows >= pc * nslot, GWB_ERR_SHAPE, "basis_fused_ring: W holds %d rows, the ring needs %d", wrows,
+                  pc * nslot);
     cudaStream_t s = (cudaStream_t)stream;
     GWB_CUDA(cudaMemsetAsync(sync, 0, sizeof(int32_t) * gwb_basis_ring_sync_ints(rows), s));
     PersistArgs a;
+    a.pc = pc;
+    a.nslot = nslot;
+    a.look = look;
     a.Vp = reinterpret_cast<const float2*>(Vp);
     a.ldvp = ldvp;
     a.rows = rows;

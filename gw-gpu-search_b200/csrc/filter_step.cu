@@ -75,6 +75,7 @@ struct StepWork {
     void* sort_work;
     int32_t* sort_status;
     long long gemm_bytes, sort_bytes, npartials, sync_ints;
+    int wrows;
 };
 
 long long carve(const StepShapes& s, int M, int nseg, long long tlen, int flen, int kmin, const GwbStepConfig* cfg,
@@ -85,7 +86,8 @@ long long carve(const StepShapes& s, int M, int nseg, long long tlen, int flen, 
     w->part = c.take<double>((long long)M * nseg * 16);
     w->Dp = c.take<float>(2ll * nseg * s.ldp);
     w->tw = c.take<float>(2ll * tlen);
-    w->W = c.take<float>(2ll * tlen * (s.ring ? gwb_basis_ring_rows() : s.rmax));
+    w->wrows = s.ring ? gwb_basis_ring_rows() : s.rmax;
+    w->W = c.take<float>(2ll * tlen * w->wrows);
     w->npartials = std::max(1024ll, 64ll * std::max(1ll, tlen / 64));
     w->partials = c.take<double>(w->npartials);
     w->scale = c.take<float>(1);
@@ -165,7 +167,8 @@ int gwb_filter_step(const GwbTile* tiles, int ntiles, const float* H, long long 
         for (int sg = 0; sg < nseg; ++sg) {
             const float* dp = w.Dp + 2ll * sg * s.ldp;
             if (s.ring)
-                GWB_TRY(gwb_basis_fused_ring(T.Vp, T.ldvp, T.r, dp, tlen, w.tw, w.W, cfg->a0, s.Tn, pack, w.Z, w.Zlo,
+                GWB_TRY(gwb_basis_fused_ring(T.Vp, T.ldvp, T.r, dp, tlen, w.tw, w.W, w.wrows, cfg->a0, s.Tn, pack,
+                                             w.Z, w.Zlo,
                                              s.ldz, kh, 0, w.partials, w.npartials, w.scale, nullptr, nullptr, 0,
                                              w.sync, w.sync_ints, st));
             else

@@ -51,8 +51,9 @@ SIGNATURES = {
     'gwb_fourstep_order': [_P, _LL, _I, _P, _LL, _LL, _P, _LL, _P],
     'gwb_basis_fused': [_P, _LL, _I, _P, _LL, _P, _P, _I, _LL, _LL, _I, _P, _P, _LL, _I, _I, _I, _P, _LL, _P, _P, _P,
                         _P, _LL, _P],
-    'gwb_basis_fused_ring': [_P, _LL, _I, _P, _LL, _P, _P, _LL, _LL, _I, _P, _P, _LL, _I, _I, _P, _LL, _P, _P, _P, _LL,
-                             _P, _LL, _P],
+    'gwb_basis_fused_ring': [_P, _LL, _I, _P, _LL, _P, _P, _I, _LL, _LL, _I, _P, _P, _LL, _I, _I, _P, _LL, _P, _P, _P,
+                             _LL, _P, _LL, _P],
+    'gwb_basis_ring_set_config': [_I, _I, _I],
     'gwb_basis_ring_rows': [],
     'gwb_basis_ring_sync_ints': [_I],
     'gwb_basis_pack': [_P, _LL, _I, _I, _I, _LL, _LL, _P, _I, _P, _P, _LL, _P],
@@ -162,6 +163,12 @@ def stream_ptr(device=None):
 def ptr(t):
     """Device pointer of a tensor (None -> NULL)."""
     return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def row_stride(t):
+    """Row stride (elements) of a 2-D tensor whose rows are contiguous; a single row may carry any stride in torch
+    (a size-1 dimension's stride is free), so its row length is passed instead."""
+    return t.stride(0) if t.shape[0] > 1 else t.shape[1]
 
 
 def device_error(clear=True):

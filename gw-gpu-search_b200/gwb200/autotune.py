@@ -7,14 +7,17 @@ The reference's counterpart is fp_gemm.pick_cfg (pipeline/fp_gemm.py:47-64): it 
 (BM, BK, warps, stages) once on one shape and keeps the fastest. Here every candidate is timed with CUDA events on
 synthetic operands of the exact shape (a warm-up launch, then `reps` launches), the fastest is written into the
 library's table (gwb_gemm_set_config) and kept in a cache keyed by (device, form, n, Kh, Tn), so a later bank or
-MatchedFilter of the same shapes reuses it without timing. Every candidate gives the same V and I (the tests check
-it), so tuning changes speed only.
+MatchedFilter of the same shapes reuses it without timing. The candidates compute the same products; only the order
+of the fp32 accumulation differs between MMA orders (identical V and I where the sums are exact, as in the tests;
+otherwise the last bits of V and, at near-ties, I), so tuning changes speed, not precision.
 """
 import torch
 
 from . import _lib, fp_filter
 
 FORM_CODE = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}
+# the persistent basis series' (rows per chunk, W slots, lookahead): W in L2 holds rows x slots rows of 8 MB at 2^20
+RING_CONFIGS = [(2, 3, 1), (2, 4, 2), (1, 4, 2), (1, 6, 3), (4, 2, 1), (3, 3, 2)]
 _CACHE = {}
 
 
@@ -92,7 +95,10 @@ def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
     rows or in batches of 32; returns (best: dict(ring, wrows), {candidate: ms})."""
     key = (torch.cuda.get_device_name(device), 'basis', int(tlen), int(r), form)
     if key in _CACHE:
-        return _CACHE[key]
+        out = _CACHE[key]
+        if out[0]['ring_config'] is not None:
+            _lib.call('gwb_basis_ring_set_config', *out[0]['ring_config'])
+        return out
     flen = tlen // 2 + 1
     g = torch.Generator(device=device).manual_seed(2)
     Vh = torch.randn((r, flen), generator=g, device=device, dtype=torch.complex64)
@@ -104,18 +110,22 @@ def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
     Zlo = torch.zeros_like(Z) if form == 'bf16x3' else None
     Vp = fp_filter.fourstep_order(Vh, tlen)
     Dp = fp_filter.fourstep_order(D, tlen, isw)
-    cands = [(False, None), (False, 32)]
+    cands = [(False, None, None), (False, 32, None)]
     if tlen == fp_filter.RING_N:
-        cands.insert(0, (True, None))
+        cands = [(True, None, rc) for rc in RING_CONFIGS] + cands
     res, best = {}, None
-    for ring, wrows in cands:
+    for ring, wrows, rc in cands:
+        if rc is not None:
+            _lib.call('gwb_basis_ring_set_config', *rc)
         ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, device=device, wrows=wrows, ring=ring)
         ms = _events_ms(lambda: fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo, form, im_off=Kh), reps)
-        res[(ring, wrows)] = ms
+        res[(ring, wrows, rc)] = ms
         if best is None or ms < res[best]:
-            best = (ring, wrows)
+            best = (ring, wrows, rc)
         del ws
-    out = (dict(ring=best[0], wrows=best[1]), res)
+    if best[2] is not None:
+        _lib.call('gwb_basis_ring_set_config', *best[2])
+    out = (dict(ring=best[0], wrows=best[1], ring_config=best[2]), res)
     _CACHE[key] = out
     return out
 

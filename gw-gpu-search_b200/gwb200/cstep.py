@@ -55,8 +55,8 @@ class CStep:
         b = self.bank
         assert D.shape[0] == self.nseg and IP.shape[0] == self.nseg
         _lib.call('gwb_filter_step', ctypes.addressof(self.tiles), len(b.svd), _lib.ptr(b.H), b.H.stride(0), b.M,
-                  _lib.ptr(b.kmax), _lib.ptr(b.nbins), b.kmin, float(b.df), _lib.ptr(D), _lib.ptr(IP), D.stride(0),
-                  IP.stride(0), self.nseg, _lib.ptr(isw), self.tlen, b.flen, ctypes.addressof(self.c),
+                  _lib.ptr(b.kmax), _lib.ptr(b.nbins), b.kmin, float(b.df), _lib.ptr(D), _lib.ptr(IP),
+                  _lib.row_stride(D), _lib.row_stride(IP), self.nseg, _lib.ptr(isw), self.tlen, b.flen, ctypes.addressof(self.c),
                   _lib.ptr(self.work), self.work.numel(), _lib.ptr(self.cands), _lib.ptr(self.peaks),
                   _lib.ptr(self.counters), _lib.ptr(self.sig), _lib.stream_ptr())
         return self.sig

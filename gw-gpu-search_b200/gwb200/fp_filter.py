@@ -31,7 +31,7 @@ def derive_sw(IPall):
     nseg, flen = IPall.shape
     sw = torch.empty(flen, dtype=torch.float32, device=IPall.device)
     isw = torch.empty_like(sw)
-    _lib.call('gwb_sw', _lib.ptr(IPall), IPall.stride(0), nseg, flen, _lib.ptr(sw), _lib.ptr(isw), _s())
+    _lib.call('gwb_sw', _lib.ptr(IPall), _lib.row_stride(IPall), nseg, flen, _lib.ptr(sw), _lib.ptr(isw), _s())
     return sw, isw
 
 
@@ -43,7 +43,7 @@ def sigma2(H, IPall, df, kmin=0):
     part_elems = n * nseg * 64
     part = torch.empty(part_elems, dtype=torch.float64, device=H.device)
     sig = torch.empty((n, nseg), dtype=torch.float64, device=H.device)
-    _lib.call('gwb_sigma2', _lib.ptr(H), H.stride(0), n, _lib.ptr(IPall), IPall.stride(0), nseg, int(kmin), flen,
+    _lib.call('gwb_sigma2', _lib.ptr(H), H.stride(0), n, _lib.ptr(IPall), _lib.row_stride(IPall), nseg, int(kmin), flen,
               float(df), _lib.ptr(part), part_elems, _lib.ptr(sig), sig.stride(0), _s())
     return sig, (4.0 * df) / torch.sqrt(sig)
 
@@ -115,8 +115,8 @@ def fourstep_order(X, N, isw=None, out=None):
     if out is None:
         # rows padded to an even length: 16-byte aligned rows for the fused pass's asynchronous copies
         out = torch.empty((rows, N // 2 + 2), dtype=torch.complex64, device=X.device)[:, :N // 2 + 1]
-    _lib.call('gwb_fourstep_order', _lib.ptr(X2), X2.stride(0), rows, _lib.ptr(isw), flen, int(N), _lib.ptr(out),
-              out.stride(0), _lib.stream_ptr(X.device))
+    _lib.call('gwb_fourstep_order', _lib.ptr(X2), _lib.row_stride(X2), rows, _lib.ptr(isw), flen, int(N),
+              _lib.ptr(out), _lib.row_stride(out), _lib.stream_ptr(X.device))
     return out if X.dim() == 2 else out[0]
 
 
@@ -160,7 +160,7 @@ def basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo=None, form='f16', im_off=None)
     if ws.ring:
         # one persistent launch, W in an L2-resident ring; the scale from the first two rows
         _lib.call('gwb_basis_fused_ring', _lib.ptr(Vp), Vp.stride(0), r, _lib.ptr(Dp), ws.tlen, _lib.ptr(ws.tw),
-                  _lib.ptr(ws.W), int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0), int(im_off),
+                  _lib.ptr(ws.W), ws.W.shape[0], int(a0), int(Tn), FORMS[form], _lib.ptr(Z), _lib.ptr(Zlo), Z.stride(0), int(im_off),
                   0, _lib.ptr(ws.partials), ws.partials.numel(), _lib.ptr(ws.scale), _lib.ptr(ws.rowscale),
                   _lib.ptr(ws.rowpart), ws.rowpart.numel(), _lib.ptr(ws.sync), ws.sync.numel(), _lib.stream_ptr())
         return ws.scale

@@ -267,7 +267,7 @@ class MatchedFilter:
         sig = torch.empty((b.M, nseg), dtype=torch.float64, device=IP.device)
         part_elems = b.M * nseg * 16
         part = torch.empty(part_elems, dtype=torch.float64, device=IP.device)
-        _lib.call('gwb_sigma2', _lib.ptr(b.H), b.H.stride(0), b.M, _lib.ptr(IP), IP.stride(0), nseg, b.kmin, b.flen,
+        _lib.call('gwb_sigma2', _lib.ptr(b.H), b.H.stride(0), b.M, _lib.ptr(IP), _lib.row_stride(IP), nseg, b.kmin, b.flen,
                   float(b.df), _lib.ptr(part), part_elems, _lib.ptr(sig), sig.stride(0), _lib.stream_ptr())
         self.kernel_launches += 2
         return sig
@@ -297,20 +297,20 @@ class MatchedFilter:
             self.kernel_launches += 1
         cap = self.slot_cap                    # the exact stage's lists
         _lib.call('gwb_edges', _lib.ptr(self.units), _lib.ptr(cnt[2:]), cap, _lib.ptr(b.H), b.H.stride(0),
-                  _lib.ptr(IP), IP.stride(0), _lib.ptr(b.nbins), _lib.ptr(b.kmax), b.kmin, self.B, 0, _lib.ptr(self.E), s)
+                  _lib.ptr(IP), _lib.row_stride(IP), _lib.ptr(b.nbins), _lib.ptr(b.kmax), b.kmin, self.B, 0, _lib.ptr(self.E), s)
         if self.slots is None:
             # every slot the finalisation reads is written by the binned sums: no clearing between steps
             self.slots = torch.empty((self.slot_cap, self.nchunk, self.B, 2), dtype=torch.float32, device=D.device)
         if self.cfg.exact_order:
             _lib.call('gwb_bin_sums_ordered', _lib.ptr(self.groups), _lib.ptr(cnt[1:]), cap, _lib.ptr(self.units),
                       _lib.ptr(self.cands), _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), b.M, _lib.ptr(b.H),
-                      b.H.stride(0), _lib.ptr(D), D.stride(0), b.kmin, b.flen, self.tlen, _lib.ptr(self.sort_work),
+                      b.H.stride(0), _lib.ptr(D), _lib.row_stride(D), b.kmin, b.flen, self.tlen, _lib.ptr(self.sort_work),
                       self.sort_work.numel(), _lib.ptr(self.sort_status), _lib.ptr(self.slots), s)
             self.kernel_launches += 3
         else:
             _lib.call('gwb_bin_sums', _lib.ptr(self.groups), _lib.ptr(cnt[1:]), cap, _lib.ptr(self.units),
                       _lib.ptr(self.cands), _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), _lib.ptr(b.H),
-                      b.H.stride(0), _lib.ptr(D), D.stride(0), b.kmin, b.flen, self.tlen, _lib.ptr(self.slots), s)
+                      b.H.stride(0), _lib.ptr(D), _lib.row_stride(D), b.kmin, b.flen, self.tlen, _lib.ptr(self.slots), s)
         _lib.call('gwb_exact_finalize', _lib.ptr(self.cands), _lib.ptr(cnt[0:]), cap, _lib.ptr(self.units),
                   _lib.ptr(self.E), self.B, _lib.ptr(b.nbins), b.kmin, b.flen, _lib.ptr(self.slots), _lib.ptr(sig),
                   sig.stride(0), float(b.df), _lib.ptr(self.peaks), s)

@@ -131,7 +131,7 @@ GWB_API long long gwb_fused_peaks_cplx_work_bytes(int M);
  * step grouped by A half; 2: per Z chunk all real-part MMAs, then all imaginary-part ones; 3: per Z chunk one product
  * at a time). Forms 4 and 5 are the stacked drop-in kernels (gwb_fused_peaks_f16, gwb_fused_peaks_bf16x3; kh = K;
  * only stages applies). Process-wide, guarded by a mutex; a shape without an entry uses pair 1, stages 0, order 0.
- * Every entry gives the same V and I. */
+ * Every entry computes the same products; the MMA order only changes the order of the fp32 accumulation. */
 GWB_API int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order);
 GWB_API int gwb_gemm_clear_configs(void);
 GWB_API int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo, long long lda, const void* Z_hi,
@@ -286,19 +286,21 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
                             int im_off, int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket,
                             float* scale, float* rowscale, float* rowpart, long long rowpart_elems, void* stream);
 /* The same basis series for N = 2^20 in one persistent launch that keeps W in L2 (same reference call,
- * fp_filter.py:597-613): rows go in chunks of 2 through a ring of gwb_basis_ring_rows() rows of W (W: that many rows
- * of N complex, 128-byte aligned), pass 1 of one chunk running beside pass 2 of the previous one; each W tile's L2
- * lines are dropped after pass 2 has read it, so per row HBM carries the basis filters in and Z out. Work items are
- * taken in order from a ticket; an item waits (bounded, one second, then GWB_ERR_TIMEOUT in the device error word)
- * only for items earlier in that order. The scale is the Parseval rms of the first chunk's rows (min(2, rows) rows)
- * instead of min(nfirst, wrows) rows. partials: >= 1024 doubles; sync: gwb_basis_ring_sync_ints(rows) int32, cleared
- * by the call on the stream; fp8: rowpart >= rows x 1024 floats, rowscale rows floats. Other arguments as
- * gwb_basis_fused. */
+ * fp_filter.py:597-613): rows go in chunks of pc through a ring of nslot slots of W (pc x nslot rows of N complex,
+ * 128-byte aligned; wrows = the rows W holds), pass 1 running `look` chunks ahead of pass 2; each W tile's L2 lines
+ * are dropped after pass 2 has read it, so per row HBM carries the basis filters in and Z out. Work items are taken in
+ * order from a ticket; an item waits (bounded, one second, then GWB_ERR_TIMEOUT in the device error word) only for
+ * items earlier in that order. The scale is the Parseval rms of the first chunk's rows (min(pc, rows) rows) instead
+ * of min(nfirst, wrows) rows. partials: >= 1024 doubles; sync: gwb_basis_ring_sync_ints(rows) int32, cleared by the
+ * call on the stream; fp8: rowpart >= rows x 1024 floats, rowscale rows floats. Other arguments as gwb_basis_fused.
+ * gwb_basis_ring_set_config sets (pc in 1..4, nslot > look, look >= 1) process-wide (default 2, 3, 1; the autotuner
+ * times the choices); gwb_basis_ring_rows and gwb_basis_ring_sync_ints size W and sync for the current one. */
+GWB_API int gwb_basis_ring_set_config(int pc, int nslot, int look);
 GWB_API int gwb_basis_ring_rows(void);
 GWB_API int gwb_basis_ring_sync_ints(int rows);
 GWB_API int gwb_basis_fused_ring(const float* Vp, long long ldvp, int rows, const float* Dp, long long N,
-                                 const float* tw, float* W, long long a0, long long Tn, int form, void* Z, void* Zlo,
-                                 long long ldz, int im_off, int row0, double* partials, long long npartials,
+                                 const float* tw, float* W, int wrows, long long a0, long long Tn, int form, void* Z,
+                                 void* Zlo, long long ldz, int im_off, int row0, double* partials, long long npartials,
                                  float* scale, float* rowscale, float* rowpart, long long rowpart_elems,
                                  int32_t* sync, long long sync_ints, void* stream);
 

@@ -105,14 +105,18 @@ def basis(a):
         out[f'hbm_gbs_w{fws.wrows}'] = r * (8 * flen + zb) / msf / 1e6
     if tlen == fp_filter.RING_N:
         ref, ref_scale = Z.double() * fws.scale.double(), fws.scale.double()
-        rws = fp_filter.FusedBasisWorkspace(tlen, flen, r, ring=True)
-        msr = _time(lambda: fp_filter.basis_series_fused(rws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
-        out['us_per_row_ring'] = msr * 1e3 / r
-        out['hbm_gbs_ring'] = r * (8 * flen + zb) / msr / 1e6
-        # the ring form's scale comes from 2 rows instead of 64: compare the series times their scales
-        got = Z.double() * rws.scale.double()
-        out['ring_vs_two_pass_max_rel'] = float(((got - ref).abs().max() / ref.abs().max()).item())
-        out['ring_scale_over_two_pass'] = float((rws.scale.double() / ref_scale).item())
+        for rc in [tuple(int(v) for v in x.split(':')) for x in a.ring_cfgs.split(',')]:
+            _lib.call('gwb_basis_ring_set_config', *rc)
+            rws = fp_filter.FusedBasisWorkspace(tlen, flen, r, ring=True)
+            msr = _time(lambda: fp_filter.basis_series_fused(rws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh),
+                        a.reps)
+            tag = 'ring_%d_%d_%d' % rc
+            out['us_per_row_' + tag] = msr * 1e3 / r
+            # the ring form's scale comes from pc rows instead of 64: compare the series times their scales
+            got = Z.double() * rws.scale.double()
+            out['max_rel_vs_two_pass_' + tag] = float(((got - ref).abs().max() / ref.abs().max()).item())
+            del rws
+        _lib.call('gwb_basis_ring_set_config', 2, 3, 1)
     return out
 
 
@@ -388,7 +392,11 @@ def fp64_exact_at(H, rows, samples, D_seg, IP_seg, kmin, kmax, nbins, sig, df, t
     row (int), sig per bank row (float64 of this segment). Returns (snr, chisq) float64 numpy arrays."""
     dev = H.device
     flen = H.shape[1]
-    rows = torch.as_tensor(np.asarray(rows, np.int64), device=dev)
+    rh = np.asarray(rows, np.int64)
+    assert rh.size == 0 or (rh.min() >= 0 and rh.max() < min(H.shape[0], len(kmax), len(nbins), len(sig))), \
+        'rows index the bank: kmax, nbins and sig are per bank row'
+    assert len(samples) == len(rh)
+    rows = torch.as_tensor(rh, device=dev)
     samples = torch.as_tensor(np.asarray(samples, np.int64), device=dev)
     kmax = torch.as_tensor(np.asarray(kmax, np.int64), device=dev)
     nbins = torch.as_tensor(np.asarray(nbins, np.int64), device=dev)
@@ -501,10 +509,10 @@ def precision_c2(B, cond, x, isw, forms, form_config, g, seg=0, n_chisq=256, see
             rows = np.array([p[0] for p in pick])
             s64 = np.array([g['a0'] + I64[p] for p in pick])
             sf = np.array([kept[p][2] for p in pick])
-            snr_a, chi_a = fp64_exact_at(B.H, rows, s64, Dd[seg], IPd[seg], B.kmin, kmax[rows], nbins[rows],
-                                         sig_seg[rows], g['df'], g['tlen'])
-            snr_b, chi_b = fp64_exact_at(B.H, rows, sf, Dd[seg], IPd[seg], B.kmin, kmax[rows], nbins[rows],
-                                         sig_seg[rows], g['df'], g['tlen'])
+            snr_a, chi_a = fp64_exact_at(B.H, rows, s64, Dd[seg], IPd[seg], B.kmin, kmax, nbins, sig_seg, g['df'],
+                                         g['tlen'])
+            snr_b, chi_b = fp64_exact_at(B.H, rows, sf, Dd[seg], IPd[seg], B.kmin, kmax, nbins, sig_seg, g['df'],
+                                         g['tlen'])
             cf = np.array([kept[p][1] for p in pick])
             snf = np.array([kept[p][0] for p in pick])
             chi = dict(n=len(pick), rel_vs_fp64_argmax=_stats(np.abs(cf - chi_a) / np.maximum(np.abs(chi_a), 1e-30)),
@@ -545,6 +553,8 @@ def main():
     ap.add_argument('--pair', default='1', help='gemm: comma list, 1 CTA pairs, 0 one CTA per M block')
     ap.add_argument('--stages', default='0', help='gemm: comma list of Z ring depths (0: the most that fit)')
     ap.add_argument('--orders', default='0', help='gemm: comma list of MMA orders of the CTA-pair kernel (0-3)')
+    ap.add_argument('--ring-cfgs', default='2:3:1,2:4:2,1:4:2,1:6:3,4:2:1,3:3:2',
+                    help='basis: comma list of rows:slots:lookahead of the persistent ring form (2^20)')
     a = ap.parse_args()
     print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact, 'adjoint': adjoint, 'c4': c4}[a.what](a)))
 

@@ -57,8 +57,8 @@ def test_fp64_exact_reference_matches_the_oracle():
     rows = rng.integers(0, B.M, 40)
     samples = rng.integers(0, TLEN, 40)
     nb = np.full(B.M, 16)
-    snr, chi = microbench.fp64_exact_at(B.H, rows, samples, Dd[seg], IPd[seg], B.kmin, B.kmax_h[rows], nb[rows],
-                                        sig[rows, seg], DF, TLEN)
+    snr, chi = microbench.fp64_exact_at(B.H, rows, samples, Dd[seg], IPd[seg], B.kmin, B.kmax_h, nb, sig[:, seg],
+                                        DF, TLEN)
     H = B.H.cpu().numpy()
     z, pw, _, _ = oc.exact_dense(H, nb, B.kmin, B.kmax_h, D[seg], IP[seg], DF, TLEN, rows, samples)
     snr_o, chi_o, _ = of.finalize(z, pw, 4.0 * DF / np.sqrt(sig[rows, seg]), nb[rows])
