@@ -164,6 +164,15 @@ class Clocks:
                     samples=len(sm))
 
 
+def _plain(o):
+    """JSON for the numpy scalars and arrays a report may hold."""
+    if isinstance(o, np.generic):
+        return o.item()
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError('not JSON serialisable: %r' % type(o))
+
+
 def peaks_file():
     p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
     if os.path.exists(p):
@@ -503,6 +512,19 @@ def run_c2(a):
                 autotune={f: (None if t is None else dict(gemm={str(k): v['best'] for k, v in t['gemm'].items()},
                                                             basis=t['basis'] and t['basis']['best']))
                           for f, t in tunings.items()})
+    if rank == 0 and world == 1 and not a.no_c4:
+        # the batched form (300 uneven segments, autogating, the whole run as one graph) on the same bank and GPU
+        import microbench
+        try:
+            ns = argparse.Namespace(segments=300, batch=32, seed=4, no_graph=False, production=False,
+                                    form='bf16x3', bank_obj=B, isw=isw)
+            r4 = microbench.c4(ns)
+            line['c4'] = {k: r4[k] for k in ('workload', 'value', 'unit', 'ms', 'analysed_s', 'chunks', 'batches',
+                                             'one_graph', 'graph_capture_s', 'glitches', 'glitches_gated',
+                                             'injections_snr8_in_analysed', 'injections_found')}
+        except Exception as ex:     # reported in the line; the C2 measurement above stands
+            line['c4'] = dict(error=repr(ex)[:300])
+        torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not a.no_cpu:
         S = cpu_setup(bank if len(bank['mass1']) == N_TEMPLATES else make_bank())
         cpu_step(S, 0)
@@ -515,7 +537,7 @@ def run_c2(a):
                                     sample=cpu_sample_desc(S, a.cpu_steps) + ' (after one untimed step)',
                                     ms_per_step=float(np.mean(times)) * 1e3)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=_plain), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
@@ -568,6 +590,7 @@ def main():
     ap.add_argument('--form-steps', type=int, default=3, help='timed steps of each form after the first')
     ap.add_argument('--production', action='store_true', help='c4: production selection and consolidation')
     ap.add_argument('--no-autotune', action='store_true', help='c2: default launch shapes instead of tuned ones')
+    ap.add_argument('--no-c4', action='store_true', help='c2: skip the batched-form run reported under "c4"')
     a = ap.parse_args()
     a.forms_given = any(x == '--forms' or x.startswith('--forms=') for x in sys.argv[1:])
     if a.impl == 'reference':

@@ -888,11 +888,24 @@ __global__ void __launch_bounds__(256, 2) basis_persist(const __grid_constant__ 
     int* abort_word = a.sync + 1;
     int* p1done = a.sync + 2;
     int* p2done = p1done + nch;
+    // look = 0: split roles, the first half of the grid takes only pass-1 items (ticket), the second half only pass-2
+    // items (ticket2), each in chunk order; pass 1 then runs ahead of pass 2 as far as the ring's free slots allow
+    const bool split = a.look == 0;
+    const bool p1role = (int)blockIdx.x < (int)gridDim.x / 2;
+    int* ticket2 = p2done + nch;
     while (true) {
-        if (threadIdx.x == 0) s_t = *(volatile int*)abort_word ? 0x7fffffff : atomicAdd(ticket, 1);
+        if (threadIdx.x == 0)
+            s_t = *(volatile int*)abort_word ? 0x7fffffff : atomicAdd(split && !p1role ? ticket2 : ticket, 1);
         __syncthreads();
         int type = 0, c = 0, g = 0;
-        if (!persist_item(s_t, nch, a.look, type, c, g)) break;   // uniform over the CTA
+        if (split) {
+            if (s_t >= nch * PG) break;                           // uniform over the CTA
+            type = p1role ? 1 : 2;
+            c = s_t / PG;
+            g = s_t % PG;
+        } else if (!persist_item(s_t, nch, a.look, type, c, g)) {
+            break;
+        }
         if (threadIdx.x == 0) {
             bool ok = true;
             if (type == 1 && c >= a.nslot) ok = wait_count(&p2done[c - a.nslot], PG, abort_word);
@@ -929,7 +942,9 @@ int launch_persist(const PersistArgs& a, cudaStream_t s) {
     GWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
     GWB_CHECK_ARG(per_sm >= 1, GWB_ERR_CUDA, "basis_persist: no CTA fits on an SM");
     const int nch = (a.rows + a.pc - 1) / a.pc;
-    const int grid = std::min(per_sm * num_sms(), 2 * PG * nch);
+    int grid = per_sm * num_sms();
+    if (a.look > 0) grid = std::min(grid, 2 * PG * nch);
+    else grid = std::max(2, grid & ~1);                // split roles: two equal halves
     k<<<grid, 256, smem, s>>>(a);
     GWB_LAUNCH_CHECK("basis_persist");
     return GWB_OK;
@@ -1046,9 +1061,9 @@ std::atomic<int> g_ring_pc{2}, g_ring_nslot{3}, g_ring_look{1};
 
 int gwb_basis_ring_set_config(int pc, int nslot, int look) {
     using namespace gwb;
-    GWB_CHECK_ARG(pc >= 1 && pc <= PC_MAX && look >= 1 && nslot > look && nslot <= 16, GWB_ERR_ARG,
-                  "basis_ring_set_config: pc=%d (1..%d) nslot=%d (> look, <= 16) look=%d (>= 1)", pc, PC_MAX, nslot,
-                  look);
+    GWB_CHECK_ARG(pc >= 1 && pc <= PC_MAX && look >= 0 && nslot > look && nslot >= 2 && nslot <= 16, GWB_ERR_ARG,
+                  "basis_ring_set_config: pc=%d (1..%d) nslot=%d (> look, 2..16) look=%d (>= 0; 0: split roles)", pc,
+                  PC_MAX, nslot, look);
     g_ring_pc.store(pc);
     g_ring_nslot.store(nslot);
     g_ring_look.store(look);
@@ -1059,7 +1074,7 @@ int gwb_basis_ring_rows(void) { return gwb::g_ring_pc.load() * gwb::g_ring_nslot
 
 int gwb_basis_ring_sync_ints(int rows) {
     const int pc = gwb::g_ring_pc.load();
-    return 2 + 2 * ((rows + pc - 1) / pc);
+    return 3 + 2 * ((rows + pc - 1) / pc);
 }
 
 int gwb_basis_fused_ring(const float* Vp, long long ldvp, int rows, const float* Dp, long long N, const float* tw,

@@ -155,6 +155,10 @@ int gwb_filter_step(const GwbTile* tiles, int ntiles, const float* H, long long 
     const int pack = cfg->form == 0 ? 0 : (cfg->form == 1 ? 3 : 2);     // Z / A encodings: f16, bf16, split bf16
     GWB_CUDA(cudaMemsetAsync(counters, 0, 5 * sizeof(int32_t), st));
     GWB_CUDA(cudaMemsetAsync(w.ticket, 0, sizeof(uint32_t), st));
+    // the Z rows past a tile's rank (up to its 16-row K step) are read by the GEMM against zero columns of A: they must
+    // hold finite values, so the planes start at zero (a smaller rank later leaves finite values there)
+    GWB_CUDA(cudaMemsetAsync(w.Z, 0, 2ll * s.K * s.ldz, st));
+    if (w.Zlo) GWB_CUDA(cudaMemsetAsync(w.Zlo, 0, 2ll * s.K * s.ldz, st));
     // template norms (float64) and every segment's D isw in four-step order
     GWB_TRY(gwb_sigma2(H, ldh, M, IP, ldip, nseg, kmin, flen, df, w.part, (long long)M * nseg * 16, sig, nseg, st));
     GWB_TRY(gwb_fourstep_order(D, ldd, nseg, isw, flen, tlen, w.Dp, s.ldp, st));

@@ -17,7 +17,8 @@ from . import _lib, fp_filter
 
 FORM_CODE = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}
 # the persistent basis series' (rows per chunk, W slots, lookahead): W in L2 holds rows x slots rows of 8 MB at 2^20
-RING_CONFIGS = [(2, 3, 1), (2, 4, 2), (1, 4, 2), (1, 6, 3), (4, 2, 1), (3, 3, 2)]
+# (lookahead 0: split roles, half the CTAs on each pass)
+RING_CONFIGS = [(2, 3, 1), (2, 4, 2), (4, 2, 1), (2, 3, 0), (2, 2, 0), (4, 2, 0), (1, 4, 0)]
 _CACHE = {}
 
 

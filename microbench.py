@@ -262,7 +262,11 @@ def c4(a):
     del cond
     torch.cuda.synchronize()
     t_b = time.perf_counter()
-    B = pipeline.Bank(bank, flen, df, sw, cfg)
+    if getattr(a, 'bank_obj', None) is not None:
+        # a bank built by the caller for the same chunk length (the C2 bank of bench.py), with its own SVD metric
+        B, isw = a.bank_obj, a.isw
+    else:
+        B = pipeline.Bank(bank, flen, df, sw, cfg)
     torch.cuda.synchronize()
     bank_s = time.perf_counter() - t_b
     F = sg.SegmentFilter(B, cfg, batch=a.batch, isw=isw, graph=not a.no_graph, consolidation=co)
@@ -553,7 +557,7 @@ def main():
     ap.add_argument('--pair', default='1', help='gemm: comma list, 1 CTA pairs, 0 one CTA per M block')
     ap.add_argument('--stages', default='0', help='gemm: comma list of Z ring depths (0: the most that fit)')
     ap.add_argument('--orders', default='0', help='gemm: comma list of MMA orders of the CTA-pair kernel (0-3)')
-    ap.add_argument('--ring-cfgs', default='2:3:1,2:4:2,1:4:2,1:6:3,4:2:1,3:3:2',
+    ap.add_argument('--ring-cfgs', default='2:3:1,2:4:2,4:2:1,2:3:0,2:2:0,4:2:0,1:4:0',
                     help='basis: comma list of rows:slots:lookahead of the persistent ring form (2^20)')
     a = ap.parse_args()
     print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact, 'adjoint': adjoint, 'c4': c4}[a.what](a)))

@@ -13,7 +13,7 @@ PG = 128                          # items per chunk and pass (csrc/fft_basis.cu)
 N = 1 << 20
 N1 = N2 = 1024
 TB = 8
-CONFIGS = [(2, 3, 1), (2, 4, 2), (1, 4, 2), (1, 6, 3), (4, 2, 1), (3, 3, 2)]   # gwb200.autotune.RING_CONFIGS
+CONFIGS = [(2, 3, 1), (2, 4, 2), (1, 4, 2), (1, 6, 3), (4, 2, 1), (3, 3, 2)]   # shared-ticket rings (look >= 1)
 
 
 def persist_item(t, nch, look):
@@ -134,3 +134,43 @@ def test_index_arithmetic_stays_inside_the_buffers():
     SC = 32 * SB + ((2 - (32 * SB) % 16) + 16) % 16
     p2 = N1 + TB * SC
     assert p2 <= p1 and p1 * 8 == 110592
+
+
+@pytest.mark.parametrize('rows,ctas,seed,pc,nslot', [(128, 148, 0, 2, 3), (192, 148, 1, 2, 2), (7, 148, 2, 1, 4),
+                                                      (78, 3, 3, 4, 2), (40, 1, 4, 3, 3)])
+def test_split_roles_complete_and_respect_the_ring(rows, ctas, seed, pc, nslot):
+    """look = 0: half the grid takes pass-1 items in chunk order from one ticket, the other half pass-2 items from a
+    second ticket; a pass-1 item of chunk c waits for the pass-2 items of chunk c - nslot, a pass-2 item for the
+    pass-1 items of its chunk (and of chunk 0). Random interleavings complete and no slot is overwritten while read."""
+    rng = np.random.default_rng(seed)
+    nch = (rows + pc - 1) // pc
+    queues = {1: [(1, c, g) for c in range(nch) for g in range(PG)], 2: [(2, c, g) for c in range(nch) for g in range(PG)]}
+    done, running, steps = {}, [], 0
+    free = {1: ctas, 2: ctas}
+    pos = {1: 0, 2: 0}
+    while any(pos[k] < len(queues[k]) for k in (1, 2)) or running:
+        steps += 1
+        assert steps < 10 ** 6, 'no progress'
+        for k in (1, 2):
+            while free[k] and pos[k] < len(queues[k]):
+                running.append([queues[k][pos[k]], None])
+                pos[k] += 1
+                free[k] -= 1
+        rng.shuffle(running)
+        for r in running:
+            if r[1] is None and all(done.get(d, 0) == PG for d in deps(r[0], nslot)):
+                r[1] = int(rng.integers(1, 5))
+                if r[0][0] == 1:
+                    c = r[0][1]
+                    for o in running:
+                        if o[0][0] == 2 and o[1] is not None and o[0][1] != c and o[0][1] % nslot == c % nslot:
+                            raise AssertionError(('slot overwritten while read', r[0], o[0]))
+        for r in list(running):
+            if r[1] is not None:
+                r[1] -= 1
+                if r[1] == 0:
+                    k = r[0][:2]
+                    done[k] = done.get(k, 0) + 1
+                    running.remove(r)
+                    free[r[0][0]] += 1
+    assert all(done[(ty, c)] == PG for ty in (1, 2) for c in range(nch))
