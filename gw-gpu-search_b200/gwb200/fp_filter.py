@@ -59,17 +59,51 @@ def gram(H, sw, kmin):
     return G
 
 
-def svd_tile(H, sw, kmin, eps):
-    """fp_filter.py:576-593: Gram matrix (float64, device), normalised, Hermitian eigendecomposition (float64 LAPACK on
-    the host), rank r = smallest with worst lost power <= eps, basis filters Vh (device). Returns (r, A, Vh, worst)
-    with A (n, r) and Vh (r, flen) complex64 CUDA tensors."""
+EIGH_TOL, EIGH_SWEEPS = 1e-13, 40
+
+
+def eigh_device(Gn):
+    """Eigenvalues (descending, float64 numpy) and eigenvectors (columns, complex128 numpy) of a Hermitian positive
+    semi-definite matrix (n <= 256, complex128 CUDA tensor) by the device's one-sided Jacobi in float64
+    (gwb_eigh_jacobi_sweep: sweeps until one rotates no pair with cosine above EIGH_TOL)."""
+    n = Gn.shape[0]
+    U = Gn.transpose(0, 1).contiguous()                 # column-major: U[j, i] = G[i, j]
+    V = torch.empty_like(U)
+    nv = torch.tensor([n], dtype=torch.int32, device=Gn.device)
+    rot = torch.zeros(1, dtype=torch.int32, device=Gn.device)
+    for sweep in range(EIGH_SWEEPS):
+        _lib.call('gwb_eigh_jacobi_sweep', _lib.ptr(U), _lib.ptr(V), _lib.ptr(nv), 1, n, int(sweep == 0),
+                  EIGH_TOL, _lib.ptr(rot), _s())
+        if int(rot.item()) == 0:
+            break
+    else:
+        raise _lib.GwbError('eigh_jacobi_sweep', _lib.GWB_ERR_SHAPE,
+                            'no convergence in %d sweeps (%d rotations in the last)' % (EIGH_SWEEPS, int(rot.item())))
+    lam = torch.empty(n, dtype=torch.float64, device=Gn.device)
+    _lib.call('gwb_eigh_values', _lib.ptr(U), _lib.ptr(nv), 1, n, _lib.ptr(lam), _s())
+    lam, Vm = lam.cpu().numpy(), V.cpu().numpy().T       # Vm[:, j] = eigenvector j
+    o = np.argsort(-lam, kind='stable')
+    return lam[o], Vm[:, o]
+
+
+def svd_tile(H, sw, kmin, eps, eigh='device'):
+    """fp_filter.py:576-593: Gram matrix (float64, device), normalised, Hermitian eigendecomposition (float64 on the
+    device by one-sided Jacobi, eigh_device; eigh='host' uses LAPACK on the host instead), rank r = smallest with worst
+    lost power <= eps, basis filters Vh (device). Returns (r, A, Vh, worst) with A (n, r) and Vh (r, flen) complex64
+    CUDA tensors."""
     _lib.require_cuda(H, sw)
     H = H.contiguous()
     n, flen = H.shape
-    G = gram(H, sw, kmin).cpu().numpy()
+    Gd = gram(H, sw, kmin)
+    G = Gd.cpu().numpy()
     nrm = np.sqrt(np.maximum(G.diagonal().real, 1e-30))
-    lam, W = np.linalg.eigh(G / (nrm[:, None] * nrm[None, :]))
-    lam, W = np.maximum(lam[::-1], 0), W[:, ::-1]
+    if eigh == 'host' or n > 256 or n < 2:
+        lam, W = np.linalg.eigh(G / (nrm[:, None] * nrm[None, :]))
+        lam, W = np.maximum(lam[::-1], 0), W[:, ::-1]
+    else:
+        nd = torch.from_numpy(nrm).to(H.device)
+        lam, W = eigh_device(Gd / (nd[:, None] * nd[None, :]))
+        lam = np.maximum(lam, 0)
     worst = (1 - ((np.abs(W) ** 2) * lam[None, :]).cumsum(1)).max(0)
     r = min(int((worst > eps).sum()) + 1, n)
     Wr = W[:, :r]

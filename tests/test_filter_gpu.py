@@ -204,3 +204,42 @@ def test_ring_basis_series_16bit_forms(form):
     zb = of.basis_series_complex(Vh, D * isw, a0, Tn, tlen)
     err = np.abs(got - zb) / np.abs(zb).max()
     assert err.max() < {'f16': 1e-3, 'bf16': 8e-3, 'bf16x3': 3e-5}[form], err.max()
+
+
+@pytest.mark.parametrize('n,spread', [(64, 6), (248, 12), (256, 14)])
+def test_device_jacobi_eigh_matches_lapack(n, spread):
+    """The device's one-sided Jacobi (fp_filter.eigh_device, float64) against LAPACK on Hermitian positive
+    semi-definite matrices with eigenvalues over `spread` decades: eigenvalues within 1e-12 of the largest, the
+    projector onto the eigenvectors of the eigenvalues above 1e-4 of the largest within 1e-9, unitary eigenvectors."""
+    from gwb200 import fp_filter
+    rng = np.random.default_rng(n)
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    lam = np.logspace(0, -spread, n)
+    G = (Q * lam[None, :]) @ Q.conj().T
+    G = (G + G.conj().T) / 2
+    l_d, W_d = fp_filter.eigh_device(torch.from_numpy(G).cuda())
+    l_h, W_h = np.linalg.eigh(G)
+    l_h, W_h = l_h[::-1], W_h[:, ::-1]
+    assert np.abs(l_d - l_h).max() < 1e-12 * l_h[0]
+    k = int((l_h > 1e-4 * l_h[0]).sum())
+    P_d = W_d[:, :k] @ W_d[:, :k].conj().T
+    P_h = W_h[:, :k] @ W_h[:, :k].conj().T
+    assert np.abs(P_d - P_h).max() < 1e-9
+    assert np.abs(W_d.conj().T @ W_d - np.eye(n)).max() < 1e-11
+
+
+def test_svd_tile_device_eigh_matches_host(golden):
+    """svd_tile with the device eigendecomposition gives the same rank, worst lost power and reconstruction as with
+    LAPACK on the host, on the reference's svd_tile fixture."""
+    from gwb200 import fp_filter
+    g = golden('filt_tile')
+    H = torch.from_numpy(g['H']).cuda()
+    sw = torch.from_numpy(g['sw']).cuda()
+    out = {}
+    for e in ('host', 'device'):
+        r, A, Vh, worst = fp_filter.svd_tile(H, sw, int(g['kmin']), float(g['eps']), eigh=e)
+        out[e] = (r, worst, (A.to(torch.complex128) @ Vh.to(torch.complex128)).cpu().numpy())
+    assert out['host'][0] == out['device'][0]
+    assert abs(out['host'][1] - out['device'][1]) < 1e-9
+    rec_h, rec_d = out['host'][2], out['device'][2]
+    assert np.abs(rec_d - rec_h).max() < 1e-4 * np.abs(rec_h).max()
