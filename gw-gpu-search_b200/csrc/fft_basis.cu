@@ -1004,6 +1004,7 @@ template <int N2>
 int launch_pass2(int form, const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn,
                  const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
     // row-chunk form for the long transforms; the split bf16 form (four Z planes) runs faster on the per-row kernel
+    // (measured at N = 2^20, r = 128: 8.3 against 10.6 us per row)
     if constexpr (N2 >= 512) {
         switch (form) {
             case 0: return launch_pass2_p<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);

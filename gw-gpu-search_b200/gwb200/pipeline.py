@@ -208,6 +208,23 @@ class MatchedFilter:
                       _lib.ptr(self.Z), self.Z.stride(0), n, K, self.Tn, self.group, _lib.ptr(self.V), _lib.ptr(self.I),
                       self.V.stride(0), s)
 
+    def clear_padding(self, t):
+        """Zeroes the rows of Z (and Zlo) that tile t's GEMM reads but its basis series does not write: between its r
+        basis rows and its width Kh in the real and the imaginary half (compact forms), or from 2 r to Kp. The GEMM
+        multiplies them by A's zero columns, so whatever another tile or step left there must not be a NaN or an
+        infinity (a step on empty data leaves both)."""
+        r = self.bank.svd[t]['r']
+        if self.compact:
+            Kh = self.khs[t]
+            spans = [(r, Kh), (Kh + r, 2 * Kh)] if Kh > r else []
+        else:
+            Kp = self.bank.svd[t]['Kp']
+            spans = [(2 * r, Kp)] if Kp > 2 * r else []
+        for Zp in (self.Z, self.Zlo):
+            if Zp is not None:
+                for a, b in spans:
+                    Zp[a:b].zero_()
+
     def tile_segment(self, t, D, isw, sig, seg):
         """Basis series, stacked A, fused GEMM and window selection of tile t against segment seg (row of D)."""
         b = self.bank
@@ -347,6 +364,7 @@ class MatchedFilter:
             prof.setdefault('parts', []).append(('fourstep', e_f))
         segs = range(D.shape[0]) if seg_ids is None else seg_ids
         for t in range(len(self.bank.tiles)):
+            self.clear_padding(t)
             for s in segs:
                 self.tile_segment(t, D, isw, sig, s)
         if prof is not None:

@@ -150,7 +150,11 @@ class SegmentFilter:
                           work=torch.zeros(2, dtype=torch.int32, device=dev),
                           meta=torch.zeros((max(nb, 1), 8), dtype=torch.int32, device=dev), cap=arena_cap)
         A = self.arena
-        self._step()                           # warm-up: plans, workspaces and cached tables outside the capture
+        # warm-up on the first batch's chunks: plans, workspaces and cached tables outside the capture
+        for r in range(self.batch):
+            i, (s0, s1), _ = chunks[min(r, len(chunks) - 1)]
+            self.X[r].copy_(segments[i]['x'][s0:s1])
+        self._step()
         torch.cuda.synchronize()
         self.run_graph_ = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.run_graph_):

@@ -311,7 +311,7 @@ def c4(a):
                      peaks_after_consolidation=res['n_peaks_out'], injections_found_in_tables=found_t)
     return dict(workload='C4: %d segments, log-uniform 64-4096 s, 2 detectors, %d injections, %d glitches; 5880 '
                          'templates, %s' % (a.segments, len(inj), len(glitches), a.form),
-                value=weeks / (ms / 1e3 / 3600.0), unit='2-det weeks / GPU-hour', ms=ms, wall_s=wall,
+                value=weeks / (ms / 1e3 / 3600.0), unit='2-det weeks / hour', ms=ms, wall_s=wall,
                 analysed_s=res['analysed_s'], skipped_s=res['skipped_s'], skipped_segments=len(res['skipped']),
                 total_s=float(lens.sum()), chunks=res['n_chunks'], batches=res['batches'], graph=not a.no_graph,
                 kept=int(kept.sum()), candidates=len(res['cands']), glitches=len(glitches), glitches_gated=gated,
@@ -454,9 +454,11 @@ def precision_c2(B, cond, x, isw, forms, form_config, g, seg=0, n_chisq=256, see
     """Precision of each form against float64 over every tile of one segment (seg) of a C2 step:
     windows: the window maxima of the rebuilt SNR from the form's fused GEMM against the float64 series' (all tiles);
     kept: the peaks kept after the form's exact stage (one step of every tile against seg) against the float64
-      series' window maxima above the threshold: set agreement (away = beyond 0.2% of the threshold in float64),
-      relative SNR error at the common windows, and relative chi-squared error against the float64 exact stage at
-      the float64 argmax for up to n_chisq sampled common windows (the loudest 32 always among them), and at the
+      exact stage's: float64 transform and product, window argmax, float64 exact SNR at that sample for every window
+      whose float64 window maximum is above 0.95 of the threshold (the rebuilt and exact SNR differ by about 1%),
+      kept when above the threshold. Set agreement (away = beyond 3% of the threshold in the float64 exact SNR),
+      relative exact-SNR error at the common windows, and relative chi-squared error against the float64 exact stage
+      at the float64 argmax for up to n_chisq sampled common windows (the loudest 32 always among them), and at the
       form's own sample (the exact stage's own error).
     form_config(form): the FilterConfig of a form. g: dict(df, tlen, a0, an (analysed span), cw, thr)."""
     from gwb200 import pipeline
@@ -475,10 +477,19 @@ def precision_c2(B, cond, x, isw, forms, form_config, g, seg=0, n_chisq=256, see
         i64.append(i)
     V64, I64 = np.concatenate(v64), np.concatenate(i64)                     # (M, nw), bank rows in tile order
     thr = g['thr']
-    set64 = {tuple(p) for p in np.argwhere(V64 > thr).tolist()}
     sig_seg = sig[:, seg].double()
     kmax = B.kmax_h
     nbins = np.full(B.M, B.cfg.nbins)
+    # the float64 exact stage: exact SNR at the float64 argmax of every window near or above the threshold
+    near = np.argwhere(V64 > 0.95 * thr)
+    ex_snr, _ = fp64_exact_at(B.H, near[:, 0], g['a0'] + I64[near[:, 0], near[:, 1]], Dd[seg], IPd[seg], B.kmin, kmax,
+                              nbins, sig_seg, g['df'], g['tlen'], batch=64)
+    EX64 = {(int(r_), int(w_)): float(v_) for (r_, w_), v_ in zip(near.tolist(), ex_snr)}
+    set64 = {p for p, v_ in EX64.items() if v_ > thr}
+    rep['fp64_exact'] = dict(windows_evaluated=len(EX64), kept=len(set64),
+                             rebuilt_vs_exact=_stats(np.abs(ex_snr - V64[near[:, 0], near[:, 1]]) / ex_snr)
+                             if len(ex_snr) else None)
+    AWAY = 0.03
     rng = np.random.default_rng(seed)
     for form in forms:
         cfg = form_config(form)
@@ -500,9 +511,8 @@ def precision_c2(B, cond, x, isw, forms, form_config, g, seg=0, n_chisq=256, see
                 for r_, w_, s_, c_, t_ in zip(kc['row'], kc['window'], kp['snr'], kp['chisq'], kc['sample'])}
         ks = set(kept)
         only64, onlyf = set64 - ks, ks - set64
-        away = 2e-3 * thr
         common = sorted(ks & set64)
-        rel_snr = [abs(kept[p][0] - V64[p]) / V64[p] for p in common]
+        rel_snr = [abs(kept[p][0] - EX64[p]) / EX64[p] for p in common]
         # chi-squared against float64 at a sample of the common windows
         chi = dict(n=0)
         if common:
@@ -527,8 +537,8 @@ def precision_c2(B, cond, x, isw, forms, form_config, g, seg=0, n_chisq=256, see
                        sample_agree=float(np.mean(s64 == sf)))
         rep[form] = dict(windows=win, kept=dict(
             fp64=len(set64), form=len(ks), both=len(common), only_fp64=len(only64), only_form=len(onlyf),
-            only_fp64_away=sum(V64[p] > thr + away for p in only64),
-            only_form_away=sum(V64[p] < thr - away for p in onlyf),
+            only_fp64_away=sum(EX64[p] > thr * (1 + AWAY) for p in only64),
+            only_form_away=sum(EX64.get(p, 0.0) < thr * (1 - AWAY) for p in onlyf),
             snr_rel_common=_stats(rel_snr)), chisq=chi)
         del mf
         torch.cuda.empty_cache()

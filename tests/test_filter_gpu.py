@@ -52,8 +52,10 @@ def test_svd_tile_matches_reference(golden):
     r, A, Vh, worst = fp_filter.svd_tile(H, sw, int(g['kmin']), float(g['eps']))
     assert r == int(g['r'])
     assert abs(worst - float(g['worst'])) < 2e-5
-    rec = A.cpu().numpy().astype(np.complex128) @ Vh.cpu().numpy().astype(np.complex128)
-    rec_ref = g['A'].astype(np.complex128) @ g['Vh'].astype(np.complex128)
+    # the reconstruction conj(A) Vh = W W^H H' is independent of the eigenvectors' phases (the device solver's differ
+    # from LAPACK's); the filter uses A with conj(Vh) (fp_filter.py:592)
+    rec = A.cpu().numpy().astype(np.complex128).conj() @ Vh.cpu().numpy().astype(np.complex128)
+    rec_ref = g['A'].astype(np.complex128).conj() @ g['Vh'].astype(np.complex128)
     assert (np.linalg.norm(rec - rec_ref, axis=1) / np.linalg.norm(rec_ref, axis=1)).max() < 2e-5
 
 
@@ -238,7 +240,7 @@ def test_svd_tile_device_eigh_matches_host(golden):
     out = {}
     for e in ('host', 'device'):
         r, A, Vh, worst = fp_filter.svd_tile(H, sw, int(g['kmin']), float(g['eps']), eigh=e)
-        out[e] = (r, worst, (A.to(torch.complex128) @ Vh.to(torch.complex128)).cpu().numpy())
+        out[e] = (r, worst, (A.to(torch.complex128).conj() @ Vh.to(torch.complex128)).cpu().numpy())
     assert out['host'][0] == out['device'][0]
     assert abs(out['host'][1] - out['device'][1]) < 1e-9
     rec_h, rec_d = out['host'][2], out['device'][2]
