@@ -283,17 +283,29 @@ def top_peak_sets(kept, thr):
     return out
 
 
-def traffic_ratios():
-    """Measured DRAM bytes over algorithmic bytes, from the committed ncu summaries (lines 'traffic_ratio: X')."""
-    out = {}
-    for key, name in (('basis', 'basis_passes_c2_r128.md'), ('gemm', 'umma_cplx2_kernel_c2_r128.md')):
+# the committed ncu summaries of each form's two dominant kernels (DRAM bytes over algorithmic bytes)
+PROFILES = {'basis': {'bf16x3': 'basis_passes_c2_r128_bf16x3.md'},
+            'gemm': {'bf16x3': 'umma_cplx_kernel_c2_r192_bf16x3.md', 'f16': 'umma_cplx_kernel_c2_r128.md',
+                     'bf16': 'umma_cplx_kernel_c2_r128.md'}}
+BASIS_DEFAULT = 'basis_passes_c2_r128.md'
+
+
+def traffic_ratios(form):
+    """Measured DRAM bytes over algorithmic bytes of the form's basis series and GEMM, from the committed ncu
+    summaries (lines 'traffic_ratio: X'); returns ({kernel: ratio}, {kernel: summary file})."""
+    out, src = {}, {}
+    names = dict(basis=PROFILES['basis'].get(form, BASIS_DEFAULT), gemm=PROFILES['gemm'].get(form))
+    for key, name in names.items():
+        if name is None:
+            continue
         try:
             for ln in open(os.path.join(ROOT, 'profiles', name)):
                 if ln.startswith('traffic_ratio:'):
                     out[key] = float(ln.split(':')[1])
+                    src[key] = 'profiles/' + name
         except OSError:
             pass
-    return out
+    return out, src
 
 
 def form_config(form, autotune=False):
@@ -464,23 +476,24 @@ def run_c2(a):
     main_form = forms[0]
     R = results[main_form]
     peaks, kind = peaks_file()
-    ratios = traffic_ratios()
-    # dominant kernel: the fused basis series (basis_pass1_w + basis_pass2_p, one call per (tile, segment)), HBM-bound
+    ratios, rsrc = traffic_ratios(main_form)
+    # dominant kernel: the fused basis series (pass 1 + pass 2, one call per (tile, segment)), HBM-bound
     hbm = peaks.get('hbm_gbs', 6650.0)
     b_ach = R['basis_bytes'] / (R['basis_ms'] / 1e3) / 1e9
     b_tr = ratios.get('basis') and ratios['basis'] * R['basis_bytes']
-    roof = dict(kernel='basis series: basis_pass1_w + basis_pass2_p (%s)' % main_form, bound='hbm', achieved=b_ach,
+    p2 = 'basis_pass2 (per row)' if main_form == 'bf16x3' else 'basis_pass2_p'
+    roof = dict(kernel='basis series: basis_pass1_w + %s (%s)' % (p2, main_form), bound='hbm', achieved=b_ach,
                 peak=hbm, unit='GB/s', frac=b_ach / hbm, traffic=b_tr, bytes_per_call=R['basis_bytes'],
                 avg_call_ms=R['basis_ms'], calls=R['n_gemm'], share_of_step=R['basis_total_ms'] / R['ms'],
                 peak_kind='%s hbm copy' % kind,
-                traffic_source='profiles/basis_passes_c2_r128.md (dram bytes / algorithmic bytes, scaled)')
+                traffic_source='%s (dram bytes / algorithmic bytes, scaled)' % rsrc.get('basis'))
     # the fused GEMM, timed inside a seconds-long step: against the sustained bf16 peak (the burst one beside it)
     ach = R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
     pk = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops', 1590.0)) if main_form != 'f32' else None
     pkb = peaks.get('bf16_tflops') if main_form != 'f32' else None
     g_tr = ratios.get('gemm') and ratios['gemm'] * R['z_bytes']
-    gname = {'f16': 'umma_cplx2_kernel (f16, CTA pairs)', 'bf16': 'umma_cplx2_kernel (bf16, CTA pairs)',
-             'f32': 'simt_absmax_kernel'}.get(main_form, 'umma_cplx_kernel (%s)' % main_form)
+    gname = {'f32': 'simt_absmax_kernel'}.get(main_form, 'umma_cplx_kernel / umma_cplx2_kernel (%s, the launch '
+                                                         'shape the autotuner picked per Kh)' % main_form)
     roof_gemm = dict(kernel=gname,
                      bound='tensor', achieved=ach, peak=pk, unit='TFLOP/s', frac=(ach / pk) if pk else None,
                      frac_of_burst=(ach / pkb) if pkb else None,
@@ -488,7 +501,7 @@ def run_c2(a):
                      issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
                      launches=R['n_gemm'], share_of_step=R['gemm_total_ms'] / R['ms'],
                      peak_kind='%s sustained bf16 (cuBLAS loop under the power cap)' % kind,
-                     traffic_source='profiles/umma_cplx2_kernel_c2_r128.md (dram bytes / Z bytes, scaled)')
+                     traffic_source='%s (dram bytes / Z bytes, scaled)' % rsrc.get('gemm'))
     fp32 = results.get('f32')
     line = dict(metric=METRIC, value=R['value'], unit=UNIT, n_gpus=world, steps=a.steps,
                 warmup=a.warmup, ms_per_step=R['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,

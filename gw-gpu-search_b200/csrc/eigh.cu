@@ -10,6 +10,10 @@
 // block sums); when |gamma| > tol sqrt(alpha beta), zeta = (beta - alpha) / (2 |gamma|), t = sign(zeta) / (|zeta| +
 // sqrt(1 + zeta^2)), c = 1 / sqrt(1 + t^2), s = c t gamma / |gamma|, and u_p <- c u_p - conj(s) u_q, u_q <- s u_p +
 // c u_q (the same for v), which makes u_p^H u_q zero. The caller repeats sweeps until a sweep rotates nothing.
+// Columns whose norm is below `floor` (an absolute norm, about 1e-12 of the largest column of G) are numerically null:
+// U = G V holds only to rounding error eps ||G||, so their directions are noise and no rotation can make them
+// orthogonal to a relative 1e-13; pairs with such a column are not rotated (V stays unitary, their eigenvalues are the
+// noise-level column norms).
 #include "common.cuh"
 
 namespace gwb {
@@ -21,7 +25,8 @@ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_doub
 
 __global__ void __launch_bounds__(kEigThreads) jacobi_round_kernel(double2* __restrict__ U, double2* __restrict__ V,
                                                                     const int* __restrict__ nv, int ld, long long mstride,
-                                                                    int round, double tol, int* __restrict__ rotated) {
+                                                                    int round, double tol, double floor2,
+                                                                    int* __restrict__ rotated) {
     __shared__ double red[3][kEigThreads / 32];
     __shared__ double coef[4];
     const int mat = blockIdx.y, j = blockIdx.x;
@@ -77,7 +82,7 @@ __global__ void __launch_bounds__(kEigThreads) jacobi_round_kernel(double2* __re
             Gi += redi[w];
         }
         const double g = sqrt(Gr * Gr + Gi * Gi);
-        if (g > tol * sqrt(A * Bv) && g > 0.0) {
+        if (g > tol * sqrt(A * Bv) && g > 0.0 && A > floor2 && Bv > floor2) {
             const double zeta = (Bv - A) / (2.0 * g);
             const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
             const double c = 1.0 / sqrt(1.0 + t * t);
@@ -142,12 +147,13 @@ __global__ void identity_kernel(double2* __restrict__ V, const int* __restrict__
 
 extern "C" {
 
-int gwb_eigh_jacobi_sweep(double* U, double* V, const int* n, int nmat, int ld, int init, double tol, int* rotated,
-                          void* stream) {
+int gwb_eigh_jacobi_sweep(double* U, double* V, const int* n, int nmat, int ld, int init, double tol, double floor,
+                          int* rotated, void* stream) {
     using namespace gwb;
     GWB_CHECK_ARG(U && V && n && rotated, GWB_ERR_ARG, "eigh_jacobi_sweep: null pointer");
-    GWB_CHECK_ARG(nmat > 0 && nmat < 65536 && ld >= 2 && ld <= kEigThreads && tol > 0.0, GWB_ERR_SHAPE,
-                  "eigh_jacobi_sweep: nmat=%d ld=%d (2..%d) tol=%g", nmat, ld, kEigThreads, tol);
+    GWB_CHECK_ARG(nmat > 0 && nmat < 65536 && ld >= 2 && ld <= kEigThreads && tol > 0.0 && floor >= 0.0,
+                  GWB_ERR_SHAPE, "eigh_jacobi_sweep: nmat=%d ld=%d (2..%d) tol=%g floor=%g", nmat, ld, kEigThreads, tol,
+                  floor);
     cudaStream_t s = (cudaStream_t)stream;
     const long long ms = (long long)ld * ld;
     double2* u = reinterpret_cast<double2*>(U);
@@ -159,7 +165,8 @@ int gwb_eigh_jacobi_sweep(double* U, double* V, const int* n, int nmat, int ld, 
     GWB_CUDA(cudaMemsetAsync(rotated, 0, sizeof(int), s));
     const int ne = ld + (ld & 1);
     for (int r = 0; r < ne - 1; ++r) {
-        jacobi_round_kernel<<<dim3(ne / 2, nmat), kEigThreads, 0, s>>>(u, v, n, ld, ms, r, tol, rotated);
+        jacobi_round_kernel<<<dim3(ne / 2, nmat), kEigThreads, 0, s>>>(u, v, n, ld, ms, r, tol, floor * floor,
+                                                                        rotated);
         GWB_LAUNCH_CHECK("jacobi_round_kernel");
     }
     return GWB_OK;

@@ -82,7 +82,7 @@ SIGNATURES = {
     'gwb_sigma2': [_P, _LL, _I, _P, _LL, _I, _I, _I, _D, _P, _LL, _P, _LL, _P],
     'gwb_sigma2_noalloc': [_P, _LL, _I, _P, _LL, _I, _I, _I, _D, _P, _LL, _P],
     'gwb_gram': [_P, _LL, _I, _P, _I, _I, _P, _LL, _P, _P],
-    'gwb_eigh_jacobi_sweep': [_P, _P, _P, _I, _I, _I, _D, _P, _P],
+    'gwb_eigh_jacobi_sweep': [_P, _P, _P, _I, _I, _I, _D, _D, _P, _P],
     'gwb_eigh_values': [_P, _P, _I, _I, _P, _P],
     'gwb_basis_vh': [_P, _LL, _I, _I, _P, _LL, _P, _I, _I, _P, _LL, _P],
     'gwb_taylorf2': [_P, _P, _P, _P, _P, _P, _I, _D, _I, _I, _D, _P, _LL, _P],

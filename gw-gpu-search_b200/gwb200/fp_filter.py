@@ -59,21 +59,24 @@ def gram(H, sw, kmin):
     return G
 
 
-EIGH_TOL, EIGH_SWEEPS = 1e-13, 40
+# rotation threshold (cosine of a column pair), null-column floor (relative to the largest column of G), sweep limit
+EIGH_TOL, EIGH_FLOOR, EIGH_SWEEPS = 1e-13, 1e-12, 40
 
 
 def eigh_device(Gn):
     """Eigenvalues (descending, float64 numpy) and eigenvectors (columns, complex128 numpy) of a Hermitian positive
     semi-definite matrix (n <= 256, complex128 CUDA tensor) by the device's one-sided Jacobi in float64
-    (gwb_eigh_jacobi_sweep: sweeps until one rotates no pair with cosine above EIGH_TOL)."""
+    (gwb_eigh_jacobi_sweep: sweeps until one rotates no pair with cosine above EIGH_TOL; columns below EIGH_FLOOR of
+    the largest column of G are numerically null and not rotated)."""
     n = Gn.shape[0]
     U = Gn.transpose(0, 1).contiguous()                 # column-major: U[j, i] = G[i, j]
     V = torch.empty_like(U)
     nv = torch.tensor([n], dtype=torch.int32, device=Gn.device)
     rot = torch.zeros(1, dtype=torch.int32, device=Gn.device)
+    floor = EIGH_FLOOR * float(torch.linalg.vector_norm(Gn, dim=0).max().item())
     for sweep in range(EIGH_SWEEPS):
         _lib.call('gwb_eigh_jacobi_sweep', _lib.ptr(U), _lib.ptr(V), _lib.ptr(nv), 1, n, int(sweep == 0),
-                  EIGH_TOL, _lib.ptr(rot), _s())
+                  EIGH_TOL, floor, _lib.ptr(rot), _s())
         if int(rot.item()) == 0:
             break
     else:

@@ -233,10 +233,11 @@ GWB_API int gwb_gram(const float* H, long long ldh, int n, const float* sw, int 
  * one-sided Jacobi on the device: nmat matrices of n[m] <= ld <= 256 rows, stored column-major complex128 in U
  * (U[(m ld + j) ld + i] = G_m[i, j]); one call runs one sweep (every column pair rotated once, n - 1 rounds of n/2
  * disjoint pairs) over U and V (V set to the identity when init != 0); *rotated counts the pairs rotated (cosine
- * above tol), 0 when the sweep found U's columns orthogonal. Then G_m V_m = U_m: the eigenvectors are V's columns and
- * gwb_eigh_values gives the eigenvalues, lam[m ld + j] = ||U_m[:, j]|| (unsorted). */
+ * above tol, both column norms above floor: columns below it, about 1e-12 of the largest, are numerically null), 0 when
+ * the sweep found U's columns orthogonal. Then G_m V_m = U_m: the eigenvectors are V's columns and gwb_eigh_values
+ * gives the eigenvalues, lam[m ld + j] = ||U_m[:, j]|| (unsorted). */
 GWB_API int gwb_eigh_jacobi_sweep(double* U, double* V, const int* n, int nmat, int ld, int init, double tol,
-                                  int* rotated, void* stream);
+                                  double floor, int* rotated, void* stream);
 GWB_API int gwb_eigh_values(const double* U, const int* n, int nmat, int ld, double* lam, void* stream);
 /* Basis filters (svd_tile, fp_filter.py:589-591): Vh[j, k] = sum_i Bm[j, i] H[i, k] sw[k] for k >= kmin, else 0;
  * Bm (r x n complex64). */

@@ -103,8 +103,9 @@ def basis(a):
         # HBM bytes of the fused form when W stays in L2: Vh read and Z written (D isw stays in L2)
         out[f'us_per_row_fused_w{fws.wrows}'] = msf * 1e3 / r
         out[f'hbm_gbs_w{fws.wrows}'] = r * (8 * flen + zb) / msf / 1e6
-    if tlen == fp_filter.RING_N:
-        ref, ref_scale = Z.double() * fws.scale.double(), fws.scale.double()
+    full = (lambda: Z.double() + Zlo.double()) if Zlo is not None else (lambda: Z.double())
+    if tlen == fp_filter.RING_N and a.ring_cfgs:
+        ref = full() * fws.scale.double()
         for rc in [tuple(int(v) for v in x.split(':')) for x in a.ring_cfgs.split(',')]:
             _lib.call('gwb_basis_ring_set_config', *rc)
             rws = fp_filter.FusedBasisWorkspace(tlen, flen, r, ring=True)
@@ -113,7 +114,7 @@ def basis(a):
             tag = 'ring_%d_%d_%d' % rc
             out['us_per_row_' + tag] = msr * 1e3 / r
             # the ring form's scale comes from pc rows instead of 64: compare the series times their scales
-            got = Z.double() * rws.scale.double()
+            got = full() * rws.scale.double()
             out['max_rel_vs_two_pass_' + tag] = float(((got - ref).abs().max() / ref.abs().max()).item())
             del rws
         _lib.call('gwb_basis_ring_set_config', 2, 3, 1)
@@ -568,7 +569,8 @@ def main():
     ap.add_argument('--stages', default='0', help='gemm: comma list of Z ring depths (0: the most that fit)')
     ap.add_argument('--orders', default='0', help='gemm: comma list of MMA orders of the CTA-pair kernel (0-3)')
     ap.add_argument('--ring-cfgs', default='2:3:1,2:4:2,4:2:1,2:3:0,2:2:0,4:2:0,1:4:0',
-                    help='basis: comma list of rows:slots:lookahead of the persistent ring form (2^20)')
+                    help='basis: comma list of rows:slots:lookahead of the persistent ring form (2^20; empty: '
+                         'none)')
     a = ap.parse_args()
     print(json.dumps({'gemm': gemm, 'basis': basis, 'exact': exact, 'adjoint': adjoint, 'c4': c4}[a.what](a)))
 
