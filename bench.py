@@ -487,8 +487,10 @@ def run_c2(a):
                 avg_call_ms=R['basis_ms'], calls=R['n_gemm'], share_of_step=R['basis_total_ms'] / R['ms'],
                 peak_kind='%s hbm copy' % kind,
                 traffic_source='%s (dram bytes / algorithmic bytes, scaled)' % rsrc.get('basis'))
-    # the fused GEMM, timed inside a seconds-long step: against the sustained bf16 peak (the burst one beside it)
-    ach = R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
+    # the fused GEMM, timed inside a seconds-long step: against the sustained bf16 peak (the burst one beside it).
+    # Algorithmic flop of a launch: 8 n r Tn per product (the split form computes three), without the K padding
+    nprod = {'bf16x3': 3}.get(main_form, 1)
+    ach = nprod * R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
     pk = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops', 1590.0)) if main_form != 'f32' else None
     pkb = peaks.get('bf16_tflops') if main_form != 'f32' else None
     g_tr = ratios.get('gemm') and ratios['gemm'] * R['z_bytes']
@@ -497,7 +499,9 @@ def run_c2(a):
     roof_gemm = dict(kernel=gname,
                      bound='tensor', achieved=ach, peak=pk, unit='TFLOP/s', frac=(ach / pk) if pk else None,
                      frac_of_burst=(ach / pkb) if pkb else None,
-                     traffic=g_tr, flops_per_launch_useful=R['useful'], flops_per_launch_issued=R['issued'],
+                     traffic=g_tr, products=nprod, flops_per_launch_algorithmic=nprod * R['useful'],
+                     flops_per_launch_useful=R['useful'], flops_per_launch_issued=R['issued'],
+                     useful_tflops=R['useful'] / (R['gemm_ms'] / 1e3) / 1e12,
                      issued_tflops=R['issued'] / (R['gemm_ms'] / 1e3) / 1e12, avg_launch_ms=R['gemm_ms'],
                      launches=R['n_gemm'], share_of_step=R['gemm_total_ms'] / R['ms'],
                      peak_kind='%s sustained bf16 (cuBLAS loop under the power cap)' % kind,
