@@ -593,6 +593,93 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
     }
 }
 
+// Pass 2 over row chunks with TBW = 16 columns per CTA (two adjacent W blocks, 128 KB contiguous). Each Z store
+// instruction of a warp covers two runs of 16 consecutive samples (32 bytes for 16-bit Z: whole L2 sectors) instead
+// of four runs of 8, halving the write requests of the pass, which bound it with four 16-bit planes. One CTA of
+// 16 R2 threads per SM (the tile and exchange buffer take 135 KB). Thread index bits: step 1 (c, b) with
+// c = (t & 7) + 8 ((t >> 4) & 1), b = ((t >> 3) & 1) + 2 (t >> 5), so a half-warp reads 16 consecutive tile words;
+// step 2 (c2, u) with the same c and u = ((t >> 3) & 1) + 2 (t >> 5); SC = 2 (mod 16) keeps both exchange accesses
+// free of bank conflicts.
+constexpr int TBW = 16;
+
+template <int N2>
+struct SplitW {
+    using S = Split<N2, 2>;
+    static constexpr int R1 = S::R1, R2 = S::R2, SB = S::SB;
+    static constexpr int NT = TBW * R2;
+    static constexpr int SC = R2 * SB + ((2 - (R2 * SB) % 16) + 16) % 16;
+    static_assert(R1 == R2, "the 16-column pass 2 is for square splits (N2 = 1024, 256, 64)");
+    static_assert(SC >= N2, "the exchange buffer holds the W tile");
+};
+
+template <int N2, int FORM>
+__global__ void __launch_bounds__(SplitW<N2>::NT, 1) basis_pass2_w(
+    const float2* __restrict__ W, int rows, int N, int N1, const float2* __restrict__ tw, int a0, int Tn,
+    const float* __restrict__ scale, void* __restrict__ Z, void* __restrict__ Zlo, long long ldz, int im_off,
+    int row0) {
+    using S = SplitW<N2>;
+    constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC;
+    constexpr int ES = FORM == 1 ? 4 : (FORM == 4 ? 1 : 2);   // bytes per Z element
+    constexpr int CP = TBW * N2 * 8 / 16 / NT;   // 16-byte copies per thread per tile
+    extern __shared__ float2 sm[];
+    float2* Bt = sm;                              // W tile (two blocks of TB columns), then the exchange tile
+    float2* tw2 = Bt + TBW * SC;                  // tw2[u R2 + b] = e^{2 pi i b u / N2}
+    const int tid = threadIdx.x, t10 = blockIdx.x * TBW;
+    const int j0 = blockIdx.y * RC, j1 = min(j0 + RC, rows);
+    auto fetch = [&](int j) {
+        const char* g = reinterpret_cast<const char*>(W + (long long)j * N + (long long)blockIdx.x * (N2 * TBW));
+        char* d = reinterpret_cast<char*>(Bt);
+#pragma unroll
+        for (int i = 0; i < CP; ++i) cp_async16(d + (i * NT + tid) * 16, g + (i * NT + tid) * 16);
+        cp_async_commit();
+    };
+    fetch(j0);
+    for (int e = tid; e < N2; e += NT) tw2[e] = tw[(e % R2) * (e / R2) * (N / N2)];
+    const float inv0 = FORM == 4 ? 0.f : 1.0f / *scale;    // fp8: scale holds one scale per row
+    const int c = (tid & 7) + 8 * ((tid >> 4) & 1);
+    const int lo = (tid >> 3) & 1, hi = tid >> 5;
+    const int b = lo + 2 * hi;                    // step 1: b < R2
+    const int u2 = lo + 2 * hi;                   // step 2: u < R1 (= R2)
+    const int cblk = (c >> 3) * (N2 * TB) + (c & 7);
+    char* zb = static_cast<char*>(Z);
+    char* zl = static_cast<char*>(Zlo);
+    for (int j = j0; j < j1; ++j) {
+        const float inv = FORM == 4 ? 1.0f / scale[j] : inv0;
+        cp_async_wait_all();
+        __syncthreads();
+        float2 x[R1];
+#pragma unroll
+        for (int a = 0; a < R1; ++a) x[a] = Bt[cblk + (R2 * a + b) * TB];
+        __syncthreads();
+        dft_reg<R1>(x);
+        static_for<R1>([&](auto U) {
+            constexpr int u = decltype(U)::value;
+            Bt[c * SC + b * SB + u] = cmul(x[brev(u, ilog2(R1))], tw2[u * R2 + b]);
+        });
+        __syncthreads();
+        float2 y[R2];
+#pragma unroll
+        for (int bb = 0; bb < R2; ++bb) y[bb] = Bt[c * SC + bb * SB + u2];
+        __syncthreads();
+        if (j + 1 < j1) fetch(j + 1);
+        const long long re_off = (long long)(row0 + j) * ldz * ES, im_off_b = (long long)(im_off + row0 + j) * ldz * ES;
+        void* Zr = zb + re_off;
+        void* Zi = zb + im_off_b;
+        void* Zlr = FORM == 2 ? (void*)(zl + re_off) : nullptr;
+        void* Zli = FORM == 2 ? (void*)(zl + im_off_b) : nullptr;
+        dft_reg<R2>(y);
+        const int t0 = t10 + c + N1 * u2 - a0;
+        static_for<R2>([&](auto V) {
+            constexpr int vv = decltype(V)::value;
+            const int t = t0 + N1 * (R1 * vv);
+            if (t >= 0 && t < Tn) {
+                const float2 z = y[brev(vv, ilog2(R2))];
+                store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * inv, z.y * inv);
+            }
+        });
+    }
+}
+
 // ---------------------------------------------------------------------------------------------------------------------
 // Persistent form of the two passes for N = 2^20 (N1 = N2 = 1024): W stays in L2.
 // Rows go in chunks of pc rows through a ring of nslot slots of W (pc rows of N each). Work items, taken in order from
@@ -1000,9 +1087,37 @@ int launch_pass2_p(const float2* W, int N, int N1, int rows, const float2* tw, i
     return GWB_OK;
 }
 
+template <int N2, int FORM>
+int launch_pass2_w(const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn, const float* scale,
+                   void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
+    using S = SplitW<N2>;
+    const size_t smem = (size_t)(TBW * S::SC + N2) * sizeof(float2);
+    auto k = basis_pass2_w<N2, FORM>;
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<dim3(N1 / TBW, (rows + RC - 1) / RC), S::NT, smem, s>>>(W, rows, N, N1, tw, a0, Tn, scale, Z, Zlo, ldz,
+                                                                 im_off, row0);
+    GWB_LAUNCH_CHECK("basis_pass2_w");
+    return GWB_OK;
+}
+
+// columns per pass-2 CTA at N2 = 1024 (gwb_basis_set_pass2_columns): 8 (basis_pass2_p, or the per-row kernel for
+// the split form) or 16 (basis_pass2_w)
+std::atomic<int> g_pass2_cols{8};
+
 template <int N2>
 int launch_pass2(int form, const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn,
                  const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
+    if constexpr (N2 == 1024) {
+        if (g_pass2_cols.load() == 16) {
+            switch (form) {
+                case 0: return launch_pass2_w<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+                case 1: return launch_pass2_w<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+                case 2: return launch_pass2_w<N2, 2>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+                case 3: return launch_pass2_w<N2, 3>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+                default: return launch_pass2_w<N2, 4>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+            }
+        }
+    }
     // row-chunk form for the long transforms; the split bf16 form (four Z planes) runs faster on the per-row kernel
     // (measured at N = 2^20, r = 128: 8.3 against 10.6 us per row)
     if constexpr (N2 >= 512) {
@@ -1070,6 +1185,15 @@ int gwb_basis_ring_set_config(int pc, int nslot, int look) {
     g_ring_look.store(look);
     return GWB_OK;
 }
+
+int gwb_basis_set_pass2_columns(int cols) {
+    using namespace gwb;
+    GWB_CHECK_ARG(cols == 8 || cols == 16, GWB_ERR_ARG, "basis_set_pass2_columns: cols=%d (8 or 16)", cols);
+    g_pass2_cols.store(cols);
+    return GWB_OK;
+}
+
+int gwb_basis_pass2_columns(void) { return gwb::g_pass2_cols.load(); }
 
 int gwb_basis_ring_rows(void) { return gwb::g_ring_pc.load() * gwb::g_ring_nslot.load(); }
 

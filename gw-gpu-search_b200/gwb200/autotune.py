@@ -92,13 +92,13 @@ def tune_gemm(form, n, Kh, Tn, group=16, reps=3, device='cuda'):
 
 
 def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
-    """Times the basis-series forms for r rows of length tlen: the ring (tlen = 2^20) and two passes with W for all
-    rows or in batches of 32; returns (best: dict(ring, wrows), {candidate: ms})."""
+    """Times the basis-series forms for r rows of length tlen: the ring (tlen = 2^20, RING_CONFIGS) and two passes with
+    W for all rows or in batches of 32, with 8 or 16 columns per pass-2 CTA (16 at tlen = 2^20 only); sets the fastest
+    and returns (best: dict(ring, wrows, ring_config, pass2_cols), {candidate: ms})."""
     key = (torch.cuda.get_device_name(device), 'basis', int(tlen), int(r), form)
     if key in _CACHE:
         out = _CACHE[key]
-        if out[0]['ring_config'] is not None:
-            _lib.call('gwb_basis_ring_set_config', *out[0]['ring_config'])
+        _apply_basis(out[0])
         return out
     flen = tlen // 2 + 1
     g = torch.Generator(device=device).manual_seed(2)
@@ -111,24 +111,30 @@ def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
     Zlo = torch.zeros_like(Z) if form == 'bf16x3' else None
     Vp = fp_filter.fourstep_order(Vh, tlen)
     Dp = fp_filter.fourstep_order(D, tlen, isw)
-    cands = [(False, None, None), (False, 32, None)]
+    cands = [(False, None, None, 8), (False, 32, None, 8)]
     if tlen == fp_filter.RING_N:
-        cands = [(True, None, rc) for rc in RING_CONFIGS] + cands
+        cands = ([(True, None, rc, 8) for rc in RING_CONFIGS] + cands +
+                 [(False, None, None, 16), (False, 32, None, 16)])
     res, best = {}, None
-    for ring, wrows, rc in cands:
-        if rc is not None:
-            _lib.call('gwb_basis_ring_set_config', *rc)
+    for ring, wrows, rc, cols in cands:
+        _apply_basis(dict(ring_config=rc, pass2_cols=cols))
         ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, device=device, wrows=wrows, ring=ring)
         ms = _events_ms(lambda: fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo, form, im_off=Kh), reps)
-        res[(ring, wrows, rc)] = ms
+        res[(ring, wrows, rc, cols)] = ms
         if best is None or ms < res[best]:
-            best = (ring, wrows, rc)
+            best = (ring, wrows, rc, cols)
         del ws
-    if best[2] is not None:
-        _lib.call('gwb_basis_ring_set_config', *best[2])
-    out = (dict(ring=best[0], wrows=best[1], ring_config=best[2]), res)
+    out = (dict(ring=best[0], wrows=best[1], ring_config=best[2], pass2_cols=best[3]), res)
+    _apply_basis(out[0])
     _CACHE[key] = out
     return out
+
+
+def _apply_basis(choice):
+    """Sets a basis-series choice's process-wide knobs in the library (ring configuration, pass-2 columns)."""
+    if choice.get('ring_config') is not None:
+        _lib.call('gwb_basis_ring_set_config', *choice['ring_config'])
+    _lib.call('gwb_basis_set_pass2_columns', int(choice.get('pass2_cols') or 8))
 
 
 def tune_filter(bank, tlen, Tn, form, group, device='cuda'):

@@ -295,6 +295,11 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
                             float* W, int wrows, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz,
                             int im_off, int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket,
                             float* scale, float* rowscale, float* rowpart, long long rowpart_elems, void* stream);
+/* Columns of the transform per pass-2 CTA of gwb_basis_fused at N = 2^20, process-wide: 8 (default; a CTA writes runs
+ * of 8 consecutive Z samples) or 16 (runs of 16: whole 32-byte sectors for 16-bit Z, half the write requests, one
+ * 512-thread CTA per SM). Same results either way; the autotuner times both. */
+GWB_API int gwb_basis_set_pass2_columns(int cols);
+GWB_API int gwb_basis_pass2_columns(void);
 /* The same basis series for N = 2^20 in one persistent launch that keeps W in L2 (same reference call,
  * fp_filter.py:597-613): rows go in chunks of pc through a ring of nslot slots of W (pc x nslot rows of N complex,
  * 128-byte aligned; wrows = the rows W holds), pass 1 running `look` chunks ahead of pass 2; each W tile's L2 lines
@@ -303,8 +308,8 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
  * items earlier in that order. The scale is the Parseval rms of the first chunk's rows (min(pc, rows) rows) instead
  * of min(nfirst, wrows) rows. partials: >= 1024 doubles; sync: gwb_basis_ring_sync_ints(rows) int32, cleared by the
  * call on the stream; fp8: rowpart >= rows x 1024 floats, rowscale rows floats. Other arguments as gwb_basis_fused.
- * gwb_basis_ring_set_config sets (pc in 1..4, nslot > look, look >= 1) process-wide (default 2, 3, 1; the autotuner
- * times the choices); gwb_basis_ring_rows and gwb_basis_ring_sync_ints size W and sync for the current one. */
+ * gwb_basis_ring_set_config sets (pc in 1..4, nslot > look, look >= 0; 0 splits the grid into pass-1 and pass-2
+ * CTAs) process-wide (default 2, 3, 1; the autotuner times the choices); gwb_basis_ring_rows and gwb_basis_ring_sync_ints size W and sync for the current one. */
 GWB_API int gwb_basis_ring_set_config(int pc, int nslot, int look);
 GWB_API int gwb_basis_ring_rows(void);
 GWB_API int gwb_basis_ring_sync_ints(int rows);

@@ -208,6 +208,41 @@ def test_ring_basis_series_16bit_forms(form):
     assert err.max() < {'f16': 1e-3, 'bf16': 8e-3, 'bf16x3': 3e-5}[form], err.max()
 
 
+@pytest.mark.parametrize('form', ['f16', 'bf16', 'bf16x3', 'f32', 'fp8'])
+def test_pass2_sixteen_columns_bit_identical(form):
+    """The 16-column pass 2 (gwb_basis_set_pass2_columns(16)) writes the same Z bits as the 8-column kernels at
+    N = 2^20, for every Z encoding, with rows that end mid-chunk (r = 11) and an analysed span that starts and ends
+    inside a column block."""
+    from gwb200 import _lib, fp_filter
+    tlen = 1 << 20
+    rng = np.random.default_rng(8)
+    flen = tlen // 2 + 1
+    r = 11
+    Vh = (rng.standard_normal((r, flen)) + 1j * rng.standard_normal((r, flen))).astype(np.complex64)
+    D = (rng.standard_normal(flen) + 1j * rng.standard_normal(flen)).astype(np.complex64)
+    isw = rng.uniform(0.5, 2, flen).astype(np.float32)
+    a0, Tn = 98304 + 8, 917504 - 24
+    Kh = fp_filter.kh_of(r, form)
+    dt = fp_filter._z_dtype(form)
+    Vp = fp_filter.fourstep_order(torch.from_numpy(Vh).cuda(), tlen)
+    Dp = fp_filter.fourstep_order(torch.from_numpy(D).cuda(), tlen, torch.from_numpy(isw).cuda())
+    out = {}
+    try:
+        for cols in (8, 16):
+            _lib.call('gwb_basis_set_pass2_columns', cols)
+            ws = fp_filter.FusedBasisWorkspace(tlen, flen, r)
+            Z = torch.full((2 * Kh, -(-Tn // 16) * 16), 7 if dt == torch.uint8 else 3.0, dtype=dt, device='cuda')
+            Zlo = torch.full_like(Z, 5.0) if form == 'bf16x3' else None
+            fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo, form, im_off=Kh)
+            out[cols] = [Z.cpu()] + ([Zlo.cpu()] if Zlo is not None else []) + [ws.scale.cpu()]
+            if form == 'fp8':
+                out[cols].append(ws.rowscale[:r].cpu())
+    finally:
+        _lib.call('gwb_basis_set_pass2_columns', 8)
+    for x, y in zip(out[8], out[16]):
+        assert torch.equal(x.view(torch.uint8), y.view(torch.uint8))
+
+
 @pytest.mark.parametrize('n,spread', [(64, 6), (248, 12), (256, 14)])
 def test_device_jacobi_eigh_matches_lapack(n, spread):
     """The device's one-sided Jacobi (fp_filter.eigh_device, float64) against LAPACK on Hermitian positive
