@@ -1100,9 +1100,10 @@ int launch_pass2_w(const float2* W, int N, int N1, int rows, const float2* tw, i
     return GWB_OK;
 }
 
-// columns per pass-2 CTA at N2 = 1024 (gwb_basis_set_pass2_columns): 8 (basis_pass2_p, or the per-row kernel for
-// the split form) or 16 (basis_pass2_w)
-std::atomic<int> g_pass2_cols{8};
+// columns per pass-2 CTA at N2 = 1024 (gwb_basis_set_pass2_columns): 16 (basis_pass2_w, the default: measured at
+// r = 128, 5.3 against 6.0 us per row for fp16 Z and 6.1 against 8.6 for split bf16) or 8 (basis_pass2_p, or the
+// per-row kernel for the split form)
+std::atomic<int> g_pass2_cols{16};
 
 template <int N2>
 int launch_pass2(int form, const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn,

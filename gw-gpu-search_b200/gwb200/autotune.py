@@ -111,10 +111,10 @@ def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
     Zlo = torch.zeros_like(Z) if form == 'bf16x3' else None
     Vp = fp_filter.fourstep_order(Vh, tlen)
     Dp = fp_filter.fourstep_order(D, tlen, isw)
-    cands = [(False, None, None, 8), (False, 32, None, 8)]
+    cands = [(False, None, None, 16), (False, 32, None, 16)]
     if tlen == fp_filter.RING_N:
-        cands = ([(True, None, rc, 8) for rc in RING_CONFIGS] + cands +
-                 [(False, None, None, 16), (False, 32, None, 16)])
+        cands = ([(True, None, rc, 16) for rc in RING_CONFIGS] + cands +
+                 [(False, None, None, 8), (False, 32, None, 8)])
     res, best = {}, None
     for ring, wrows, rc, cols in cands:
         _apply_basis(dict(ring_config=rc, pass2_cols=cols))
@@ -134,7 +134,7 @@ def _apply_basis(choice):
     """Sets a basis-series choice's process-wide knobs in the library (ring configuration, pass-2 columns)."""
     if choice.get('ring_config') is not None:
         _lib.call('gwb_basis_ring_set_config', *choice['ring_config'])
-    _lib.call('gwb_basis_set_pass2_columns', int(choice.get('pass2_cols') or 8))
+    _lib.call('gwb_basis_set_pass2_columns', int(choice.get('pass2_cols') or 16))
 
 
 def tune_filter(bank, tlen, Tn, form, group, device='cuda'):

@@ -103,7 +103,7 @@ def basis(a):
         for wr in [int(x) for x in a.wrows.split(',')]:
             fws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wr or None, ring=False)
             msf = _time(lambda: fp_filter.basis_series_fused(fws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
-            tag = f'w{fws.wrows}' + ('' if cols == 8 else f'_c{cols}')
+            tag = f'w{fws.wrows}_c{cols}'
             # HBM bytes of the fused form when W stays in L2: Vh read and Z written (D isw stays in L2)
             out['us_per_row_fused_' + tag] = msf * 1e3 / r
             out['hbm_gbs_' + tag] = r * (8 * flen + zb) / msf / 1e6
@@ -112,7 +112,7 @@ def basis(a):
                 first = got
             else:
                 out['bit_identical_' + tag] = all(torch.equal(x, y) for x, y in zip(got, first))
-    _lib.call('gwb_basis_set_pass2_columns', 8)
+    _lib.call('gwb_basis_set_pass2_columns', 16)
     full = (lambda: Z.double() + Zlo.double()) if Zlo is not None else (lambda: Z.double())
     if tlen == fp_filter.RING_N and a.ring_cfgs:
         ref = full() * fws.scale.double()
@@ -575,7 +575,7 @@ def main():
     ap.add_argument('--peaks', type=int, default=1)
     ap.add_argument('--reps', type=int, default=10)
     ap.add_argument('--wrows', default='0', help='basis: comma list of W row batches (0: all rows at once)')
-    ap.add_argument('--pass2-cols', default='8,16', help='basis: comma list of columns per pass-2 CTA (8, 16)')
+    ap.add_argument('--pass2-cols', default='16,8', help='basis: comma list of columns per pass-2 CTA (8, 16)')
     ap.add_argument('--pair', default='1', help='gemm: comma list, 1 CTA pairs, 0 one CTA per M block')
     ap.add_argument('--stages', default='0', help='gemm: comma list of Z ring depths (0: the most that fit)')
     ap.add_argument('--orders', default='0', help='gemm: comma list of MMA orders of the CTA-pair kernel (0-3)')

@@ -238,7 +238,7 @@ def test_pass2_sixteen_columns_bit_identical(form):
             if form == 'fp8':
                 out[cols].append(ws.rowscale[:r].cpu())
     finally:
-        _lib.call('gwb_basis_set_pass2_columns', 8)
+        _lib.call('gwb_basis_set_pass2_columns', 16)
     for x, y in zip(out[8], out[16]):
         assert torch.equal(x.view(torch.uint8), y.view(torch.uint8))
 
