@@ -481,9 +481,10 @@ def run_c2(a):
     hbm = peaks.get('hbm_gbs', 6650.0)
     b_ach = R['basis_bytes'] / (R['basis_ms'] / 1e3) / 1e9
     b_tr = ratios.get('basis') and ratios['basis'] * R['basis_bytes']
-    from gwb200 import _lib as glib
-    p2 = ('basis_pass2_w' if glib.load().gwb_basis_pass2_columns() == 16 else
-          'basis_pass2 (per row)' if main_form == 'bf16x3' else 'basis_pass2_p')
+    # the pass-2 kernel the headline form ran with: its tuned column count (the library default, 16, untuned)
+    tb = tunings.get(main_form)
+    cols = ((tb or {}).get('basis') or {}).get('best', {}).get('pass2_cols') or 16
+    p2 = 'basis_pass2_w' if cols == 16 else 'basis_pass2 (per row)' if main_form == 'bf16x3' else 'basis_pass2_p'
     roof = dict(kernel='basis series: basis_pass1_w + %s (%s)' % (p2, main_form), bound='hbm', achieved=b_ach,
                 peak=hbm, unit='GB/s', frac=b_ach / hbm, traffic=b_tr, bytes_per_call=R['basis_bytes'],
                 avg_call_ms=R['basis_ms'], calls=R['n_gemm'], share_of_step=R['basis_total_ms'] / R['ms'],
