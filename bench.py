@@ -540,7 +540,7 @@ def run_c2(a):
         import microbench
         try:
             ns = argparse.Namespace(segments=300, batch=32, seed=4, no_graph=False, production=False,
-                                    form='bf16x3', bank_obj=B, isw=isw)
+                                    form='bf16x3', bank_obj=B, isw=isw, autotune=not a.no_autotune)
             r4 = microbench.c4(ns)
             line['c4'] = {k: r4[k] for k in ('workload', 'value', 'unit', 'ms', 'analysed_s', 'chunks', 'batches',
                                              'one_graph', 'graph_capture_s', 'glitches', 'glitches_gated',
@@ -575,7 +575,8 @@ def run_c4(a):
         return
     # the batched form's configuration names the split-bf16 GEMM; --forms overrides it
     form = a.forms.split(',')[0] if a.forms_given else 'bf16x3'
-    ns = argparse.Namespace(segments=300, batch=32, seed=4, no_graph=False, production=a.production, form=form)
+    ns = argparse.Namespace(segments=300, batch=32, seed=4, no_graph=False, production=a.production, form=form,
+                            autotune=not a.no_autotune)
     r = microbench.c4(ns)
     print(json.dumps(dict(metric=METRIC, value=r['value'], unit=UNIT, n_gpus=1, steps=1, warmup=1,
                           ms_per_step=r['ms'], higher_is_better=True, scaling='weak', vs_baseline=None,
@@ -612,7 +613,7 @@ def main():
     ap.add_argument('--forms', default='bf16x3,f16,bf16,fp8,f32', help='forms timed (the first gives value)')
     ap.add_argument('--form-steps', type=int, default=3, help='timed steps of each form after the first')
     ap.add_argument('--production', action='store_true', help='c4: production selection and consolidation')
-    ap.add_argument('--no-autotune', action='store_true', help='c2: default launch shapes instead of tuned ones')
+    ap.add_argument('--no-autotune', action='store_true', help='c2, c4: default launch shapes instead of tuned ones')
     ap.add_argument('--no-c4', action='store_true', help='c2: skip the batched-form run reported under "c4"')
     a = ap.parse_args()
     a.forms_given = any(x == '--forms' or x.startswith('--forms=') for x in sys.argv[1:])

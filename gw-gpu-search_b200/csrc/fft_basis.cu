@@ -1100,16 +1100,16 @@ int launch_pass2_w(const float2* W, int N, int N1, int rows, const float2* tw, i
     return GWB_OK;
 }
 
-// columns per pass-2 CTA at N2 = 1024 (gwb_basis_set_pass2_columns): 16 (basis_pass2_w, the default: measured at
-// r = 128, 5.3 against 6.0 us per row for fp16 Z and 6.1 against 8.6 for split bf16) or 8 (basis_pass2_p, or the
-// per-row kernel for the split form)
-std::atomic<int> g_pass2_cols{16};
+// columns per pass-2 CTA at N2 = 1024, per Z encoding (gwb_basis_set_pass2_columns): 16 (basis_pass2_w, the default:
+// measured at r = 128, 5.3 against 6.0 us per row for fp16 Z and 6.1 against 8.6 for split bf16) or 8
+// (basis_pass2_p, or the per-row kernel for the split form)
+std::atomic<int> g_pass2_cols[5] = {{16}, {16}, {16}, {16}, {16}};
 
 template <int N2>
 int launch_pass2(int form, const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn,
                  const float* scale, void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
     if constexpr (N2 == 1024) {
-        if (g_pass2_cols.load() == 16) {
+        if (form >= 0 && form <= 4 && g_pass2_cols[form].load() == 16) {
             switch (form) {
                 case 0: return launch_pass2_w<N2, 0>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
                 case 1: return launch_pass2_w<N2, 1>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
@@ -1187,14 +1187,16 @@ int gwb_basis_ring_set_config(int pc, int nslot, int look) {
     return GWB_OK;
 }
 
-int gwb_basis_set_pass2_columns(int cols) {
+int gwb_basis_set_pass2_columns(int form, int cols) {
     using namespace gwb;
     GWB_CHECK_ARG(cols == 8 || cols == 16, GWB_ERR_ARG, "basis_set_pass2_columns: cols=%d (8 or 16)", cols);
-    g_pass2_cols.store(cols);
+    GWB_CHECK_ARG(form >= -1 && form <= 4, GWB_ERR_ARG, "basis_set_pass2_columns: form=%d (0-4, -1: all)", form);
+    for (int f = 0; f < 5; ++f)
+        if (form < 0 || f == form) g_pass2_cols[f].store(cols);
     return GWB_OK;
 }
 
-int gwb_basis_pass2_columns(void) { return gwb::g_pass2_cols.load(); }
+int gwb_basis_pass2_columns(int form) { return form >= 0 && form <= 4 ? gwb::g_pass2_cols[form].load() : -1; }
 
 int gwb_basis_ring_rows(void) { return gwb::g_ring_pc.load() * gwb::g_ring_nslot.load(); }
 

@@ -55,8 +55,8 @@ SIGNATURES = {
                              _LL, _P, _LL, _P],
     'gwb_basis_ring_set_config': [_I, _I, _I],
     'gwb_basis_ring_rows': [],
-    'gwb_basis_set_pass2_columns': [_I],
-    'gwb_basis_pass2_columns': [],
+    'gwb_basis_set_pass2_columns': [_I, _I],
+    'gwb_basis_pass2_columns': [_I],
     'gwb_basis_ring_sync_ints': [_I],
     'gwb_basis_pack': [_P, _LL, _I, _I, _I, _LL, _LL, _P, _I, _P, _P, _LL, _P],
     'gwb_stacked_a': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _I, _I, _P, _P, _P, _P, _LL, _P],

@@ -98,7 +98,7 @@ def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
     key = (torch.cuda.get_device_name(device), 'basis', int(tlen), int(r), form)
     if key in _CACHE:
         out = _CACHE[key]
-        _apply_basis(out[0])
+        _apply_basis(out[0], form)
         return out
     flen = tlen // 2 + 1
     g = torch.Generator(device=device).manual_seed(2)
@@ -117,7 +117,7 @@ def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
                  [(False, None, None, 8), (False, 32, None, 8)])
     res, best = {}, None
     for ring, wrows, rc, cols in cands:
-        _apply_basis(dict(ring_config=rc, pass2_cols=cols))
+        _apply_basis(dict(ring_config=rc, pass2_cols=cols), form)
         ws = fp_filter.FusedBasisWorkspace(tlen, flen, r, device=device, wrows=wrows, ring=ring)
         ms = _events_ms(lambda: fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo, form, im_off=Kh), reps)
         res[(ring, wrows, rc, cols)] = ms
@@ -125,16 +125,17 @@ def tune_basis(tlen, r, form='f16', reps=2, device='cuda'):
             best = (ring, wrows, rc, cols)
         del ws
     out = (dict(ring=best[0], wrows=best[1], ring_config=best[2], pass2_cols=best[3]), res)
-    _apply_basis(out[0])
+    _apply_basis(out[0], form)
     _CACHE[key] = out
     return out
 
 
-def _apply_basis(choice):
-    """Sets a basis-series choice's process-wide knobs in the library (ring configuration, pass-2 columns)."""
+def _apply_basis(choice, form):
+    """Sets a basis-series choice's knobs in the library: the ring configuration (process-wide) and the form's
+    pass-2 columns."""
     if choice.get('ring_config') is not None:
         _lib.call('gwb_basis_ring_set_config', *choice['ring_config'])
-    _lib.call('gwb_basis_set_pass2_columns', int(choice.get('pass2_cols') or 16))
+    _lib.call('gwb_basis_set_pass2_columns', fp_filter.FORMS[form], int(choice.get('pass2_cols') or 16))
 
 
 def tune_filter(bank, tlen, Tn, form, group, device='cuda'):

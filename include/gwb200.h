@@ -295,11 +295,12 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
                             float* W, int wrows, long long a0, long long Tn, int form, void* Z, void* Zlo, long long ldz,
                             int im_off, int row0, int nfirst, double* partials, long long npartials, uint32_t* ticket,
                             float* scale, float* rowscale, float* rowpart, long long rowpart_elems, void* stream);
-/* Columns of the transform per pass-2 CTA of gwb_basis_fused at N = 2^20, process-wide: 16 (default; a CTA writes
- * runs of 16 consecutive Z samples: whole 32-byte sectors for 16-bit Z, one 512-thread CTA per SM) or 8 (runs of 8,
- * twice the L2 write requests). Bit-identical results either way; the autotuner times both. */
-GWB_API int gwb_basis_set_pass2_columns(int cols);
-GWB_API int gwb_basis_pass2_columns(void);
+/* Columns of the transform per pass-2 CTA of gwb_basis_fused at N = 2^20, process-wide per Z form (0-4 as
+ * gwb_basis_fused's `form`; -1 sets every form): 16 (default; a CTA writes runs of 16 consecutive Z samples: whole
+ * 32-byte sectors for 16-bit Z, one 512-thread CTA per SM) or 8 (runs of 8, twice the L2 write requests).
+ * Bit-identical results either way; the autotuner times both. gwb_basis_pass2_columns returns a form's setting. */
+GWB_API int gwb_basis_set_pass2_columns(int form, int cols);
+GWB_API int gwb_basis_pass2_columns(int form);
 /* The same basis series for N = 2^20 in one persistent launch that keeps W in L2 (same reference call,
  * fp_filter.py:597-613): rows go in chunks of pc through a ring of nslot slots of W (pc x nslot rows of N complex,
  * 128-byte aligned; wrows = the rows W holds), pass 1 running `look` chunks ahead of pass 2; each W tile's L2 lines

@@ -99,7 +99,7 @@ def basis(a):
     zb = 2 * Tn * {'f16': 2, 'bf16': 2, 'fp8': 1}.get(a.form, 4)
     first = None
     for cols in [int(x) for x in a.pass2_cols.split(',')]:
-        _lib.call('gwb_basis_set_pass2_columns', cols)
+        _lib.call('gwb_basis_set_pass2_columns', -1, cols)
         for wr in [int(x) for x in a.wrows.split(',')]:
             fws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wr or None, ring=False)
             msf = _time(lambda: fp_filter.basis_series_fused(fws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
@@ -112,7 +112,7 @@ def basis(a):
                 first = got
             else:
                 out['bit_identical_' + tag] = all(torch.equal(x, y) for x, y in zip(got, first))
-    _lib.call('gwb_basis_set_pass2_columns', 16)
+    _lib.call('gwb_basis_set_pass2_columns', -1, 16)
     full = (lambda: Z.double() + Zlo.double()) if Zlo is not None else (lambda: Z.double())
     if tlen == fp_filter.RING_N and a.ring_cfgs:
         ref = full() * fws.scale.double()
@@ -255,12 +255,13 @@ def c4(a):
             glitches.append((i, tg, f0, snr))
         segs.append(dict(x=x.to(torch.float32).contiguous(), start_gps=gps, det=i % 2))
         gps += int(n_s) + 100
-    cfg = pipeline.FilterConfig(form=a.form)
+    tune = bool(getattr(a, 'autotune', False))
+    cfg = pipeline.FilterConfig(form=a.form, autotune=tune)
     co = None
     if a.production:
         # production's selection (threshold 4, exact stage above 5.5 (1 - margin), the rest rebuilt) and
         # consolidation (newsnr 4, 30 loudest per 1.072 s, SNR >= 5 exempt): ops/run_prod_o4a.sh's flags
-        cfg = pipeline.FilterConfig(form=a.form, snr_threshold=4.0, exact_snr=5.5, rebuilt_cap=1 << 24)
+        cfg = pipeline.FilterConfig(form=a.form, snr_threshold=4.0, exact_snr=5.5, rebuilt_cap=1 << 24, autotune=tune)
         co = sg.Consolidation()
     # SVD metric of the run from a first batch of chunks, then the bank (as bench.py builds it)
     from gwb200 import gpu_prep

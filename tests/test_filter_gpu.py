@@ -210,7 +210,7 @@ def test_ring_basis_series_16bit_forms(form):
 
 @pytest.mark.parametrize('form', ['f16', 'bf16', 'bf16x3', 'f32', 'fp8'])
 def test_pass2_sixteen_columns_bit_identical(form):
-    """The 16-column pass 2 (gwb_basis_set_pass2_columns(16)) writes the same Z bits as the 8-column kernels at
+    """The 16-column pass 2 (gwb_basis_set_pass2_columns(form, 16)) writes the same Z bits as the 8-column kernels at
     N = 2^20, for every Z encoding, with rows that end mid-chunk (r = 11) and an analysed span that starts and ends
     inside a column block."""
     from gwb200 import _lib, fp_filter
@@ -229,7 +229,7 @@ def test_pass2_sixteen_columns_bit_identical(form):
     out = {}
     try:
         for cols in (8, 16):
-            _lib.call('gwb_basis_set_pass2_columns', cols)
+            _lib.call('gwb_basis_set_pass2_columns', -1, cols)
             ws = fp_filter.FusedBasisWorkspace(tlen, flen, r)
             Z = torch.full((2 * Kh, -(-Tn // 16) * 16), 7 if dt == torch.uint8 else 3.0, dtype=dt, device='cuda')
             Zlo = torch.full_like(Z, 5.0) if form == 'bf16x3' else None
@@ -238,7 +238,7 @@ def test_pass2_sixteen_columns_bit_identical(form):
             if form == 'fp8':
                 out[cols].append(ws.rowscale[:r].cpu())
     finally:
-        _lib.call('gwb_basis_set_pass2_columns', 16)
+        _lib.call('gwb_basis_set_pass2_columns', -1, 16)
     for x, y in zip(out[8], out[16]):
         assert torch.equal(x.view(torch.uint8), y.view(torch.uint8))
 
