@@ -159,6 +159,35 @@ __device__ __forceinline__ void dft_reg(float2 (&x)[R]) {
     });
 }
 
+// dft_reg for inputs whose upper half past R/2 is zero (x[R/2] may not be): the first stage's butterflies (j, j + R/2)
+// reduce to a copy and a rotation for j >= 1, so its additions are skipped. Same output as dft_reg on those inputs
+// (up to the sign of exact zeros).
+template <int R>
+__device__ __forceinline__ void dft_reg_upper_zero(float2 (&x)[R]) {
+    constexpr int h0 = R / 2;
+    {
+        const float2 a = x[0], b = x[h0];
+        x[0] = make_float2(a.x + b.x, a.y + b.y);
+        x[h0] = make_float2(a.x - b.x, a.y - b.y);
+    }
+    static_for<h0 - 1>([&](auto J) {
+        constexpr int j = decltype(J)::value + 1;
+        x[j + h0] = rot<j, R>(x[j]);
+    });
+    static_for<ilog2(R) - 1>([&](auto S) {
+        constexpr int h = R >> (decltype(S)::value + 2);
+        static_for<R / (2 * h)>([&](auto B) {
+            constexpr int base = decltype(B)::value * 2 * h;
+            static_for<h>([&](auto J) {
+                constexpr int j = decltype(J)::value;
+                const float2 a = x[base + j], b = x[base + j + h];
+                x[base + j] = make_float2(a.x + b.x, a.y + b.y);
+                x[base + j + h] = rot<j, 2 * h>(make_float2(a.x - b.x, a.y - b.y));
+            });
+        });
+    });
+}
+
 // Two-level split of a DFT of length L over TB columns. Shared buffer Y[c][b][u] at c * SC + b * SB + u (float2):
 // SB = 1 (mod 16 eight-byte words) and SC = SCM (mod 16), chosen per pass so that each half-warp of a 64-bit access
 // hits 16 distinct bank pairs.
@@ -265,29 +294,30 @@ __global__ void __launch_bounds__(256, 2) basis_pass1_w(
         for (int a = 0; a < R / 2; ++a) x[a] = Vs[R * a + lane];
         __syncwarp();
         if (j + 1 < j1) fetch(j + 1);
-        float part = 0.f;
 #pragma unroll
         for (int a = 0; a < R / 2; ++a) {
             const float2 av = x[a];
             x[a] = make_float2(fmaf(av.x, dk[a].x, av.y * dk[a].y), fmaf(av.x, dk[a].y, -(av.y * dk[a].x)));
-            part = fmaf(x[a].x, x[a].x, fmaf(x[a].y, x[a].y, part));
         }
         x[R / 2] = make_float2(0.f, 0.f);
         if (k2 == 0 && lane == 0) {                         // the bin N / 2
             const float2 av = Vp[(long long)j * ldvp + N / 2];
             x[R / 2] = make_float2(fmaf(av.x, dN.x, av.y * dN.y), fmaf(av.x, dN.y, -(av.y * dN.x)));
-            part = fmaf(x[R / 2].x, x[R / 2].x, fmaf(x[R / 2].y, x[R / 2].y, part));
         }
+        // sums of |q|^2 only where they are used: the scale's first rows, the fp8 form's per-row sums (warp-uniform)
+        if (j < nf || rowpart) {
+            float part = 0.f;
 #pragma unroll
-        for (int a = R / 2 + 1; a < R; ++a) x[a] = make_float2(0.f, 0.f);
-        if (j < nf) acc += (double)part;
-        if (rowpart) {                                      // per-row sums of |q|^2: rowpart[j][k2]
-            float ps = part;
+            for (int a = 0; a <= R / 2; ++a) part = fmaf(x[a].x, x[a].x, fmaf(x[a].y, x[a].y, part));
+            if (j < nf) acc += (double)part;
+            if (rowpart) {                                  // per-row sums of |q|^2: rowpart[j][k2]
+                float ps = part;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, off);
-            if (lane == 0) rowpart[(long long)j * N2 + k2] = ps;
+                for (int off = 16; off > 0; off >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, off);
+                if (lane == 0) rowpart[(long long)j * N2 + k2] = ps;
+            }
         }
-        dft_reg<R>(x);
+        dft_reg_upper_zero<R>(x);                           // q is zero for k1 > N1 / 2
         static_for<R>([&](auto U) {
             constexpr int u = decltype(U)::value;
             Yw[lane * (R + 1) + u] = cmul(x[brev(u, ilog2(R))], tw2[u * R + lane]);

@@ -205,43 +205,84 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                 *abort_flag = 1;
             }
             tc_fence_after();
-            // the MMAs of one item (M block mb) on one Z chunk
+            // the MMAs of one item (M block mb) on one Z chunk. One-product forms: every descriptor of the chunk is
+            // formed first, then the MMAs go out back to back in the same order (sk, four real products), so the one
+            // issuing thread spends no address arithmetic between them (measured 0.266 -> 0.253 ms at n = 256,
+            // r = 128, fp16). The split form keeps descriptors and MMAs interleaved (the burst measured slower there:
+            // one K step per chunk when A lo is streamed).
             auto issue = [&](int kc, int mb, int b, uint32_t st) {
-                const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
-                const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
-                for (int sk = 0; sk < nsteps; ++sk) {
-                    const int k = kc * KC + sk * C::KSTEP;
-                    for (int pr = 0; pr < C::NPROD; ++pr) {
-                        const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
-                        const uint32_t abase = a_base + (mb * nres + ha) * L.a_tiles * kATile;
+                if constexpr (C::NPROD == 1) {
+                    constexpr int MAXS = 4;                      // K steps per chunk: KC / KSTEP (64/16, 128/32)
+                    const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
+                    const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
+                    const uint32_t abase = a_base + mb * L.a_tiles * kATile;
+                    uint64_t dAre[MAXS], dAim[MAXS], dZre[MAXS], dZim[MAXS];
+#pragma unroll
+                    for (int sk = 0; sk < MAXS; ++sk) {
+                        const int k = kc * KC + sk * C::KSTEP;
                         const uint32_t are = abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
                         const uint32_t aim = abase + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
                         // K step = KSTEP rows of 128 bytes (2048 bytes for 16-bit, 4096 for 8-bit)
-                        const uint32_t zre = st + ((0 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
-                        const uint32_t zim = st + ((1 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
-                        uint64_t dAre, dAim;
-                        if (los && ha == 1) {
-                            // A lo of this stage: 128 rows x 16 columns, 32-byte rows, 32-byte swizzle (8-row atoms
-                            // of 256 bytes)
-                            dAre = smem_desc(st + zst_bytes, 16, 256, 6);
-                            dAim = smem_desc(st + zst_bytes + 128 * KC * 2, 16, 256, 6);
-                        } else {
-                            dAre = smem_desc(are, 16, 1024, 2);
-                            dAim = smem_desc(aim, 16, 1024, 2);
-                        }
-                        const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
-                        const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
-                        const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
+                        const uint32_t zre = st + sk * C::KSTEP * 128;
+                        const uint32_t zim = st + C::HALVES * KC * 128 + sk * C::KSTEP * 128;
+                        dAre[sk] = smem_desc(are, 16, 1024, 2);
+                        dAim[sk] = smem_desc(aim, 16, 1024, 2);
+                        dZre[sk] = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
+                        dZim[sk] = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                    }
+#pragma unroll
+                    for (int sk = 0; sk < MAXS; ++sk) {
+                        if (sk >= nsteps) break;
+                        const uint32_t acc = (kc > 0 || sk > 0) ? 1u : 0u;
                         if constexpr (C::F8) {
-                            umma_f8(dre, dAre, dZre, idesc, acc);
-                            umma_f8(dre, dAim, dZim, idesc_neg, 1u);
-                            umma_f8(dim, dAim, dZre, idesc, acc);
-                            umma_f8(dim, dAre, dZim, idesc, 1u);
+                            umma_f8(dre, dAre[sk], dZre[sk], idesc, acc);
+                            umma_f8(dre, dAim[sk], dZim[sk], idesc_neg, 1u);
+                            umma_f8(dim, dAim[sk], dZre[sk], idesc, acc);
+                            umma_f8(dim, dAre[sk], dZim[sk], idesc, 1u);
                         } else {
-                            umma_f16(dre, dAre, dZre, idesc, acc);
-                            umma_f16(dre, dAim, dZim, idesc_neg, 1u);
-                            umma_f16(dim, dAim, dZre, idesc, acc);
-                            umma_f16(dim, dAre, dZim, idesc, 1u);
+                            umma_f16(dre, dAre[sk], dZre[sk], idesc, acc);
+                            umma_f16(dre, dAim[sk], dZim[sk], idesc_neg, 1u);
+                            umma_f16(dim, dAim[sk], dZre[sk], idesc, acc);
+                            umma_f16(dim, dAre[sk], dZim[sk], idesc, 1u);
+                        }
+                    }
+                } else {
+                    const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
+                    const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
+                    for (int sk = 0; sk < nsteps; ++sk) {
+                        const int k = kc * KC + sk * C::KSTEP;
+                        for (int pr = 0; pr < C::NPROD; ++pr) {
+                            const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
+                            const uint32_t abase = a_base + (mb * nres + ha) * L.a_tiles * kATile;
+                            const uint32_t are = abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
+                            const uint32_t aim = abase + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
+                            // K step = KSTEP rows of 128 bytes (2048 bytes for 16-bit, 4096 for 8-bit)
+                            const uint32_t zre = st + ((0 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
+                            const uint32_t zim = st + ((1 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
+                            uint64_t dAre, dAim;
+                            if (los && ha == 1) {
+                                // A lo of this stage: 128 rows x 16 columns, 32-byte rows, 32-byte swizzle (8-row atoms
+                                // of 256 bytes)
+                                dAre = smem_desc(st + zst_bytes, 16, 256, 6);
+                                dAim = smem_desc(st + zst_bytes + 128 * KC * 2, 16, 256, 6);
+                            } else {
+                                dAre = smem_desc(are, 16, 1024, 2);
+                                dAim = smem_desc(aim, 16, 1024, 2);
+                            }
+                            const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
+                            const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                            const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
+                            if constexpr (C::F8) {
+                                umma_f8(dre, dAre, dZre, idesc, acc);
+                                umma_f8(dre, dAim, dZim, idesc_neg, 1u);
+                                umma_f8(dim, dAim, dZre, idesc, acc);
+                                umma_f8(dim, dAre, dZim, idesc, 1u);
+                            } else {
+                                umma_f16(dre, dAre, dZre, idesc, acc);
+                                umma_f16(dre, dAim, dZim, idesc_neg, 1u);
+                                umma_f16(dim, dAim, dZre, idesc, acc);
+                                umma_f16(dim, dAre, dZim, idesc, 1u);
+                            }
                         }
                     }
                 }
