@@ -24,7 +24,6 @@ struct Carve {
 struct StepShapes {
     int rmax, nmax, khmax, K, lda, nw;
     long long ldz, Tn, ldp;
-    bool ring;
 };
 
 int shapes_of(const GwbTile* tiles, int ntiles, long long tlen, const GwbStepConfig* cfg, StepShapes* s) {
@@ -53,7 +52,6 @@ int shapes_of(const GwbTile* tiles, int ntiles, long long tlen, const GwbStepCon
     s->Tn = (long long)s->nw * cfg->cw;
     s->ldz = (s->Tn + 15) / 16 * 16;
     s->ldp = tlen / 2 + 2;
-    s->ring = tlen == (1 << 20);
     return GWB_OK;
 }
 
@@ -63,7 +61,6 @@ struct StepWork {
     float *Dp, *tw, *W, *scale;
     double* partials;
     uint32_t* ticket;
-    int32_t* sync;
     uint16_t *Z, *Zlo, *Are, *Are_lo;
     float* V;
     int32_t* I;
@@ -74,7 +71,7 @@ struct StepWork {
     float* slots;
     void* sort_work;
     int32_t* sort_status;
-    long long gemm_bytes, sort_bytes, npartials, sync_ints;
+    long long gemm_bytes, sort_bytes, npartials;
     int wrows;
 };
 
@@ -86,14 +83,12 @@ long long carve(const StepShapes& s, int M, int nseg, long long tlen, int flen, 
     w->part = c.take<double>((long long)M * nseg * 16);
     w->Dp = c.take<float>(2ll * nseg * s.ldp);
     w->tw = c.take<float>(2ll * tlen);
-    w->wrows = s.ring ? gwb_basis_ring_rows() : s.rmax;
+    w->wrows = s.rmax;           // the two-pass basis series, W for all of a tile's rows (the ring measured slower)
     w->W = c.take<float>(2ll * tlen * w->wrows);
     w->npartials = std::max(1024ll, 64ll * std::max(1ll, tlen / 64));
     w->partials = c.take<double>(w->npartials);
     w->scale = c.take<float>(1);
     w->ticket = c.take<uint32_t>(1);
-    w->sync_ints = gwb_basis_ring_sync_ints(s.rmax);
-    w->sync = c.take<int32_t>(w->sync_ints);
     w->Z = c.take<uint16_t>((long long)s.K * s.ldz);
     w->Zlo = split ? c.take<uint16_t>((long long)s.K * s.ldz) : nullptr;
     w->Are = c.take<uint16_t>((long long)s.nmax * s.lda);
@@ -170,15 +165,9 @@ int gwb_filter_step(const GwbTile* tiles, int ntiles, const float* H, long long 
         const int kh = (T.r + 15) / 16 * 16;
         for (int sg = 0; sg < nseg; ++sg) {
             const float* dp = w.Dp + 2ll * sg * s.ldp;
-            if (s.ring)
-                GWB_TRY(gwb_basis_fused_ring(T.Vp, T.ldvp, T.r, dp, tlen, w.tw, w.W, w.wrows, cfg->a0, s.Tn, pack,
-                                             w.Z, w.Zlo,
-                                             s.ldz, kh, 0, w.partials, w.npartials, w.scale, nullptr, nullptr, 0,
-                                             w.sync, w.sync_ints, st));
-            else
-                GWB_TRY(gwb_basis_fused(T.Vp, T.ldvp, T.r, dp, tlen, w.tw, w.W, s.rmax, cfg->a0, s.Tn, pack, w.Z,
-                                        w.Zlo, s.ldz, kh, 0, std::min(64, T.r), w.partials, w.npartials, w.ticket,
-                                        w.scale, nullptr, nullptr, 0, st));
+            GWB_TRY(gwb_basis_fused(T.Vp, T.ldvp, T.r, dp, tlen, w.tw, w.W, s.rmax, cfg->a0, s.Tn, pack, w.Z, w.Zlo,
+                                    s.ldz, kh, 0, std::min(64, T.r), w.partials, w.npartials, w.ticket, w.scale,
+                                    nullptr, nullptr, 0, st));
             GWB_TRY(gwb_stacked_a(T.A, T.lda, T.n, T.r, sig + (long long)T.row0 * nseg + sg, nseg, 4.0 * df,
                                   w.scale, 2 * kh, kh, pack, w.Are, nullptr, w.Are_lo, nullptr, s.lda, st));
             GWB_TRY(gwb_fused_peaks_cplx(cfg->form, w.Are, w.Are_lo, s.lda, w.Z, w.Zlo, s.ldz, T.n, kh, s.Tn,

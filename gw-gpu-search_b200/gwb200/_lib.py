@@ -75,6 +75,9 @@ SIGNATURES = {
     'gwb_exact_set_staging': [_I],
     'gwb_append_results': [_P, _P, _P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P],
     'gwb_filter_step_work_bytes': [_P, _I, _I, _I, _LL, _I, _I, _P],
+    'gwb_filter_batch_work_bytes': [_P, _I, _I, _I, _LL, _P, _P],
+    'gwb_filter_batch': [_P, _P, _LL, _I, _LL, _P, _P, _I, _P, _LL, _I, _P, _P, _P, _P, _P, _LL, _P, _P, _P, _P, _P, _P,
+                         _P],
     'gwb_filter_step': [_P, _I, _P, _LL, _I, _P, _P, _I, _D, _P, _P, _LL, _LL, _I, _P, _LL, _I, _P, _P, _LL, _P, _P, _P,
                         _P, _P],
     'gwb_select_top': [_P, _P, _P, _P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _I, _P, _LL, _P],
@@ -139,6 +142,7 @@ def load():
         lib.gwb_fused_peaks_cplx_work_bytes.restype = ctypes.c_longlong
         lib.gwb_select_top_work_bytes.restype = ctypes.c_longlong
         lib.gwb_filter_step_work_bytes.restype = ctypes.c_longlong
+        lib.gwb_filter_batch_work_bytes.restype = ctypes.c_longlong
         _lib = lib
     return _lib
 

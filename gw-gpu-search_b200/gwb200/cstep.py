@@ -69,3 +69,43 @@ class CStep:
         cands = _exact.from_dev(self.cands, _exact.CAND, n)
         peaks = _exact.from_dev(self.peaks, _exact.PEAK, n)
         return dict(n_candidates=n, cands=cands, peaks=peaks, keep=peaks['snr'] > self.cfg.snr_threshold)
+
+
+class GwbCondConfig(ctypes.Structure):
+    _fields_ = [('sr', ctypes.c_double), ('f_low', ctypes.c_double), ('psd_len', ctypes.c_int),
+                ('psd_stride', ctypes.c_int), ('median', ctypes.c_int), ('inv_len', ctypes.c_int),
+                ('inv_taper', ctypes.c_int)]
+
+
+class CBatch(CStep):
+    """gwb_filter_batch: a batch of raw chunks (nseg x tlen float32 strain) conditioned as
+    gpu_prep.BatchConditioner(nseg, tlen, sr, f_low, psd_seg_len, psd_seg_stride, ..., psd_inverse_length) conditions
+    them, then filtered as CStep.step, in one C call. D and IP stay on the device (self.D, self.IP)."""
+
+    def __init__(self, bank, tlen, a0, Tn, nseg, cfg, psd_seg_len=16.0, psd_seg_stride=8.0, psd_inverse_length=16.0,
+                 median=True, taper=False, device='cuda'):
+        super().__init__(bank, tlen, a0, Tn, nseg, cfg, device)
+        sr = float(cfg.sr)
+        self.cond = GwbCondConfig(sr, float(cfg.f_low), int(psd_seg_len * sr + 0.5), int(psd_seg_stride * sr + 0.5),
+                                  int(median), int(psd_inverse_length * sr) if psd_inverse_length else 0, int(taper))
+        wb = _lib.load().gwb_filter_batch_work_bytes(ctypes.addressof(self.tiles), len(bank.svd), bank.M, nseg, tlen,
+                                                     ctypes.addressof(self.cond), ctypes.addressof(self.c))
+        if wb < 0:
+            raise _lib.GwbError('gwb_filter_batch_work_bytes', _lib.GWB_ERR_SHAPE,
+                                _lib.load().gwb_last_error().decode())
+        del self.work
+        self.work = torch.empty(wb, dtype=torch.uint8, device=device)
+        flen = tlen // 2 + 1
+        self.D = torch.empty((nseg, flen), dtype=torch.complex64, device=device)
+        self.IP = torch.empty((nseg, flen), dtype=torch.float32, device=device)
+
+    def batch(self, x, isw):
+        """x: (nseg, tlen) float32 CUDA strain; isw: 1 / sw of the bank's SVD metric. Returns sig."""
+        b = self.bank
+        assert tuple(x.shape) == (self.nseg, self.tlen) and x.dtype == torch.float32 and x.stride(1) == 1
+        _lib.call('gwb_filter_batch', _lib.handle(), _lib.ptr(x), x.stride(0), self.nseg, self.tlen,
+                  ctypes.addressof(self.cond), ctypes.addressof(self.tiles), len(b.svd), _lib.ptr(b.H), b.H.stride(0),
+                  b.M, _lib.ptr(b.kmax), _lib.ptr(b.nbins), _lib.ptr(isw), ctypes.addressof(self.c),
+                  _lib.ptr(self.work), self.work.numel(), _lib.ptr(self.D), _lib.ptr(self.IP), _lib.ptr(self.cands),
+                  _lib.ptr(self.peaks), _lib.ptr(self.counters), _lib.ptr(self.sig), _lib.stream_ptr())
+        return self.sig

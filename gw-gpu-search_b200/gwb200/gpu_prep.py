@@ -492,7 +492,9 @@ class BatchConditioner:
         self.bias = median_bias(nseg)
         w = np.hanning(self.L).astype(np.float32)
         self.w = torch.from_numpy(w).to(device)
-        self.fac = float(np.float32(2 * (1. / (1. / sr) / self.L) * self.L / (w * w).sum()))
+        # the Welch scale 2 / (dt sum w^2) with dt = 1 / sr, the window's float values squared and summed in double
+        # (gwb_filter_batch forms the same number)
+        self.fac = float(np.float32(2.0 * sr / np.sum(w.astype(np.float64) ** 2)))
         self.pdf = 1. / (1. / sr) / self.L
         self.mfl = int(psd_inverse_length * sr) if psd_inverse_length else 0
         self.tw = torch.from_numpy(np.hanning(self.mfl).astype(np.float32)).to(device) if trunc_method == 'hann' else None

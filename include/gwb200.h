@@ -452,7 +452,7 @@ typedef struct {
 } GwbStepConfig;
 /* One step of the compressed filter over a batch of conditioned segments (the loop of fp_filter.py:700-888, run_group
  * :741-836, with every candidate sent to the exact stage): template norms sig (M x nseg, float64, out), D isw in
- * four-step order, then for every tile and segment the fused basis series (the ring form for tlen = 2^20), stacked A,
+ * four-step order, then for every tile and segment the fused basis series (two passes, gwb_basis_fused), stacked A,
  * the fused GEMM with |z|^2 and windowed argmax, the window selection; then edges, binned sums in template-row order
  * and the finalisation into cands / peaks (cand_cap each) with counters[0..4] as gwb_select_windows (counters[3] = 1:
  * a list overflowed). H (M x ldh complex), kmax and nbins per bank row; D, IP (nseg rows); isw = 1 / sw of the SVD
@@ -464,6 +464,31 @@ GWB_API int gwb_filter_step(const GwbTile* tiles, int ntiles, const float* H, lo
                             const float* IP, long long ldd, long long ldip, int nseg, const float* isw, long long tlen,
                             int flen, const GwbStepConfig* cfg, void* work, long long work_bytes, GwbCand* cands,
                             GwbPeak* peaks, int32_t* counters, double* sig, void* stream);
+
+/* The conditioning of a batch of raw chunks, each one dataset holding one analysis segment and one PSD span
+ * (gpu_stage2, gpu_prep.py:405-454, as gwb200.gpu_prep.BatchConditioner runs it). */
+typedef struct {
+    double sr;           /* sample rate (Hz); df = sr / tlen */
+    double f_low;        /* low-frequency cutoff (Hz); kmin = (int)(f_low / df) */
+    int psd_len;         /* Welch frame length (samples), Hann window; the frames must tile the chunk */
+    int psd_stride;      /* Welch frame stride (samples) */
+    int median;          /* 1: median average with PyCBC's bias (the reference's default); 0: mean */
+    int inv_len;         /* inverse spectrum truncation length (samples); 0: none */
+    int inv_taper;       /* 1: Hann taper in the truncation; 0: none (the reference's default) */
+} GwbCondConfig;
+/* A batch of nseg raw float32 chunks x (DYN_RANGE_FAC units, row stride ldx, tlen samples each) through the whole
+ * path in one call (the batched entry behind the batched form, the per-dataset loop of fp_filter.py:700-888):
+ * median-Welch PSD, interpolation, inverse spectrum truncation, segment rFFT, D and IP into the caller's D (nseg x
+ * flen complex) and IP (nseg x flen), then gwb_filter_step (kmin and df from cond). h: a handle (cuFFT plans).
+ * work: gwb_filter_batch_work_bytes(...) bytes; nothing is allocated except the handle's plans on first use, and
+ * nothing is copied to the host. */
+GWB_API long long gwb_filter_batch_work_bytes(const GwbTile* tiles, int ntiles, int M, int nseg, long long tlen,
+                                              const GwbCondConfig* cond, const GwbStepConfig* cfg);
+GWB_API int gwb_filter_batch(gwb_handle_t h, const float* x, long long ldx, int nseg, long long tlen,
+                             const GwbCondConfig* cond, const GwbTile* tiles, int ntiles, const float* H,
+                             long long ldh, int M, const int32_t* kmax, const int32_t* nbins, const float* isw,
+                             const GwbStepConfig* cfg, void* work, long long work_bytes, float* D, float* IP,
+                             GwbCand* cands, GwbPeak* peaks, int32_t* counters, double* sig, void* stream);
 
 /* ---- consolidation (downstream of the exact stage) -------------------------------------------------------- */
 /* Workspace bytes of gwb_consolidate for n items and nwin keep-loudest windows. */
