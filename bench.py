@@ -58,6 +58,7 @@ LINES = ((60.0, 1e3, 0.02), (120.0, 1e3, 0.02), (180.0, 1e3, 0.02))
 CW = 2048
 THR, MARGIN = 5.5, 0.04
 DTYPES = {'bf16x3': 'bf16 hi+lo, 3 products (fp32 accumulate)', 'f16': 'f16 (fp32 accumulate)',
+          'f16x2': 'f16, A as f16 hi+lo, 2 products (fp32 accumulate)',
           'bf16': 'bf16 (fp32 accumulate)', 'f32': 'f32',
           'fp8': 'fp8 e4m3 screen (fp32 accumulate) + float64 exact stage'}
 
@@ -434,10 +435,10 @@ def run_c2(a):
         # algorithmic HBM bytes of one basis-series call (both passes): Vp read (tlen/2 + 1 complex per row), W
         # written and read back (tlen complex per row), Z written (re + im over Tn, one or two 16-bit planes, fp32 or
         # fp8)
-        zb = {'bf16x3': 8, 'f16': 4, 'bf16': 4, 'f32': 8, 'fp8': 2}[form]
+        zb = {'bf16x3': 8, 'f16': 4, 'f16x2': 4, 'bf16': 4, 'f32': 8, 'fp8': 2}[form]
         b_bytes = [r * (8 * (mf.tlen // 2 + 1) + 16 * mf.tlen + zb * mf.Tn) for e, n, r, kp in L]
         useful = [8.0 * n * r * mf.Tn for e, n, r, kp in L]
-        nprod = {'bf16x3': 3, 'f16': 1, 'bf16': 1, 'f32': 1, 'fp8': 1}[form]
+        nprod = {'bf16x3': 3, 'f16x2': 2}.get(form, 1)
         issued = [nprod * 4.0 * n * kp * mf.Tn for e, n, r, kp in L]
         mf.profile = None
         val = world * (analysed / WEEK2) / (ms / 1e3 / 3600.0)
@@ -492,7 +493,7 @@ def run_c2(a):
                 traffic_source='%s (dram bytes / algorithmic bytes, scaled)' % rsrc.get('basis'))
     # the fused GEMM, timed inside a seconds-long step: against the sustained bf16 peak (the burst one beside it).
     # Algorithmic flop of a launch: 8 n r Tn per product (the split form computes three), without the K padding
-    nprod = {'bf16x3': 3}.get(main_form, 1)
+    nprod = {'bf16x3': 3, 'f16x2': 2}.get(main_form, 1)
     ach = nprod * R['useful'] / (R['gemm_ms'] / 1e3) / 1e12
     pk = peaks.get('bf16_tflops_sustained', peaks.get('bf16_tflops', 1590.0)) if main_form != 'f32' else None
     pkb = peaks.get('bf16_tflops') if main_form != 'f32' else None
@@ -610,7 +611,7 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--cpu-steps', type=int, default=3, help='timed steps of the CPU baseline sample')
     ap.add_argument('--no-precision', action='store_true', help='skip the float64 precision comparison')
-    ap.add_argument('--forms', default='bf16x3,f16,bf16,fp8,f32', help='forms timed (the first gives value)')
+    ap.add_argument('--forms', default='bf16x3,f16x2,f16,bf16,fp8,f32', help='forms timed (the first gives value)')
     ap.add_argument('--form-steps', type=int, default=3, help='timed steps of each form after the first')
     ap.add_argument('--production', action='store_true', help='c4: production selection and consolidation')
     ap.add_argument('--no-autotune', action='store_true', help='c2, c4: default launch shapes instead of tuned ones')

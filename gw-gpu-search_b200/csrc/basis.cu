@@ -136,6 +136,11 @@ __global__ void stacked_a_kernel(const float2* __restrict__ A, long long lda, in
         if (kh > 0) {
             if (FORM == 0) static_cast<__half*>(Are)[o] = __float2half_rn(re);
             else if (FORM == 1) static_cast<float*>(Are)[o] = re;
+            else if (FORM == 5) {       // fp16 hi + lo (the fp16 form with split A)
+                const __half hr = __float2half_rn(re);
+                static_cast<__half*>(Are)[o] = hr;
+                static_cast<__half*>(Are_lo)[o] = __float2half_rn(re - __half2float(hr));
+            }
             else {
                 const __nv_bfloat16 hr = __float2bfloat16_rn(re);
                 static_cast<__nv_bfloat16*>(Are)[o] = hr;
@@ -195,7 +200,7 @@ __global__ void stacked_a8_kernel(const float2* __restrict__ A, long long lda, i
 }
 
 __device__ __forceinline__ float ld_as_float(const void* p, long long i, int form) {
-    if (form == 0) return __half2float(static_cast<const __half*>(p)[i]);
+    if (form == 0 || form == 5) return __half2float(static_cast<const __half*>(p)[i]);
     if (form == 1) return static_cast<const float*>(p)[i];
     if (form == 4)
         return __half2float(__half(__nv_cvt_fp8_to_halfraw(static_cast<const __nv_fp8_storage_t*>(p)[i], __NV_E4M3)));
@@ -317,7 +322,7 @@ __global__ void select_kernel(const float* __restrict__ vw, const int32_t* __res
     };
     auto lda_ = [&](const void* hi, const void* lo, long long c) {
         return ld_as_float(hi, (long long)row * lda + c, form) +
-               (form == 2 ? ld_as_float(lo, (long long)row * lda + c, 2) : 0.f);
+               (form == 2 || form == 5 ? ld_as_float(lo, (long long)row * lda + c, form) : 0.f);
     };
     const int ne = (okf & 1) ? total : 0, nr = (okf & 2) ? rtotal : 0;
     for (int i = warp; i < ne + nr; i += kThreads / 32) {
@@ -409,8 +414,10 @@ int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm
                   long long ldo, void* stream) {
     using namespace gwb;
     GWB_CHECK_ARG(A && nrm && scale && Are && (kh > 0 || Aim) &&
-                  (form != 2 || (Are_lo && (kh > 0 || Aim_lo))), GWB_ERR_ARG, "stacked_a: null pointer");
-    GWB_CHECK_ARG(form >= 0 && form <= 3, GWB_ERR_ARG, "stacked_a: form %d", form);
+                  (form != 2 || (Are_lo && (kh > 0 || Aim_lo))) && (form != 5 || Are_lo), GWB_ERR_ARG,
+                  "stacked_a: null pointer");
+    GWB_CHECK_ARG(form >= 0 && form <= 5 && form != 4 && (form != 5 || kh > 0), GWB_ERR_ARG,
+                  "stacked_a: form %d (0 fp16, 1 fp32, 2 split bf16, 3 bf16, 5 fp16 with split A, compact)", form);
     GWB_CHECK_ARG(n > 0 && r > 0 && lda >= r && ldo >= Kp && (kh > 0 ? (kh >= r && Kp == 2 * kh) : Kp >= 2 * r),
                   GWB_ERR_SHAPE, "stacked_a: n=%d r=%d Kp=%d kh=%d", n, r, Kp, kh);
     cudaStream_t s = (cudaStream_t)stream;
@@ -418,6 +425,7 @@ int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm
     if (form == 0) stacked_a_kernel<0><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
     else if (form == 1) stacked_a_kernel<1><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
     else if (form == 2) stacked_a_kernel<2><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
+    else if (form == 5) stacked_a_kernel<5><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
     else stacked_a_kernel<3><<<n, 128, 0, s>>>(a, lda, n, r, nrm, nrm_stride, df4, scale, Kp, kh, Are, Aim, Are_lo, Aim_lo, ldo);
     GWB_LAUNCH_CHECK("stacked_a_kernel");
     return GWB_OK;
@@ -445,8 +453,9 @@ int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n,
     using namespace gwb;
     GWB_CHECK_ARG(vw && iw && Are && (kh > 0 || Aim) && Z && cands && groups && units && counters, GWB_ERR_ARG,
                   "select_windows: null pointer");
-    GWB_CHECK_ARG(form >= 0 && form <= 4 && (form != 2 || (Are_lo && (kh > 0 || Aim_lo) && Zlo)) &&
-                      (form != 4 || (kh > 0 && rowscale)), GWB_ERR_ARG, "select_windows: form %d", form);
+    GWB_CHECK_ARG(form >= 0 && form <= 5 && (form != 2 || (Are_lo && (kh > 0 || Aim_lo) && Zlo)) &&
+                      (form != 4 || (kh > 0 && rowscale)) && (form != 5 || (Are_lo && kh > 0)), GWB_ERR_ARG,
+                  "select_windows: form %d", form);
     GWB_CHECK_ARG(kh == 0 || Kp == 2 * kh, GWB_ERR_SHAPE, "select_windows: Kp=%d with kh=%d", Kp, kh);
     GWB_CHECK_ARG(n > 0 && nw >= 0 && ldv >= nw && Kp > 0 && lda >= Kp, GWB_ERR_SHAPE, "select_windows: n=%d nw=%d", n,
                   nw);

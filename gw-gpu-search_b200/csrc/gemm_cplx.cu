@@ -46,11 +46,19 @@ struct __align__(64) CplxArgs {
     DeviceError* err;
 };
 
+// Forms: 0 fp16, 1 bf16, 2 split bf16 (A and Z as hi + lo, products hi.hi + hi.lo + lo.hi), 3 fp8 e4m3, 6 fp16 with A
+// split (A hi + lo in fp16, Z in fp16, products hi.Z + lo.Z).
 template <int FORM>
 struct Cfg {
-    static constexpr int NH = FORM == 2 ? 2 : 1;          // hi (and lo) copies of each operand
-    static constexpr int NPROD = FORM == 2 ? 3 : 1;
+    static constexpr bool SPLIT_A = FORM == 2 || FORM == 6;           // A as hi + lo
+    static constexpr int NHA = SPLIT_A ? 2 : 1;                       // copies of A
+    static constexpr int NHZ = FORM == 2 ? 2 : 1;                     // copies of Z
+    static constexpr int NH = NHA > NHZ ? NHA : NHZ;                  // tensor maps per operand
+    static constexpr int NPROD = FORM == 2 ? 3 : (FORM == 6 ? 2 : 1);
     static constexpr uint32_t FMT = FORM == 1 || FORM == 2 ? 1u : 0u;   // kind::f16: 0 f16, 1 bf16; kind::f8f6f4: 0 e4m3
+    // product pr: A copy ha, Z copy hz (split bf16: (0,0), (0,1), (1,0); fp16 with split A: (0,0), (1,0))
+    static constexpr int ha(int pr) { return SPLIT_A && pr == NPROD - 1 ? 1 : 0; }
+    static constexpr int hz(int pr) { return FORM == 2 && pr == 1 ? 1 : 0; }
     static constexpr bool F8 = FORM == 3;
     static constexpr int ES = F8 ? 1 : 2;                 // bytes per element
     static constexpr int KSTEP = F8 ? 32 : 16;            // K per MMA
@@ -62,27 +70,27 @@ struct Layout {
     uint32_t a_tiles, a_bytes, z_off, stage_bytes, x_off, bar_off, total;
 };
 
-__host__ __device__ inline Layout layout_of(int nh, int MB, int Kh, int KC, int stages, int rowel = 64) {
+__host__ __device__ inline Layout layout_of(int nha, int nhz, int MB, int Kh, int KC, int stages, int rowel = 64) {
     Layout L;
     L.a_tiles = (uint32_t)((2 * Kh + rowel - 1) / rowel);
-    L.a_bytes = (uint32_t)MB * nh * L.a_tiles * kATile;
+    L.a_bytes = (uint32_t)MB * nha * L.a_tiles * kATile;
     L.z_off = L.a_bytes;
     // (re, im) x (hi, lo) x the 128-sample tile as 128-byte rows (two 64-sample halves for 16-bit, one for 8-bit)
-    L.stage_bytes = 2u * nh * (uint32_t)(128 / rowel) * (uint32_t)KC * 128u;
+    L.stage_bytes = 2u * nhz * (uint32_t)(128 / rowel) * (uint32_t)KC * 128u;
     L.x_off = L.z_off + (uint32_t)stages * L.stage_bytes;
     L.bar_off = L.x_off + 2048u;
     L.total = L.bar_off + (uint32_t)(2 * stages + 6) * 8u + 16u;
     return L;
 }
 
-// The split bf16 form with A lo streamed: A hi resident (128 rows x 2 Kh), stages of Z (re, im) x (hi, lo) x KC rows
-// x 128 samples followed by A lo (re, im) x 128 rows x KC columns (KC = 16: one 32-byte swizzle atom per row).
-__host__ __device__ inline Layout layout_split_stream(int Kh, int KC, int stages) {
+// The split-A forms with A lo streamed: A hi resident (128 rows x 2 Kh), stages of Z (re, im) x (its nhz copies) x
+// KC rows x 128 samples followed by A lo (re, im) x 128 rows x KC columns (KC = 16: one 32-byte swizzle atom per row).
+__host__ __device__ inline Layout layout_split_stream(int Kh, int KC, int stages, int nhz) {
     Layout L;
     L.a_tiles = (uint32_t)((2 * Kh + 63) / 64);
     L.a_bytes = L.a_tiles * kATile;
     L.z_off = L.a_bytes;
-    L.stage_bytes = 2u * 2u * 2u * (uint32_t)KC * 128u + 2u * 128u * (uint32_t)KC * 2u;
+    L.stage_bytes = 2u * (uint32_t)nhz * 2u * (uint32_t)KC * 128u + 2u * 128u * (uint32_t)KC * 2u;
     L.x_off = L.z_off + (uint32_t)stages * L.stage_bytes;
     L.bar_off = L.x_off + 2048u;
     L.total = L.bar_off + (uint32_t)(2 * stages + 6) * 8u + 16u;
@@ -95,10 +103,10 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int Kh = args.Kh, KC = args.KC, S = args.stages, MB = args.MB;
-    const bool los = FORM == 2 && args.lo_stream != 0;    // A lo streamed (MB = 1, KC = 16)
-    const int nres = los ? 1 : C::NH;                     // resident copies of A
-    const Layout L = los ? layout_split_stream(Kh, KC, S) : layout_of(C::NH, MB, Kh, KC, S, C::ROWEL);
-    const uint32_t zst_bytes = 2u * C::NH * C::HALVES * (uint32_t)KC * 128u;   // the Z part of a stage
+    const bool los = C::SPLIT_A && args.lo_stream != 0;   // A lo streamed (MB = 1, KC = 16)
+    const int nres = los ? 1 : C::NHA;                    // resident copies of A
+    const Layout L = los ? layout_split_stream(Kh, KC, S, C::NHZ) : layout_of(C::NHA, C::NHZ, MB, Kh, KC, S, C::ROWEL);
+    const uint32_t zst_bytes = 2u * C::NHZ * C::HALVES * (uint32_t)KC * 128u;   // the Z part of a stage
     const int nkc = (Kh + KC - 1) / KC;
     uint8_t* sA = smem;
     uint8_t* sZ = smem + L.z_off;
@@ -156,10 +164,8 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
 
     if (warp == 0) {
         if (lane == 0) {
-            for (int h = 0; h < C::NH; ++h) {
-                prefetch_tmap(&args.tA[h]);
-                prefetch_tmap(&args.tZ[h]);
-            }
+            for (int h = 0; h < C::NHA; ++h) prefetch_tmap(&args.tA[h]);
+            for (int h = 0; h < C::NHZ; ++h) prefetch_tmap(&args.tZ[h]);
             mbar_arrive_expect_tx(barA, (uint32_t)(MBe * nres * L.a_tiles * kATile));
             for (int mb = 0; mb < MBe; ++mb)
                 for (int h = 0; h < nres; ++h)
@@ -180,9 +186,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                 const int x = (t_begin + i) * kTile;
                 uint8_t* st = sZ + s * L.stage_bytes;
                 for (int ri = 0; ri < 2; ++ri)
-                    for (int h = 0; h < C::NH; ++h)
+                    for (int h = 0; h < C::NHZ; ++h)
                         for (int half = 0; half < C::HALVES; ++half)
-                            tma_load_2d(st + ((ri * C::NH + h) * C::HALVES + half) * KC * 128, &args.tZ[h],
+                            tma_load_2d(st + ((ri * C::NHZ + h) * C::HALVES + half) * KC * 128, &args.tZ[h],
                                         &full[s], x + C::ROWEL * half, ri * Kh + kc * KC);
                 if (los)            // A lo, re then im columns of this K chunk (x a multiple of 16 elements)
                     for (int ri = 0; ri < 2; ++ri)
@@ -252,13 +258,13 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                     for (int sk = 0; sk < nsteps; ++sk) {
                         const int k = kc * KC + sk * C::KSTEP;
                         for (int pr = 0; pr < C::NPROD; ++pr) {
-                            const int ha = (pr == 2) ? 1 : 0, hz = (pr == 1) ? 1 : 0;
+                            const int ha = C::ha(pr), hz = C::hz(pr);
                             const uint32_t abase = a_base + (mb * nres + ha) * L.a_tiles * kATile;
                             const uint32_t are = abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
                             const uint32_t aim = abase + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
                             // K step = KSTEP rows of 128 bytes (2048 bytes for 16-bit, 4096 for 8-bit)
-                            const uint32_t zre = st + ((0 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
-                            const uint32_t zim = st + ((1 * C::NH + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
+                            const uint32_t zre = st + ((0 * C::NHZ + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
+                            const uint32_t zim = st + ((1 * C::NHZ + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
                             uint64_t dAre, dAim;
                             if (los && ha == 1) {
                                 // A lo of this stage: 128 rows x 16 columns, 32-byte rows, 32-byte swizzle (8-row atoms
@@ -886,10 +892,10 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     GWB_CHECK_ARG((lda * C::ES) % 16 == 0 && (ldz * C::ES) % 16 == 0, GWB_ERR_ALIGN,
                   "fused_peaks_cplx: lda=%lld and ldz=%lld must be multiples of 16 bytes", lda, ldz);
     GWB_CHECK_ARG(!C::F8 || rowscale, GWB_ERR_ARG, "fused_peaks_cplx: the fp8 form needs the row scales of A");
-    for (int h = 0; h < C::NH; ++h) {
+    for (int h = 0; h < C::NHA; ++h)
         GWB_CHECK_ARG(A[h] && aligned(A[h], 16), GWB_ERR_ALIGN, "fused_peaks_cplx: A operand %d misaligned", h);
+    for (int h = 0; h < C::NHZ; ++h)
         GWB_CHECK_ARG(Zp[h] && aligned(Zp[h], 16), GWB_ERR_ALIGN, "fused_peaks_cplx: Z operand %d misaligned", h);
-    }
     GWB_CHECK_ARG(V && I, GWB_ERR_ARG, "fused_peaks_cplx: null output");
     const long long ntiles = cdiv(Tn, kTile);
     GWB_CHECK_ARG(ntiles * kTile < (1ll << 31), GWB_ERR_SHAPE, "fused_peaks_cplx: Tn too large for int32 indices");
@@ -897,7 +903,9 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     GWB_CHECK_ARG(ldv >= nout, GWB_ERR_SHAPE, "fused_peaks_cplx: ldv=%lld < outputs per row %lld", ldv, nout);
     const uint32_t max_smem = 227 * 1024;
     int KC = FORM == 2 ? 32 : (C::F8 ? 128 : 64);          // K rows per Z stage (32 KB per stage in every form)
-    auto fits = [&](int mb, int st) { return layout_of(C::NH, mb, Kh, KC, st, C::ROWEL).total + 1024 <= max_smem; };
+    auto fits = [&](int mb, int st) {
+        return layout_of(C::NHA, C::NHZ, mb, Kh, KC, st, C::ROWEL).total + 1024 <= max_smem;
+    };
     auto most_stages = [&](int mb) {
         int st = 6;
         while (st > 0 && !fits(mb, st)) --st;
@@ -910,12 +918,12 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     const GemmTune tune = gemm_tune(FORM, Kh);
     int stages = most_stages(MB);
     if (tune.stages >= 2 && stages >= 2) stages = std::min(stages, tune.stages);
-    // split bf16 beyond Kh = 128: A hi + lo no longer fit beside the Z ring, so A lo is streamed with it
-    const bool los = FORM == 2 && stages < 2;
+    // split A beyond Kh = 128: A hi + lo no longer fit beside the Z ring, so A lo is streamed with it
+    const bool los = C::SPLIT_A && stages < 2;
     if (los) {
         KC = 16;
         stages = 8;
-        while (stages > 0 && layout_split_stream(Kh, KC, stages).total + 1024 > max_smem) --stages;
+        while (stages > 0 && layout_split_stream(Kh, KC, stages, C::NHZ).total + 1024 > max_smem) --stages;
         if (tune.stages >= 2) stages = std::min(stages, tune.stages);
     }
     GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d does not fit in shared memory for this form",
@@ -923,16 +931,18 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     CplxArgs args;
     memset(&args, 0, sizeof(args));
     const CUtensorMapDataType dt = C::F8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
-                                   : FORM == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-    for (int h = 0; h < C::NH; ++h) {
+                                   : C::FMT == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    for (int h = 0; h < C::NHA; ++h) {
         // A lo streamed: boxes of 16 columns (32 bytes) x 128 rows, 32-byte swizzle
         const bool lo_box = los && h == 1;
-        int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)(lda * C::ES),
-                               lo_box ? 16u : (uint32_t)C::ROWEL, 128,
-                               lo_box ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_128B);
+        const int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)(lda * C::ES),
+                                     lo_box ? 16u : (uint32_t)C::ROWEL, 128,
+                                     lo_box ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_128B);
         if (r) return r;
-        r = encode_tmap_2d(&args.tZ[h], dt, Zp[h], (uint64_t)Tn, (uint64_t)(2 * Kh), (uint64_t)(ldz * C::ES), C::ROWEL,
-                           (uint32_t)KC, CU_TENSOR_MAP_SWIZZLE_128B);
+    }
+    for (int h = 0; h < C::NHZ; ++h) {
+        const int r = encode_tmap_2d(&args.tZ[h], dt, Zp[h], (uint64_t)Tn, (uint64_t)(2 * Kh), (uint64_t)(ldz * C::ES),
+                                     C::ROWEL, (uint32_t)KC, CU_TENSOR_MAP_SWIZZLE_128B);
         if (r) return r;
     }
     args.V = V;
@@ -950,8 +960,8 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     args.KC = KC;
     args.lo_stream = los ? 1 : 0;
     args.err = device_error_ptr();
-    const uint32_t smem = (los ? layout_split_stream(Kh, KC, stages) : layout_of(C::NH, MB, Kh, KC, stages,
-                                                                                  C::ROWEL)).total + 1024;
+    const uint32_t smem = (los ? layout_split_stream(Kh, KC, stages, C::NHZ)
+                               : layout_of(C::NHA, C::NHZ, MB, Kh, KC, stages, C::ROWEL)).total + 1024;
     auto kern = umma_cplx_kernel<FORM>;
     GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if constexpr (FORM == 0 || FORM == 1) {
@@ -1014,8 +1024,12 @@ extern "C" int gwb_fused_peaks_cplx(int form, const void* A_hi, const void* A_lo
         case 3:
             return gwb::launch_cplx<3>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, work, work_bytes,
                                         s);
+        case 6:
+            return gwb::launch_cplx<6>(A, Z, lda, ldz, M, Kh, Tn, group, V, I, ldv, rowscale, work, work_bytes,
+                                        s);
         default:
-            gwb::set_error("fused_peaks_cplx: form %d (0 fp16, 1 bf16, 2 split bf16, 3 fp8 e4m3)", form);
+            gwb::set_error("fused_peaks_cplx: form %d (0 fp16, 1 bf16, 2 split bf16, 3 fp8 e4m3, 6 fp16 with A "
+                           "split)", form);
             return GWB_ERR_ARG;
     }
 }

@@ -165,7 +165,7 @@ int gwb_num_sms(void) { return gwb::num_sms(); }
 
 extern "C" int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order) {
     using namespace gwb;
-    GWB_CHECK_ARG(form >= 0 && form <= 5 && kh > 0 && (pair == 0 || pair == 1) && stages >= 0 && stages <= 8 &&
+    GWB_CHECK_ARG(form >= 0 && form <= 6 && kh > 0 && (pair == 0 || pair == 1) && stages >= 0 && stages <= 8 &&
                       order >= 0 && order <= 3, GWB_ERR_ARG,
                   "gemm_set_config: form=%d kh=%d pair=%d stages=%d order=%d", form, kh, pair, stages, order);
     std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -15,7 +15,7 @@ import torch
 
 from . import _lib, fp_filter
 
-FORM_CODE = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}
+FORM_CODE = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3, 'f16x2': 6}
 # the persistent basis series' (rows per chunk, W slots, lookahead): W in L2 holds rows x slots rows of 8 MB at 2^20
 # (lookahead 0: split roles, half the CTAs on each pass)
 RING_CONFIGS = [(2, 3, 1), (2, 4, 2), (4, 2, 1), (2, 3, 0), (2, 2, 0), (4, 2, 0), (1, 4, 0)]
@@ -58,9 +58,9 @@ def tune_gemm(form, n, Kh, Tn, group=16, reps=3, device='cuda'):
     if form == 'fp8':
         A, Z = A.to(torch.float8_e4m3fn).view(torch.uint8), Z.to(torch.float8_e4m3fn).view(torch.uint8)
     else:
-        dt = torch.float16 if form == 'f16' else torch.bfloat16
+        dt = torch.float16 if form in ('f16', 'f16x2') else torch.bfloat16
         A, Z = A.to(dt), Z.to(dt)
-    lo = (A.clone(), Z.clone()) if form == 'bf16x3' else (None, None)
+    lo = (A.clone(), Z.clone()) if form == 'bf16x3' else ((A.clone(), None) if form == 'f16x2' else (None, None))
     rs = torch.ones(n, device=device)
     ntiles = -(-Tn // 128)
     nout = -(-ntiles // group)

@@ -15,9 +15,11 @@ from . import _lib
 
 CH = 1 << 16       # fp_filter.py:42 (kept for reference; the kernels do not chunk)
 RB = 64            # basis rows per inverse-FFT batch (fp_filter.py:43)
-# operand encodings of the pack / stacked-A / selection kernels; fp8 (e4m3 with per-row scales, the screening form)
-# exists in the fused basis series and the compact GEMM only
-FORMS = {'f16': 0, 'f32': 1, 'bf16x3': 2, 'bf16': 3, 'fp8': 4}
+# Z encodings of the basis-series and pack kernels; fp8 (e4m3 with per-row scales, the screening form) exists in the
+# fused basis series and the compact GEMM only. f16x2: fp16 Z with A split into fp16 hi + lo (two GEMM products)
+FORMS = {'f16': 0, 'f32': 1, 'bf16x3': 2, 'bf16': 3, 'fp8': 4, 'f16x2': 0}
+# operand (A and Z) encodings of the stacked-A and selection kernels
+A_FORMS = dict(FORMS, f16x2=5)
 
 
 def _s():
@@ -254,7 +256,7 @@ def basis_series_into(ws, Vh, D, isw, a0, Tn, Z, Zlo=None, form='f16', im_off=No
 
 def _z_dtype(form):
     return {'f16': torch.float16, 'f32': torch.float32, 'bf16x3': torch.bfloat16, 'bf16': torch.bfloat16,
-            'fp8': torch.uint8}[form]
+            'fp8': torch.uint8, 'f16x2': torch.float16}[form]
 
 
 def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='f16', df4=0.0, kh=0):
@@ -264,7 +266,7 @@ def stacked_A_into(A, nrm, scale, Kp, Are, Aim, Are_lo=None, Aim_lo=None, form='
     n, r = A.shape
     _lib.call('gwb_stacked_a', _lib.ptr(A), A.stride(0), n, r, _lib.ptr(nrm), nrm.stride(0), float(df4),
               _lib.ptr(scale), Kp, int(kh),
-              FORMS[form], _lib.ptr(Are), _lib.ptr(Aim), _lib.ptr(Are_lo), _lib.ptr(Aim_lo), Are.stride(0), _s())
+              A_FORMS[form], _lib.ptr(Are), _lib.ptr(Aim), _lib.ptr(Are_lo), _lib.ptr(Aim_lo), Are.stride(0), _s())
 
 
 def stacked_A8_into(A, nrm, zscale, kh, A8, sa, df4):

@@ -37,7 +37,7 @@ class FilterConfig:
     snr_threshold: float = 5.5
     margin: float = 0.04
     screen_margin: float = 0.10   # fp8 form: candidates down to thr (1 - screen_margin); the exact stage decides
-    form: str = 'bf16x3'
+    form: str = 'bf16x3'          # GEMM operands: f16, bf16, bf16x3 (split bf16), f16x2 (fp16, A hi + lo), fp8, f32
     cand_cap: int = 1 << 21
     seg_batch: int = 16
     # the reference's --exact-snr split (fp_filter.py:769-781): windows whose rebuilt SNR is below
@@ -140,7 +140,7 @@ class MatchedFilter:
         lda = -(-K // 16) * 16
         self.Are = torch.zeros((nmax, lda), dtype=dt, device=device)
         self.Aim = None if self.compact else torch.zeros_like(self.Are)
-        self.Are_lo = torch.zeros_like(self.Are) if self.form == 'bf16x3' else None
+        self.Are_lo = torch.zeros_like(self.Are) if self.form in ('bf16x3', 'f16x2') else None
         self.Aim_lo = None
         self.sa = torch.empty(nmax, dtype=torch.float32, device=device) if self.fp8 else None   # A row scales
         self.V = torch.empty((nmax, self.nw), dtype=torch.float32, device=device)
@@ -198,7 +198,7 @@ class MatchedFilter:
     def _gemm(self, n, K, Kh):
         s = _lib.stream_ptr()
         if self.compact:
-            code = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}[self.form]
+            code = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3, 'f16x2': 6}[self.form]
             _lib.call('gwb_fused_peaks_cplx', code, _lib.ptr(self.Are), _lib.ptr(self.Are_lo), self.Are.stride(0),
                       _lib.ptr(self.Z), _lib.ptr(self.Zlo), self.Z.stride(0), n, Kh, self.Tn, self.group,
                       _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), _lib.ptr(self.sa),
@@ -258,7 +258,7 @@ class MatchedFilter:
         if prof is not None:
             e[2].record()
             prof.setdefault('launches', []).append((e, n, r, K))
-        f = fp_filter.FORMS[self.form]
+        f = fp_filter.A_FORMS[self.form]
         cap = self.cfg.cand_cap
         _lib.call('gwb_select_windows', _lib.ptr(self.V), _lib.ptr(self.I), self.V.stride(0), n, self.nw, self.thr2,
                   self.ecut, self.rthr, self.a0, b.row0[t], seg, _lib.ptr(self.Are), _lib.ptr(self.Aim),

@@ -115,9 +115,10 @@ GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long ld
  * reference's stacked Are/Aim (pipeline/fp_filter.py:615-621) and stays in shared memory. form 0: fp16 A_hi, Z_hi;
  * 1: bf16; 2: split bf16 with A_lo, Z_lo (hi.hi + hi.lo + lo.hi); 3: fp8 e4m3 (the screening form, no reference
  * counterpart; Kh a multiple of 32), V = rowscale[i]^2 max |z|^2 with rowscale the per-row scale of A
- * (gwb_stacked_a8); rowscale is ignored by the other forms (may be NULL). Kh <= 192 (forms 0, 1, 3); form 2 keeps
- * A hi and lo in shared memory up to Kh = 128 and beyond that keeps A hi there and streams A lo with the Z chunks
- * (Kh <= 320). lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
+ * (gwb_stacked_a8); rowscale is ignored by the other forms (may be NULL); 6: fp16 Z with A split into fp16 hi + lo
+ * (A_lo; Z_lo unused), two products hi.Z + lo.Z (no reference counterpart: the rounding of A is removed, that of Z
+ * kept). Kh <= 192 (forms 0, 1, 3); forms 2 and 6 keep A hi and lo in shared memory up to Kh = 128 and beyond that
+ * keep A hi there and stream A lo with the Z chunks (Kh <= 320). lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
  * be NULL): with it the CTAs take tile-granular ranges of the time axis (balanced to one 128-sample tile) and windows
  * cut by a range boundary are merged by a second kernel, bit for bit the same V and I; without it every CTA takes
  * whole windows (up to one window of imbalance between CTAs). With work, forms 0 and 1 run on CTA pairs (clusters
@@ -260,7 +261,7 @@ GWB_API int gwb_basis_pack(const float* zb, long long ldzb, int rows, int im_off
 /* As = A (norm_i scale); Are = [Re As, -Im As, 0...], Aim = [Im As, Re As, 0...] padded to Kp columns, or with
  * kh > 0 the compact single operand Are = [Re As (kh) | Im As (kh)] (Kp = 2 kh; Aim unused). nrm is read at
  * nrm[i * nrm_stride] (float64): the norm itself when df4 <= 0, else sigma^2 with norm = df4 / sqrt(sigma^2)
- * (df4 = 4 df). form as gwb_basis_pack. */
+ * (df4 = 4 df). form as gwb_basis_pack, plus 5 = compact fp16 hi in Are and lo in Are_lo (for the GEMM's form 6). */
 GWB_API int gwb_stacked_a(const float* A, long long lda, int n, int r, const double* nrm, long long nrm_stride,
                           double df4, const float* scale, int Kp, int kh, int form, void* Are, void* Aim,
                           void* Are_lo, void* Aim_lo, long long ldo, void* stream);
@@ -354,7 +355,7 @@ GWB_API int gwb_refine_step(const double* params, const double* res, long long l
  * exceeded; the row's list is then dropped), rebuilt peaks. Operands in the layout the GEMM used: stacked Are/Aim
  * (kh = 0, K = Kp) or compact A = [ReA | ImA] with Z = [ReZ ; ImZ] (kh > 0, Kp = 2 kh); form as gwb_basis_pack,
  * plus 4 = fp8 e4m3 (compact only), whose rebuilt z is multiplied by rowscale[i] (gwb_stacked_a8's sa; NULL for the
- * other forms). */
+ * other forms), and 5 = fp16 Z with A as fp16 hi + lo (compact only). */
 GWB_API int gwb_select_windows(const float* vw, const int32_t* iw, long long ldv, int n, int nw, float thr2,
                                float ecut, float rthr, long long a0, int row0, int seg, const void* Are,
                                const void* Aim, const void* Are_lo, const void* Aim_lo, long long lda, const void* Z,

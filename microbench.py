@@ -35,7 +35,7 @@ def _time(fn, reps):
 
 def gemm(a):
     n, r, Tn = a.n, a.r, a.tn
-    code = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3}[a.form]
+    code = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'fp8': 3, 'f16x2': 6}[a.form]
     Kh = fp_filter.kh_of(r, a.form)
     g = torch.Generator(device='cuda').manual_seed(0)
     A = torch.randn((n, 2 * Kh), generator=g, device='cuda')
@@ -43,10 +43,10 @@ def gemm(a):
     if code == 3:
         A, Z = A.to(torch.float8_e4m3fn).view(torch.uint8), Z.to(torch.float8_e4m3fn).view(torch.uint8)
     else:
-        dt = torch.float16 if a.form == 'f16' else torch.bfloat16
+        dt = torch.float16 if a.form in ('f16', 'f16x2') else torch.bfloat16
         A, Z = A.to(dt), Z.to(dt)
     rs = torch.ones(n, device='cuda')
-    lo = (A.clone(), Z.clone()) if code == 2 else (None, None)
+    lo = (A.clone(), Z.clone()) if code == 2 else ((A.clone(), None) if code == 6 else (None, None))
     nw = Tn // 2048
     V = torch.empty((n, nw), dtype=torch.float32, device='cuda')
     I = torch.empty((n, nw), dtype=torch.int32, device='cuda')
@@ -58,7 +58,7 @@ def gemm(a):
                   Z.stride(0), n, Kh, Tn, 16, _lib.ptr(V), _lib.ptr(I), V.stride(0), _lib.ptr(rs), _lib.ptr(wk),
                   0 if wk is None else wk.numel(), _lib.stream_ptr())
     useful = 8.0 * n * r * Tn
-    issued = (3 if code == 2 else 1) * 4.0 * n * 2 * Kh * Tn
+    issued = {2: 3, 6: 2}.get(code, 1) * 4.0 * n * 2 * Kh * Tn
     zbytes = 2 * Kh * Tn * (1 if code == 3 else 2) * (2 if code == 2 else 1)
     out = dict(kernel='umma_cplx_kernel', form=a.form, n=n, r=r, Kh=Kh, Tn=Tn)
     # launch configurations (gwb_gemm_set_config): pair x stages x order; results must not depend on them

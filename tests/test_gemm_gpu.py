@@ -225,6 +225,43 @@ def test_cplx_bf16_forms_against_oracle(form, r):
         assert (I.cpu().numpy() == Ir).mean() > (0.99 if form == 2 else 0.8)
 
 
+@pytest.mark.parametrize('r', [40, 120, 150, 192])
+def test_cplx_f16_split_a_against_oracle(r):
+    """fp16 Z with A split into fp16 hi + lo (form 6: two products; A hi and lo resident for Kh <= 128, A lo streamed
+    with Z beyond) against the float64 product of the fp16 Z values with the unrounded A."""
+    from gwb200 import _lib
+    rng = np.random.default_rng(600 + r)
+    M, Tn, group = 256, 2048 * 8, 16
+    Kh = -(-r // 16) * 16
+    As = (rng.standard_normal((M, r)) + 1j * rng.standard_normal((M, r))).astype(np.complex64)
+    zb = (rng.standard_normal((r, Tn)) + 1j * rng.standard_normal((r, Tn))).astype(np.complex64)
+    A = np.zeros((M, 2 * Kh), np.float32)
+    A[:, :r], A[:, Kh:Kh + r] = As.real, As.imag
+    Z = np.zeros((2 * Kh, Tn), np.float32)
+    Z[:r], Z[Kh:Kh + r] = zb.real, zb.imag
+    Z = Z.astype(np.float16).astype(np.float32)                # the Z values the kernel sees
+    At = torch.from_numpy(A).cuda()
+    Ah = At.to(torch.float16)
+    Al = (At - Ah.float()).to(torch.float16)
+    Zh = torch.from_numpy(Z).cuda().to(torch.float16)
+    nout = -(-(Tn // 128) // group)
+    V = torch.empty((M, nout), dtype=torch.float32, device='cuda')
+    I = torch.empty((M, nout), dtype=torch.int32, device='cuda')
+    Are = np.concatenate([A[:, :Kh], -A[:, Kh:]], 1)
+    Aim = np.concatenate([A[:, Kh:], A[:, :Kh]], 1)
+    Vr, Ir = og.group_reduce(*og.gemm_absmax(Are, Aim, Z, M, Tn), group)
+    work = torch.empty(_lib.load().gwb_fused_peaks_cplx_work_bytes(M), dtype=torch.uint8, device='cuda')
+    for wk in (None, work):
+        V.fill_(-7.0)
+        _lib.call('gwb_fused_peaks_cplx', 6, _lib.ptr(Ah), _lib.ptr(Al), Ah.stride(0), _lib.ptr(Zh), None,
+                  Zh.stride(0), M, Kh, Tn, group, _lib.ptr(V), _lib.ptr(I), V.stride(0), None, _lib.ptr(wk),
+                  0 if wk is None else wk.numel(), _lib.stream_ptr())
+        rel = np.abs(V.cpu().numpy() - Vr) / Vr
+        # A carries ~22 bits (hi + lo); Z's own rounding is in the oracle's operands
+        assert rel.max() < 5e-5, rel.max()
+        assert (I.cpu().numpy() == Ir).mean() > 0.99
+
+
 def test_cplx_rejects_oversized_kh():
     from gwb200 import _lib
     with pytest.raises(_lib.GwbError, match='shared memory'):

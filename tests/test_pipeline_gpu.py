@@ -42,7 +42,7 @@ def _case(seed=3):
     return bank, D, IP, kmin, inj
 
 
-@pytest.mark.parametrize('form', ['bf16x3', 'f16', 'f32'])
+@pytest.mark.parametrize('form', ['bf16x3', 'f16x2', 'f16', 'f32'])
 def test_pipeline_matches_oracle(form):
     from gwb200 import pipeline
     bank, D, IP, kmin, inj = _case()
