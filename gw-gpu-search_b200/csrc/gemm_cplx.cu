@@ -84,7 +84,8 @@ __host__ __device__ inline Layout layout_of(int nha, int nhz, int MB, int Kh, in
 }
 
 // The split-A forms with A lo streamed: A hi resident (128 rows x 2 Kh), stages of Z (re, im) x (its nhz copies) x
-// KC rows x 128 samples followed by A lo (re, im) x 128 rows x KC columns (KC = 16: one 32-byte swizzle atom per row).
+// KC rows x 128 samples followed by A lo (re, im) x 128 rows x KC columns (KC = 16: one 32-byte swizzle atom per row;
+// KC = 32: 64-byte rows in the 64-byte swizzle).
 __host__ __device__ inline Layout layout_split_stream(int Kh, int KC, int stages, int nhz) {
     Layout L;
     L.a_tiles = (uint32_t)((2 * Kh + 63) / 64);
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int Kh = args.Kh, KC = args.KC, S = args.stages, MB = args.MB;
-    const bool los = C::SPLIT_A && args.lo_stream != 0;   // A lo streamed (MB = 1, KC = 16)
+    const bool los = C::SPLIT_A && args.lo_stream != 0;   // A lo streamed (MB = 1, KC = 16 or 32)
     const int nres = los ? 1 : C::NHA;                    // resident copies of A
     const Layout L = los ? layout_split_stream(Kh, KC, S, C::NHZ) : layout_of(C::NHA, C::NHZ, MB, Kh, KC, S, C::ROWEL);
     const uint32_t zst_bytes = 2u * C::NHZ * C::HALVES * (uint32_t)KC * 128u;   // the Z part of a stage
@@ -267,10 +268,17 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                             const uint32_t zim = st + ((1 * C::NHZ + hz) * C::HALVES) * KC * 128 + sk * C::KSTEP * 128;
                             uint64_t dAre, dAim;
                             if (los && ha == 1) {
-                                // A lo of this stage: 128 rows x 16 columns, 32-byte rows, 32-byte swizzle (8-row atoms
-                                // of 256 bytes)
-                                dAre = smem_desc(st + zst_bytes, 16, 256, 6);
-                                dAim = smem_desc(st + zst_bytes + 128 * KC * 2, 16, 256, 6);
+                                // A lo of this stage: 128 rows x KC columns; KC = 16: 32-byte rows, 32-byte swizzle
+                                // (8-row atoms of 256 bytes); KC = 32: 64-byte rows, 64-byte swizzle (atoms of 512
+                                // bytes), K step sk 32 bytes into the row
+                                const uint32_t lo_re = st + zst_bytes + sk * 32, lo_im = lo_re + 128 * KC * 2;
+                                if (KC == 16) {
+                                    dAre = smem_desc(lo_re, 16, 256, 6);
+                                    dAim = smem_desc(lo_im, 16, 256, 6);
+                                } else {
+                                    dAre = smem_desc(lo_re, 16, 512, 4);
+                                    dAim = smem_desc(lo_im, 16, 512, 4);
+                                }
                             } else {
                                 dAre = smem_desc(are, 16, 1024, 2);
                                 dAim = smem_desc(aim, 16, 1024, 2);
@@ -921,9 +929,17 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     // split A beyond Kh = 128: A hi + lo no longer fit beside the Z ring, so A lo is streamed with it
     const bool los = C::SPLIT_A && stages < 2;
     if (los) {
-        KC = 16;
-        stages = 8;
-        while (stages > 0 && layout_split_stream(Kh, KC, stages, C::NHZ).total + 1024 > max_smem) --stages;
+        // K chunks of 32 (A lo in 64-byte rows) when at least three stages fit, or two and the launch table asks for
+        // two; else of 16 (32-byte rows). Measured at n = 256, r = 192, fp16 with split A: 0.64 ms with chunks of 32
+        // against 0.90 with chunks of 16
+        auto most_split = [&](int kc) {
+            int st = 8;
+            while (st > 0 && layout_split_stream(Kh, kc, st, C::NHZ).total + 1024 > max_smem) --st;
+            return st;
+        };
+        const int s32 = most_split(32);
+        KC = (s32 >= 3 || (s32 == 2 && tune.stages == 2)) ? 32 : 16;
+        stages = most_split(KC);
         if (tune.stages >= 2) stages = std::min(stages, tune.stages);
     }
     GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d does not fit in shared memory for this form",
@@ -933,11 +949,12 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
     const CUtensorMapDataType dt = C::F8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
                                    : C::FMT == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     for (int h = 0; h < C::NHA; ++h) {
-        // A lo streamed: boxes of 16 columns (32 bytes) x 128 rows, 32-byte swizzle
+        // A lo streamed: boxes of KC columns (32 or 64 bytes) x 128 rows, 32- or 64-byte swizzle
         const bool lo_box = los && h == 1;
         const int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)(lda * C::ES),
-                                     lo_box ? 16u : (uint32_t)C::ROWEL, 128,
-                                     lo_box ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_128B);
+                                     lo_box ? (uint32_t)KC : (uint32_t)C::ROWEL, 128,
+                                     !lo_box ? CU_TENSOR_MAP_SWIZZLE_128B
+                                             : KC == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
         if (r) return r;
     }
     for (int h = 0; h < C::NHZ; ++h) {
