@@ -29,8 +29,8 @@ struct StepShapes {
 int shapes_of(const GwbTile* tiles, int ntiles, long long tlen, const GwbStepConfig* cfg, StepShapes* s) {
     using namespace gwb;
     GWB_CHECK_ARG(tiles && ntiles > 0 && cfg, GWB_ERR_ARG, "filter_step: null tiles or config");
-    GWB_CHECK_ARG(cfg->form >= 0 && cfg->form <= 2, GWB_ERR_ARG,
-                  "filter_step: form %d (0 fp16, 1 bf16, 2 split bf16)", cfg->form);
+    GWB_CHECK_ARG((cfg->form >= 0 && cfg->form <= 2) || cfg->form == 6, GWB_ERR_ARG,
+                  "filter_step: form %d (0 fp16, 1 bf16, 2 split bf16, 6 fp16 with split A)", cfg->form);
     GWB_CHECK_ARG(is_pow2(tlen) && tlen >= (1 << 12) && tlen <= (1 << 20), GWB_ERR_NOT_POW2,
                   "filter_step: tlen=%lld must be a power of two in [2^12, 2^20]", tlen);
     GWB_CHECK_ARG(cfg->cw > 0 && cfg->cw % 128 == 0 && cfg->a0 >= 0 && cfg->Tn >= cfg->cw &&
@@ -78,7 +78,7 @@ struct StepWork {
 long long carve(const StepShapes& s, int M, int nseg, long long tlen, int flen, int kmin, const GwbStepConfig* cfg,
                 void* base, StepWork* w) {
     Carve c{static_cast<char*>(base), 0, 0};
-    const int split = cfg->form == 2;
+    const int split = cfg->form == 2, split_a = cfg->form == 2 || cfg->form == 6;
     const long long cap = cfg->cand_cap;
     w->part = c.take<double>((long long)M * nseg * 16);
     w->Dp = c.take<float>(2ll * nseg * s.ldp);
@@ -92,7 +92,7 @@ long long carve(const StepShapes& s, int M, int nseg, long long tlen, int flen, 
     w->Z = c.take<uint16_t>((long long)s.K * s.ldz);
     w->Zlo = split ? c.take<uint16_t>((long long)s.K * s.ldz) : nullptr;
     w->Are = c.take<uint16_t>((long long)s.nmax * s.lda);
-    w->Are_lo = split ? c.take<uint16_t>((long long)s.nmax * s.lda) : nullptr;
+    w->Are_lo = split_a ? c.take<uint16_t>((long long)s.nmax * s.lda) : nullptr;
     w->V = c.take<float>((long long)s.nmax * s.nw);
     w->I = c.take<int32_t>((long long)s.nmax * s.nw);
     w->gemm_bytes = gwb_fused_peaks_cplx_work_bytes(s.nmax);
@@ -147,7 +147,10 @@ int gwb_filter_step(const GwbTile* tiles, int ntiles, const float* H, long long 
     carve(s, M, nseg, tlen, flen, kmin, cfg, base, &w);
     cudaStream_t st = (cudaStream_t)stream;
     const int cap = cfg->cand_cap, B = cfg->nbins_max;
-    const int pack = cfg->form == 0 ? 0 : (cfg->form == 1 ? 3 : 2);     // Z / A encodings: f16, bf16, split bf16
+    // Z encoding of the basis series and operand encoding of stacked A and the selection: f16, bf16, split bf16, and
+    // for the fp16 form with split A, fp16 Z with fp16 hi + lo A
+    const int pack = cfg->form == 0 ? 0 : (cfg->form == 1 ? 3 : (cfg->form == 2 ? 2 : 0));
+    const int apack = cfg->form == 6 ? 5 : pack;
     GWB_CUDA(cudaMemsetAsync(counters, 0, 5 * sizeof(int32_t), st));
     GWB_CUDA(cudaMemsetAsync(w.ticket, 0, sizeof(uint32_t), st));
     // the Z rows past a tile's rank (up to its 16-row K step) are read by the GEMM against zero columns of A: they must
@@ -169,11 +172,11 @@ int gwb_filter_step(const GwbTile* tiles, int ntiles, const float* H, long long 
                                     s.ldz, kh, 0, std::min(64, T.r), w.partials, w.npartials, w.ticket, w.scale,
                                     nullptr, nullptr, 0, st));
             GWB_TRY(gwb_stacked_a(T.A, T.lda, T.n, T.r, sig + (long long)T.row0 * nseg + sg, nseg, 4.0 * df,
-                                  w.scale, 2 * kh, kh, pack, w.Are, nullptr, w.Are_lo, nullptr, s.lda, st));
+                                  w.scale, 2 * kh, kh, apack, w.Are, nullptr, w.Are_lo, nullptr, s.lda, st));
             GWB_TRY(gwb_fused_peaks_cplx(cfg->form, w.Are, w.Are_lo, s.lda, w.Z, w.Zlo, s.ldz, T.n, kh, s.Tn,
                                          cfg->cw / 128, w.V, w.I, s.nw, nullptr, w.gemm_work, w.gemm_bytes, st));
             GWB_TRY(gwb_select_windows(w.V, w.I, s.nw, T.n, s.nw, thr2, 0.f, cfg->snr_threshold, cfg->a0, T.row0, sg,
-                                       w.Are, nullptr, w.Are_lo, nullptr, s.lda, w.Z, w.Zlo, s.ldz, 2 * kh, kh, pack,
+                                       w.Are, nullptr, w.Are_lo, nullptr, s.lda, w.Z, w.Zlo, s.ldz, 2 * kh, kh, apack,
                                        nullptr, cands, cap, w.groups, cap, w.units, cap, nullptr, 0, counters, st));
         }
     }

@@ -9,7 +9,7 @@ import torch
 
 from . import _exact, _lib, fp_filter
 
-FORM_CODE = {'f16': 0, 'bf16': 1, 'bf16x3': 2}
+FORM_CODE = {'f16': 0, 'bf16': 1, 'bf16x3': 2, 'f16x2': 6}
 
 
 class GwbTile(ctypes.Structure):
@@ -27,7 +27,7 @@ class CStep:
     """gwb_filter_step for one bank (pipeline.Bank), one transform length and analysed span, one batch size."""
 
     def __init__(self, bank, tlen, a0, Tn, nseg, cfg, device='cuda'):
-        assert cfg.form in FORM_CODE, 'the C step runs the fp16, bf16 and split-bf16 forms'
+        assert cfg.form in FORM_CODE, 'the C step runs the fp16, bf16, split-bf16 and fp16 split-A forms'
         self.bank, self.cfg, self.tlen, self.nseg = bank, cfg, tlen, nseg
         self.vp = [fp_filter.fourstep_order(s['Vh'], tlen) for s in bank.svd]
         self.A = [s['A'].contiguous() for s in bank.svd]

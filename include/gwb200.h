@@ -443,7 +443,7 @@ typedef struct {
     int r, n, row0;      /* rank, templates, first row of the tile in the bank arrays */
 } GwbTile;
 typedef struct {
-    int form;            /* GEMM precision: 0 fp16, 1 bf16, 2 split bf16 */
+    int form;            /* GEMM precision: 0 fp16, 1 bf16, 2 split bf16, 6 fp16 with A split into hi + lo */
     int cw;              /* cluster window in samples, a multiple of 128 */
     long long a0, Tn;    /* analysed span of each segment: samples [a0, a0 + Tn) (Tn cut to whole windows) */
     float snr_threshold; /* exact-stage threshold; windows above (thr (1 - margin))^2 are candidates */

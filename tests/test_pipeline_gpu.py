@@ -232,7 +232,7 @@ def test_fp8_screen_with_local_search_keeps_the_fp32_peaks():
                     assert abs(out[b][k][0] - v) <= 2e-2 * v, (k, v, out[b][k])
 
 
-@pytest.mark.parametrize('form', ['f16', 'bf16x3'])
+@pytest.mark.parametrize('form', ['f16', 'bf16x3', 'f16x2'])
 def test_c_filter_step_matches_the_python_step(form):
     """The whole step through the one C entry gwb_filter_step (gwb200.cstep) gives the same candidates and exact
     values as MatchedFilter.step, which calls the same kernels one by one from Python."""
