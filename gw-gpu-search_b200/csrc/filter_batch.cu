@@ -40,7 +40,6 @@ int cond_shapes(long long tlen, const GwbCondConfig* c, CondShapes* s) {
 struct CondWork {
     float *frames, *F, *psd_w, *psd, *inv, *q, *pt, *st, *w, *tw;
     int32_t* pick;
-    char* step;
 };
 
 long long cond_carve(const CondShapes& s, int nseg, const GwbCondConfig* c, char* base, CondWork* w) {
@@ -63,7 +62,6 @@ long long cond_carve(const CondShapes& s, int nseg, const GwbCondConfig* c, char
     w->w = reinterpret_cast<float*>(take(4ll * c->psd_len));
     w->tw = reinterpret_cast<float*>(take(4ll * (c->inv_len > 0 ? c->inv_len : 1)));
     w->pick = reinterpret_cast<int32_t*>(take(4ll * nseg));
-    w->step = take(0);
     return (off + 255) & ~255ll;
 }
 
