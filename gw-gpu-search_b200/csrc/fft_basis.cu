@@ -501,7 +501,13 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT) basis_pass2(
     float2* twL = Y + TB * SC;
     const int row = blockIdx.y, t10 = blockIdx.x * TB, tid = threadIdx.x;
     const int stride = N / N2;
-    for (int m = tid; m < N2; m += NT) twL[m] = tw[m * stride];
+    // 1 / scale: folded into the step-1 twiddles (one rms per call), applied per row at the store for fp8
+    const float inv = 1.0f / (FORM == 4 ? scale[row] : *scale);
+    const float tsc = FORM == 4 ? 1.f : inv, zsc = FORM == 4 ? inv : 1.f;
+    for (int m = tid; m < N2; m += NT) {
+        const float2 w = tw[m * stride];
+        twL[m] = make_float2(w.x * tsc, w.y * tsc);
+    }
     // step 1: thread (c, b), c fastest: the block's W[k2][c] at k2 = R2 a + b, 256 contiguous bytes per warp
     const int c = tid % TB, b = tid / TB;
     const float2* wc = W + (long long)row * N + (long long)blockIdx.x * (N2 * TB) + b * TB + c;
@@ -516,7 +522,6 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT) basis_pass2(
     });
     __syncthreads();
     // step 2: thread (c, u), c fastest so the Z stores run along t. fp8: scale holds one scale per row
-    const float inv = 1.0f / (FORM == 4 ? scale[row] : *scale);
     char* zb = static_cast<char*>(Z);
     char* zl = static_cast<char*>(Zlo);
     const long long re_off = (long long)(row0 + row) * ldz * ES, im_off_b = (long long)(im_off + row0 + row) * ldz * ES;
@@ -538,7 +543,8 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT) basis_pass2(
             const int t = t0 + N1 * (R1 * vv);
             if (t >= 0 && t < Tn) {
                 const float2 z = y[brev(vv, ilog2(R2))];
-                store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * inv, z.y * inv);
+                if constexpr (FORM == 4) store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * zsc, z.y * zsc);
+                else store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x, z.y);
             }
         });
     }
@@ -571,13 +577,17 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
         cp_async_commit();
     };
     fetch(j0);
-    for (int e = tid; e < N2; e += NT) tw2[e] = tw[(e % R2) * (e / R2) * (N / N2)];
-    const float inv0 = FORM == 4 ? 0.f : 1.0f / *scale;    // fp8: scale holds one scale per row
+    // 1 / scale folded into the step-1 twiddles; fp8: scale holds one scale per row, applied at the store
+    const float inv0 = FORM == 4 ? 1.f : 1.0f / *scale;
+    for (int e = tid; e < N2; e += NT) {
+        const float2 w = tw[(e % R2) * (e / R2) * (N / N2)];
+        tw2[e] = make_float2(w.x * inv0, w.y * inv0);
+    }
     const int c = tid % TB, b = tid / TB;
     char* zb = static_cast<char*>(Z);
     char* zl = static_cast<char*>(Zlo);
     for (int j = j0; j < j1; ++j) {
-        const float inv = FORM == 4 ? 1.0f / scale[j] : inv0;
+        const float inv = FORM == 4 ? 1.0f / scale[j] : 1.f;
         cp_async_wait_all();
         __syncthreads();
         float2 x[R1];
@@ -616,7 +626,8 @@ __global__ void __launch_bounds__(Split<N2, 2>::NT, 2) basis_pass2_p(
                 const int t = t0 + N1 * (R1 * vv);
                 if (t >= 0 && t < Tn) {
                     const float2 z = y[p][brev(vv, ilog2(R2))];
-                    store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * inv, z.y * inv);
+                    if constexpr (FORM == 4) store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * inv, z.y * inv);
+                    else store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x, z.y);
                 }
             });
         }
@@ -642,18 +653,72 @@ struct SplitW {
     static_assert(SC >= N2, "the exchange buffer holds the W tile");
 };
 
-template <int N2, int FORM>
+// Paired Z stores (PAIR): the lanes c and c + 1 (c even, lane ^ 1) hold the samples t and t + 1 of every vv. Each
+// lane packs its (re, im), the two swap one 32-bit word by a shuffle, and the even lane stores the two real parts,
+// the odd lane the two imaginary parts, one word per plane (two 16-bit samples, or 64 bits of fp32): half the store
+// instructions of one 16-bit store per plane and sample. Needs an even a0, Tn and ldz and word-aligned planes.
+// Split bf16: hi = bf16(x), lo = bf16(x - hi), as store_z.
+template <int FORM>
+struct PairStore {
+    unsigned hsel, lsel, ssel;
+    bool odd;
+    __device__ __forceinline__ explicit PairStore(bool o) : odd(o) {
+        // __byte_perm(x, y, s): bytes 0-3 of x, 4-7 of y
+        hsel = o ? 0x3276u : 0x5410u;                      // 16-bit forms: own re | partner re, partner im | own im
+        if constexpr (FORM == 2) {
+            ssel = o ? 0x5410u : 0x7632u;                  // send: odd (re hi, re lo), even (im hi, im lo)
+            hsel = o ? 0x3254u : 0x5410u;
+            lsel = o ? 0x3276u : 0x7610u;
+        }
+    }
+    // one sample (scaled); writes through the lane's plane pointers ph, pl (element pairs) at pair index k
+    template <int K>
+    __device__ __forceinline__ void store(float xr, float xi, unsigned* ph, unsigned* pl, bool ok) const {
+        if constexpr (FORM == 1) {
+            const float snd = odd ? xr : xi;
+            const float rcv = __shfl_xor_sync(0xffffffffu, snd, 1);
+            const float2 w = odd ? make_float2(rcv, xi) : make_float2(xr, rcv);
+            if (ok) __stcs(reinterpret_cast<float2*>(ph) + K, w);
+        } else if constexpr (FORM == 2) {
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(xr, xi);
+            const unsigned H = *reinterpret_cast<const unsigned*>(&h2);
+            const float hr = __uint_as_float(H << 16), hm = __uint_as_float(H & 0xffff0000u);
+            const __nv_bfloat162 l2 = __floats2bfloat162_rn(xr - hr, xi - hm);
+            const unsigned L = *reinterpret_cast<const unsigned*>(&l2);
+            const unsigned R = __shfl_xor_sync(0xffffffffu, __byte_perm(H, L, ssel), 1);
+            if (ok) {
+                __stcs(ph + K, __byte_perm(H, R, hsel));
+                __stcs(pl + K, __byte_perm(L, R, lsel));
+            }
+        } else {
+            unsigned H;
+            if constexpr (FORM == 0) {
+                const __half2 h2 = __floats2half2_rn(xr, xi);
+                H = *reinterpret_cast<const unsigned*>(&h2);
+            } else {
+                const __nv_bfloat162 h2 = __floats2bfloat162_rn(xr, xi);
+                H = *reinterpret_cast<const unsigned*>(&h2);
+            }
+            const unsigned R = __shfl_xor_sync(0xffffffffu, H, 1);
+            if (ok) __stcs(ph + K, __byte_perm(H, R, hsel));
+        }
+    }
+};
+
+template <int N2, int FORM, bool PAIR>
 __global__ void __launch_bounds__(SplitW<N2>::NT, 1) basis_pass2_w(
-    const float2* __restrict__ W, int rows, int N, int N1, const float2* __restrict__ tw, int a0, int Tn,
+    const float2* __restrict__ W, int rows, int N, const float2* __restrict__ tw, int a0, int Tn,
     const float* __restrict__ scale, void* __restrict__ Z, void* __restrict__ Zlo, long long ldz, int im_off,
     int row0) {
     using S = SplitW<N2>;
     constexpr int R1 = S::R1, R2 = S::R2, NT = S::NT, SB = S::SB, SC = S::SC;
+    constexpr int N1 = N2;                        // square split: t = t1 + N1 (u + R1 v)
     constexpr int ES = FORM == 1 ? 4 : (FORM == 4 ? 1 : 2);   // bytes per Z element
     constexpr int CP = TBW * N2 * 8 / 16 / NT;   // 16-byte copies per thread per tile
+    static_assert(!PAIR || FORM != 4, "fp8 Z is stored per sample");
     extern __shared__ float2 sm[];
     float2* Bt = sm;                              // W tile (two blocks of TB columns), then the exchange tile
-    float2* tw2 = Bt + TBW * SC;                  // tw2[u R2 + b] = e^{2 pi i b u / N2}
+    float2* tw2 = Bt + TBW * SC;                  // tw2[u R2 + b] = e^{2 pi i b u / N2} / scale
     const int tid = threadIdx.x, t10 = blockIdx.x * TBW;
     const int j0 = blockIdx.y * RC, j1 = min(j0 + RC, rows);
     auto fetch = [&](int j) {
@@ -664,17 +729,32 @@ __global__ void __launch_bounds__(SplitW<N2>::NT, 1) basis_pass2_w(
         cp_async_commit();
     };
     fetch(j0);
-    for (int e = tid; e < N2; e += NT) tw2[e] = tw[(e % R2) * (e / R2) * (N / N2)];
-    const float inv0 = FORM == 4 ? 0.f : 1.0f / *scale;    // fp8: scale holds one scale per row
+    // 1 / scale folded into the step-1 twiddles; fp8: scale holds one scale per row, applied at the store
+    const float inv0 = FORM == 4 ? 1.f : 1.0f / *scale;
+    for (int e = tid; e < N2; e += NT) {
+        const float2 w = tw[(e % R2) * (e / R2) * (N / N2)];
+        tw2[e] = make_float2(w.x * inv0, w.y * inv0);
+    }
     const int c = (tid & 7) + 8 * ((tid >> 4) & 1);
     const int lo = (tid >> 3) & 1, hi = tid >> 5;
     const int b = lo + 2 * hi;                    // step 1: b < R2
     const int u2 = lo + 2 * hi;                   // step 2: u < R1 (= R2)
     const int cblk = (c >> 3) * (N2 * TB) + (c & 7);
+    const int t0 = t10 + c + N1 * u2 - a0;        // sample of vv = 0; vv steps by N1 R1
+    const bool odd = c & 1;
+    const int te = t0 - (PAIR && odd ? 1 : 0);    // the pair's even sample
+    unsigned vmask = 0;                           // bit vv: the sample (pair) lies in [0, Tn)
+#pragma unroll
+    for (int v = 0; v < R2; ++v) {
+        const int t = te + N1 * R1 * v;
+        if (t >= 0 && t < Tn) vmask |= 1u << v;
+    }
+    const PairStore<PAIR ? FORM : 0> ps(odd);
+    const int prow = row0 + (PAIR && odd ? im_off : 0);    // paired: the odd lane writes the imaginary planes
     char* zb = static_cast<char*>(Z);
     char* zl = static_cast<char*>(Zlo);
     for (int j = j0; j < j1; ++j) {
-        const float inv = FORM == 4 ? 1.0f / scale[j] : inv0;
+        const float inv = FORM == 4 ? 1.0f / scale[j] : 1.f;
         cp_async_wait_all();
         __syncthreads();
         float2 x[R1];
@@ -692,21 +772,31 @@ __global__ void __launch_bounds__(SplitW<N2>::NT, 1) basis_pass2_w(
         for (int bb = 0; bb < R2; ++bb) y[bb] = Bt[c * SC + bb * SB + u2];
         __syncthreads();
         if (j + 1 < j1) fetch(j + 1);
-        const long long re_off = (long long)(row0 + j) * ldz * ES, im_off_b = (long long)(im_off + row0 + j) * ldz * ES;
-        void* Zr = zb + re_off;
-        void* Zi = zb + im_off_b;
-        void* Zlr = FORM == 2 ? (void*)(zl + re_off) : nullptr;
-        void* Zli = FORM == 2 ? (void*)(zl + im_off_b) : nullptr;
         dft_reg<R2>(y);
-        const int t0 = t10 + c + N1 * u2 - a0;
-        static_for<R2>([&](auto V) {
-            constexpr int vv = decltype(V)::value;
-            const int t = t0 + N1 * (R1 * vv);
-            if (t >= 0 && t < Tn) {
+        if constexpr (PAIR) {
+            const long long off = ((long long)(prow + j) * ldz + te) * ES;
+            unsigned* ph = reinterpret_cast<unsigned*>(zb + off);
+            unsigned* pl = FORM == 2 ? reinterpret_cast<unsigned*>(zl + off) : nullptr;
+            static_for<R2>([&](auto V) {
+                constexpr int vv = decltype(V)::value;
+                constexpr int K = N1 * R1 * vv / 2;    // pair index of vv (64-bit pairs for fp32: same count)
                 const float2 z = y[brev(vv, ilog2(R2))];
-                store_z<FORM>(Zr, Zi, Zlr, Zli, t, z.x * inv, z.y * inv);
-            }
-        });
+                ps.template store<K>(z.x, z.y, ph, pl, (vmask >> vv) & 1u);
+            });
+        } else {
+            const long long re_off = (long long)(row0 + j) * ldz * ES, im_off_b = (long long)(im_off + row0 + j) * ldz * ES;
+            void* Zr = zb + re_off;
+            void* Zi = zb + im_off_b;
+            void* Zlr = FORM == 2 ? (void*)(zl + re_off) : nullptr;
+            void* Zli = FORM == 2 ? (void*)(zl + im_off_b) : nullptr;
+            static_for<R2>([&](auto V) {
+                constexpr int vv = decltype(V)::value;
+                if ((vmask >> vv) & 1u) {
+                    const float2 z = y[brev(vv, ilog2(R2))];
+                    store_z<FORM>(Zr, Zi, Zlr, Zli, t0 + N1 * R1 * vv, z.x * inv, z.y * inv);
+                }
+            });
+        }
     }
 }
 
@@ -1117,17 +1207,36 @@ int launch_pass2_p(const float2* W, int N, int N1, int rows, const float2* tw, i
     return GWB_OK;
 }
 
+// paired Z stores when every pair of samples (t, t + 1), t even, is one aligned word of each plane
+bool pair_ok(int form, int a0, int Tn, long long ldz, const void* Z, const void* Zlo) {
+    const int es = form == 1 ? 4 : (form == 4 ? 1 : 2);
+    const auto al = [&](const void* p) { return p == nullptr || reinterpret_cast<uintptr_t>(p) % (2 * es) == 0; };
+    return form != 4 && a0 % 2 == 0 && Tn % 2 == 0 && ldz % 2 == 0 && al(Z) && (form != 2 || al(Zlo));
+}
+std::atomic<int> g_pass2_pair{1};            // 0: per-sample stores only (gwb_basis_set_pass2_pairs)
+
+template <int N2, int FORM, bool PAIR>
+int launch_pass2_wp(const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn, const float* scale,
+                    void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
+    using S = SplitW<N2>;
+    GWB_CHECK_ARG(N1 == N2, GWB_ERR_SHAPE, "basis_pass2_w: N1=%d must equal N2=%d", N1, N2);
+    const size_t smem = (size_t)(TBW * S::SC + N2) * sizeof(float2);
+    auto k = basis_pass2_w<N2, FORM, PAIR>;
+    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<dim3(N1 / TBW, (rows + RC - 1) / RC), S::NT, smem, s>>>(W, rows, N, tw, a0, Tn, scale, Z, Zlo, ldz, im_off,
+                                                                 row0);
+    GWB_LAUNCH_CHECK("basis_pass2_w");
+    return GWB_OK;
+}
+
 template <int N2, int FORM>
 int launch_pass2_w(const float2* W, int N, int N1, int rows, const float2* tw, int a0, int Tn, const float* scale,
                    void* Z, void* Zlo, long long ldz, int im_off, int row0, cudaStream_t s) {
-    using S = SplitW<N2>;
-    const size_t smem = (size_t)(TBW * S::SC + N2) * sizeof(float2);
-    auto k = basis_pass2_w<N2, FORM>;
-    GWB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<dim3(N1 / TBW, (rows + RC - 1) / RC), S::NT, smem, s>>>(W, rows, N, N1, tw, a0, Tn, scale, Z, Zlo, ldz,
-                                                                 im_off, row0);
-    GWB_LAUNCH_CHECK("basis_pass2_w");
-    return GWB_OK;
+    if constexpr (FORM != 4) {
+        if (g_pass2_pair.load() && pair_ok(FORM, a0, Tn, ldz, Z, Zlo))
+            return launch_pass2_wp<N2, FORM, true>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
+    }
+    return launch_pass2_wp<N2, FORM, false>(W, N, N1, rows, tw, a0, Tn, scale, Z, Zlo, ldz, im_off, row0, s);
 }
 
 // columns per pass-2 CTA at N2 = 1024, per Z encoding (gwb_basis_set_pass2_columns): 16 (basis_pass2_w, the default:
@@ -1227,6 +1336,13 @@ int gwb_basis_set_pass2_columns(int form, int cols) {
 }
 
 int gwb_basis_pass2_columns(int form) { return form >= 0 && form <= 4 ? gwb::g_pass2_cols[form].load() : -1; }
+
+int gwb_basis_set_pass2_pairs(int on) {
+    using namespace gwb;
+    GWB_CHECK_ARG(on == 0 || on == 1, GWB_ERR_ARG, "basis_set_pass2_pairs: on=%d (0 or 1)", on);
+    g_pass2_pair.store(on);
+    return GWB_OK;
+}
 
 int gwb_basis_ring_rows(void) { return gwb::g_ring_pc.load() * gwb::g_ring_nslot.load(); }
 

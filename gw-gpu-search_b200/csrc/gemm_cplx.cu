@@ -478,7 +478,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
-// The CTA-pair form (fp16 / bf16): a cluster of two CTAs along x, M blocks 2p (rank 0) and 2p + 1 (rank 1) of the
+// The CTA-pair form (fp16, bf16, and the split forms 2 and 6 with their two or three products per K step; their A lo
+// resident beside A hi where three stages of 32 K rows fit, else streamed per CTA beside each Z stage): a cluster of
+// two CTAs along x, M blocks 2p (rank 0) and 2p + 1 (rank 1) of the
 // same time range (grid y). Each CTA keeps its own 128 rows of A resident and loads its own 64-sample half of every Z tile; rank 0
 // issues tcgen05.mma.cta_group::2 with M = 256 (each SM computes its 128 rows over all 128 samples, the Z halves
 // shared between the SMs), so per SM the MMAs read half the Z bytes from shared memory. Barriers: the loads of both
@@ -486,14 +488,16 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
 // CTAs (empty, tfull, done); both CTAs' epilogue warps arrive on rank 0's tempty. Every wait is bounded; every path
 // reaches the final cluster barrier.
 // ---------------------------------------------------------------------------------------------------------------------
-// Shared memory of one CTA of a pair: A (128 rows x 2 Kh, 128-byte rows of 64 elements), stages of (re, im) x KC
-// rows x 64 samples (one 128-byte row each), the epilogue's exchange, the barriers.
-__host__ __device__ inline Layout layout_pair(int Kh, int KC, int stages) {
+// Shared memory of one CTA of a pair: A (nres resident copies of 128 rows x 2 Kh, 128-byte rows of 64 elements),
+// stages of (re, im) x (nhz copies of Z) x KC rows x 64 samples (one 128-byte row each), followed, when A lo is
+// streamed (los), by A lo (re, im) x 128 rows x KC columns as in the one-CTA kernel; the epilogue's exchange, the
+// barriers.
+__host__ __device__ inline Layout layout_pair(int Kh, int KC, int stages, int nres = 1, int nhz = 1, bool los = false) {
     Layout L;
     L.a_tiles = (uint32_t)((2 * Kh + 63) / 64);
-    L.a_bytes = L.a_tiles * kATile;
+    L.a_bytes = (uint32_t)nres * L.a_tiles * kATile;
     L.z_off = L.a_bytes;
-    L.stage_bytes = 2u * (uint32_t)KC * 128u;
+    L.stage_bytes = 2u * (uint32_t)nhz * (uint32_t)KC * 128u + (los ? 2u * 128u * (uint32_t)KC * 2u : 0u);
     L.x_off = L.z_off + (uint32_t)stages * L.stage_bytes;
     L.bar_off = L.x_off + 2048u;
     L.total = L.bar_off + (uint32_t)(2 * stages + 6) * 8u + 16u;
@@ -504,11 +508,14 @@ template <int FORM>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     umma_cplx2_kernel(const __grid_constant__ CplxArgs args) {
     using C = Cfg<FORM>;
-    static_assert(C::NH == 1 && !C::F8, "the CTA-pair form takes one 16-bit product");
+    static_assert(!C::F8, "the CTA-pair form takes 16-bit products");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
     const int Kh = args.Kh, KC = args.KC, S = args.stages;
-    const Layout L = layout_pair(Kh, KC, S);
+    const bool los = C::SPLIT_A && args.lo_stream != 0;   // A lo streamed beside each Z stage (KC = 16 or 32)
+    const int nres = los ? 1 : C::NHA;                    // resident copies of A
+    const Layout L = layout_pair(Kh, KC, S, nres, C::NHZ, los);
+    const uint32_t zst_bytes = 2u * C::NHZ * (uint32_t)KC * 128u;   // the Z part of a stage
     const int nkc = (Kh + KC - 1) / KC;
     uint8_t* sA = smem;
     uint8_t* sZ = smem + L.z_off;
@@ -540,7 +547,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
     const int t_end = (int)((long long)(tr + 1) * args.ntiles / gridDim.y);
     const int ntl = t_end - t_begin;                         // the same in both CTAs of the pair
     const int nfill = ntl * nkc;
-    const uint32_t a_bytes = (uint32_t)(L.a_tiles * kATile);
+    const uint32_t a_bytes = L.a_bytes;                      // one CTA's resident A
     const uint32_t half_stage = L.stage_bytes;               // one CTA's half of a stage
 
     if (threadIdx.x == 0) {
@@ -569,12 +576,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 
     if (ntl > 0 && warp == 0) {
         if (lane == 0) {
-            prefetch_tmap(&args.tA[0]);
-            prefetch_tmap(&args.tZ[0]);
+            for (int h = 0; h < C::NHA; ++h) prefetch_tmap(&args.tA[h]);
+            for (int h = 0; h < C::NHZ; ++h) prefetch_tmap(&args.tZ[h]);
             const uint32_t barA_l = mapa_shared(smem_u32(barA), 0);
             if (leader) mbar_arrive_expect_tx(barA, 2u * a_bytes);
-            for (int a = 0; a < (int)L.a_tiles; ++a)
-                tma_load_2d_pair(sA + a * kATile, &args.tA[0], barA_l, a * C::ROWEL, m0);
+            for (int h = 0; h < nres; ++h)
+                for (int a = 0; a < (int)L.a_tiles; ++a)
+                    tma_load_2d_pair(sA + (h * L.a_tiles + a) * kATile, &args.tA[h], barA_l, a * C::ROWEL, m0);
             int issued = 0;
             for (int f = 0; f < nfill; ++f) {
                 const int s = f % S;
@@ -591,7 +599,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 const int x = (t_begin + i) * kTile + 64 * (int)rank;
                 uint8_t* st = sZ + s * half_stage;
                 for (int ri = 0; ri < 2; ++ri)
-                    tma_load_2d_pair(st + ri * KC * 128, &args.tZ[0], full_l, x, ri * Kh + kc * KC);
+                    for (int h = 0; h < C::NHZ; ++h)
+                        tma_load_2d_pair(st + (ri * C::NHZ + h) * KC * 128, &args.tZ[h], full_l, x, ri * Kh + kc * KC);
+                if (los)            // this CTA's 128 rows of A lo, re then im columns of the K chunk
+                    for (int ri = 0; ri < 2; ++ri)
+                        tma_load_2d_pair(st + zst_bytes + ri * 128 * KC * 2, &args.tA[1], full_l, ri * Kh + kc * KC,
+                                         m0);
                 issued = f + 1;
             }
             // the loads of both CTAs complete on the leader's full barriers: before the final cluster barrier (after
@@ -639,43 +652,80 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                     tc_fence_after();
                     const uint32_t st = z_base + (f % S) * half_stage;
                     const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
-                    // descriptors of K step sk: A re / im halves (K-major), Z re / im halves (sample-major)
-                    auto dA = [&](int sk, int im) {
-                        const int k = (im ? Kh : 0) + kc * KC + sk * C::KSTEP;
-                        return smem_desc(a_base + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES, 16, 1024, 2);
-                    };
-                    auto dZ = [&](int sk, int im) {
-                        return smem_desc(st + (im ? KC * 128 : 0) + sk * C::KSTEP * 128, (uint32_t)KC * 128u, 1024, 2);
-                    };
-                    // the first MMA into each accumulator of a tile overwrites it
-                    auto acc0 = [&](int sk) { return (kc > 0 || sk > 0) ? 1u : 0u; };
-                    if (order == 1) {            // per K step, grouped by A half
-                        for (int sk = 0; sk < nsteps; ++sk) {
-                            umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
-                            umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
-                            umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
-                            umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
+                    if constexpr (C::NPROD == 1) {
+                        // descriptors of K step sk: A re / im halves (K-major), Z re / im halves (sample-major)
+                        auto dA = [&](int sk, int im) {
+                            const int k = (im ? Kh : 0) + kc * KC + sk * C::KSTEP;
+                            return smem_desc(a_base + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES, 16, 1024, 2);
+                        };
+                        auto dZ = [&](int sk, int im) {
+                            return smem_desc(st + (im ? KC * 128 : 0) + sk * C::KSTEP * 128, (uint32_t)KC * 128u, 1024, 2);
+                        };
+                        // the first MMA into each accumulator of a tile overwrites it
+                        auto acc0 = [&](int sk) { return (kc > 0 || sk > 0) ? 1u : 0u; };
+                        if (order == 1) {            // per K step, grouped by A half
+                            for (int sk = 0; sk < nsteps; ++sk) {
+                                umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                                umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
+                                umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                                umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
+                            }
+                        } else if (order == 2) {     // the chunk's real-part MMAs, then its imaginary-part MMAs
+                            for (int sk = 0; sk < nsteps; ++sk) {
+                                umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                                umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                            }
+                            for (int sk = 0; sk < nsteps; ++sk) {
+                                umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
+                                umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
+                            }
+                        } else if (order == 3) {     // one product at a time over the chunk's K steps
+                            for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                            for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                            for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
+                            for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
+                        } else {                     // per K step: re += ReA ReZ, re -= ImA ImZ, im += ImA ReZ, += ReA ImZ
+                            for (int sk = 0; sk < nsteps; ++sk) {
+                                umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
+                                umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
+                                umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, acc0(sk));
+                                umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, 1u);
+                            }
                         }
-                    } else if (order == 2) {     // the chunk's real-part MMAs, then its imaginary-part MMAs
+                    } else {
+                        // split forms: per K step the products (ha, hz) in order, each as the four real MMAs;
+                        // A hi (and A lo when resident) from the resident copies, A lo streamed from the stage
                         for (int sk = 0; sk < nsteps; ++sk) {
-                            umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
-                            umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
-                        }
-                        for (int sk = 0; sk < nsteps; ++sk) {
-                            umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
-                            umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
-                        }
-                    } else if (order == 3) {     // one product at a time over the chunk's K steps
-                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
-                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
-                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, acc0(sk));
-                        for (int sk = 0; sk < nsteps; ++sk) umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, 1u);
-                    } else {                     // per K step: re += ReA ReZ, re -= ImA ImZ, im += ImA ReZ, += ReA ImZ
-                        for (int sk = 0; sk < nsteps; ++sk) {
-                            umma_f16_pair(dre, dA(sk, 0), dZ(sk, 0), idesc, acc0(sk));
-                            umma_f16_pair(dre, dA(sk, 1), dZ(sk, 1), idesc_neg, 1u);
-                            umma_f16_pair(dim, dA(sk, 1), dZ(sk, 0), idesc, acc0(sk));
-                            umma_f16_pair(dim, dA(sk, 0), dZ(sk, 1), idesc, 1u);
+                            const int k = kc * KC + sk * C::KSTEP;
+                            for (int pr = 0; pr < C::NPROD; ++pr) {
+                                const int ha = C::ha(pr), hz = C::hz(pr);
+                                uint64_t dAre, dAim;
+                                if (los && ha == 1) {
+                                    const uint32_t lo_re = st + zst_bytes + sk * 32, lo_im = lo_re + 128 * KC * 2;
+                                    if (KC == 16) {
+                                        dAre = smem_desc(lo_re, 16, 256, 6);
+                                        dAim = smem_desc(lo_im, 16, 256, 6);
+                                    } else {
+                                        dAre = smem_desc(lo_re, 16, 512, 4);
+                                        dAim = smem_desc(lo_im, 16, 512, 4);
+                                    }
+                                } else {
+                                    const uint32_t abase = a_base + ha * L.a_tiles * kATile;
+                                    dAre = smem_desc(abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES, 16,
+                                                     1024, 2);
+                                    dAim = smem_desc(abase + ((Kh + k) / C::ROWEL) * kATile +
+                                                         ((Kh + k) % C::ROWEL) * C::ES, 16, 1024, 2);
+                                }
+                                const uint32_t zre = st + (0 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128;
+                                const uint32_t zim = st + (1 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128;
+                                const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
+                                const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                                const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
+                                umma_f16_pair(dre, dAre, dZre, idesc, acc);
+                                umma_f16_pair(dre, dAim, dZim, idesc_neg, 1u);
+                                umma_f16_pair(dim, dAim, dZre, idesc, acc);
+                                umma_f16_pair(dim, dAre, dZim, idesc, 1u);
+                            }
                         }
                     }
                     umma_commit_pair(&empty[f % S]);
@@ -830,20 +880,74 @@ struct GemmTune {
 };
 
 GemmTune gemm_tune(int form, int kh) {
-    GemmTune t{form, kh, 1, 0, 0};
+    // without a table entry: CTA pairs, except for fp16 with split A (one CTA per M block: measured 0.368 against
+    // 0.404 ms at n = 256, Kh = 128; the pair is faster at Kh = 192, 0.569 against 0.616, where the autotuner picks it)
+    GemmTune t{form, kh, form == 6 ? 0 : 1, 0, 0};
     tune_lookup(form, kh, &t.pair, &t.stages, &t.order);
     return t;
 }
 
+// The tensor maps of the CTA-pair form: A (hi, lo) in boxes of 64 columns x 128 rows (128-byte swizzle), or A lo in
+// boxes of KC columns when it is streamed; Z in boxes of 64 samples x KC rows.
 template <int FORM>
-int launch_pair(CplxArgs args, int M, long long ntiles, long long nout, int group, float* V, int32_t* I,
-                long long ldv, void* work, long long work_bytes, const GemmTune& tune, cudaStream_t stream) {
+int encode_pair_maps(CplxArgs& args, const void* const* A, const void* const* Zp, long long lda, long long ldz, int M,
+                     long long Tn, bool los, int KC) {
+    using C = Cfg<FORM>;
+    const CUtensorMapDataType dt = C::FMT == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const int Kh = args.Kh;
+    for (int h = 0; h < C::NHA; ++h) {
+        const bool lo_box = los && h == 1;
+        const int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)(lda * C::ES),
+                                     lo_box ? (uint32_t)KC : (uint32_t)C::ROWEL, 128,
+                                     !lo_box ? CU_TENSOR_MAP_SWIZZLE_128B
+                                             : KC == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
+        if (r) return r;
+    }
+    for (int h = 0; h < C::NHZ; ++h) {
+        const int r = encode_tmap_2d(&args.tZ[h], dt, Zp[h], (uint64_t)Tn, (uint64_t)(2 * Kh), (uint64_t)(ldz * C::ES),
+                                     C::ROWEL, (uint32_t)KC, CU_TENSOR_MAP_SWIZZLE_128B);
+        if (r) return r;
+    }
+    return GWB_OK;
+}
+
+template <int FORM>
+int launch_pair(CplxArgs args, const void* const* A, const void* const* Zp, long long lda, long long ldz, int M,
+                long long ntiles, long long nout, int group, float* V, int32_t* I, long long ldv, void* work,
+                long long work_bytes, const GemmTune& tune, cudaStream_t stream) {
+    using C = Cfg<FORM>;
     const uint32_t max_smem = 227 * 1024;
-    const int KC = 64;
-    int stages = 8;
-    while (stages > 0 && layout_pair(args.Kh, KC, stages).total + 1024 > max_smem) --stages;
+    const int Kh = args.Kh;
+    auto most = [&](int kc, int nres, bool ls) {
+        int st = 8;
+        while (st > 0 && layout_pair(Kh, kc, st, nres, C::NHZ, ls).total + 1024 > max_smem) --st;
+        return st;
+    };
+    int KC = 64, stages = 0;
+    bool los = false;
+    if constexpr (C::SPLIT_A) {
+        // A hi and lo resident where three stages of 32 K rows fit beside them (or two, if the launch table asks for
+        // two); else A lo streamed in K chunks of 32 (64-byte swizzle) beside each Z stage, or of 16
+        KC = 32;
+        const int sres = most(32, 2, false);
+        if (sres >= 3 || (sres == 2 && tune.stages == 2)) {
+            stages = sres;
+        } else {
+            los = true;
+            stages = most(32, 1, true);
+            if (stages < 2) {
+                KC = 16;
+                stages = most(16, 1, true);
+            }
+        }
+        const int r = encode_pair_maps<FORM>(args, A, Zp, lda, ldz, M, args.Tn, los, KC);
+        if (r) return r;
+    } else {
+        stages = most(KC, 1, false);
+    }
     if (tune.stages >= 2) stages = std::min(stages, tune.stages);
     args.order = tune.order;
+    args.lo_stream = los ? 1 : 0;
     GWB_CHECK_ARG(stages >= 2, GWB_ERR_SHAPE, "fused_peaks_cplx: Kh=%d does not fit the CTA-pair form", args.Kh);
     const int npair = (M + 255) / 256;
     const long long per = (long long)std::max(1, num_sms() / (2 * npair));
@@ -855,7 +959,7 @@ int launch_pair(CplxArgs args, int M, long long ntiles, long long nout, int grou
     args.MB = 1;
     args.pv = static_cast<float*>(work);
     args.pi = reinterpret_cast<int32_t*>(static_cast<char*>(work) + 8ll * M * gx);
-    const uint32_t smem = layout_pair(args.Kh, KC, stages).total + 1024;
+    const uint32_t smem = layout_pair(args.Kh, KC, stages, los ? 1 : C::NHA, C::NHZ, los).total + 1024;
     auto kern = umma_cplx2_kernel<FORM>;
     GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<dim3(2 * npair, gx), kThreads, smem, stream>>>(args);
@@ -981,9 +1085,10 @@ int launch_cplx(const void* const* A, const void* const* Zp, long long lda, long
                                : layout_of(C::NHA, C::NHZ, MB, Kh, KC, stages, C::ROWEL)).total + 1024;
     auto kern = umma_cplx_kernel<FORM>;
     GWB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if constexpr (FORM == 0 || FORM == 1) {
-        if (work != nullptr && tune.pair) return launch_pair<FORM>(args, M, ntiles, nout, group, V, I, ldv, work,
-                                                                   work_bytes, tune, stream);
+    if constexpr (!C::F8) {
+        if (work != nullptr && tune.pair)
+            return launch_pair<FORM>(args, A, Zp, lda, ldz, M, ntiles, nout, group, V, I, ldv, work, work_bytes, tune,
+                                     stream);
     }
     const int mgroups = (M + 128 * MB - 1) / (128 * MB);
     const long long per = (long long)std::max(1, num_sms() / mgroups);

@@ -57,6 +57,7 @@ SIGNATURES = {
     'gwb_basis_ring_rows': [],
     'gwb_basis_set_pass2_columns': [_I, _I],
     'gwb_basis_pass2_columns': [_I],
+    'gwb_basis_set_pass2_pairs': [_I],
     'gwb_basis_ring_sync_ints': [_I],
     'gwb_basis_pack': [_P, _LL, _I, _I, _I, _LL, _LL, _P, _I, _P, _P, _LL, _P],
     'gwb_stacked_a': [_P, _LL, _I, _I, _P, _LL, _D, _P, _I, _I, _I, _P, _P, _P, _P, _LL, _P],

@@ -121,17 +121,18 @@ GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long ld
  * keep A hi there and stream A lo with the Z chunks (Kh <= 320). lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
  * be NULL): with it the CTAs take tile-granular ranges of the time axis (balanced to one 128-sample tile) and windows
  * cut by a range boundary are merged by a second kernel, bit for bit the same V and I; without it every CTA takes
- * whole windows (up to one window of imbalance between CTAs). With work, forms 0 and 1 run on CTA pairs (clusters
- * of two CTAs, tcgen05.mma.cta_group::2 with M = 256 over two SMs, each SM loading half of every Z tile) unless the
- * launch table says otherwise (gwb_gemm_set_config). */
+ * whole windows (up to one window of imbalance between CTAs). With work, forms 0, 1 and 2 run on CTA pairs (clusters
+ * of two CTAs, tcgen05.mma.cta_group::2 with M = 256 over two SMs, each SM loading half of every Z tile; the split
+ * form's A lo resident or streamed per CTA) unless the launch table says otherwise (gwb_gemm_set_config); form 6 runs
+ * one CTA per M block unless the table asks for pairs. */
 GWB_API long long gwb_fused_peaks_cplx_work_bytes(int M);
 /* Launch table of gwb_fused_peaks_cplx, per (form, Kh), filled by the autotuner (no reference counterpart; the
- * reference's own tuner is fp_gemm.pick_cfg, pipeline/fp_gemm.py:47-64): pair 1 = CTA pairs (forms 0, 1 with a
+ * reference's own tuner is fp_gemm.pick_cfg, pipeline/fp_gemm.py:47-64): pair 1 = CTA pairs (forms 0, 1, 2, 6 with a
  * work buffer), 0 = one CTA per M block; stages = depth of the Z ring (0 = the most that fit, else at most that);
  * order = the CTA-pair kernel's MMA order (0: per K step re+=ReA.ReZ, re-=ImA.ImZ, im+=ImA.ReZ, im+=ReA.ImZ; 1: per K
  * step grouped by A half; 2: per Z chunk all real-part MMAs, then all imaginary-part ones; 3: per Z chunk one product
  * at a time). Forms 4 and 5 are the stacked drop-in kernels (gwb_fused_peaks_f16, gwb_fused_peaks_bf16x3; kh = K;
- * only stages applies). Process-wide, guarded by a mutex; a shape without an entry uses pair 1, stages 0, order 0.
+ * only stages applies). Process-wide, guarded by a mutex; a shape without an entry uses pair 1 (0 for form 6), stages 0, order 0.
  * Every entry computes the same products; the MMA order only changes the order of the fp32 accumulation. */
 GWB_API int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order);
 GWB_API int gwb_gemm_clear_configs(void);
@@ -302,6 +303,10 @@ GWB_API int gwb_basis_fused(const float* Vp, long long ldvp, int rows, const flo
  * Bit-identical results either way; the autotuner times both. gwb_basis_pass2_columns returns a form's setting. */
 GWB_API int gwb_basis_set_pass2_columns(int form, int cols);
 GWB_API int gwb_basis_pass2_columns(int form);
+/* Z stores of the 16-column pass 2: 1 (default) pairs the samples (t, t + 1), t even, into one 32-bit word per plane
+ * (64-bit for fp32) through a lane shuffle, wherever a0, Tn and ldz are even and the planes word-aligned (fp8 and
+ * other shapes store per sample); 0 stores every sample separately. Bit-identical results either way. */
+GWB_API int gwb_basis_set_pass2_pairs(int on);
 /* The same basis series for N = 2^20 in one persistent launch that keeps W in L2 (same reference call,
  * fp_filter.py:597-613): rows go in chunks of pc through a ring of nslot slots of W (pc x nslot rows of N complex,
  * 128-byte aligned; wrows = the rows W holds), pass 1 running `look` chunks ahead of pass 2; each W tile's L2 lines

@@ -98,12 +98,15 @@ def basis(a):
         out.update(ms_cufft_path=ms, us_per_row_cufft=ms * 1e3 / r)
     zb = 2 * Tn * {'f16': 2, 'bf16': 2, 'fp8': 1}.get(a.form, 4)
     first = None
-    for cols in [int(x) for x in a.pass2_cols.split(',')]:
+    runs = [(c, p) for c in [int(x) for x in a.pass2_cols.split(',')]
+            for p in ([int(x) for x in a.pass2_pairs.split(',')] if c == 16 else [1])]
+    for cols, pairs in runs:
         _lib.call('gwb_basis_set_pass2_columns', -1, cols)
+        _lib.call('gwb_basis_set_pass2_pairs', pairs)
         for wr in [int(x) for x in a.wrows.split(',')]:
             fws = fp_filter.FusedBasisWorkspace(tlen, flen, r, wrows=wr or None, ring=False)
             msf = _time(lambda: fp_filter.basis_series_fused(fws, Vp, Dp, a0, Tn, Z, Zlo, a.form, im_off=Kh), a.reps)
-            tag = f'w{fws.wrows}_c{cols}'
+            tag = f'w{fws.wrows}_c{cols}' + ('' if pairs else '_unpaired')
             # HBM bytes of the fused form when W stays in L2: Vh read and Z written (D isw stays in L2)
             out['us_per_row_fused_' + tag] = msf * 1e3 / r
             out['hbm_gbs_' + tag] = r * (8 * flen + zb) / msf / 1e6
@@ -113,6 +116,7 @@ def basis(a):
             else:
                 out['bit_identical_' + tag] = all(torch.equal(x, y) for x, y in zip(got, first))
     _lib.call('gwb_basis_set_pass2_columns', -1, 16)
+    _lib.call('gwb_basis_set_pass2_pairs', 1)
     full = (lambda: Z.double() + Zlo.double()) if Zlo is not None else (lambda: Z.double())
     if tlen == fp_filter.RING_N and a.ring_cfgs:
         ref = full() * fws.scale.double()
@@ -577,6 +581,8 @@ def main():
     ap.add_argument('--reps', type=int, default=10)
     ap.add_argument('--wrows', default='0', help='basis: comma list of W row batches (0: all rows at once)')
     ap.add_argument('--pass2-cols', default='16,8', help='basis: comma list of columns per pass-2 CTA (8, 16)')
+    ap.add_argument('--pass2-pairs', default='1,0',
+                    help='basis: comma list of Z store modes of the 16-column pass 2 (1 paired, 0 per sample)')
     ap.add_argument('--pair', default='1', help='gemm: comma list, 1 CTA pairs, 0 one CTA per M block')
     ap.add_argument('--stages', default='0', help='gemm: comma list of Z ring depths (0: the most that fit)')
     ap.add_argument('--orders', default='0', help='gemm: comma list of MMA orders of the CTA-pair kernel (0-3)')

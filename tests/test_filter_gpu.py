@@ -209,10 +209,12 @@ def test_ring_basis_series_16bit_forms(form):
 
 
 @pytest.mark.parametrize('form', ['f16', 'bf16', 'bf16x3', 'f32', 'fp8'])
-def test_pass2_sixteen_columns_bit_identical(form):
+@pytest.mark.parametrize('da0,dtn', [(8, -24), (9, -23)])
+def test_pass2_sixteen_columns_bit_identical(form, da0, dtn):
     """The 16-column pass 2 (gwb_basis_set_pass2_columns(form, 16)) writes the same Z bits as the 8-column kernels at
     N = 2^20, for every Z encoding, with rows that end mid-chunk (r = 11) and an analysed span that starts and ends
-    inside a column block."""
+    inside a column block; with its paired stores (even a0 and Tn) and with per-sample stores
+    (gwb_basis_set_pass2_pairs(0), and odd a0 and Tn, where pairs do not apply)."""
     from gwb200 import _lib, fp_filter
     tlen = 1 << 20
     rng = np.random.default_rng(8)
@@ -221,26 +223,29 @@ def test_pass2_sixteen_columns_bit_identical(form):
     Vh = (rng.standard_normal((r, flen)) + 1j * rng.standard_normal((r, flen))).astype(np.complex64)
     D = (rng.standard_normal(flen) + 1j * rng.standard_normal(flen)).astype(np.complex64)
     isw = rng.uniform(0.5, 2, flen).astype(np.float32)
-    a0, Tn = 98304 + 8, 917504 - 24
+    a0, Tn = 98304 + da0, 917504 + dtn
     Kh = fp_filter.kh_of(r, form)
     dt = fp_filter._z_dtype(form)
     Vp = fp_filter.fourstep_order(torch.from_numpy(Vh).cuda(), tlen)
     Dp = fp_filter.fourstep_order(torch.from_numpy(D).cuda(), tlen, torch.from_numpy(isw).cuda())
     out = {}
     try:
-        for cols in (8, 16):
+        for cols, pairs in ((8, 1), (16, 0), (16, 1)):
             _lib.call('gwb_basis_set_pass2_columns', -1, cols)
+            _lib.call('gwb_basis_set_pass2_pairs', pairs)
             ws = fp_filter.FusedBasisWorkspace(tlen, flen, r)
             Z = torch.full((2 * Kh, -(-Tn // 16) * 16), 7 if dt == torch.uint8 else 3.0, dtype=dt, device='cuda')
             Zlo = torch.full_like(Z, 5.0) if form == 'bf16x3' else None
             fp_filter.basis_series_fused(ws, Vp, Dp, a0, Tn, Z, Zlo, form, im_off=Kh)
-            out[cols] = [Z.cpu()] + ([Zlo.cpu()] if Zlo is not None else []) + [ws.scale.cpu()]
+            out[cols, pairs] = [Z.cpu()] + ([Zlo.cpu()] if Zlo is not None else []) + [ws.scale.cpu()]
             if form == 'fp8':
-                out[cols].append(ws.rowscale[:r].cpu())
+                out[cols, pairs].append(ws.rowscale[:r].cpu())
     finally:
         _lib.call('gwb_basis_set_pass2_columns', -1, 16)
-    for x, y in zip(out[8], out[16]):
-        assert torch.equal(x.view(torch.uint8), y.view(torch.uint8))
+        _lib.call('gwb_basis_set_pass2_pairs', 1)
+    for key in ((16, 0), (16, 1)):
+        for x, y in zip(out[8, 1], out[key]):
+            assert torch.equal(x.view(torch.uint8), y.view(torch.uint8)), key
 
 
 @pytest.mark.parametrize('n,spread', [(64, 6), (248, 12), (256, 14)])

@@ -190,10 +190,31 @@ def test_cplx_f16_against_oracle(M, r, Tn, group, split):
     _check(V.cpu().numpy(), I.cpu().numpy(), Vr, Ir, tie)
 
 
-@pytest.mark.parametrize('form,r', [(1, 120), (2, 120), (2, 40), (2, 150), (2, 192), (2, 250)])
-def test_cplx_bf16_forms_against_oracle(form, r):
+_PAIR_CFGS = [None, (1, 0), (1, 2)]
+
+
+def _with_config(form, Kh, cfg, fn):
+    """Runs fn with the launch table entry (pair, stages) for (form, Kh), or the default without one."""
+    from gwb200 import _lib
+    if cfg is None:
+        return fn()
+    _lib.call('gwb_gemm_set_config', form, Kh, cfg[0], cfg[1], 0)
+    try:
+        return fn()
+    finally:
+        _lib.call('gwb_gemm_clear_configs')
+
+
+@pytest.mark.parametrize('form,r,cfg', [(1, 120, None)] +
+                         [(2, r, c) for r in (40, 120, 150, 192, 250) for c in _PAIR_CFGS])
+def test_cplx_bf16_forms_against_oracle(form, r, cfg):
     """bf16 and split bf16 (Kh <= 128: A hi and lo resident; beyond: A hi resident, A lo streamed with Z) against
-    the float64 stacked product, with whole windows per CTA and with tile-granular ranges (merged windows)."""
+    the float64 stacked product, with whole windows per CTA and with tile-granular ranges (merged windows); the split
+    form also on CTA pairs (launch table pair 1; A lo resident or streamed, the most stages or two)."""
+    _with_config(form, -(-r // 16) * 16, cfg, lambda: _bf16_forms_case(form, r))
+
+
+def _bf16_forms_case(form, r):
     from gwb200 import _lib
     rng = np.random.default_rng(form * 100 + r)
     M, Tn, group = 256, 2048 * 8, 16
@@ -226,9 +247,14 @@ def test_cplx_bf16_forms_against_oracle(form, r):
 
 
 @pytest.mark.parametrize('r', [40, 120, 150, 192])
-def test_cplx_f16_split_a_against_oracle(r):
+@pytest.mark.parametrize('cfg', _PAIR_CFGS)
+def test_cplx_f16_split_a_against_oracle(r, cfg):
     """fp16 Z with A split into fp16 hi + lo (form 6: two products; A hi and lo resident for Kh <= 128, A lo streamed
-    with Z beyond) against the float64 product of the fp16 Z values with the unrounded A."""
+    with Z beyond) against the float64 product of the fp16 Z values with the unrounded A; also on CTA pairs."""
+    _with_config(6, -(-r // 16) * 16, cfg, lambda: _f16_split_a_case(r))
+
+
+def _f16_split_a_case(r):
     from gwb200 import _lib
     rng = np.random.default_rng(600 + r)
     M, Tn, group = 256, 2048 * 8, 16
