@@ -41,6 +41,7 @@ SIGNATURES = {
     'gwb_fused_peaks_f16': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_bf16x3': [_P, _P, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
     'gwb_fused_peaks_f32': [_P, _P, _LL, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P],
+    'gwb_f32_set_async': [_I],
     'gwb_fused_peaks_cplx': [_I, _P, _P, _LL, _P, _P, _LL, _I, _I, _LL, _I, _P, _P, _LL, _P, _P, _LL, _P],
     'gwb_fused_peaks_cplx_work_bytes': [_I],
     'gwb_gemm_set_config': [_I, _I, _I, _I, _I],

@@ -108,6 +108,10 @@ GWB_API int gwb_fused_peaks_bf16x3(const uint16_t* Are_hi, const uint16_t* Are_l
                            long long ldv, void* stream);
 GWB_API int gwb_fused_peaks_f32(const float* Are, const float* Aim, long long lda, const float* Z, long long ldz, int M,
                         int K, long long Tn, int group, float* V, int32_t* I, long long ldv, void* stream);
+/* The fp32 form's kernel: 1 (default) copies the operand tiles by cp.async through a three-stage ring (needs K, lda,
+ * ldz multiples of 4 and 16-byte aligned operands, else the synchronous kernel runs), 0 the synchronous kernel. Both
+ * give the same V and I up to the order of the fp32 sums (identical K order: the same bits). */
+GWB_API int gwb_f32_set_async(int on);
 
 /* Compact complex form (same outputs): A = [Re As | Im As] (M, 2 Kh), Z = [Re zb ; Im zb] (2 Kh, Tn), each half Kh
  * wide (Kh a multiple of 16, halves zero-padded past r). z_re = ReA.ReZ - ImA.ImZ and z_im = ImA.ReZ + ReA.ImZ are

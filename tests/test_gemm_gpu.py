@@ -101,7 +101,7 @@ def test_f16_integer_operands_bit_exact_with_ties():
     assert np.array_equal(I.cpu().numpy(), Ir)
 
 
-@pytest.mark.parametrize('M,K,Tn,group', [(256, 64, 32768, 1), (130, 40, 5000, 16)])
+@pytest.mark.parametrize('M,K,Tn,group', [(256, 64, 32768, 1), (130, 40, 5000, 16), (70, 37, 3001, 4)])
 def test_f32_form_against_oracle(M, K, Tn, group):
     from gwb200 import fp_gemm
     rng = np.random.default_rng(11)
@@ -115,6 +115,32 @@ def test_f32_form_against_oracle(M, K, Tn, group):
     if group > 1:
         Vr, Ir, tie = _grouped(Vr, Ir, tie, group)
     _check(V.cpu().numpy(), I.cpu().numpy(), Vr, Ir, tie)
+
+
+@pytest.mark.parametrize('M,K,Tn,group', [(256, 384, 40000, 16), (200, 72, 4998, 3), (64, 16, 130, 1)])
+def test_f32_async_kernel_bit_identical(M, K, Tn, group):
+    """The fp32 form's cp.async kernel (the default where K, lda, ldz are multiples of 4) gives the same V and I bits
+    as the synchronous kernel (gwb_f32_set_async(0)): the same fp32 sums in the same K order, samples past Tn (inside
+    the last 16-byte copy and past it) ignored."""
+    from gwb200 import _lib, fp_gemm
+    rng = np.random.default_rng(K + Tn)
+    Are = _dev(rng.standard_normal((M, K)).astype(np.float32), torch.float32)
+    Aim = _dev(rng.standard_normal((M, K)).astype(np.float32), torch.float32)
+    ldz = -(-Tn // 4) * 4
+    Zf = torch.zeros((K, ldz), dtype=torch.float32, device='cuda')
+    Zf[:, :Tn] = _dev(rng.standard_normal((K, Tn)).astype(np.float32), torch.float32)
+    Zf[:, Tn:] = float('nan')                    # never read as a sample: NaN there would show in V
+    Z = Zf[:, :Tn]
+    out = {}
+    try:
+        for mode in (0, 1):
+            _lib.call('gwb_f32_set_async', mode)
+            out[mode] = [x.cpu() for x in fp_gemm.fused_peaks(Are, Aim, Z, M, Tn, group=group)]
+    finally:
+        _lib.call('gwb_f32_set_async', 1)
+    assert torch.equal(out[0][0].view(torch.int32), out[1][0].view(torch.int32))
+    assert torch.equal(out[0][1], out[1][1])
+    assert torch.isfinite(out[1][0]).all()
 
 
 def test_bf16x3_form_close_to_fp32():
