@@ -286,7 +286,7 @@ def top_peak_sets(kept, thr):
 
 # the committed ncu summaries of each form's two dominant kernels (DRAM bytes over algorithmic bytes)
 PROFILES = {'basis': {'bf16x3': 'basis_passes_c2_r128_bf16x3.md'},
-            'gemm': {'bf16x3': 'umma_cplx_kernel_c2_r192_bf16x3.md', 'f16': 'umma_cplx_kernel_c2_r128.md',
+            'gemm': {'bf16x3': 'umma_cplx2_kernel_c2_r192_bf16x3.md', 'f16': 'umma_cplx_kernel_c2_r128.md',
                      'bf16': 'umma_cplx_kernel_c2_r128.md'}}
 BASIS_DEFAULT = 'basis_passes_c2_r128.md'
 
