@@ -694,37 +694,49 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         }
                     } else {
                         // split forms: per K step the products (ha, hz) in order, each as the four real MMAs;
-                        // A hi (and A lo when resident) from the resident copies, A lo streamed from the stage
-                        for (int sk = 0; sk < nsteps; ++sk) {
+                        // A hi (and A lo when resident) from the resident copies, A lo streamed from the stage. The
+                        // chunk's descriptors (KC <= 32: at most two K steps) are formed first, then its MMAs go out
+                        // back to back
+                        constexpr int MAXS = 2;
+                        uint64_t dAr[MAXS][C::NPROD], dAi[MAXS][C::NPROD], dZr[MAXS][C::NPROD], dZi[MAXS][C::NPROD];
+#pragma unroll
+                        for (int sk = 0; sk < MAXS; ++sk) {
                             const int k = kc * KC + sk * C::KSTEP;
+#pragma unroll
                             for (int pr = 0; pr < C::NPROD; ++pr) {
                                 const int ha = C::ha(pr), hz = C::hz(pr);
-                                uint64_t dAre, dAim;
                                 if (los && ha == 1) {
                                     const uint32_t lo_re = st + zst_bytes + sk * 32, lo_im = lo_re + 128 * KC * 2;
                                     if (KC == 16) {
-                                        dAre = smem_desc(lo_re, 16, 256, 6);
-                                        dAim = smem_desc(lo_im, 16, 256, 6);
+                                        dAr[sk][pr] = smem_desc(lo_re, 16, 256, 6);
+                                        dAi[sk][pr] = smem_desc(lo_im, 16, 256, 6);
                                     } else {
-                                        dAre = smem_desc(lo_re, 16, 512, 4);
-                                        dAim = smem_desc(lo_im, 16, 512, 4);
+                                        dAr[sk][pr] = smem_desc(lo_re, 16, 512, 4);
+                                        dAi[sk][pr] = smem_desc(lo_im, 16, 512, 4);
                                     }
                                 } else {
                                     const uint32_t abase = a_base + ha * L.a_tiles * kATile;
-                                    dAre = smem_desc(abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES, 16,
-                                                     1024, 2);
-                                    dAim = smem_desc(abase + ((Kh + k) / C::ROWEL) * kATile +
-                                                         ((Kh + k) % C::ROWEL) * C::ES, 16, 1024, 2);
+                                    dAr[sk][pr] = smem_desc(abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES,
+                                                            16, 1024, 2);
+                                    dAi[sk][pr] = smem_desc(abase + ((Kh + k) / C::ROWEL) * kATile +
+                                                                ((Kh + k) % C::ROWEL) * C::ES, 16, 1024, 2);
                                 }
-                                const uint32_t zre = st + (0 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128;
-                                const uint32_t zim = st + (1 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128;
-                                const uint64_t dZre = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
-                                const uint64_t dZim = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                                dZr[sk][pr] = smem_desc(st + (0 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128,
+                                                        (uint32_t)KC * 128u, 1024, 2);
+                                dZi[sk][pr] = smem_desc(st + (1 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128,
+                                                        (uint32_t)KC * 128u, 1024, 2);
+                            }
+                        }
+#pragma unroll
+                        for (int sk = 0; sk < MAXS; ++sk) {
+                            if (sk >= nsteps) break;
+#pragma unroll
+                            for (int pr = 0; pr < C::NPROD; ++pr) {
                                 const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
-                                umma_f16_pair(dre, dAre, dZre, idesc, acc);
-                                umma_f16_pair(dre, dAim, dZim, idesc_neg, 1u);
-                                umma_f16_pair(dim, dAim, dZre, idesc, acc);
-                                umma_f16_pair(dim, dAre, dZim, idesc, 1u);
+                                umma_f16_pair(dre, dAr[sk][pr], dZr[sk][pr], idesc, acc);
+                                umma_f16_pair(dre, dAi[sk][pr], dZi[sk][pr], idesc_neg, 1u);
+                                umma_f16_pair(dim, dAi[sk][pr], dZr[sk][pr], idesc, acc);
+                                umma_f16_pair(dim, dAr[sk][pr], dZi[sk][pr], idesc, 1u);
                             }
                         }
                     }
