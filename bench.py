@@ -454,18 +454,18 @@ def run_c2(a):
         if ms_e2e is not None:
             results[form].update(e2e=world * (analysed / WEEK2) / (ms_e2e / 1e3 / 3600.0), ms_e2e=ms_e2e)
         if head:
-            # the exact stage with its bands staged in shared memory by bulk copies (TMA) instead of direct loads
+            # the exact stage with direct loads instead of its bands staged in shared memory by bulk copies (TMA)
             from gwb200 import _lib as glib
-            glib.call('gwb_exact_set_staging', 1)
+            glib.call('gwb_exact_set_staging', 0)
             mf.profile = {}
             Dd, IPd = cond(x)
             mf.step(Dd, IPd, isw)
             torch.cuda.synchronize()
-            results[form]['exact_ms_bulk'] = [a_.elapsed_time(b_) for nm, (a_, b_) in mf.profile['parts']
-                                              if nm == 'exact'][0]
-            results[form]['exact_ms_direct'] = split.get('exact')
+            results[form]['exact_ms_direct'] = [a_.elapsed_time(b_) for nm, (a_, b_) in mf.profile['parts']
+                                                if nm == 'exact'][0]
+            results[form]['exact_ms_bulk'] = split.get('exact')
             mf.profile = None
-            glib.call('gwb_exact_set_staging', 0)
+            glib.call('gwb_exact_set_staging', 1)
         del mf
         torch.cuda.empty_cache()
     precision_rep = None

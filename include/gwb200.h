@@ -432,8 +432,9 @@ GWB_API int gwb_append_results(const GwbCand* cands, const GwbPeak* peaks, const
                                GwbCand* out_cands, GwbPeak* out_peaks, int32_t* out_tag, int32_t* out_count,
                                int out_cap, int32_t* work, int32_t* meta, void* stream);
 /* Process-wide choice of gwb_bin_sums_ordered's loads (the TMA-staged chi-squared tiles; no reference counterpart):
- * bulk 1 stages every tile of 2048 bins of the template and data bands in shared memory with cp.async.bulk copies
- * (double-buffered, bounded waits) instead of loading them straight from L2; the slots are bit for bit the same. */
+ * bulk 1 (the default) stages every tile of 2048 bins of the template and data bands in shared memory with
+ * cp.async.bulk copies (double-buffered, bounded waits), 0 loads them straight from L2; the slots are bit for bit the
+ * same. */
 GWB_API int gwb_exact_set_staging(int bulk);
 /* Per candidate: z, pw from the slots (float64 sums), and with sig given (float64, sig[row * ldsig + seg]) snr,
  * chisq, dof, newsnr (fp_filter.py:837-853, coinc_rank.py:39-46); fpeak (exact_stage.py:236-238). */

@@ -140,7 +140,7 @@ def test_bulk_staged_bin_sums_are_bit_identical():
             torch.cuda.synchronize()
             out.append(mf.results())
     finally:
-        _lib.call('gwb_exact_set_staging', 0)
+        _lib.call('gwb_exact_set_staging', 1)
     assert out[0]['n_candidates'] > 500
     # candidate order follows the selection's atomics: compare by (row, segment, window)
     key = lambda r: {(int(c['row']), int(c['seg']), int(c['window'])): (int(c['sample']), p.tobytes())
