@@ -624,6 +624,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             const uint32_t idesc_neg = idesc | (1u << 13);  // negate A
             const int order = args.order;
             const uint32_t a_base = smem_u32(sA), z_base = smem_u32(sZ);
+            // descriptors of the resident A copies at K column 0 (the split forms add offsets to them)
+            uint64_t ad0[2];
+            for (int h = 0; h < 2; ++h) ad0[h] = smem_desc(a_base + (h < nres ? h : 0) * L.a_tiles * kATile, 16, 1024, 2);
             bool ok = mbar_wait_bounded(barA, 0);
             if (!ok) {
                 record_error(args.err, GWB_ERR_TIMEOUT, 212, tr, 0);
@@ -696,35 +699,35 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         // split forms: per K step the products (ha, hz) in order, each as the four real MMAs;
                         // A hi (and A lo when resident) from the resident copies, A lo streamed from the stage. The
                         // chunk's descriptors (KC <= 32: at most two K steps) are formed first, then its MMAs go out
-                        // back to back
+                        // back to back. A descriptor's start address is bits 0-13 (address >> 4), so a descriptor of
+                        // the same layout at a higher address is the base descriptor plus the byte offset >> 4:
+                        // one base per operand and chunk, the rest by additions (shared-memory addresses stay below
+                        // 2^18, so the field does not carry)
                         constexpr int MAXS = 2;
                         uint64_t dAr[MAXS][C::NPROD], dAi[MAXS][C::NPROD], dZr[MAXS][C::NPROD], dZi[MAXS][C::NPROD];
+                        const uint64_t zd = smem_desc(st, (uint32_t)KC * 128u, 1024, 2);
+                        const uint64_t lod = los ? (KC == 16 ? smem_desc(st + zst_bytes, 16, 256, 6)
+                                                             : smem_desc(st + zst_bytes, 16, 512, 4))
+                                                 : 0ull;
+                        const auto koff = [](int kk) {     // byte offset of K column kk in the 64-column tiles
+                            return (uint32_t)((kk / C::ROWEL) * kATile + (kk % C::ROWEL) * C::ES);
+                        };
 #pragma unroll
                         for (int sk = 0; sk < MAXS; ++sk) {
                             const int k = kc * KC + sk * C::KSTEP;
+                            const uint32_t ore = koff(k) >> 4, oim = koff(Kh + k) >> 4;
 #pragma unroll
                             for (int pr = 0; pr < C::NPROD; ++pr) {
                                 const int ha = C::ha(pr), hz = C::hz(pr);
                                 if (los && ha == 1) {
-                                    const uint32_t lo_re = st + zst_bytes + sk * 32, lo_im = lo_re + 128 * KC * 2;
-                                    if (KC == 16) {
-                                        dAr[sk][pr] = smem_desc(lo_re, 16, 256, 6);
-                                        dAi[sk][pr] = smem_desc(lo_im, 16, 256, 6);
-                                    } else {
-                                        dAr[sk][pr] = smem_desc(lo_re, 16, 512, 4);
-                                        dAi[sk][pr] = smem_desc(lo_im, 16, 512, 4);
-                                    }
+                                    dAr[sk][pr] = lod + (uint64_t)(sk * 2);
+                                    dAi[sk][pr] = lod + (uint64_t)(sk * 2 + ((128 * KC * 2) >> 4));
                                 } else {
-                                    const uint32_t abase = a_base + ha * L.a_tiles * kATile;
-                                    dAr[sk][pr] = smem_desc(abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES,
-                                                            16, 1024, 2);
-                                    dAi[sk][pr] = smem_desc(abase + ((Kh + k) / C::ROWEL) * kATile +
-                                                                ((Kh + k) % C::ROWEL) * C::ES, 16, 1024, 2);
+                                    dAr[sk][pr] = ad0[ha] + (uint64_t)ore;
+                                    dAi[sk][pr] = ad0[ha] + (uint64_t)oim;
                                 }
-                                dZr[sk][pr] = smem_desc(st + (0 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128,
-                                                        (uint32_t)KC * 128u, 1024, 2);
-                                dZi[sk][pr] = smem_desc(st + (1 * C::NHZ + hz) * KC * 128 + sk * C::KSTEP * 128,
-                                                        (uint32_t)KC * 128u, 1024, 2);
+                                dZr[sk][pr] = zd + (uint64_t)((((0 * C::NHZ + hz) * KC * 128) >> 4) + sk * C::KSTEP * 8);
+                                dZi[sk][pr] = zd + (uint64_t)((((1 * C::NHZ + hz) * KC * 128) >> 4) + sk * C::KSTEP * 8);
                             }
                         }
 #pragma unroll
