@@ -703,8 +703,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         // the same layout at a higher address is the base descriptor plus the byte offset >> 4:
                         // one base per operand and chunk, the rest by additions (shared-memory addresses stay below
                         // 2^18, so the field does not carry)
+                        // (K chunks of 64 with A resident: the chunk goes out in groups of two K steps)
                         constexpr int MAXS = 2;
-                        uint64_t dAr[MAXS][C::NPROD], dAi[MAXS][C::NPROD], dZr[MAXS][C::NPROD], dZi[MAXS][C::NPROD];
                         const uint64_t zd = smem_desc(st, (uint32_t)KC * 128u, 1024, 2);
                         const uint64_t lod = los ? (KC == 16 ? smem_desc(st + zst_bytes, 16, 256, 6)
                                                              : smem_desc(st + zst_bytes, 16, 512, 4))
@@ -712,34 +712,41 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         const auto koff = [](int kk) {     // byte offset of K column kk in the 64-column tiles
                             return (uint32_t)((kk / C::ROWEL) * kATile + (kk % C::ROWEL) * C::ES);
                         };
+                        for (int s0 = 0; s0 < nsteps; s0 += MAXS) {
+                            uint64_t dAr[MAXS][C::NPROD], dAi[MAXS][C::NPROD], dZr[MAXS][C::NPROD],
+                                dZi[MAXS][C::NPROD];
 #pragma unroll
-                        for (int sk = 0; sk < MAXS; ++sk) {
-                            const int k = kc * KC + sk * C::KSTEP;
-                            const uint32_t ore = koff(k) >> 4, oim = koff(Kh + k) >> 4;
+                            for (int sk = 0; sk < MAXS; ++sk) {
+                                const int ks = s0 + sk;             // K step within the chunk
+                                const int k = kc * KC + ks * C::KSTEP;
+                                const uint32_t ore = koff(k) >> 4, oim = koff(Kh + k) >> 4;
 #pragma unroll
-                            for (int pr = 0; pr < C::NPROD; ++pr) {
-                                const int ha = C::ha(pr), hz = C::hz(pr);
-                                if (los && ha == 1) {
-                                    dAr[sk][pr] = lod + (uint64_t)(sk * 2);
-                                    dAi[sk][pr] = lod + (uint64_t)(sk * 2 + ((128 * KC * 2) >> 4));
-                                } else {
-                                    dAr[sk][pr] = ad0[ha] + (uint64_t)ore;
-                                    dAi[sk][pr] = ad0[ha] + (uint64_t)oim;
+                                for (int pr = 0; pr < C::NPROD; ++pr) {
+                                    const int ha = C::ha(pr), hz = C::hz(pr);
+                                    if (los && ha == 1) {
+                                        dAr[sk][pr] = lod + (uint64_t)(ks * 2);
+                                        dAi[sk][pr] = lod + (uint64_t)(ks * 2 + ((128 * KC * 2) >> 4));
+                                    } else {
+                                        dAr[sk][pr] = ad0[ha] + (uint64_t)ore;
+                                        dAi[sk][pr] = ad0[ha] + (uint64_t)oim;
+                                    }
+                                    dZr[sk][pr] = zd + (uint64_t)((((0 * C::NHZ + hz) * KC * 128) >> 4) +
+                                                                  ks * C::KSTEP * 8);
+                                    dZi[sk][pr] = zd + (uint64_t)((((1 * C::NHZ + hz) * KC * 128) >> 4) +
+                                                                  ks * C::KSTEP * 8);
                                 }
-                                dZr[sk][pr] = zd + (uint64_t)((((0 * C::NHZ + hz) * KC * 128) >> 4) + sk * C::KSTEP * 8);
-                                dZi[sk][pr] = zd + (uint64_t)((((1 * C::NHZ + hz) * KC * 128) >> 4) + sk * C::KSTEP * 8);
                             }
-                        }
 #pragma unroll
-                        for (int sk = 0; sk < MAXS; ++sk) {
-                            if (sk >= nsteps) break;
+                            for (int sk = 0; sk < MAXS; ++sk) {
+                                if (s0 + sk >= nsteps) break;
 #pragma unroll
-                            for (int pr = 0; pr < C::NPROD; ++pr) {
-                                const uint32_t acc = (kc > 0 || sk > 0 || pr > 0) ? 1u : 0u;
-                                umma_f16_pair(dre, dAr[sk][pr], dZr[sk][pr], idesc, acc);
-                                umma_f16_pair(dre, dAi[sk][pr], dZi[sk][pr], idesc_neg, 1u);
-                                umma_f16_pair(dim, dAi[sk][pr], dZr[sk][pr], idesc, acc);
-                                umma_f16_pair(dim, dAr[sk][pr], dZi[sk][pr], idesc, 1u);
+                                for (int pr = 0; pr < C::NPROD; ++pr) {
+                                    const uint32_t acc = (kc > 0 || s0 + sk > 0 || pr > 0) ? 1u : 0u;
+                                    umma_f16_pair(dre, dAr[sk][pr], dZr[sk][pr], idesc, acc);
+                                    umma_f16_pair(dre, dAi[sk][pr], dZi[sk][pr], idesc_neg, 1u);
+                                    umma_f16_pair(dim, dAi[sk][pr], dZr[sk][pr], idesc, acc);
+                                    umma_f16_pair(dim, dAr[sk][pr], dZi[sk][pr], idesc, 1u);
+                                }
                             }
                         }
                     }
@@ -896,8 +903,9 @@ struct GemmTune {
 
 GemmTune gemm_tune(int form, int kh) {
     // without a table entry: CTA pairs, except for fp16 with split A (one CTA per M block: measured 0.368 against
-    // 0.404 ms at n = 256, Kh = 128; the pair is faster at Kh = 192, 0.569 against 0.616, where the autotuner picks it)
-    GemmTune t{form, kh, form == 6 ? 0 : 1, 0, 0};
+    // 0.404 ms at n = 256, Kh = 128; the pair is faster at Kh = 192, 0.569 against 0.616, where the autotuner picks
+    // it); split bf16 with order 1, K chunks of 64 where A hi and lo stay resident (0.526 -> 0.488 ms at Kh = 128)
+    GemmTune t{form, kh, form == 6 ? 0 : 1, 0, form == 2 ? 1 : 0};
     tune_lookup(form, kh, &t.pair, &t.stages, &t.order);
     return t;
 }
@@ -941,11 +949,16 @@ int launch_pair(CplxArgs args, const void* const* A, const void* const* Zp, long
     int KC = 64, stages = 0;
     bool los = false;
     if constexpr (C::SPLIT_A) {
+        // order 1: A hi and lo resident with K chunks of 64 where two stages fit. Otherwise:
         // A hi and lo resident where three stages of 32 K rows fit beside them (or two, if the launch table asks for
         // two); else A lo streamed in K chunks of 32 (64-byte swizzle) beside each Z stage, or of 16
         KC = 32;
         const int sres = most(32, 2, false);
-        if (sres >= 3 || (sres == 2 && tune.stages == 2)) {
+        if (tune.order == 1 && most(64, 2, false) >= 2) {
+            // order 1: K chunks of 64 (A hi and lo resident), half the barrier round trips per MMA
+            KC = 64;
+            stages = most(64, 2, false);
+        } else if (sres >= 3 || (sres == 2 && tune.stages == 2)) {
             stages = sres;
         } else {
             los = true;

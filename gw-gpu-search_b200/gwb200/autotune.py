@@ -40,7 +40,7 @@ def gemm_space(form):
         return ([(1, st, o) for st in (0, 4) for o in (0, 1, 2, 3)] +
                 [(0, st, 0) for st in (0, 3)])
     if form in ('bf16x3', 'f16x2'):        # the split forms: one CTA per M block, or CTA pairs
-        return [(0, st, 0) for st in (0, 4, 3, 2)] + [(1, st, 0) for st in (0, 3, 2)]
+        return [(0, st, 0) for st in (0, 4, 3, 2)] + [(1, st, 0) for st in (0, 3, 2)] + [(1, 0, 1)]
     return [(0, st, 0) for st in (0, 4, 3, 2)]
 
 

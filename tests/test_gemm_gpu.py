@@ -216,15 +216,15 @@ def test_cplx_f16_against_oracle(M, r, Tn, group, split):
     _check(V.cpu().numpy(), I.cpu().numpy(), Vr, Ir, tie)
 
 
-_PAIR_CFGS = [None, (1, 0), (1, 2)]
+_PAIR_CFGS = [None, (1, 0), (1, 2), (1, 0, 1)]
 
 
 def _with_config(form, Kh, cfg, fn):
-    """Runs fn with the launch table entry (pair, stages) for (form, Kh), or the default without one."""
+    """Runs fn with the launch table entry (pair, stages[, order]) for (form, Kh), or the default without one."""
     from gwb200 import _lib
     if cfg is None:
         return fn()
-    _lib.call('gwb_gemm_set_config', form, Kh, cfg[0], cfg[1], 0)
+    _lib.call('gwb_gemm_set_config', form, Kh, cfg[0], cfg[1], cfg[2] if len(cfg) > 2 else 0)
     try:
         return fn()
     finally:
