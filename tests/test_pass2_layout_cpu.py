@@ -62,3 +62,43 @@ def test_warp_stores_are_two_runs_of_sixteen():
         samples = np.sort(c[s] + N1 * u[s])
         runs = np.split(samples, np.flatnonzero(np.diff(samples) != 1) + 1)
         assert [len(x) for x in runs] == [16, 16]
+
+
+def _byte_perm(x, y, s):
+    """__byte_perm(x, y, s): byte i of the result is byte (s >> 4 i) & 7 of the 8 bytes {y:x}."""
+    b = (int(x) | (int(y) << 32)).to_bytes(8, 'little')
+    return int.from_bytes(bytes(b[(s >> (4 * i)) & 7] for i in range(4)), 'little')
+
+
+def _bf16_bits(v):
+    """Round-to-nearest-even bf16 bits of float32 values."""
+    u = np.asarray(v, np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint32)
+
+
+def test_paired_z_stores_place_every_sample():
+    """The paired stores of pass 2 (PairStore in csrc/fft_basis.cu), emulated on the CPU for a lane pair (c even and
+    odd, samples t and t + 1): the even lane's word holds the two real parts, the odd lane's the two imaginary parts,
+    for 16-bit Z (selector 0x5410 / 0x3276) and for split bf16 (hi 0x5410 / 0x3254, lo 0x7610 / 0x3276, sent word
+    0x7632 / 0x5410), the same bits as one 16-bit store per plane and sample."""
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        x = rng.standard_normal(4).astype(np.float32)          # (re, im) of sample t, then of sample t + 1
+        hr = _bf16_bits(x)                                     # hi of re_t, im_t, re_t1, im_t1
+        back = (hr.astype(np.uint64) << 16).astype(np.uint32).view(np.float32)
+        lo = _bf16_bits(x - back)
+        H = [int(hr[0]) | int(hr[1]) << 16, int(hr[2]) | int(hr[3]) << 16]     # lane even, lane odd
+        L = [int(lo[0]) | int(lo[1]) << 16, int(lo[2]) | int(lo[3]) << 16]
+        # 16-bit forms: each lane sends its packed (re, im) word
+        R = [H[1], H[0]]
+        w_even = _byte_perm(H[0], R[0], 0x5410)
+        w_odd = _byte_perm(H[1], R[1], 0x3276)
+        assert w_even == int(hr[0]) | int(hr[2]) << 16                           # re of t, t + 1
+        assert w_odd == int(hr[1]) | int(hr[3]) << 16                            # im of t, t + 1
+        # split bf16: even sends (im hi, im lo), odd sends (re hi, re lo)
+        S = [_byte_perm(H[0], L[0], 0x7632), _byte_perm(H[1], L[1], 0x5410)]
+        R = [S[1], S[0]]
+        assert _byte_perm(H[0], R[0], 0x5410) == int(hr[0]) | int(hr[2]) << 16   # re hi plane
+        assert _byte_perm(L[0], R[0], 0x7610) == int(lo[0]) | int(lo[2]) << 16   # re lo plane
+        assert _byte_perm(H[1], R[1], 0x3254) == int(hr[1]) | int(hr[3]) << 16   # im hi plane
+        assert _byte_perm(L[1], R[1], 0x3276) == int(lo[1]) | int(lo[3]) << 16   # im lo plane
