@@ -112,3 +112,24 @@ def test_order_keys_follow_the_reference_append_order():
     by_fields = np.lexsort((f['window'], f['row'], f['exact'], f['chunk'], f['tile']))
     assert np.array_equal(keys[by_key], keys[by_fields])
     assert (keys >= 0).all()
+
+
+def test_autotune_candidates_are_valid_launch_table_entries():
+    """Every launch shape the autotuner times (gwb200.autotune.gemm_space) is accepted by gwb_gemm_set_config (a
+    host-only table), the split forms include CTA pairs with 64-row K chunks (order 1), and out-of-range entries are
+    refused with a status."""
+    from gwb200 import autotune
+    lib = _lib.load()
+    try:
+        for form, code in autotune.FORM_CODE.items():
+            space = autotune.gemm_space(form)
+            assert space and len(set(space)) == len(space)
+            for pair, stages, order in space:
+                assert lib.gwb_gemm_set_config(code, 128, pair, stages, order) == 0
+            if form in ('bf16x3', 'f16x2'):
+                assert (1, 0, 1) in space and any(p == 0 for p, _, _ in space)
+        assert lib.gwb_gemm_set_config(2, 128, 2, 0, 0) == _lib.GWB_ERR_ARG
+        assert lib.gwb_gemm_set_config(2, 128, 1, 9, 0) == _lib.GWB_ERR_ARG
+        assert lib.gwb_gemm_set_config(2, 128, 1, 0, 4) == _lib.GWB_ERR_ARG
+    finally:
+        lib.gwb_gemm_clear_configs()
