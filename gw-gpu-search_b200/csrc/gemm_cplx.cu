@@ -706,9 +706,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                         // (K chunks of 64 with A resident: the chunk goes out in groups of two K steps)
                         constexpr int MAXS = 2;
                         const uint64_t zd = smem_desc(st, (uint32_t)KC * 128u, 1024, 2);
-                        const uint64_t lod = los ? (KC == 16 ? smem_desc(st + zst_bytes, 16, 256, 6)
-                                                             : smem_desc(st + zst_bytes, 16, 512, 4))
-                                                 : 0ull;
+                        // A lo streamed: KC-column rows in the 32-, 64- or 128-byte swizzle (KC = 16, 32, 64)
+                        const uint64_t lod = !los ? 0ull
+                                             : KC == 16 ? smem_desc(st + zst_bytes, 16, 256, 6)
+                                             : KC == 32 ? smem_desc(st + zst_bytes, 16, 512, 4)
+                                                        : smem_desc(st + zst_bytes, 16, 1024, 2);
                         const auto koff = [](int kk) {     // byte offset of K column kk in the 64-column tiles
                             return (uint32_t)((kk / C::ROWEL) * kATile + (kk % C::ROWEL) * C::ES);
                         };
@@ -922,8 +924,9 @@ int encode_pair_maps(CplxArgs& args, const void* const* A, const void* const* Zp
         const bool lo_box = los && h == 1;
         const int r = encode_tmap_2d(&args.tA[h], dt, A[h], (uint64_t)(2 * Kh), (uint64_t)M, (uint64_t)(lda * C::ES),
                                      lo_box ? (uint32_t)KC : (uint32_t)C::ROWEL, 128,
-                                     !lo_box ? CU_TENSOR_MAP_SWIZZLE_128B
-                                             : KC == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
+                                     !lo_box || KC == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                     : KC == 32          ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                         : CU_TENSOR_MAP_SWIZZLE_32B);
         if (r) return r;
     }
     for (int h = 0; h < C::NHZ; ++h) {
@@ -958,6 +961,12 @@ int launch_pair(CplxArgs args, const void* const* A, const void* const* Zp, long
             // order 1: K chunks of 64 (A hi and lo resident), half the barrier round trips per MMA
             KC = 64;
             stages = most(64, 2, false);
+        } else if (tune.order == 1 && most(64, 1, true) >= 2) {
+            // order 1 where A hi and lo do not fit beside two stages of 64: A lo streamed in chunks of 64
+            // (128-byte swizzle)
+            KC = 64;
+            los = true;
+            stages = most(64, 1, true);
         } else if (sres >= 3 || (sres == 2 && tune.stages == 2)) {
             stages = sres;
         } else {

@@ -135,8 +135,9 @@ GWB_API long long gwb_fused_peaks_cplx_work_bytes(int M);
  * work buffer), 0 = one CTA per M block; stages = depth of the Z ring (0 = the most that fit, else at most that);
  * order = the CTA-pair kernel's MMA order (0: per K step re+=ReA.ReZ, re-=ImA.ImZ, im+=ImA.ReZ, im+=ReA.ImZ; 1: per K
  * step grouped by A half; 2: per Z chunk all real-part MMAs, then all imaginary-part ones; 3: per Z chunk one product
- * at a time; for the split forms 2 and 6 on pairs, order 1 takes K chunks of 64 where A hi and lo stay resident
- * beside two stages, else the chunks of 32 as order 0). Forms 4 and 5 are the stacked drop-in kernels (gwb_fused_peaks_f16, gwb_fused_peaks_bf16x3; kh = K;
+ * at a time; for the split forms 2 and 6 on pairs, order 1 takes K chunks of 64: A hi and lo resident beside two
+ * stages where they fit, else A lo streamed in chunks of 64 where two such stages fit, else the chunks of 32 as order
+ * 0). Forms 4 and 5 are the stacked drop-in kernels (gwb_fused_peaks_f16, gwb_fused_peaks_bf16x3; kh = K;
  * only stages applies). Process-wide, guarded by a mutex; a shape without an entry uses pair 1 (0 for form 6), stages 0, order 0 (1 for form 2).
  * Every entry computes the same products; the MMA order only changes the order of the fp32 accumulation. */
 GWB_API int gwb_gemm_set_config(int form, int kh, int pair, int stages, int order);
