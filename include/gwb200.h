@@ -121,8 +121,10 @@ GWB_API int gwb_f32_set_async(int on);
  * counterpart; Kh a multiple of 32), V = rowscale[i]^2 max |z|^2 with rowscale the per-row scale of A
  * (gwb_stacked_a8); rowscale is ignored by the other forms (may be NULL); 6: fp16 Z with A split into fp16 hi + lo
  * (A_lo; Z_lo unused), two products hi.Z + lo.Z (no reference counterpart: the rounding of A is removed, that of Z
- * kept). Kh <= 192 (forms 0, 1, 3); forms 2 and 6 keep A hi and lo in shared memory up to Kh = 128 and beyond that
- * keep A hi there and stream A lo with the Z chunks (Kh <= 320). lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes, 16-byte aligned, may
+ * kept). Kh <= 192 (forms 0, 1, 3); forms 2 and 6 keep A hi and lo in shared memory where they fit beside the Z
+ * stages (one CTA: Kh <= 128; CTA pairs: Kh <= 160) and beyond that keep A hi there and stream A lo with the Z
+ * chunks (Kh <= 320). lda, ldz in elements, multiples of 16 bytes. work (gwb_fused_peaks_cplx_work_bytes(M) bytes,
+ * 16-byte aligned, may
  * be NULL): with it the CTAs take tile-granular ranges of the time axis (balanced to one 128-sample tile) and windows
  * cut by a range boundary are merged by a second kernel, bit for bit the same V and I; without it every CTA takes
  * whole windows (up to one window of imbalance between CTAs). With work, forms 0, 1 and 2 run on CTA pairs (clusters
