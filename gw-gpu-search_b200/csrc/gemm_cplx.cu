@@ -213,9 +213,9 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
             }
             tc_fence_after();
             // the MMAs of one item (M block mb) on one Z chunk. One-product forms: every descriptor of the chunk is
-            // formed first, then the MMAs go out back to back in the same order (sk, four real products), so the one
-            // issuing thread spends no address arithmetic between them (measured 0.266 -> 0.253 ms at n = 256,
-            // r = 128, fp16). The split form keeps descriptors and MMAs interleaved (the burst measured slower there:
+            // formed first (base descriptors plus offsets), then the MMAs go out back to back in the same order (sk,
+            // four real products), so the one issuing thread spends no address arithmetic between them (measured
+            // 0.266 -> 0.253 ms at n = 256, r = 128, fp16). The split form keeps descriptors and MMAs interleaved (the burst measured slower there:
             // one K step per chunk when A lo is streamed).
             auto issue = [&](int kc, int mb, int b, uint32_t st) {
                 if constexpr (C::NPROD == 1) {
@@ -223,19 +223,21 @@ __global__ void __launch_bounds__(kThreads, 1) umma_cplx_kernel(const __grid_con
                     const uint32_t dre = tmem + (uint32_t)(b * 256), dim = dre + 128;
                     const int nsteps = min(KC, Kh - kc * KC) / C::KSTEP;
                     const uint32_t abase = a_base + mb * L.a_tiles * kATile;
+                    // base descriptors of the chunk plus byte offsets >> 4 (the start-address field, bits 0-13;
+                    // shared-memory addresses stay below 2^18, so it does not carry)
+                    const uint64_t ad = smem_desc(abase, 16, 1024, 2);
+                    const uint64_t zd = smem_desc(st, (uint32_t)KC * 128u, 1024, 2);
                     uint64_t dAre[MAXS], dAim[MAXS], dZre[MAXS], dZim[MAXS];
 #pragma unroll
                     for (int sk = 0; sk < MAXS; ++sk) {
                         const int k = kc * KC + sk * C::KSTEP;
-                        const uint32_t are = abase + (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
-                        const uint32_t aim = abase + ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
+                        const uint32_t are = (k / C::ROWEL) * kATile + (k % C::ROWEL) * C::ES;
+                        const uint32_t aim = ((Kh + k) / C::ROWEL) * kATile + ((Kh + k) % C::ROWEL) * C::ES;
                         // K step = KSTEP rows of 128 bytes (2048 bytes for 16-bit, 4096 for 8-bit)
-                        const uint32_t zre = st + sk * C::KSTEP * 128;
-                        const uint32_t zim = st + C::HALVES * KC * 128 + sk * C::KSTEP * 128;
-                        dAre[sk] = smem_desc(are, 16, 1024, 2);
-                        dAim[sk] = smem_desc(aim, 16, 1024, 2);
-                        dZre[sk] = smem_desc(zre, (uint32_t)KC * 128u, 1024, 2);
-                        dZim[sk] = smem_desc(zim, (uint32_t)KC * 128u, 1024, 2);
+                        dAre[sk] = ad + (uint64_t)(are >> 4);
+                        dAim[sk] = ad + (uint64_t)(aim >> 4);
+                        dZre[sk] = zd + (uint64_t)(sk * C::KSTEP * 8);
+                        dZim[sk] = zd + (uint64_t)(((C::HALVES * KC * 128) >> 4) + sk * C::KSTEP * 8);
                     }
 #pragma unroll
                     for (int sk = 0; sk < MAXS; ++sk) {
