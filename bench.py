@@ -51,7 +51,7 @@ A0, A1 = int(START_PAD * SR), int((CHUNK_S - END_PAD) * SR)
 F_LOW = 20.0
 WEEK2 = 2 * 604800.0
 N_TEMPLATES = 5880
-METRIC = "2-det weeks filtered per GPU-hour, 5,880 templates, SNR err<=1e-3: FP32 vs BF16"
+METRIC = "2-det weeks filtered per GPU-hour, 5,880 templates, SNR err\u22641e-3: FP32 vs BF16"
 UNIT = '2-det weeks / hour'
 DYN = 5.9029581035870565e+20
 LINES = ((60.0, 1e3, 0.02), (120.0, 1e3, 0.02), (180.0, 1e3, 0.02))
